@@ -1,0 +1,157 @@
+/* neo_fft_b200 — C ABI of the B200 (sm_100a) per-plane spectral pipeline.
+ *
+ * This header is the drop-in boundary for neo-fft's core `Plan`
+ * (src/algorithms/plan.hpp:49-140 in the reference). Everything below is plain C:
+ * pointers, sizes and status codes, no C++ or CUDA types. A C++ facade with the
+ * reference's class signature (include/neo_fft_b200/plan.hpp) is built on it.
+ *
+ * Memory: plane pointers passed to the *_device entry points are CUDA device
+ * pointers; the *_host entry points take host memory and stage it through the
+ * plan's device buffers. `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).
+ *
+ * Errors: every call returns nf_status and, when `err` is non-NULL, writes a
+ * NUL-terminated message of at most err_len bytes. NF_INVALID_ARGUMENT mirrors the
+ * reference's std::invalid_argument (src/base/checked.hpp:13-20) with the same
+ * message texts; NF_NON_FINITE mirrors std::runtime_error("non-finite sample or
+ * intermediate") (checked.hpp:37-41). On any error the destination contents are
+ * unspecified; no Kalman state or model is published by a failed call.
+ */
+#ifndef NEO_FFT_B200_H
+#define NEO_FFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NF_ABI_VERSION 1
+
+typedef enum nf_status {
+  NF_OK = 0,
+  NF_INVALID_ARGUMENT = 1, /* configuration, geometry, shape or aliasing error */
+  NF_NON_FINITE = 2,       /* non-finite sample or intermediate */
+  NF_DEVICE_ERROR = 3      /* CUDA launch/allocation failure or device unavailable */
+} nf_status;
+
+/* SampleFormat (plan.hpp:20-23): integer bits 8..16, or floating with bits 32. */
+typedef struct nf_format {
+  int bits;
+  int floating;
+  int chroma;
+} nf_format;
+
+/* FFT3DConfig (plan.hpp:24-36) with EnhancementConfig (fft3d_profile.hpp:6-9).
+ * Optional sigma2..4 are "unset" when the has_* flag is 0. */
+typedef struct nf_fft3d_config {
+  int bw, bh, ow, oh, wintype, opt, bt;
+  float sigma, beta, degrid, kratio;
+  int has_sigma2, has_sigma3, has_sigma4;
+  float sigma2, sigma3, sigma4;
+  float sharpen, scutoff, svr, smin, smax, dehalo, hr, ht;
+  float pfactor, pcutoff;
+  int pframe, px, py, pshow;
+  int left, top, right, bottom, interlaced;
+  int cache_frames, cache_mb, kalman_warmup;
+} nf_fft3d_config;
+
+/* DFTConfig (plan.hpp:37-46) with DFTCurves (profile.hpp:7-12). Curves are
+ * frequency/value pairs; NULL/0 means empty. nlocation holds (frame, plane, y, x)
+ * tuples (dft_noise.hpp:10). */
+typedef struct nf_dft_config {
+  int block, overlap, mode, swin, twin, ftype, opt, tbsize;
+  float sbeta, tbeta, sigma, sigma2, pmin, pmax, f0beta;
+  int zmean, temporal_mode, temporal_overlap, dither, dither_seed;
+  const float* slocation; int n_slocation;
+  const float* ssx; int n_ssx;
+  const float* ssy; int n_ssy;
+  const float* sst; int n_sst;
+  int ssystem;
+  const int* nlocation; int n_nlocation;
+  int has_alpha; float alpha;
+} nf_dft_config;
+
+/* Axis (src/spectral/geometry.hpp:6-8). */
+typedef struct nf_axis {
+  int length, block, overlap, step, count, cover, offset;
+} nf_axis;
+
+/* span2d::Plane equivalent: signed byte stride (bottom-up planes allowed). */
+typedef struct nf_const_plane {
+  const void* data;
+  int width, height;
+  ptrdiff_t stride_bytes;
+} nf_const_plane;
+typedef struct nf_plane {
+  void* data;
+  int width, height;
+  ptrdiff_t stride_bytes;
+} nf_plane;
+
+typedef struct nf_plan nf_plan;
+typedef struct nf_kalman_state nf_kalman_state;
+
+/* Defaults of FFT3DConfig{} / DFTConfig{} (plan.hpp:24-46). */
+void nf_fft3d_config_default(nf_fft3d_config* c);
+void nf_dft_config_default(nf_dft_config* c);
+
+/* Plan(int w, int h, SampleFormat, const FFT3DConfig&) — plan.hpp:51, plan.cpp:91-169. */
+nf_status nf_plan_create_fft3d(int width, int height, nf_format format, const nf_fft3d_config* config,
+                               nf_plan** plan, char* err, size_t err_len);
+/* Plan(int w, int h, SampleFormat, const DFTConfig&) — plan.hpp:52, plan.cpp:170-226. */
+nf_status nf_plan_create_dft(int width, int height, nf_format format, const nf_dft_config* config,
+                             nf_plan** plan, char* err, size_t err_len);
+void nf_plan_destroy(nf_plan* plan);
+
+/* Public members geometry/temporal_size/fft.bins() (plan.hpp:53-57; read by
+ * filter.hpp:97-98). `bins` is the spatial half-spectrum bin count. */
+nf_status nf_plan_geometry(const nf_plan* plan, nf_axis* x, nf_axis* y, int* temporal_size, int* bins);
+
+/* Plan::process_at<T>(sources, dst, frame, plane, targets) — plan.hpp:77-80, run()
+ * plan.cpp:331-640. `sources` holds nsources logical temporal slots (they may alias
+ * each other, never dst). For DFTTest tmode=1, sources holds ntargets blocks of
+ * tbsize slots and targets the slice of each block (temporal_grid.hpp:24-40).
+ * Device pointers; asynchronous on `stream`. The non-finite check of this call is
+ * accumulated on the plan and reported by nf_plan_sync_status. */
+nf_status nf_plan_process_device(const nf_plan* plan, const nf_const_plane* sources, int nsources,
+                                 const int* targets, int ntargets, nf_plane dst, int frame, int plane,
+                                 void* stream, char* err, size_t err_len);
+/* Same as above with host planes: copies in, launches, copies out and synchronises;
+ * returns NF_NON_FINITE like the reference's frame evaluation. */
+nf_status nf_plan_process_host(const nf_plan* plan, const nf_const_plane* sources, int nsources,
+                               const int* targets, int ntargets, nf_plane dst, int frame, int plane,
+                               void* stream, char* err, size_t err_len);
+/* Synchronises `stream` and returns NF_NON_FINITE if any launch since the last call
+ * met a non-finite sample or intermediate (then clears the flag). */
+nf_status nf_plan_sync_status(const nf_plan* plan, void* stream, char* err, size_t err_len);
+
+/* Kalman (bt=0): initial_kalman / advance_kalman / render_kalman — plan.hpp:84-88,
+ * plan.cpp:293-321, kernels/scalar/kalman.cpp:3-24. The state (complex L, float C,
+ * float Q per bin; kernels/kalman.hpp:5-14) lives in device memory. `fp64_variance`
+ * = 1 keeps C and Q in binary64 (state then holds 24 bytes per bin). */
+nf_status nf_kalman_state_create(const nf_plan* plan, int fp64_variance, nf_kalman_state** state, char* err,
+                                 size_t err_len);
+void nf_kalman_state_destroy(nf_kalman_state* state);
+nf_status nf_kalman_state_copy(nf_kalman_state* dst, const nf_kalman_state* src, void* stream);
+nf_status nf_kalman_advance_device(const nf_plan* plan, nf_const_plane source, nf_kalman_state* state, void* stream,
+                                   char* err, size_t err_len);
+nf_status nf_kalman_render_device(const nf_plan* plan, nf_const_plane source, nf_plane dst,
+                                  const nf_kalman_state* state, void* stream, char* err, size_t err_len);
+/* Read back the state (host arrays of `count` bins; C/Q as float). */
+nf_status nf_kalman_state_read(const nf_kalman_state* state, float* last_interleaved, float* covariance,
+                               float* process, size_t count);
+
+/* KernelInfo (docs/api/en/kernel-info.md; vapoursynth.cpp:64-69): labels of the
+ * active implementation. Each string buffer receives at most len bytes. */
+nf_status nf_kernel_info(char* fft_backend, size_t fft_backend_len, char* target, size_t target_len, char* fft,
+                         size_t fft_len, int* fft_lanes);
+
+/* Library/ABI version for loaders. */
+int nf_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEO_FFT_B200_H */

@@ -1,0 +1,554 @@
+// FFT arithmetic shared by the sm_100a tile kernels and the host-side table builders.
+//
+// Every floating-point operation is spelled out with round-to-nearest intrinsics
+// (device) or plain operators compiled with -ffp-contract=off (host), so the same
+// source produces bit-identical results on both sides.
+//
+// Two families live here:
+//
+//  * Codelet-order transforms for 8, 16 and 32 points (fft8/fft16/fft32). The
+//    neo-fft reference computes 8x8, 16x16 and 32x32 real 2-D FFTs with hand
+//    written AVX2 codelets (src/spectral/codelets/fft8x8_avx2.cpp:42-138,
+//    fft16x16_avx2.cpp:29-194, fft32x32_avx2.cpp:96-260; dispatched from
+//    src/spectral/fft_backend.cpp:260-367). Parity with the reference's rounding
+//    requires the same butterfly network, so these functions follow the codelets'
+//    stage order, twiddle constants and fused multiply-adds step for step.
+//
+//  * A project mixed-radix decimation-in-time FFT for every other length (the
+//    reference uses PocketFFT there, which is not available to restate). Factors
+//    are taken outermost-first as 4,4,...,(2),3,...,5,..., then remaining primes by
+//    direct DFT. Radix-3 and radix-5 butterflies use the same formulas as the
+//    reference's temporal butterflies (src/spectral/fft_backend.cpp:396-420).
+//
+// Conventions (docs/knowledge/en/shared/fft-conventions.md): forward is
+// unnormalised with exp(-2*pi*i*jk/N); inverse uses exp(+...) and the caller
+// applies the 1/V scale once.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define NF_HD __host__ __device__ __forceinline__
+#else
+#define NF_HD inline
+#endif
+
+#if !defined(__CUDACC__)
+#include <cmath>
+#endif
+
+namespace nf {
+
+struct cf {
+  float r, i;
+};
+
+// Round-to-nearest float primitives that are never contracted.
+NF_HD float fadd(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+NF_HD float fsub(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
+NF_HD float fmul(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+NF_HD float ffma(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+  return __fmaf_rn(a, b, c);
+#else
+  return std::fma(a, b, c);
+#endif
+}
+NF_HD float fdiv(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fdiv_rn(a, b);
+#else
+  return a / b;
+#endif
+}
+NF_HD float fsqrt(float a) {
+#if defined(__CUDA_ARCH__)
+  return __fsqrt_rn(a);
+#else
+  return std::sqrt(a);
+#endif
+}
+
+NF_HD cf cadd(cf a, cf b) { return {fadd(a.r, b.r), fadd(a.i, b.i)}; }
+NF_HD cf csub(cf a, cf b) { return {fsub(a.r, b.r), fsub(a.i, b.i)}; }
+
+// ---------------------------------------------------------------------------
+// Codelet-order transforms (8/16/32 points).
+// ---------------------------------------------------------------------------
+
+// cos/sin(k*pi/8) and cos/sin(k*pi/16) rounded to binary32: the codelets' tables
+// (fft16x16_avx2.cpp:12-24, fft32x32_avx2.cpp:12-46), which evaluate cos/sin of
+// float(pi)*k/8 and float(pi)*k/16. Literal values; a host test checks them against
+// the same expressions evaluated by the host compiler.
+NF_HD float tw16r(int k) {
+  const float t[8] = {0x1p+0f,         0x1.d906bcp-1f, 0x1.6a09e6p-1f,  0x1.87de2ap-2f,
+                      -0x1.777a5cp-25f, -0x1.87de3p-2f, -0x1.6a09e6p-1f, -0x1.d906cp-1f};
+  return t[k];
+}
+NF_HD float tw16i(int k) {
+  const float t[8] = {0x0p+0f, 0x1.87de2cp-2f, 0x1.6a09e6p-1f, 0x1.d906bcp-1f,
+                      0x1p+0f, 0x1.d906bcp-1f, 0x1.6a09e6p-1f, 0x1.87de2p-2f};
+  return t[k];
+}
+NF_HD float tw32r(int k) {
+  const float t[16] = {0x1p+0f,         0x1.f6297cp-1f,  0x1.d906bcp-1f,  0x1.a9b662p-1f,
+                       0x1.6a09e6p-1f,  0x1.1c73b2p-1f,  0x1.87de2ap-2f,  0x1.8f8b78p-3f,
+                       -0x1.777a5cp-25f, -0x1.8f8b84p-3f, -0x1.87de3p-2f, -0x1.1c73b8p-1f,
+                       -0x1.6a09e6p-1f, -0x1.a9b664p-1f, -0x1.d906cp-1f, -0x1.f6297ep-1f};
+  return t[k];
+}
+NF_HD float tw32i(int k) {
+  const float t[16] = {0x0p+0f,        0x1.8f8b84p-3f, 0x1.87de2cp-2f, 0x1.1c73b4p-1f,
+                       0x1.6a09e6p-1f, 0x1.a9b664p-1f, 0x1.d906bcp-1f, 0x1.f6297ep-1f,
+                       0x1p+0f,        0x1.f6297cp-1f, 0x1.d906bcp-1f, 0x1.a9b66p-1f,
+                       0x1.6a09e6p-1f, 0x1.1c73b2p-1f, 0x1.87de2p-2f,  0x1.8f8b82p-3f};
+  return t[k];
+}
+
+// (in * w) with w = (wr, FORWARD ? -wi : wi), using the codelets' fused form:
+// re = fma(in.r, wr, -(in.i*wi)), im = fma(in.r, wi, in.i*wr).
+template <bool FORWARD>
+NF_HD cf cmul_codelet(cf in, float wr, float wi_raw) {
+  const float wi = FORWARD ? -wi_raw : wi_raw;
+  return {ffma(in.r, wr, -fmul(in.i, wi)), ffma(in.r, wi, fmul(in.i, wr))};
+}
+// Multiplication by -j (forward) or +j (inverse); the negation is 0-x.
+template <bool FORWARD>
+NF_HD cf mul_j(cf z) {
+  return FORWARD ? cf{z.i, fsub(0.0f, z.r)} : cf{fsub(0.0f, z.i), z.r};
+}
+NF_HD void bfly2(cf& x, cf& y) {
+  const cf u = x, v = y;
+  x = cadd(u, v);
+  y = csub(u, v);
+}
+
+// 8-point transform, codelet order (fft8x8_avx2.cpp:42-138). The codelets are
+// built with -ffp-contract=fast (CMakeLists.txt:91-101), which fuses the W8^1 and
+// W8^3 products by sqrt(1/2) into the following butterfly's sum and difference;
+// the fused form is written out here (checked bit-exact against the codelet).
+template <bool FORWARD>
+NF_HD void fft8(cf* v) {
+  const float s = 0.70710678118654752440f;
+  cf a0 = v[0], a1 = v[4], a2 = v[2], a3 = v[6], a4 = v[1], a5 = v[5], a6 = v[3], a7 = v[7];
+  bfly2(a0, a1);
+  bfly2(a2, a3);
+  bfly2(a4, a5);
+  bfly2(a6, a7);
+  bfly2(a0, a2);
+  bfly2(a4, a6);
+  a3 = mul_j<FORWARD>(a3);
+  a7 = mul_j<FORWARD>(a7);
+  bfly2(a1, a3);
+  bfly2(a5, a7);
+  bfly2(a0, a4);
+  {
+    // a5*W8 then the (a1, a5) butterfly; the product is fused into both sums.
+    const cf u = a5, x = a1;
+    const float tr = FORWARD ? fadd(u.r, u.i) : fsub(u.r, u.i);
+    const float ti = FORWARD ? fsub(u.i, u.r) : fadd(u.i, u.r);
+    a1 = {ffma(s, tr, x.r), ffma(s, ti, x.i)};
+    a5 = {ffma(-s, tr, x.r), ffma(-s, ti, x.i)};
+  }
+  a6 = mul_j<FORWARD>(a6);
+  bfly2(a2, a6);
+  {
+    // a7*W8^3 then the (a3, a7) butterfly, fused the same way.
+    const cf u = a7, x = a3;
+    const float tr = FORWARD ? fsub(u.i, u.r) : fsub(fsub(0.0f, u.r), u.i);
+    const float ti = FORWARD ? fsub(fsub(0.0f, u.r), u.i) : fsub(u.r, u.i);
+    a3 = {ffma(s, tr, x.r), ffma(s, ti, x.i)};
+    a7 = {ffma(-s, tr, x.r), ffma(-s, ti, x.i)};
+  }
+  v[0] = a0; v[1] = a1; v[2] = a2; v[3] = a3; v[4] = a4; v[5] = a5; v[6] = a6; v[7] = a7;
+}
+
+// 16-point transform, codelet order (fft16x16_avx2.cpp:29-194): bit-reversed
+// load, radix-2 stages of span 2, 4, 8 and 16 with the W16 table.
+template <bool FORWARD>
+NF_HD void fft16(cf* v) {
+  cf a[16] = {v[0], v[8], v[4], v[12], v[2], v[10], v[6], v[14], v[1], v[9], v[5], v[13], v[3], v[11], v[7], v[15]};
+#pragma unroll
+  for (int k = 0; k < 16; k += 2) bfly2(a[k], a[k + 1]);
+  // span 4: (x0,x2) plain, (x1, j*x3)
+#pragma unroll
+  for (int g = 0; g < 16; g += 4) {
+    bfly2(a[g], a[g + 2]);
+    const cf v1 = mul_j<FORWARD>(a[g + 3]);
+    const cf u1 = a[g + 1];
+    a[g + 1] = cadd(u1, v1);
+    a[g + 3] = csub(u1, v1);
+  }
+  // span 8: (x0,x4) plain, (x1, W2*x5), (x2, j*x6), (x3, W6*x7)
+#pragma unroll
+  for (int g = 0; g < 16; g += 8) {
+    bfly2(a[g], a[g + 4]);
+    {
+      const cf v1 = cmul_codelet<FORWARD>(a[g + 5], tw16r(2), tw16i(2));
+      const cf u1 = a[g + 1];
+      a[g + 1] = cadd(u1, v1);
+      a[g + 5] = csub(u1, v1);
+    }
+    {
+      const cf v2 = mul_j<FORWARD>(a[g + 6]);
+      const cf u2 = a[g + 2];
+      a[g + 2] = cadd(u2, v2);
+      a[g + 6] = csub(u2, v2);
+    }
+    {
+      const cf v3 = cmul_codelet<FORWARD>(a[g + 7], tw16r(6), tw16i(6));
+      const cf u3 = a[g + 3];
+      a[g + 3] = cadd(u3, v3);
+      a[g + 7] = csub(u3, v3);
+    }
+  }
+  // span 16: (x0,x8) plain, (xk, Wk*x(k+8)) with x12 using j.
+  bfly2(a[0], a[8]);
+#pragma unroll
+  for (int k = 1; k < 8; ++k) {
+    const cf vk = (k == 4) ? mul_j<FORWARD>(a[12]) : cmul_codelet<FORWARD>(a[k + 8], tw16r(k), tw16i(k));
+    const cf uk = a[k];
+    a[k] = cadd(uk, vk);
+    a[k + 8] = csub(uk, vk);
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = a[k];
+}
+
+// 32-point transform, codelet order (fft32x32_avx2.cpp:220-240): two 16-point
+// transforms of the even and odd samples combined with the W32 table.
+template <bool FORWARD>
+NF_HD void fft32(cf* v) {
+  cf e[16], o[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    e[m] = v[2 * m];
+    o[m] = v[2 * m + 1];
+  }
+  fft16<FORWARD>(e);
+  fft16<FORWARD>(o);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const cf w = cmul_codelet<FORWARD>(o[k], tw32r(k), tw32i(k));
+    v[k] = cadd(e[k], w);
+    v[k + 16] = csub(e[k], w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Project mixed-radix DIT transform for arbitrary lengths.
+// ---------------------------------------------------------------------------
+
+// Twiddle table entry w_N^m = (cos(2*pi*m/N), -sin(2*pi*m/N)) for the forward
+// direction, evaluated in binary64 and rounded once to binary32. The inverse uses
+// the conjugate. Tables are built on the host and copied to the device verbatim.
+NF_HD cf cmul_plain(cf a, cf w) {
+  return {fsub(fmul(a.r, w.r), fmul(a.i, w.i)), fadd(fmul(a.r, w.i), fmul(a.i, w.r))};
+}
+template <bool FORWARD>
+NF_HD cf rot_j(cf z) {
+  // forward: multiply by -j; inverse: by +j.
+  return FORWARD ? cf{z.i, -z.r} : cf{-z.i, z.r};
+}
+
+// Radix-3/5 butterflies on t[0..r-1] (in place). Formulas follow the reference's
+// temporal butterflies (fft_backend.cpp:400-419).
+template <bool FORWARD>
+NF_HD void radix3(cf* t) {
+  const float s60 = 0.86602540378443864676f;
+  const cf sum = cadd(t[1], t[2]), diff = csub(t[1], t[2]);
+  const cf center = csub(t[0], cf{fmul(sum.r, 0.5f), fmul(sum.i, 0.5f)});
+  const cf side = rot_j<FORWARD>(cf{fmul(diff.r, s60), fmul(diff.i, s60)});
+  t[0] = cadd(t[0], sum);
+  t[1] = cadd(center, side);
+  t[2] = csub(center, side);
+}
+template <bool FORWARD>
+NF_HD void radix5(cf* v) {
+  const float c1 = 0.30901699437494742410f, c2 = 0.80901699437494742410f;
+  const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
+  const cf a = cadd(v[1], v[4]), b = cadd(v[2], v[3]), c = csub(v[1], v[4]), d = csub(v[2], v[3]);
+  const cf base1 = csub(cadd(v[0], cf{fmul(a.r, c1), fmul(a.i, c1)}), cf{fmul(b.r, c2), fmul(b.i, c2)});
+  const cf base2 = cadd(csub(v[0], cf{fmul(a.r, c2), fmul(a.i, c2)}), cf{fmul(b.r, c1), fmul(b.i, c1)});
+  const cf side1 = rot_j<FORWARD>(cadd(cf{fmul(c.r, s1), fmul(c.i, s1)}, cf{fmul(d.r, s2), fmul(d.i, s2)}));
+  const cf side2 = rot_j<FORWARD>(csub(cf{fmul(c.r, s2), fmul(c.i, s2)}, cf{fmul(d.r, s1), fmul(d.i, s1)}));
+  const cf v0 = cadd(cadd(v[0], a), b);
+  v[0] = v0;
+  v[1] = cadd(base1, side1);
+  v[4] = csub(base1, side1);
+  v[2] = cadd(base2, side2);
+  v[3] = csub(base2, side2);
+}
+template <bool FORWARD>
+NF_HD void radix4(cf* t) {
+  const cf s02 = cadd(t[0], t[2]), d02 = csub(t[0], t[2]);
+  const cf s13 = cadd(t[1], t[3]), d13 = rot_j<FORWARD>(csub(t[1], t[3]));
+  t[0] = cadd(s02, s13);
+  t[2] = csub(s02, s13);
+  t[1] = cadd(d02, d13);
+  t[3] = csub(d02, d13);
+}
+
+// ---------------------------------------------------------------------------
+// Factorisation and the iterative DIT driver.
+//
+// Definition (recursive form): a length-N transform with outermost radix r and
+// M = N/r computes r length-M transforms of x[j::r] (j = 0..r-1), then for each
+// k1 < M multiplies sub_j[k1] by w_N^(j*k1) (skipped when j*k1 == 0) and applies a
+// radix-r butterfly, writing X[k1 + M*q]. The iterative form below performs the
+// same butterflies (digit-reversed load, innermost level first), so its rounding
+// is identical. Twiddles for every level come from the length-N table:
+// w_n^e = table[e * (N/n)].
+// ---------------------------------------------------------------------------
+constexpr int kMaxFactors = 16;
+struct Factors {
+  int count;
+  int r[kMaxFactors];
+};
+NF_HD constexpr int pick_radix(int n) {
+  if (n % 4 == 0) return 4;
+  if (n % 2 == 0) return 2;
+  if (n % 3 == 0) return 3;
+  if (n % 5 == 0) return 5;
+  for (int p = 7; p * p <= n; p += 2)
+    if (n % p == 0) return p;
+  return n;
+}
+// Outermost factor first.
+NF_HD constexpr Factors factorize(int n) {
+  Factors f{0, {}};
+  while (n > 1 && f.count < kMaxFactors) {
+    const int r = pick_radix(n);
+    f.r[f.count++] = r;
+    n /= r;
+  }
+  return f;
+}
+
+// Table of w_N^m for one length, m = 0..N-1 (forward sign).
+struct TwiddleView {
+  const cf* w;  // w[m] = exp(-2*pi*i*m/N)
+  int n;
+};
+
+// Direct radix-p DFT on t[0..p-1] using the length-p twiddles embedded in a
+// length-N table (stride N/p). Sum order is j = 0..p-1.
+template <bool FORWARD>
+NF_HD void radix_direct(cf* t, int p, TwiddleView tw, cf* scratch) {
+  const int stride = tw.n / p;
+  for (int q = 0; q < p; ++q) {
+    cf acc = t[0];
+    for (int j = 1; j < p; ++j) {
+      cf w = tw.w[((j * q) % p) * stride];
+      if (!FORWARD) w.i = -w.i;
+      acc = cadd(acc, cmul_plain(t[j], w));
+    }
+    scratch[q] = acc;
+  }
+  for (int q = 0; q < p; ++q) t[q] = scratch[q];
+}
+
+template <bool FORWARD>
+NF_HD void butterfly(cf* t, int r, const cf* table, int n_top, cf* scratch) {
+  if (r == 2) {
+    bfly2(t[0], t[1]);
+  } else if (r == 3) {
+    radix3<FORWARD>(t);
+  } else if (r == 4) {
+    radix4<FORWARD>(t);
+  } else if (r == 5) {
+    radix5<FORWARD>(t);
+  } else {
+    radix_direct<FORWARD>(t, r, TwiddleView{table, n_top}, scratch);
+  }
+}
+
+// In-place project transform of a[0..n-1]. NC > 0 makes the length a
+// compile-time constant so every loop unrolls into registers; NC == 0 uses the
+// runtime length n (n <= kMaxProject). `table` holds w_n^m, m < n.
+constexpr int kMaxProject = 128;
+template <bool FORWARD, int NC>
+NF_HD void fft_project(cf* a, int n_rt, const cf* table) {
+  const int n = NC > 0 ? NC : n_rt;
+  if (n <= 1) return;
+  const Factors f = factorize(n);
+  constexpr int CAP = NC > 0 ? NC : kMaxProject;
+  cf src[CAP];
+#pragma unroll
+  for (int p = 0; p < CAP; ++p)
+    if (p < n) src[p] = a[p];
+  // Digit-reversed load: the leaf at recursion position p = sum j_l * M_l holds
+  // x[sum j_l * S_l] with M_l = n / (r_0...r_l), S_l = r_0...r_(l-1).
+#pragma unroll
+  for (int p = 0; p < CAP; ++p) {
+    if (p >= n) break;
+    int rem = p, m = n, s = 1, idx = 0;
+#pragma unroll
+    for (int l = 0; l < kMaxFactors; ++l) {
+      if (l >= f.count) break;
+      m /= f.r[l];
+      const int j = rem / m;
+      rem -= j * m;
+      idx += j * s;
+      s *= f.r[l];
+    }
+    a[p] = src[idx];
+  }
+  // Levels from innermost (count-1) to outermost (0).
+  int inner = 1;  // M_l: length of the sub-transforms combined at this level
+#pragma unroll
+  for (int lev = kMaxFactors - 1; lev >= 0; --lev) {
+    if (lev >= f.count) continue;
+    const int r = f.r[lev];
+    const int len = r * inner;
+    const int tw_step = n / len;
+#pragma unroll
+    for (int base = 0; base < CAP; base += 1) {
+      if (base >= n) break;
+      if (base % len != 0) continue;
+#pragma unroll
+      for (int k1 = 0; k1 < CAP; ++k1) {
+        if (k1 >= inner) break;
+        cf t[CAP < 16 ? CAP : 16];
+        cf scratch[CAP < 16 ? CAP : 16];
+#pragma unroll
+        for (int j = 0; j < (CAP < 16 ? CAP : 16); ++j) {
+          if (j >= r) break;
+          cf v = a[base + j * inner + k1];
+          const int e = j * k1;
+          if (e != 0) {
+            cf w = table[e * tw_step];
+            if (!FORWARD) w.i = -w.i;
+            v = cmul_plain(v, w);
+          }
+          t[j] = v;
+        }
+        butterfly<FORWARD>(t, r, table, n, scratch);
+#pragma unroll
+        for (int q = 0; q < (CAP < 16 ? CAP : 16); ++q) {
+          if (q >= r) break;
+          a[base + k1 + inner * q] = t[q];
+        }
+      }
+    }
+    inner = len;
+  }
+}
+
+// 1-D transform dispatch. The reference uses its codelets only for square 8x8,
+// 16x16 and 32x32 blocks (fft_backend.cpp:262-273); every other shape goes to
+// PocketFFT, which the project transform stands in for. The caller passes
+// `codelet` = (block is square and its side is 8, 16 or 32).
+template <bool FORWARD, int NC>
+NF_HD void fft_1d(cf* a, int n_rt, const cf* table, bool codelet) {
+  const int n = NC > 0 ? NC : n_rt;
+  if (codelet && n == 8) {
+    fft8<FORWARD>(a);
+  } else if (codelet && n == 16) {
+    fft16<FORWARD>(a);
+  } else if (codelet && n == 32) {
+    fft32<FORWARD>(a);
+  } else {
+    fft_project<FORWARD, NC>(a, n, table);
+  }
+}
+NF_HD bool is_codelet_length(int n) { return n == 8 || n == 16 || n == 32; }
+
+// ---------------------------------------------------------------------------
+// Real 2-D building blocks (half spectrum [H][W/2+1], x fastest).
+// ---------------------------------------------------------------------------
+
+// Forward transform of one real row of W samples into K = W/2+1 bins: the row is
+// transformed as complex data with zero imaginary parts (the codelets' method,
+// fft16x16_avx2.cpp:239-262). The 16- and 32-point codelets store the Nyquist
+// bin's imaginary part as exactly 0 (fft16x16_avx2.cpp:268-271,
+// fft32x32_avx2.cpp:329-335); the project transform does the same for every even W.
+template <int WC>
+NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool codelet) {
+  const int w = WC > 0 ? WC : w_rt;
+  constexpr int CAP = WC > 0 ? WC : kMaxProject;
+  cf a[CAP];
+#pragma unroll
+  for (int k = 0; k < CAP; ++k)
+    if (k < w) a[k] = cf{x[k], 0.0f};
+  fft_1d<true, WC>(a, w, table, codelet);
+  const int K = w / 2 + 1;
+#pragma unroll
+  for (int k = 0; k < CAP / 2 + 1; ++k)
+    if (k < K) bins[k] = a[k];
+  if (w % 2 == 0 && !(codelet && w == 8)) bins[w / 2].i = 0.0f;
+}
+
+// Inverse of one row: K bins -> W real samples scaled by fct. Bins 1..(W-1)/2 are
+// mirrored as conjugates (imaginary part negated as 0-x, fft16x16_avx2.cpp:420-423).
+// The codelets keep the DC and Nyquist bins as given; for the project transform
+// their imaginary parts are cleared, because a half-complex inverse defines the
+// row from their real parts only.
+template <int WC>
+NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf* table, bool codelet) {
+  const int w = WC > 0 ? WC : w_rt;
+  constexpr int CAP = WC > 0 ? WC : kMaxProject;
+  const int K = w / 2 + 1;
+  cf a[CAP];
+#pragma unroll
+  for (int k = 0; k < CAP / 2 + 1; ++k)
+    if (k < K) a[k] = bins[k];
+#pragma unroll
+  for (int k = 1; k < CAP; ++k)
+    if (k < (w + 1) / 2) a[w - k] = cf{a[k].r, fsub(0.0f, a[k].i)};
+  if (!codelet) {
+    a[0].i = 0.0f;
+    if (w % 2 == 0) a[w / 2].i = 0.0f;
+  }
+  fft_1d<false, WC>(a, w, table, codelet);
+#pragma unroll
+  for (int k = 0; k < CAP; ++k)
+    if (k < w) out[k] = fmul(a[k].r, fct);
+}
+
+// Serial reference drivers for whole blocks (host builders and CPU checks). The
+// tile kernels distribute the same row/column steps over threads.
+NF_HD void block_r2c(const float* in, int in_stride, cf* out, int out_stride, int h, int w, const cf* tw_h,
+                     const cf* tw_w) {
+  const bool codelet = (h == w) && (w == 8 || w == 16 || w == 32);
+  const int K = w / 2 + 1;
+  for (int y = 0; y < h; ++y) row_forward<0>(in + y * in_stride, w, out + y * out_stride, tw_w, codelet);
+  cf col[kMaxProject];
+  for (int k = 0; k < K; ++k) {
+    for (int y = 0; y < h; ++y) col[y] = out[y * out_stride + k];
+    fft_1d<true, 0>(col, h, tw_h, codelet);
+    for (int y = 0; y < h; ++y) out[y * out_stride + k] = col[y];
+  }
+}
+NF_HD void block_c2r(const cf* in, int in_stride, float* out, int out_stride, int h, int w, float fct,
+                     const cf* tw_h, const cf* tw_w) {
+  const bool codelet = (h == w) && (w == 8 || w == 16 || w == 32);
+  const int K = w / 2 + 1;
+  cf tmp[kMaxProject * (kMaxProject / 2 + 1)];
+  cf col[kMaxProject];
+  for (int k = 0; k < K; ++k) {
+    for (int y = 0; y < h; ++y) col[y] = in[y * in_stride + k];
+    fft_1d<false, 0>(col, h, tw_h, codelet);
+    for (int y = 0; y < h; ++y) tmp[y * K + k] = col[y];
+  }
+  for (int y = 0; y < h; ++y) row_inverse<0>(tmp + y * K, w, fct, out + y * out_stride, tw_w, codelet);
+}
+
+} // namespace nf

@@ -1,0 +1,320 @@
+"""Benchmark: DFTTest (sbsize 16, sosize 12, ftype 0, sigma 8 with a flat sigma curve,
+dither 0) over a 1920x1080 YUV420P16 clip of 60 frames — luma 1920x1080 and two
+960x540 chroma planes per frame, synthetic seeded band-limited texture in
+[4096, 60000] plus Gaussian noise sd 600.
+
+A step is one pass of the per-plane pipeline over the whole clip (60 frames x 3
+planes; ~746 MB of input and output per step, larger than the 126 MB L2, so no
+flush is needed between steps). Mpx counts luma pixels per output frame.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (one process per GPU under torchrun): every rank filters its own clip
+(weak scaling, no data-path collective); the time is the max over ranks.
+--impl reference times the reference core's CPU implementation of the same
+workload (compiled from its own sources, oracle/_ref) on all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+W, H, CW, CH, FRAMES = 1920, 1080, 960, 540, 60
+METRIC = "Mpx/s per config on 1 B200 (plain vs batched/graph), fwd+bwd Mpx/s, vs host CPU"
+WORKLOAD = "DFTTest tbsize=1 sbsize=16 sosize=12 ftype=0 sigma=8 flat curve, 1920x1080 YUV420P16, 60 frames"
+
+
+def dft_config():
+    from neo_fft_b200 import DFTConfig
+    return DFTConfig(block=16, overlap=12, mode=1, ftype=0, sigma=8.0, tbsize=1, dither=0, slocation=[0, 8, 1, 8])
+
+
+def make_plane(h, w, seed):
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    t = gaussian_filter(rng.standard_normal((h, w)), 3.0)
+    t = (t - t.min()) / max(np.ptp(t), 1e-12)
+    v = 4096 + (60000 - 4096) * t + rng.standard_normal((h, w)) * 600
+    return np.clip(np.round(v), 0, 65535).astype(np.uint16)
+
+
+def make_clip(rank: int, frames: int):
+    """Frames of (Y, U, V) planes; seeds [2, clip, frame]. Frames beyond a small
+    distinct set reuse seeds to keep host generation short (content does not change
+    the arithmetic per pixel)."""
+    distinct = min(frames, 6)
+    base = [(make_plane(H, W, [2, rank, f, 0]), make_plane(CH, CW, [2, rank, f, 1]), make_plane(CH, CW, [2, rank, f, 2]))
+            for f in range(distinct)]
+    return [base[f % distinct] for f in range(frames)]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index, self.samples, self._stop = index, [], threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in out.stdout.strip().split(",")]
+                if len(f) >= 7:
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(frames_sample: int = 2):
+    """The reference core (compiled from its own sources) on the host cores: frames
+    run concurrently, one shared plan per plane size."""
+    from neo_fft_b200 import SampleFormat
+    from oracle import ref as R
+    if not R.available():
+        return None
+    threads = os.cpu_count() or 1
+    fmt = SampleFormat(16)
+    luma = R.RefPlan(W, H, fmt, dft_config())
+    chroma = R.RefPlan(CW, CH, fmt, dft_config())
+    clip = make_clip(0, max(frames_sample, threads))
+    n = max(frames_sample, threads)
+    t0 = time.perf_counter()
+    luma.process_many([[c[0]] for c in clip[:n]], threads)
+    chroma.process_many([[c[p]] for c in clip[:n] for p in (1, 2)], threads)
+    dt = time.perf_counter() - t0
+    return {"value": n * W * H / dt / 1e6, "unit": "Mpx/s", "cores": threads, "kind": "reference",
+            "sample": f"{n} frames (Y+U+V) of the same clip, frames concurrent on {threads} threads, "
+                      "reference core built from source with its codelet FFT backend"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle library not built"}))
+        return
+    threads = os.cpu_count() or 1
+    from neo_fft_b200 import SampleFormat
+    fmt = SampleFormat(16)
+    luma = R.RefPlan(W, H, fmt, dft_config())
+    chroma = R.RefPlan(CW, CH, fmt, dft_config())
+    n = threads  # one frame per host thread per step (a bounded sample of the clip)
+    clip = make_clip(0, n)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        luma.process_many([[c[0]] for c in clip], threads)
+        chroma.process_many([[c[p]] for c in clip for p in (1, 2)], threads)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    dt = float(np.mean(times))
+    value = n * W * H / dt / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpx/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_frames_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "Mpx/s", "cores": threads, "kind": "reference",
+                         "sample": f"{n} frames per step (Y+U+V), frames concurrent on {threads} host threads"},
+        "e2e": {"value": value, "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from neo_fft_b200 import Plan, SampleFormat
+    from neo_fft_b200 import _capi as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    fmt = SampleFormat(16)
+    luma = Plan(W, H, fmt, dft_config())
+    chroma = Plan(CW, CH, fmt, dft_config())
+    lib = C.load()
+    clip = make_clip(rank, FRAMES)
+    # device-resident inputs and outputs
+    d_in = [[torch.from_numpy(p).to(dev) for p in f] for f in clip]
+    d_out = [[torch.empty_like(p) for p in f] for f in d_in]
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes_stream(stream)
+    err = __import__("ctypes").create_string_buffer(256)
+
+    def plane_call(plan, src, dst):
+        srcs = (C.NfConstPlane * 1)(C.NfConstPlane(src.data_ptr(), src.shape[1], src.shape[0], src.stride(0) * 2))
+        d = C.NfPlane(dst.data_ptr(), dst.shape[1], dst.shape[0], dst.stride(0) * 2)
+        st = lib.nf_plan_process_device(plan._h, srcs, 1, None, 0, d, 0, 0, sptr, err, 256)
+        if st:
+            C.raise_for(st, err.value)
+
+    def step():
+        for f in range(FRAMES):
+            plane_call(luma, d_in[f][0], d_out[f][0])
+            plane_call(chroma, d_in[f][1], d_out[f][1])
+            plane_call(chroma, d_in[f][2], d_out[f][2])
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    luma.sync_status()
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        barrier()
+    ms = start.elapsed_time(end)
+    luma.sync_status()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * FRAMES * W * H / (ms_step / 1e3) / 1e6
+
+    # Roofline of the dominant kernel: the luma launch timed alone on the same stream.
+    reps = 20
+    for _ in range(3):
+        plane_call(luma, d_in[0][0], d_out[0][0])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for r in range(reps):
+        plane_call(luma, d_in[r % FRAMES][0], d_out[r % FRAMES][0])
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launch_ms = e0.elapsed_time(e1) / reps
+    g = luma.geometry
+    alg_bytes = W * H * 2 * 2                      # each input sample read once + output written once
+    blocks = g.x.count * g.y.count
+    alg_flops = blocks * (2 * 10240 + 144 * 12)    # 2.5 N log2 N per real transform pair + per-bin filter
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved_gbs = alg_bytes / (launch_ms / 1e3) / 1e9
+    fp32_peak = 148 * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    achieved_tf = alg_flops / (launch_ms / 1e3) / 1e12
+
+    # End to end through the public host-memory API from pinned host buffers.
+    pinned_in = [[torch.from_numpy(p).pin_memory().numpy() for p in f] for f in clip]
+    pinned_out = [[torch.empty(p.shape, dtype=torch.uint16).pin_memory().numpy() for p in f] for f in clip]
+    for f in range(2):
+        luma.process([pinned_in[f][0]], pinned_out[f][0])
+    barrier()
+    e2e_steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for f in range(FRAMES):
+            luma.process([pinned_in[f][0]], pinned_out[f][0])
+            chroma.process([pinned_in[f][1]], pinned_out[f][1])
+            chroma.process([pinned_in[f][2]], pinned_out[f][2])
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    plane_bytes = FRAMES * (W * H + 2 * CW * CH) * 2
+    e2e_value = world * FRAMES * W * H / e2e_s / 1e6
+
+    cpu = cpu_baseline() if (rank == 0 and world == 1) else None
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "frames_per_step": FRAMES, "planes": "Y 1920x1080 + U,V 960x540 u16",
+                   "parallelism": f"clip-per-rank x{world}", "l2": "inputs larger than L2 (746 MB per step)"},
+        "e2e": {"value": e2e_value, "unit": "Mpx/s", "h2d_bytes_per_step": plane_bytes,
+                "d2h_bytes_per_step": plane_bytes},
+        "gpu_launches": FRAMES * 3 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved_gbs / hbm_peak, "traffic": None,
+                     "kernel": "spatial_tile_kernel<16,16,u16> (luma plane)", "launch_ms": launch_ms,
+                     "alg_bytes_per_launch": alg_bytes,
+                     "fp32": {"achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                              "frac": achieved_tf / fp32_peak, "alg_flops_per_launch": alg_flops,
+                              "peak_source": "148 SMs x 128 FP32 lanes x 2 x max SM clock (nominal)"}},
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def ctypes_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,7 @@
+"""neo_fft_b200 — B200 (sm_100a) implementation of neo-fft's per-plane spectral pipeline.
+
+The public surface mirrors the reference core's `Plan` API; see `plan.py`.
+"""
+from .plan import (Axis, DFTConfig, FFT3DConfig, Geometry, KalmanState, Plan, SampleFormat,  # noqa: F401
+                   kernel_info)
+from ._capi import DeviceError, NonFiniteError  # noqa: F401

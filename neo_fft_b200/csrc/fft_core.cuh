@@ -380,75 +380,150 @@ NF_HD void butterfly(cf* t, int r, const cf* table, int n_top, cf* scratch) {
   }
 }
 
-// In-place project transform of a[0..n-1]. NC > 0 makes the length a
-// compile-time constant so every loop unrolls into registers; NC == 0 uses the
-// runtime length n (n <= kMaxProject). `table` holds w_n^m, m < n.
-constexpr int kMaxProject = 128;
-template <bool FORWARD, int NC>
-NF_HD void fft_project(cf* a, int n_rt, const cf* table) {
-  const int n = NC > 0 ? NC : n_rt;
-  if (n <= 1) return;
-  const Factors f = factorize(n);
-  constexpr int CAP = NC > 0 ? NC : kMaxProject;
-  cf src[CAP];
-#pragma unroll
-  for (int p = 0; p < CAP; ++p)
-    if (p < n) src[p] = a[p];
-  // Digit-reversed load: the leaf at recursion position p = sum j_l * M_l holds
-  // x[sum j_l * S_l] with M_l = n / (r_0...r_l), S_l = r_0...r_(l-1).
-#pragma unroll
-  for (int p = 0; p < CAP; ++p) {
-    if (p >= n) break;
-    int rem = p, m = n, s = 1, idx = 0;
-#pragma unroll
-    for (int l = 0; l < kMaxFactors; ++l) {
-      if (l >= f.count) break;
-      m /= f.r[l];
-      const int j = rem / m;
-      rem -= j * m;
-      idx += j * s;
-      s *= f.r[l];
+// Compile-time form: constexpr factorisation and digit-reversal table, one
+// template instance per level; every index is a constant, so the transform is
+// fully unrolled into registers.
+template <int N>
+struct DigitReversal {
+  int v[N];
+  NF_HD constexpr DigitReversal() : v() {
+    const Factors f = factorize(N);
+    for (int p = 0; p < N; ++p) {
+      int rem = p, m = N, s = 1, idx = 0;
+      for (int l = 0; l < f.count; ++l) {
+        m /= f.r[l];
+        const int j = rem / m;
+        rem -= j * m;
+        idx += j * s;
+        s *= f.r[l];
+      }
+      v[p] = idx;
     }
-    a[p] = src[idx];
   }
-  // Levels from innermost (count-1) to outermost (0).
-  int inner = 1;  // M_l: length of the sub-transforms combined at this level
+};
+
+template <bool FORWARD, int R>
+NF_HD void butterfly_ct(cf* t, const cf* table, int n_top) {
+  if constexpr (R == 2) {
+    bfly2(t[0], t[1]);
+  } else if constexpr (R == 3) {
+    radix3<FORWARD>(t);
+  } else if constexpr (R == 4) {
+    radix4<FORWARD>(t);
+  } else if constexpr (R == 5) {
+    radix5<FORWARD>(t);
+  } else {
+    cf scratch[R];
+    const int stride = n_top / R;
 #pragma unroll
-  for (int lev = kMaxFactors - 1; lev >= 0; --lev) {
-    if (lev >= f.count) continue;
-    const int r = f.r[lev];
-    const int len = r * inner;
-    const int tw_step = n / len;
+    for (int q = 0; q < R; ++q) {
+      cf acc = t[0];
 #pragma unroll
-    for (int base = 0; base < CAP; base += 1) {
-      if (base >= n) break;
-      if (base % len != 0) continue;
+      for (int j = 1; j < R; ++j) {
+        cf w = table[((j * q) % R) * stride];
+        if (!FORWARD) w.i = -w.i;
+        acc = cadd(acc, cmul_plain(t[j], w));
+      }
+      scratch[q] = acc;
+    }
 #pragma unroll
-      for (int k1 = 0; k1 < CAP; ++k1) {
-        if (k1 >= inner) break;
-        cf t[CAP < 16 ? CAP : 16];
-        cf scratch[CAP < 16 ? CAP : 16];
+    for (int q = 0; q < R; ++q) t[q] = scratch[q];
+  }
+}
+
+template <bool FORWARD, int N, int LEV, int INNER>
+NF_HD void ct_level(cf* a, const cf* table) {
+  constexpr Factors F = factorize(N);
+  constexpr int R = F.r[LEV];
+  constexpr int LEN = R * INNER;
+  constexpr int STEP = N / LEN;
 #pragma unroll
-        for (int j = 0; j < (CAP < 16 ? CAP : 16); ++j) {
-          if (j >= r) break;
-          cf v = a[base + j * inner + k1];
-          const int e = j * k1;
-          if (e != 0) {
-            cf w = table[e * tw_step];
-            if (!FORWARD) w.i = -w.i;
-            v = cmul_plain(v, w);
-          }
-          t[j] = v;
+  for (int base = 0; base < N; base += LEN) {
+#pragma unroll
+    for (int k1 = 0; k1 < INNER; ++k1) {
+      cf t[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        cf v = a[base + j * INNER + k1];
+        if (j * k1 != 0) {
+          cf w = table[j * k1 * STEP];
+          if (!FORWARD) w.i = -w.i;
+          v = cmul_plain(v, w);
         }
-        butterfly<FORWARD>(t, r, table, n, scratch);
+        t[j] = v;
+      }
+      butterfly_ct<FORWARD, R>(t, table, N);
 #pragma unroll
-        for (int q = 0; q < (CAP < 16 ? CAP : 16); ++q) {
-          if (q >= r) break;
-          a[base + k1 + inner * q] = t[q];
+      for (int q = 0; q < R; ++q) a[base + k1 + INNER * q] = t[q];
+    }
+  }
+  if constexpr (LEV > 0) ct_level<FORWARD, N, LEV - 1, LEN>(a, table);
+}
+
+template <bool FORWARD, int N>
+NF_HD void fft_ct(cf* a, const cf* table) {
+  if constexpr (N > 1) {
+    constexpr DigitReversal<N> perm{};
+    constexpr Factors F = factorize(N);
+    cf src[N];
+#pragma unroll
+    for (int p = 0; p < N; ++p) src[p] = a[p];
+#pragma unroll
+    for (int p = 0; p < N; ++p) a[p] = src[perm.v[p]];
+    ct_level<FORWARD, N, F.count - 1, 1>(a, table);
+  }
+}
+
+// In-place project transform of a[0..n-1]; `table` holds w_n^m, m < n.
+// NC > 0: compile-time length (fft_ct above). NC == 0: the same butterflies in a
+// runtime loop nest for lengths n <= RCAP.
+constexpr int kMaxProject = 128;
+template <bool FORWARD, int NC, int RCAP = kMaxProject>
+NF_HD void fft_project(cf* a, int n_rt, const cf* table) {
+  if constexpr (NC > 0) {
+    fft_ct<FORWARD, NC>(a, table);
+  } else {
+    const int n = n_rt;
+    if (n <= 1) return;
+    const Factors f = factorize(n);
+    cf src[RCAP];
+    for (int p = 0; p < n; ++p) src[p] = a[p];
+    for (int p = 0; p < n; ++p) {
+      int rem = p, m = n, s = 1, idx = 0;
+      for (int l = 0; l < f.count; ++l) {
+        m /= f.r[l];
+        const int j = rem / m;
+        rem -= j * m;
+        idx += j * s;
+        s *= f.r[l];
+      }
+      a[p] = src[idx];
+    }
+    int inner = 1;
+    for (int lev = f.count - 1; lev >= 0; --lev) {
+      const int r = f.r[lev];
+      const int len = r * inner;
+      const int tw_step = n / len;
+      for (int base = 0; base < n; base += len) {
+        for (int k1 = 0; k1 < inner; ++k1) {
+          cf t[kMaxProject < 64 ? kMaxProject : 64];
+          cf scratch[kMaxProject < 64 ? kMaxProject : 64];
+          for (int j = 0; j < r; ++j) {
+            cf v = a[base + j * inner + k1];
+            const int e = j * k1;
+            if (e != 0) {
+              cf w = table[e * tw_step];
+              if (!FORWARD) w.i = -w.i;
+              v = cmul_plain(v, w);
+            }
+            t[j] = v;
+          }
+          butterfly<FORWARD>(t, r, table, n, scratch);
+          for (int q = 0; q < r; ++q) a[base + k1 + inner * q] = t[q];
         }
       }
+      inner = len;
     }
-    inner = len;
   }
 }
 
@@ -484,13 +559,14 @@ template <int WC>
 NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool codelet) {
   const int w = WC > 0 ? WC : w_rt;
   constexpr int CAP = WC > 0 ? WC : kMaxProject;
+  constexpr int U = WC > 0 ? CAP : 1;
   cf a[CAP];
-#pragma unroll
+#pragma unroll U
   for (int k = 0; k < CAP; ++k)
     if (k < w) a[k] = cf{x[k], 0.0f};
   fft_1d<true, WC>(a, w, table, codelet);
   const int K = w / 2 + 1;
-#pragma unroll
+#pragma unroll U
   for (int k = 0; k < CAP / 2 + 1; ++k)
     if (k < K) bins[k] = a[k];
   if (w % 2 == 0 && !(codelet && w == 8)) bins[w / 2].i = 0.0f;
@@ -505,12 +581,13 @@ template <int WC>
 NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf* table, bool codelet) {
   const int w = WC > 0 ? WC : w_rt;
   constexpr int CAP = WC > 0 ? WC : kMaxProject;
+  constexpr int U = WC > 0 ? CAP : 1;
   const int K = w / 2 + 1;
   cf a[CAP];
-#pragma unroll
+#pragma unroll U
   for (int k = 0; k < CAP / 2 + 1; ++k)
     if (k < K) a[k] = bins[k];
-#pragma unroll
+#pragma unroll U
   for (int k = 1; k < CAP; ++k)
     if (k < (w + 1) / 2) a[w - k] = cf{a[k].r, fsub(0.0f, a[k].i)};
   if (!codelet) {
@@ -518,7 +595,7 @@ NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf
     if (w % 2 == 0) a[w / 2].i = 0.0f;
   }
   fft_1d<false, WC>(a, w, table, codelet);
-#pragma unroll
+#pragma unroll U
   for (int k = 0; k < CAP; ++k)
     if (k < w) out[k] = fmul(a[k].r, fct);
 }

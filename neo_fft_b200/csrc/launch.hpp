@@ -1,0 +1,44 @@
+// Kernel launchers, one translation unit per block shape (spatial_inst.cu is
+// compiled once per shape with -DNF_BH/-DNF_BW; 0 = runtime shape).
+#pragma once
+#include "device_plan.cuh"
+
+#include <cuda_runtime.h>
+
+namespace nfd {
+struct TileShape;
+#define NF_DECLARE_SPATIAL(BH, BW)                                                                              \
+  cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const TileShape& s, dim3 grid, size_t smem,          \
+                                         const void* src, ptrdiff_t ss, void* dst, ptrdiff_t ds, const cf* L,   \
+                                         cudaStream_t st);
+NF_DECLARE_SPATIAL(8, 8)
+NF_DECLARE_SPATIAL(16, 16)
+NF_DECLARE_SPATIAL(32, 32)
+NF_DECLARE_SPATIAL(12, 12)
+NF_DECLARE_SPATIAL(48, 48)
+NF_DECLARE_SPATIAL(0, 0)
+#undef NF_DECLARE_SPATIAL
+struct KalmanArgs;
+struct VolumeShape;
+struct VolumeSources;
+#define NF_DECLARE_VOLUME(BH, BW)                                                                               \
+  cudaError_t launch_volume_##BH##x##BW(const DevPlan& d, const VolumeShape& s, dim3 grid, size_t smem,         \
+                                        const VolumeSources& v, void* dst, ptrdiff_t ds, cudaStream_t st);
+NF_DECLARE_VOLUME(8, 8)
+NF_DECLARE_VOLUME(16, 16)
+NF_DECLARE_VOLUME(32, 32)
+NF_DECLARE_VOLUME(12, 12)
+NF_DECLARE_VOLUME(48, 48)
+NF_DECLARE_VOLUME(0, 0)
+#undef NF_DECLARE_VOLUME
+#define NF_DECLARE_KALMAN(BH, BW)                                                                               \
+  cudaError_t launch_kalman_##BH##x##BW(const DevPlan& d, int nb, dim3 grid, size_t smem, const void* src,      \
+                                        ptrdiff_t ss, const KalmanArgs& a, cudaStream_t st);
+NF_DECLARE_KALMAN(8, 8)
+NF_DECLARE_KALMAN(16, 16)
+NF_DECLARE_KALMAN(32, 32)
+NF_DECLARE_KALMAN(12, 12)
+NF_DECLARE_KALMAN(48, 48)
+NF_DECLARE_KALMAN(0, 0)
+#undef NF_DECLARE_KALMAN
+} // namespace nfd

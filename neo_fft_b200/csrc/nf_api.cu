@@ -1,0 +1,623 @@
+// C ABI of the B200 pipeline (include/neo_fft_b200.h): plan creation, validation
+// and kernel launches. Host-side checks mirror neo-fft's Plan::run
+// (src/algorithms/plan.cpp:331-375) with the same error texts.
+#include "neo_fft_b200.h"
+#include "plan_build.hpp"
+#include "tile_spatial.cuh"
+#include "tile_volume.cuh"
+#include "launch.hpp"
+#include "kalman.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using nf::cf;
+
+struct nf_plan {
+  nfb::PlanTables t;
+  nfd::DevPlan dev{};
+  void* tables = nullptr;  // one device allocation holding every table
+  int* err = nullptr;      // device error word
+  int device = 0;
+  mutable std::mutex staging_mu;
+  mutable void* staging = nullptr;  // device staging for the host-memory path
+  mutable size_t staging_bytes = 0;
+  ~nf_plan() {
+    if (tables) cudaFree(tables);
+    if (err) cudaFree(err);
+    if (staging) cudaFree(staging);
+  }
+};
+
+struct nf_kalman_state {
+  const nf_plan* plan = nullptr;
+  size_t count = 0;
+  int fp64 = 0;
+  cf* last = nullptr;       // [count]
+  void* covariance = nullptr;  // float or double [count]
+  void* process = nullptr;
+  ~nf_kalman_state() {
+    if (last) cudaFree(last);
+    if (covariance) cudaFree(covariance);
+    if (process) cudaFree(process);
+  }
+};
+
+namespace {
+
+nf_status fail(char* err, size_t len, const std::string& msg, nf_status code) {
+  if (err && len) {
+    std::strncpy(err, msg.c_str(), len - 1);
+    err[len - 1] = 0;
+  }
+  return code;
+}
+nf_status cuda_fail(char* err, size_t len, cudaError_t e, const char* what) {
+  return fail(err, len, std::string(what) + ": " + cudaGetErrorString(e), NF_DEVICE_ERROR);
+}
+template <class F>
+nf_status guarded(char* err, size_t len, F&& f) {
+  try {
+    return f();
+  } catch (const std::invalid_argument& e) {
+    return fail(err, len, e.what(), NF_INVALID_ARGUMENT);
+  } catch (const std::runtime_error& e) {
+    return fail(err, len, e.what(), NF_NON_FINITE);
+  } catch (const std::bad_alloc&) {
+    return fail(err, len, "host allocation failed", NF_DEVICE_ERROR);
+  }
+}
+
+int storage_of(nf_format f) { return f.floating ? nfd::kStoreF32 : (f.bits == 8 ? nfd::kStoreU8 : nfd::kStoreU16); }
+
+// Packs host tables into one aligned blob and records each table's offset.
+struct Blob {
+  std::vector<unsigned char> bytes;
+  size_t add(const void* p, size_t n) {
+    if (!n) return SIZE_MAX;
+    const size_t off = (bytes.size() + 255) & ~size_t(255);
+    bytes.resize(off + n);
+    std::memcpy(bytes.data() + off, p, n);
+    return off;
+  }
+  template <class T>
+  size_t add(const std::vector<T>& v) {
+    return add(v.data(), v.size() * sizeof(T));
+  }
+};
+
+nfd::DevAxis dev_axis(const nfb::Axis& a) {
+  return {a.length, a.block, a.overlap, a.step, a.count, a.cover, a.offset};
+}
+
+// Temporal twiddles of the FFT3D temporal kernel (get_fft3d_twiddles,
+// src/kernels/scalar/spectral.cpp:67-88): binary64 angles, binary32 values.
+void temporal_twiddles(int T, int c, std::vector<cf>& fwd, std::vector<cf>& inv) {
+  constexpr double kPi = 3.1415926535897932384626433832795;
+  fwd.assign(size_t(T) * T, cf{0, 0});
+  inv.assign(size_t(T), cf{0, 0});
+  for (int m = 0; m < T; ++m)
+    for (int j = 0; j < T; ++j) {
+      const double angle = -2.0 * kPi * double(j * m) / double(T);
+      fwd[size_t(m) * T + j] = {float(std::cos(angle)), float(std::sin(angle))};
+    }
+  for (int m = 0; m < T; ++m) {
+    const double a = +2.0 * kPi * double(c * m) / double(T);
+    inv[size_t(m)] = {float(std::cos(a)), float(std::sin(a))};
+  }
+}
+
+nf_status finalize_plan(std::unique_ptr<nf_plan>& p, char* err, size_t len) {
+  const nfb::PlanTables& t = p->t;
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "no CUDA device");
+  Blob blob;
+  const auto twh = nfb::twiddle_table(t.bh), tww = nfb::twiddle_table(t.bw), twt = nfb::twiddle_table(t.temporal_size);
+  std::vector<cf> tfwd, tinv;
+  temporal_twiddles(std::max(1, t.temporal_size), t.temporal_size / 2, tfwd, tinv);
+  const size_t o_wxa = blob.add(t.wx.analysis), o_wya = blob.add(t.wy.analysis), o_wxs = blob.add(t.wx.synthesis),
+               o_wys = blob.add(t.wy.synthesis), o_h = blob.add(t.h), o_hs = blob.add(t.h_synthesis),
+               o_grid = blob.add(t.grid), o_prim = blob.add(t.spectral.primary),
+               o_sw = blob.add(t.enhancement.sharpen_window), o_hw = blob.add(t.enhancement.halo_window),
+               o_twh = blob.add(twh), o_tww = blob.add(tww), o_twt = blob.add(twt), o_tf = blob.add(tfwd),
+               o_ti = blob.add(tinv);
+  if ((e = cudaMalloc(&p->tables, std::max<size_t>(blob.bytes.size(), 256))) != cudaSuccess)
+    return cuda_fail(err, len, e, "device allocation failed");
+  if ((e = cudaMemcpy(p->tables, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail(err, len, e, "table upload failed");
+  if ((e = cudaMalloc(&p->err, sizeof(int))) != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
+  if ((e = cudaMemset(p->err, 0, sizeof(int))) != cudaSuccess) return cuda_fail(err, len, e, "device memset failed");
+  auto* base = static_cast<unsigned char*>(p->tables);
+  auto ptr = [&](size_t off) -> const void* { return off == SIZE_MAX ? nullptr : base + off; };
+
+  nfd::DevPlan& d = p->dev;
+  d.algo = t.algo == nfb::Algo::FFT3D ? 0 : 1;
+  d.gx = dev_axis(t.gx);
+  d.gy = dev_axis(t.gy);
+  d.bh = t.bh;
+  d.bw = t.bw;
+  d.K = t.bw / 2 + 1;
+  d.bins = t.bins;
+  d.T = t.temporal_size;
+  d.storage = storage_of(t.format);
+  const bool int_chroma = !t.format.floating && t.format.chroma;
+  if (d.algo == 0) {
+    d.dec_base = int_chroma ? float(1 << (t.format.bits - 1)) : 0.0f;
+    d.dec_scale = 1.0f;
+    d.out_base = d.dec_base;
+    d.out_scale = 1.0f;
+  } else {
+    d.dec_base = 0.0f;
+    d.dec_scale = t.format.floating ? 255.0f : 1.0f / float(1 << (t.format.bits - 8));
+    d.out_base = 0.0f;
+    d.out_scale = t.format.floating ? 1.0f / 255.0f : float(1 << (t.format.bits - 8));
+  }
+  d.out_peak = t.format.floating ? 1.0f : float((1 << t.format.bits) - 1);
+  d.wxa = static_cast<const float*>(ptr(o_wxa));
+  d.wya = static_cast<const float*>(ptr(o_wya));
+  d.wxs = static_cast<const float*>(ptr(o_wxs));
+  d.wys = static_cast<const float*>(ptr(o_wys));
+  d.h = static_cast<const float*>(ptr(o_h));
+  d.hsyn = static_cast<const float*>(ptr(o_hs));
+  d.grid = static_cast<const cf*>(ptr(o_grid));
+  d.mean_scale = t.mean_scale;
+  const auto& s = t.spectral;
+  const auto& en = t.enhancement;
+  d.filt = {s.type,  s.a, s.b, s.low, s.high, s.exponent, s.floor, static_cast<const float*>(ptr(o_prim)),
+            s.fused_enhancement ? 1 : 0,
+            en.sharpen, en.dehalo, en.a, en.b, en.c,
+            static_cast<const float*>(ptr(o_sw)), static_cast<const float*>(ptr(o_hw))};
+  d.enh = {-2, 0, 0, 0, 0, 1, 0, nullptr, en.active() ? 1 : 0, en.sharpen, en.dehalo, en.a, en.b, en.c,
+           static_cast<const float*>(ptr(o_sw)), static_cast<const float*>(ptr(o_hw))};
+  if (d.algo == 0)
+    d.fft3d_mode = !t.denoise ? nfd::kEnhanceOnly : (!s.primary.empty() ? nfd::kWienerThenEnh : nfd::kWienerFused);
+  d.codelet = (t.bh == t.bw && (t.bw == 8 || t.bw == 16 || t.bw == 32)) ? 1 : 0;
+  d.twh = static_cast<const cf*>(ptr(o_twh));
+  d.tww = static_cast<const cf*>(ptr(o_tww));
+  d.twt = static_cast<const cf*>(ptr(o_twt));
+  d.tfwd = static_cast<const cf*>(ptr(o_tf));
+  d.tinv = static_cast<const cf*>(ptr(o_ti));
+  d.center = t.center ? 1 : 0;
+  d.err = p->err;
+  d.lower = (t.beta - 1.0f) / t.beta;
+  // NoisePower of the temporal path (plan.cpp:421-425): T*sigma^2/norm or table*T.
+  d.noise_uniform = ((float(t.temporal_size) * t.sigma_eff) * t.sigma_eff) / t.norm;
+  d.noise_mult = float(t.temporal_size);
+  d.kalman_r0 = t.kalman_r0;
+  d.kalman_ratio2 = t.kalman_ratio2;
+  return NF_OK;
+}
+
+// --- plane validation (checked_plane / plane_extent, src/base/checked.hpp:43-79) ---
+size_t plane_extent(long long w, long long h, ptrdiff_t stride, size_t elem) {
+  nfb::require(w > 0 && w <= INT32_MAX && h > 0 && h <= INT32_MAX, "dimension outside int32 domain");
+  nfb::require(stride > 0 && stride % ptrdiff_t(elem) == 0 && stride / ptrdiff_t(elem) <= INT32_MAX,
+               "invalid plane byte stride");
+  const size_t row = size_t(w) * elem;
+  nfb::require(size_t(stride) >= row, "stride shorter than active row");
+  return size_t(h - 1) * size_t(stride) + row;
+}
+void check_pointer(const void* data, size_t elem) {
+  nfb::require(data && reinterpret_cast<uintptr_t>(data) % elem == 0, "invalid plane pointer alignment");
+}
+void disjoint(const void* a, size_t an, const void* b, size_t bn) {
+  const auto ap = reinterpret_cast<uintptr_t>(a), bp = reinterpret_cast<uintptr_t>(b);
+  nfb::require(ap + an <= bp || bp + bn <= ap, "partially overlapping or aliased buffers");
+}
+
+struct Checked {
+  int tslots = 1;
+  int unique = 0;
+};
+
+Checked validate_call(const nf_plan& p, const nf_const_plane* sources, int n, const int* targets, int nt,
+                      const nf_plane& dst) {
+  const auto& t = p.t;
+  nfb::require(n > 0 && sources, "sources must not be empty");
+  nfb::require(n <= 225, "too many temporal slots");
+  Checked c;
+  c.tslots = t.temporal_ola ? t.temporal_size : n;
+  if (t.temporal_ola) {
+    nfb::require(nt > 0 && nt <= 15 && n == nt * t.temporal_size, "invalid temporal block inputs");
+    for (int i = 0; i < nt; ++i) nfb::require(targets[i] >= 0 && targets[i] < c.tslots, "invalid target temporal slice");
+  }
+  if (t.algo == nfb::Algo::DFTTest)
+    nfb::require(c.tslots == t.temporal_size, "DFTTest sources size must match plan temporal_size");
+  else
+    nfb::require(c.tslots == t.temporal_size || c.tslots == 1,
+                 "FFT3D sources size must match plan temporal_size or single-frame fallback");
+  nfb::require(dst.width == t.gx.length && dst.height == t.gy.length, "frame dimensions differ from plan");
+  const size_t elem = size_t(storage_of(t.format));
+  const size_t de = plane_extent(dst.width, dst.height, dst.stride_bytes, elem);
+  check_pointer(dst.data, elem);
+  for (int j = 0; j < n; ++j) {
+    const auto& s = sources[j];
+    nfb::require(s.width == t.gx.length && s.height == t.gy.length, "frame dimensions differ from plan");
+    bool seen = false;
+    for (int i = 0; i < j; ++i)
+      if (sources[i].data == s.data && sources[i].stride_bytes == s.stride_bytes) seen = true;
+    if (seen) continue;
+    const size_t se = plane_extent(s.width, s.height, s.stride_bytes, elem);
+    check_pointer(s.data, elem);
+    disjoint(s.data, se, dst.data, de);
+    ++c.unique;
+  }
+  return c;
+}
+
+nfd::TileShape pick_tile(const nfd::DevPlan& d) {
+  nfd::TileShape S;
+  S.threads = 256;
+  const int b = std::max(d.bh, d.bw);
+  int tile = b <= 8 ? 32 : b <= 16 ? 64 : b <= 32 ? 64 : 48;
+  for (;;) {
+    S.tw = std::min(tile, d.gx.length);
+    S.th = std::min(b <= 16 ? tile / 2 : tile, d.gy.length);
+    S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
+    if (nfd::tile_smem_bytes(d.bh, d.bw, S) <= 200 * 1024 || tile <= 8) break;
+    tile /= 2;
+  }
+  return S;
+}
+
+cudaError_t run_spatial(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, void* dst, ptrdiff_t ds, const cf* L,
+                        cudaStream_t st) {
+  const nfd::TileShape S = pick_tile(d);
+  const size_t smem = nfd::tile_smem_bytes(d.bh, d.bw, S);
+  const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th);
+  if (d.bh == d.bw) {
+    switch (d.bw) {
+      case 8: return nfd::launch_spatial_8x8(d, S, grid, smem, src, ss, dst, ds, L, st);
+      case 16: return nfd::launch_spatial_16x16(d, S, grid, smem, src, ss, dst, ds, L, st);
+      case 32: return nfd::launch_spatial_32x32(d, S, grid, smem, src, ss, dst, ds, L, st);
+      case 12: return nfd::launch_spatial_12x12(d, S, grid, smem, src, ss, dst, ds, L, st);
+      case 48: return nfd::launch_spatial_48x48(d, S, grid, smem, src, ss, dst, ds, L, st);
+      default: break;
+    }
+  }
+  return nfd::launch_spatial_0x0(d, S, grid, smem, src, ss, dst, ds, L, st);
+}
+
+cudaError_t run_volume(const nfd::DevPlan& d, const nfd::VolumeSources& v, void* dst, ptrdiff_t ds, cudaStream_t st) {
+  nfd::VolumeShape S;
+  S.threads = 256;
+  const int b = std::max(d.bh, d.bw);
+  const size_t per_block = size_t(d.T) * d.bh * (d.bw / 2 + 1) * sizeof(cf);
+  int tile = b <= 16 ? 64 : b <= 32 ? 64 : 48;
+  S.tw = std::min(tile, d.gx.length);
+  S.th = std::min(b <= 16 ? tile / 2 : tile, d.gy.length);
+  S.nbc = int(std::max<size_t>(1, std::min<size_t>((96 * 1024) / per_block, (S.tw + d.bw - 1) / d.gx.step + 2)));
+  while (nfd::volume_smem_bytes(d.bh, d.bw, d.T, S) > 200 * 1024 && S.nbc > 1) --S.nbc;
+  while (nfd::volume_smem_bytes(d.bh, d.bw, d.T, S) > 200 * 1024 && S.tw > 8) {
+    S.tw /= 2;
+    S.th = std::max(1, S.th / 2);
+  }
+  const size_t smem = nfd::volume_smem_bytes(d.bh, d.bw, d.T, S);
+  const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th);
+  if (d.bh == d.bw) {
+    switch (d.bw) {
+      case 8: return nfd::launch_volume_8x8(d, S, grid, smem, v, dst, ds, st);
+      case 16: return nfd::launch_volume_16x16(d, S, grid, smem, v, dst, ds, st);
+      case 32: return nfd::launch_volume_32x32(d, S, grid, smem, v, dst, ds, st);
+      case 12: return nfd::launch_volume_12x12(d, S, grid, smem, v, dst, ds, st);
+      case 48: return nfd::launch_volume_48x48(d, S, grid, smem, v, dst, ds, st);
+      default: break;
+    }
+  }
+  return nfd::launch_volume_0x0(d, S, grid, smem, v, dst, ds, st);
+}
+
+nf_status read_error_word(const nf_plan& p, cudaStream_t st, char* err, size_t len) {
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, p.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "device synchronisation failed");
+  if (h) {
+    cudaMemsetAsync(p.err, 0, sizeof(int), st);
+    cudaStreamSynchronize(st);
+    return fail(err, len, "non-finite sample or intermediate", NF_NON_FINITE);
+  }
+  return NF_OK;
+}
+
+nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n, const int* targets, int nt,
+                          nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len) {
+  (void)frame;
+  (void)plane;
+  const Checked c = validate_call(p, sources, n, targets, nt, dst);
+  cudaError_t e;
+  if (p.t.algo == nfb::Algo::FFT3D && p.t.kalman)
+    return fail(err, len, "Kalman plans render through nf_kalman_render_device", NF_INVALID_ARGUMENT);
+  if (c.tslots == 1 && !p.t.temporal_ola) {
+    e = run_spatial(p.dev, sources[0].data, sources[0].stride_bytes, dst.data, dst.stride_bytes, nullptr, st);
+  } else {
+    nfd::VolumeSources v{};
+    for (int j = 0; j < n; ++j) {
+      v.ptr[j] = static_cast<const unsigned char*>(sources[j].data);
+      v.stride[j] = sources[j].stride_bytes;
+    }
+    v.ola = p.t.temporal_ola ? 1 : 0;
+    v.nblocks = p.t.temporal_ola ? nt : 1;
+    for (int i = 0; p.t.temporal_ola && i < nt; ++i) v.target[i] = targets[i];
+    e = run_volume(p.dev, v, dst.data, dst.stride_bytes, st);
+  }
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  return NF_OK;
+}
+
+template <class T>
+__global__ void fill_kernel(T* p, size_t n, T v) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) p[i] = v;
+}
+
+cudaError_t run_kalman_advance(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, const nfd::KalmanArgs& a,
+                               cudaStream_t st) {
+  const size_t per_block = size_t(d.bh) * d.K * sizeof(cf);
+  int nb = std::max(1, std::min(8, int((64 * 1024) / per_block)));
+  nb = std::min(nb, d.gx.count);
+  const size_t smem = per_block * size_t(nb);
+  const dim3 grid((d.gx.count + nb - 1) / nb, d.gy.count);
+  if (d.bh == d.bw) {
+    switch (d.bw) {
+      case 8: return nfd::launch_kalman_8x8(d, nb, grid, smem, src, ss, a, st);
+      case 16: return nfd::launch_kalman_16x16(d, nb, grid, smem, src, ss, a, st);
+      case 32: return nfd::launch_kalman_32x32(d, nb, grid, smem, src, ss, a, st);
+      case 12: return nfd::launch_kalman_12x12(d, nb, grid, smem, src, ss, a, st);
+      case 48: return nfd::launch_kalman_48x48(d, nb, grid, smem, src, ss, a, st);
+      default: break;
+    }
+  }
+  return nfd::launch_kalman_0x0(d, nb, grid, smem, src, ss, a, st);
+}
+
+void check_kalman_source(const nf_plan& p, const nf_const_plane& s) {
+  nfb::require(p.t.kalman, "not a Kalman plan");
+  nfb::require(s.width == p.t.gx.length && s.height == p.t.gy.length, "Kalman source shape differs");
+  const size_t elem = size_t(storage_of(p.t.format));
+  plane_extent(s.width, s.height, s.stride_bytes, elem);
+  check_pointer(s.data, elem);
+}
+
+} // namespace
+
+extern "C" {
+
+int nf_abi_version(void) { return NF_ABI_VERSION; }
+
+void nf_fft3d_config_default(nf_fft3d_config* c) {
+  *c = nf_fft3d_config{};
+  c->bw = 32; c->bh = 32; c->ow = -1; c->oh = -1; c->wintype = 0; c->opt = 0; c->bt = 1;
+  c->sigma = 2; c->beta = 1; c->degrid = 1; c->kratio = 2;
+  c->sharpen = 0; c->scutoff = .3f; c->svr = 1; c->smin = 4; c->smax = 20; c->dehalo = 0; c->hr = 2; c->ht = 50;
+  c->pfactor = 0; c->pcutoff = .1f;
+  c->cache_frames = -1; c->cache_mb = 128; c->kalman_warmup = 8;
+}
+void nf_dft_config_default(nf_dft_config* c) {
+  *c = nf_dft_config{};
+  c->block = 16; c->overlap = 12; c->mode = 1; c->swin = 0; c->twin = 7; c->ftype = 0; c->opt = 0; c->tbsize = 1;
+  c->sbeta = 2.5f; c->tbeta = 2.5f; c->sigma = 8; c->sigma2 = 8; c->pmin = 0; c->pmax = 500; c->f0beta = 1;
+  c->zmean = 1;
+}
+
+nf_status nf_plan_create_fft3d(int width, int height, nf_format format, const nf_fft3d_config* config,
+                               nf_plan** plan, char* err, size_t err_len) {
+  return guarded(err, err_len, [&]() -> nf_status {
+    nfb::require(config && plan, "missing configuration or output pointer");
+    auto p = std::make_unique<nf_plan>();
+    p->t = nfb::build_fft3d(width, height, format, *config);
+    const nf_status s = finalize_plan(p, err, err_len);
+    if (s != NF_OK) return s;
+    *plan = p.release();
+    return NF_OK;
+  });
+}
+nf_status nf_plan_create_dft(int width, int height, nf_format format, const nf_dft_config* config, nf_plan** plan,
+                             char* err, size_t err_len) {
+  return guarded(err, err_len, [&]() -> nf_status {
+    nfb::require(config && plan, "missing configuration or output pointer");
+    auto p = std::make_unique<nf_plan>();
+    p->t = nfb::build_dft(width, height, format, *config);
+    const nf_status s = finalize_plan(p, err, err_len);
+    if (s != NF_OK) return s;
+    *plan = p.release();
+    return NF_OK;
+  });
+}
+void nf_plan_destroy(nf_plan* plan) { delete plan; }
+
+nf_status nf_plan_geometry(const nf_plan* p, nf_axis* x, nf_axis* y, int* temporal_size, int* bins) {
+  if (!p) return NF_INVALID_ARGUMENT;
+  auto cp = [](const nfb::Axis& a, nf_axis* o) {
+    if (o) *o = {a.length, a.block, a.overlap, a.step, a.count, a.cover, a.offset};
+  };
+  cp(p->t.gx, x);
+  cp(p->t.gy, y);
+  if (temporal_size) *temporal_size = p->t.temporal_size;
+  if (bins) *bins = p->t.bins;
+  return NF_OK;
+}
+
+nf_status nf_plan_process_device(const nf_plan* p, const nf_const_plane* sources, int nsources, const int* targets,
+                                 int ntargets, nf_plane dst, int frame, int plane, void* stream, char* err,
+                                 size_t err_len) {
+  return guarded(err, err_len, [&]() -> nf_status {
+    nfb::require(p != nullptr, "null plan");
+    return process_device(*p, sources, nsources, targets, ntargets, dst, frame, plane,
+                          static_cast<cudaStream_t>(stream), err, err_len);
+  });
+}
+
+nf_status nf_plan_sync_status(const nf_plan* p, void* stream, char* err, size_t err_len) {
+  if (!p) return fail(err, err_len, "null plan", NF_INVALID_ARGUMENT);
+  return read_error_word(*p, static_cast<cudaStream_t>(stream), err, err_len);
+}
+
+nf_status nf_plan_process_host(const nf_plan* p, const nf_const_plane* sources, int nsources, const int* targets,
+                               int ntargets, nf_plane dst, int frame, int plane, void* stream, char* err,
+                               size_t err_len) {
+  return guarded(err, err_len, [&]() -> nf_status {
+    nfb::require(p != nullptr, "null plan");
+    const Checked c = validate_call(*p, sources, nsources, targets, ntargets, dst);
+    (void)c;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t elem = size_t(storage_of(p->t.format));
+    const size_t pitch = ((size_t(p->t.gx.length) * elem + 255) / 256) * 256;
+    const size_t plane_bytes = pitch * size_t(p->t.gy.length);
+    // Unique sources are staged once; repeated slots reuse the staged copy.
+    std::vector<int> slot_of(static_cast<size_t>(nsources), -1);
+    std::vector<int> uniq;
+    for (int j = 0; j < nsources; ++j) {
+      for (int i = 0; i < j; ++i)
+        if (sources[i].data == sources[j].data && sources[i].stride_bytes == sources[j].stride_bytes) {
+          slot_of[size_t(j)] = slot_of[size_t(i)];
+          break;
+        }
+      if (slot_of[size_t(j)] < 0) {
+        slot_of[size_t(j)] = int(uniq.size());
+        uniq.push_back(j);
+      }
+    }
+    const size_t need = plane_bytes * (uniq.size() + 1);
+    std::lock_guard<std::mutex> lock(p->staging_mu);
+    cudaError_t e;
+    if (p->staging_bytes < need) {
+      if (p->staging) cudaFree(p->staging);
+      p->staging = nullptr;
+      p->staging_bytes = 0;
+      if ((e = cudaMalloc(&p->staging, need)) != cudaSuccess) return cuda_fail(err, err_len, e, "device allocation failed");
+      p->staging_bytes = need;
+    }
+    auto* base = static_cast<unsigned char*>(p->staging);
+    std::vector<nf_const_plane> dsrc(static_cast<size_t>(nsources));
+    for (size_t u = 0; u < uniq.size(); ++u) {
+      const auto& s = sources[uniq[u]];
+      e = cudaMemcpy2DAsync(base + u * plane_bytes, pitch, s.data, size_t(s.stride_bytes), size_t(s.width) * elem,
+                            size_t(s.height), cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return cuda_fail(err, err_len, e, "host to device copy failed");
+    }
+    for (int j = 0; j < nsources; ++j)
+      dsrc[size_t(j)] = {base + size_t(slot_of[size_t(j)]) * plane_bytes, sources[j].width, sources[j].height,
+                         ptrdiff_t(pitch)};
+    nf_plane ddst{base + uniq.size() * plane_bytes, dst.width, dst.height, ptrdiff_t(pitch)};
+    nf_status s = process_device(*p, dsrc.data(), nsources, targets, ntargets, ddst, frame, plane, st, err, err_len);
+    if (s != NF_OK) return s;
+    e = cudaMemcpy2DAsync(dst.data, size_t(dst.stride_bytes), ddst.data, pitch, size_t(dst.width) * elem,
+                          size_t(dst.height), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_fail(err, err_len, e, "device to host copy failed");
+    return read_error_word(*p, st, err, err_len);
+  });
+}
+
+nf_status nf_kalman_state_create(const nf_plan* p, int fp64, nf_kalman_state** out, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && out, "null plan or output pointer");
+    nfb::require(p->t.kalman, "not a Kalman plan");
+    auto s = std::make_unique<nf_kalman_state>();
+    s->plan = p;
+    s->fp64 = fp64 ? 1 : 0;
+    s->count = size_t(p->t.gx.count) * size_t(p->t.gy.count) * size_t(p->t.bins);
+    const size_t var = s->fp64 ? sizeof(double) : sizeof(float);
+    cudaError_t e;
+    if ((e = cudaMalloc(&s->last, s->count * sizeof(cf))) != cudaSuccess ||
+        (e = cudaMalloc(&s->covariance, s->count * var)) != cudaSuccess ||
+        (e = cudaMalloc(&s->process, s->count * var)) != cudaSuccess)
+      return cuda_fail(err, len, e, "device allocation failed");
+    // initial_kalman (plan.cpp:293-300): L = 0, C = Q = R0.
+    cudaMemset(s->last, 0, s->count * sizeof(cf));
+    const int blocks = int(std::min<size_t>(4096, (s->count + 255) / 256));
+    if (s->fp64) {
+      fill_kernel<double><<<blocks, 256>>>(static_cast<double*>(s->covariance), s->count, double(p->t.kalman_r0));
+      fill_kernel<double><<<blocks, 256>>>(static_cast<double*>(s->process), s->count, double(p->t.kalman_r0));
+    } else {
+      fill_kernel<float><<<blocks, 256>>>(static_cast<float*>(s->covariance), s->count, p->t.kalman_r0);
+      fill_kernel<float><<<blocks, 256>>>(static_cast<float*>(s->process), s->count, p->t.kalman_r0);
+    }
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cuda_fail(err, len, e, "state initialisation failed");
+    *out = s.release();
+    return NF_OK;
+  });
+}
+void nf_kalman_state_destroy(nf_kalman_state* s) { delete s; }
+nf_status nf_kalman_state_copy(nf_kalman_state* dst, const nf_kalman_state* src, void* stream) {
+  if (!dst || !src || dst->count != src->count || dst->fp64 != src->fp64) return NF_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t var = src->fp64 ? sizeof(double) : sizeof(float);
+  cudaError_t e = cudaMemcpyAsync(dst->last, src->last, src->count * sizeof(cf), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dst->covariance, src->covariance, src->count * var, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dst->process, src->process, src->count * var, cudaMemcpyDeviceToDevice, st);
+  return e == cudaSuccess ? NF_OK : NF_DEVICE_ERROR;
+}
+nf_status nf_kalman_advance_device(const nf_plan* p, nf_const_plane source, nf_kalman_state* state, void* stream,
+                                   char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && state, "null plan or state");
+    check_kalman_source(*p, source);
+    nfb::require(state->count == size_t(p->t.gx.count) * p->t.gy.count * p->t.bins, "Kalman state shape differs");
+    nfd::KalmanArgs a{state->last,
+                      state->fp64 ? nullptr : static_cast<float*>(state->covariance),
+                      state->fp64 ? nullptr : static_cast<float*>(state->process),
+                      state->fp64 ? static_cast<double*>(state->covariance) : nullptr,
+                      state->fp64 ? static_cast<double*>(state->process) : nullptr,
+                      p->t.spectral.primary.empty() ? nullptr : p->dev.filt.primary, state->fp64};
+    const cudaError_t e = run_kalman_advance(p->dev, source.data, source.stride_bytes, a, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+    return NF_OK;
+  });
+}
+nf_status nf_kalman_render_device(const nf_plan* p, nf_const_plane source, nf_plane dst, const nf_kalman_state* state,
+                                  void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && state, "null plan or state");
+    check_kalman_source(*p, source);
+    nfb::require(state->count == size_t(p->t.gx.count) * p->t.gy.count * p->t.bins, "Kalman checkpoint shape differs");
+    nfb::require(dst.width == p->t.gx.length && dst.height == p->t.gy.length, "frame dimensions differ from plan");
+    const size_t elem = size_t(storage_of(p->t.format));
+    const size_t de = plane_extent(dst.width, dst.height, dst.stride_bytes, elem);
+    check_pointer(dst.data, elem);
+    disjoint(source.data, plane_extent(source.width, source.height, source.stride_bytes, elem), dst.data, de);
+    nfd::DevPlan d = p->dev;
+    d.fft3d_mode = nfd::kEnhanceOnly;  // render copies L, then enhances (plan.cpp:471-477)
+    const cudaError_t e = run_spatial(d, source.data, source.stride_bytes, dst.data, dst.stride_bytes, state->last,
+                                      static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+    return NF_OK;
+  });
+}
+nf_status nf_kalman_state_read(const nf_kalman_state* s, float* last, float* cov, float* proc, size_t count) {
+  if (!s || count != s->count) return NF_INVALID_ARGUMENT;
+  if (cudaMemcpy(last, s->last, count * sizeof(cf), cudaMemcpyDeviceToHost) != cudaSuccess) return NF_DEVICE_ERROR;
+  if (!s->fp64) {
+    if (cudaMemcpy(cov, s->covariance, count * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return NF_DEVICE_ERROR;
+    if (cudaMemcpy(proc, s->process, count * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return NF_DEVICE_ERROR;
+    return NF_OK;
+  }
+  std::vector<double> tmp(count);
+  if (cudaMemcpy(tmp.data(), s->covariance, count * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return NF_DEVICE_ERROR;
+  for (size_t i = 0; i < count; ++i) cov[i] = float(tmp[i]);
+  if (cudaMemcpy(tmp.data(), s->process, count * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return NF_DEVICE_ERROR;
+  for (size_t i = 0; i < count; ++i) proc[i] = float(tmp[i]);
+  return NF_OK;
+}
+
+nf_status nf_kernel_info(char* fft_backend, size_t fb_len, char* target, size_t t_len, char* fft, size_t f_len,
+                         int* lanes) {
+  auto put = [](char* dst, size_t n, const char* s) {
+    if (dst && n) {
+      std::strncpy(dst, s, n - 1);
+      dst[n - 1] = 0;
+    }
+  };
+  put(fft_backend, fb_len, "cuda-sm100a");
+  put(target, t_len, "sm_100a");
+  put(fft, f_len, "codelet8/16/32+project-mixed-radix");
+  if (lanes) *lanes = 32;
+  return NF_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,319 @@
+"""Python mirror of neo-fft's core `Plan` (src/algorithms/plan.hpp:18-140) over the C ABI.
+
+Same names and argument meaning as the reference: ``SampleFormat``, ``FFT3DConfig``,
+``DFTConfig`` and ``Plan(width, height, format, config)`` with ``process``,
+``process_at``, ``initial_kalman``, ``advance_kalman`` and ``render_kalman``.
+Errors follow the reference's exception types: configuration/geometry errors raise
+``ValueError`` (std::invalid_argument) and non-finite samples raise
+``NonFiniteError`` (a RuntimeError, like std::runtime_error).
+
+Planes are 2-D arrays: numpy arrays run through the host-memory entry point (copies
+in and out on the plan's stream), CUDA torch tensors through the device entry
+point (asynchronous on the current torch stream).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _capi as C
+
+
+@dataclass
+class SampleFormat:
+    bits: int = 8
+    floating: bool = False
+    chroma: bool = False
+
+
+@dataclass
+class FFT3DConfig:
+    """FFT3DConfig with EnhancementConfig fields (plan.hpp:24-36, fft3d_profile.hpp:6-9)."""
+    bw: int = 32
+    bh: int = 32
+    ow: int = -1
+    oh: int = -1
+    wintype: int = 0
+    opt: int = 0
+    bt: int = 1
+    sigma: float = 2.0
+    beta: float = 1.0
+    degrid: float = 1.0
+    kratio: float = 2.0
+    sigma2: Optional[float] = None
+    sigma3: Optional[float] = None
+    sigma4: Optional[float] = None
+    sharpen: float = 0.0
+    scutoff: float = 0.3
+    svr: float = 1.0
+    smin: float = 4.0
+    smax: float = 20.0
+    dehalo: float = 0.0
+    hr: float = 2.0
+    ht: float = 50.0
+    pfactor: float = 0.0
+    pcutoff: float = 0.1
+    pframe: int = 0
+    px: int = 0
+    py: int = 0
+    pshow: bool = False
+    left: int = 0
+    top: int = 0
+    right: int = 0
+    bottom: int = 0
+    interlaced: bool = False
+    cache_frames: int = -1
+    cache_mb: int = 128
+    kalman_warmup: int = 8
+
+    def to_c(self) -> C.NfFft3dConfig:
+        c = C.NfFft3dConfig()
+        for name, _ in C.NfFft3dConfig._fields_:
+            if name.startswith("has_"):
+                continue
+            if name in ("sigma2", "sigma3", "sigma4"):
+                v = getattr(self, name)
+                setattr(c, "has_" + name, 0 if v is None else 1)
+                setattr(c, name, 0.0 if v is None else float(v))
+            else:
+                setattr(c, name, type(getattr(c, name))(getattr(self, name)))
+        return c
+
+
+@dataclass
+class DFTConfig:
+    """DFTConfig with DFTCurves (plan.hpp:37-46, profile.hpp:7-12)."""
+    block: int = 16
+    overlap: int = 12
+    mode: int = 1
+    swin: int = 0
+    twin: int = 7
+    ftype: int = 0
+    opt: int = 0
+    tbsize: int = 1
+    sbeta: float = 2.5
+    tbeta: float = 2.5
+    sigma: float = 8.0
+    sigma2: float = 8.0
+    pmin: float = 0.0
+    pmax: float = 500.0
+    f0beta: float = 1.0
+    zmean: bool = True
+    temporal_mode: int = 0
+    temporal_overlap: int = 0
+    dither: int = 0
+    dither_seed: int = 0
+    slocation: Sequence[float] = field(default_factory=list)
+    ssx: Sequence[float] = field(default_factory=list)
+    ssy: Sequence[float] = field(default_factory=list)
+    sst: Sequence[float] = field(default_factory=list)
+    ssystem: int = 0
+    nlocation: Sequence[int] = field(default_factory=list)
+    alpha: Optional[float] = None
+
+    def to_c(self):
+        c = C.NfDftConfig()
+        keep = []
+        for name, typ in C.NfDftConfig._fields_:
+            if name.startswith("n_") or name in ("slocation", "ssx", "ssy", "sst", "nlocation", "has_alpha", "alpha"):
+                continue
+            setattr(c, name, typ(getattr(self, name)).value)
+        for name in ("slocation", "ssx", "ssy", "sst"):
+            v = np.ascontiguousarray(np.asarray(getattr(self, name), dtype=np.float32))
+            keep.append(v)
+            setattr(c, name, v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) if v.size else None)
+            setattr(c, "n_" + name, int(v.size))
+        loc = np.ascontiguousarray(np.asarray(self.nlocation, dtype=np.int32).reshape(-1))
+        keep.append(loc)
+        c.nlocation = loc.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if loc.size else None
+        c.n_nlocation = int(loc.size // 4)
+        c.has_alpha = 0 if self.alpha is None else 1
+        c.alpha = 0.0 if self.alpha is None else float(self.alpha)
+        return c, keep
+
+
+@dataclass
+class Axis:
+    length: int
+    block: int
+    overlap: int
+    step: int
+    count: int
+    cover: int
+    offset: int
+
+
+@dataclass
+class Geometry:
+    x: Axis
+    y: Axis
+
+
+_DTYPES = {1: np.uint8, 2: np.uint16, 4: np.float32}
+
+
+def _storage(fmt: SampleFormat) -> int:
+    return 4 if fmt.floating else (1 if fmt.bits == 8 else 2)
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _plane(a, const: bool):
+    """2-D array -> nf plane (data pointer, width, height, signed byte stride)."""
+    cls = C.NfConstPlane if const else C.NfPlane
+    if _is_torch(a):
+        if a.dim() != 2 or a.stride(1) != 1:
+            raise ValueError("planes must be 2-D with contiguous rows")
+        return cls(a.data_ptr(), a.shape[1], a.shape[0], a.stride(0) * a.element_size())
+    a = np.asarray(a)
+    if a.ndim != 2 or a.strides[1] != a.itemsize:
+        raise ValueError("planes must be 2-D with contiguous rows")
+    return cls(a.ctypes.data, a.shape[1], a.shape[0], a.strides[0])
+
+
+class Plan:
+    """B200 per-plane compiled filter; drop-in for neo_fft::Plan."""
+
+    def __init__(self, width: int, height: int, format: SampleFormat, config):
+        self._lib = C.load()
+        self.format = format
+        self.config = config
+        err = ctypes.create_string_buffer(512)
+        handle = ctypes.c_void_p()
+        fmt = C.NfFormat(format.bits, int(format.floating), int(format.chroma))
+        if isinstance(config, FFT3DConfig):
+            cfg = config.to_c()
+            st = self._lib.nf_plan_create_fft3d(width, height, fmt, ctypes.byref(cfg), ctypes.byref(handle), err, 512)
+            self.algorithm = "FFT3D"
+        elif isinstance(config, DFTConfig):
+            cfg, keep = config.to_c()
+            st = self._lib.nf_plan_create_dft(width, height, fmt, ctypes.byref(cfg), ctypes.byref(handle), err, 512)
+            self.algorithm = "DFTTest"
+        else:
+            raise TypeError("config must be FFT3DConfig or DFTConfig")
+        C.raise_for(st, err.value)
+        self._h = handle
+        x, y = C.NfAxis(), C.NfAxis()
+        t, b = ctypes.c_int(), ctypes.c_int()
+        self._lib.nf_plan_geometry(self._h, ctypes.byref(x), ctypes.byref(y), ctypes.byref(t), ctypes.byref(b))
+        self.geometry = Geometry(Axis(*[getattr(x, n) for n, _ in C.NfAxis._fields_]),
+                                 Axis(*[getattr(y, n) for n, _ in C.NfAxis._fields_]))
+        self.temporal_size = t.value
+        self.bins = b.value
+        self.dtype = _DTYPES[_storage(format)]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.nf_plan_destroy(h)
+            self._h = None
+
+    # -- frame processing -------------------------------------------------------
+    def process_at(self, sources, dst, frame: int = 0, plane: int = 0, targets: Sequence[int] = (),
+                   stream=None):
+        """Plan::process_at (plan.hpp:77-80): filter `sources` (temporal slots) into `dst`."""
+        if not isinstance(sources, (list, tuple)):
+            sources = [sources]
+        if not sources:
+            raise ValueError("sources must not be empty")
+        device = _is_torch(sources[0])
+        srcs = (C.NfConstPlane * len(sources))(*[_plane(s, True) for s in sources])
+        d = _plane(dst, False)
+        tg = np.ascontiguousarray(np.asarray(list(targets), dtype=np.int32))
+        tgp = tg.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if tg.size else None
+        err = ctypes.create_string_buffer(512)
+        if device:
+            import torch
+            s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+            st = self._lib.nf_plan_process_device(self._h, srcs, len(sources), tgp, int(tg.size), d, frame, plane,
+                                                  ctypes.c_void_p(s), err, 512)
+        else:
+            st = self._lib.nf_plan_process_host(self._h, srcs, len(sources), tgp, int(tg.size), d, frame, plane,
+                                                ctypes.c_void_p(stream or 0), err, 512)
+        C.raise_for(st, err.value)
+        return dst
+
+    def process(self, sources, dst=None):
+        """Plan::process (plan.hpp:58-75); allocates dst like the first source when omitted."""
+        if dst is None:
+            first = sources[0] if isinstance(sources, (list, tuple)) else sources
+            if _is_torch(first):
+                import torch
+                dst = torch.empty_like(first)
+            else:
+                dst = np.empty_like(np.asarray(first))
+        return self.process_at(sources, dst)
+
+    def sync_status(self, stream=None) -> None:
+        """Raise NonFiniteError if any device launch met a non-finite value."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_plan_sync_status(self._h, ctypes.c_void_p(s), err, 512), err.value)
+
+    # -- Kalman (bt=0) -------------------------------------------------------------
+    def initial_kalman(self, fp64_variance: bool = False) -> "KalmanState":
+        return KalmanState(self, fp64_variance)
+
+    def advance_kalman(self, source, state: "KalmanState", stream=None) -> None:
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        st = self._lib.nf_kalman_advance_device(self._h, _plane(source, True), state._h, ctypes.c_void_p(s), err, 512)
+        C.raise_for(st, err.value)
+
+    def render_kalman(self, source, dst, state: "KalmanState", stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        st = self._lib.nf_kalman_render_device(self._h, _plane(source, True), _plane(dst, False), state._h,
+                                               ctypes.c_void_p(s), err, 512)
+        C.raise_for(st, err.value)
+        return dst
+
+
+class KalmanState:
+    """Device-resident Kalman state (kernels/kalman.hpp:5-14)."""
+
+    def __init__(self, plan: Plan, fp64_variance: bool = False):
+        self._lib = plan._lib
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        st = self._lib.nf_kalman_state_create(plan._h, int(fp64_variance), ctypes.byref(self._h), err, 512)
+        C.raise_for(st, err.value)
+        g = plan.geometry
+        self.count = g.x.count * g.y.count * plan.bins
+
+    def read(self):
+        last = np.zeros((self.count, 2), np.float32)
+        cov = np.zeros(self.count, np.float32)
+        proc = np.zeros(self.count, np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        C.raise_for(self._lib.nf_kalman_state_read(self._h, last.ctypes.data_as(fp), cov.ctypes.data_as(fp),
+                                                   proc.ctypes.data_as(fp), self.count), b"state read failed")
+        return last, cov, proc
+
+    def copy_from(self, other: "KalmanState", stream=None) -> None:
+        C.raise_for(self._lib.nf_kalman_state_copy(self._h, other._h, ctypes.c_void_p(stream or 0)),
+                    b"state copy failed")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.nf_kalman_state_destroy(h)
+            self._h = None
+
+
+def kernel_info() -> dict:
+    """KernelInfo (docs/api/en/kernel-info.md): labels of the active implementation."""
+    lib = C.load()
+    a, b, c = (ctypes.create_string_buffer(64) for _ in range(3))
+    lanes = ctypes.c_int()
+    lib.nf_kernel_info(a, 64, b, 64, c, 64, ctypes.byref(lanes))
+    return {"fft_backend": a.value.decode(), "target": b.value.decode(), "fft": c.value.decode(),
+            "fft_lanes": lanes.value}

@@ -1,0 +1,81 @@
+"""Runs a few launches of one workload's dominant kernel, for profilers.
+
+  python -m neo_fft_b200.profile_case --workload dft16 --launches 3
+
+Workloads (one plane per launch, seeded synthetic content):
+  dft16    DFTTest sbsize 16 / sosize 12, ftype 0, sigma 8 flat curve, u16 1920x1080
+  dft16_4k the same on a u16 3840x2160 plane (input+output larger than L2)
+  fft3d32  FFT3D bw=bh=32, ow=oh=16, sigma 2, u8 640x360
+  fft3d48  FFT3D bt=3 bw=bh=48, ow=oh=24, sigma 3, sharpen 0.3, u16 (10-bit) 3840x2160
+  kalman32 FFT3D bt=0 (Kalman advance), bw=bh=32, float 1920x1080
+  dft12t5  DFTTest tbsize 5 tmode 1, sbsize 12 / sosize 9, ftype 1, float 1920x1080
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+
+def _plane(h, w, dtype, lo, hi, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.uniform(lo, hi, (h, w))
+    return v.astype(dtype)
+
+
+def main():
+    import torch
+
+    from . import DFTConfig, FFT3DConfig, Plan, SampleFormat
+    from .temporal import temporal_blocks
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="dft16")
+    ap.add_argument("--launches", type=int, default=3)
+    a = ap.parse_args()
+    dev = torch.device("cuda", 0)
+    wl = a.workload
+    if wl in ("dft16", "dft16_4k"):
+        w, h = (1920, 1080) if wl == "dft16" else (3840, 2160)
+        plan = Plan(w, h, SampleFormat(16), DFTConfig(block=16, overlap=12, ftype=0, sigma=8.0, slocation=[0, 8, 1, 8]))
+        srcs = [torch.from_numpy(_plane(h, w, np.uint16, 4096, 60000, 1)).to(dev)]
+        targets = ()
+    elif wl == "fft3d32":
+        w, h = 640, 360
+        plan = Plan(w, h, SampleFormat(8), FFT3DConfig(bw=32, bh=32, ow=16, oh=16, sigma=2.0))
+        srcs = [torch.from_numpy(_plane(h, w, np.uint8, 16, 235, 1)).to(dev)]
+        targets = ()
+    elif wl == "fft3d48":
+        w, h = 3840, 2160
+        plan = Plan(w, h, SampleFormat(10), FFT3DConfig(bw=48, bh=48, ow=24, oh=24, bt=3, sigma=3.0, sharpen=0.3))
+        srcs = [torch.from_numpy(_plane(h, w, np.uint16, 64, 940, f)).to(dev) for f in range(3)]
+        targets = ()
+    elif wl == "kalman32":
+        w, h = 1920, 1080
+        plan = Plan(w, h, SampleFormat(32, True), FFT3DConfig(bw=32, bh=32, bt=0, sigma=2.5, kratio=2.0))
+        state = plan.initial_kalman()
+        src = torch.from_numpy(_plane(h, w, np.float32, 0, 1, 1)).to(dev)
+        for _ in range(a.launches):
+            plan.advance_kalman(src, state)
+        torch.cuda.synchronize()
+        plan.sync_status()
+        return
+    elif wl == "dft12t5":
+        w, h = 1920, 1080
+        plan = Plan(w, h, SampleFormat(32, True), DFTConfig(block=12, overlap=9, tbsize=5, temporal_mode=1,
+                                                            ftype=1, sigma=8.0))
+        clip = [torch.from_numpy(_plane(h, w, np.float32, 0, 1, f)).to(dev) for f in range(9)]
+        blocks = temporal_blocks(4, 9, 5, 0)
+        srcs = [clip[s] for b in blocks for s in b["slots"]]
+        targets = [b["target"] for b in blocks]
+    else:
+        raise SystemExit(f"unknown workload {wl}")
+    out = torch.empty_like(srcs[0])
+    for _ in range(a.launches):
+        plan.process_at(srcs, out, targets=targets)
+    torch.cuda.synchronize()
+    plan.sync_status()
+
+
+if __name__ == "__main__":
+    main()

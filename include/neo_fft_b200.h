@@ -143,6 +143,28 @@ nf_status nf_kalman_render_device(const nf_plan* plan, nf_const_plane source, nf
 nf_status nf_kalman_state_read(const nf_kalman_state* state, float* last_interleaved, float* covariance,
                                float* process, size_t count);
 
+/* Batched / persistent form (no reference counterpart: the reference filters one
+ * plane per call, plan.cpp:331). A batch holds many single-frame planes (FFT3D
+ * bt=1/-1 and DFTTest tbsize=1 plans) of possibly different sizes and plans —
+ * luma and chroma, clips of mixed resolutions — and filters them with one
+ * persistent launch per block shape, driven by a device work queue. Planes are
+ * device memory and must stay valid while the batch is in use. Results are
+ * identical to nf_plan_process_device on each plane. Non-finite values are
+ * reported through each plan's nf_plan_sync_status. */
+typedef struct nf_batch nf_batch;
+typedef struct nf_batch_item {
+  const nf_plan* plan;
+  nf_const_plane source;
+  nf_plane dst;
+} nf_batch_item;
+nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** batch, char* err, size_t err_len);
+/* Enqueues the batch on `stream`: no allocation or synchronisation, so the call
+ * may be captured in a CUDA graph. */
+nf_status nf_batch_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
+/* Captures nf_batch_launch into a CUDA graph on first use, then replays the graph. */
+nf_status nf_batch_graph_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
+void nf_batch_destroy(nf_batch* batch);
+
 /* KernelInfo (docs/api/en/kernel-info.md; vapoursynth.cpp:64-69): labels of the
  * active implementation. Each string buffer receives at most len bytes. */
 nf_status nf_kernel_info(char* fft_backend, size_t fft_backend_len, char* target, size_t target_len, char* fft,

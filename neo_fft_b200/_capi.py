@@ -59,6 +59,10 @@ class NfPlane(ctypes.Structure):
     _fields_ = [("data", c_void_p), ("width", c_int), ("height", c_int), ("stride_bytes", c_ptrdiff)]
 
 
+class NfBatchItem(ctypes.Structure):
+    _fields_ = [("plan", c_void_p), ("source", NfConstPlane), ("dst", NfPlane)]
+
+
 # Every symbol the header declares, with its prototype: (restype, argtypes).
 PROTOTYPES = {
     "nf_abi_version": (c_int, []),
@@ -82,6 +86,11 @@ PROTOTYPES = {
     "nf_kalman_render_device": (c_int, [c_void_p, NfConstPlane, NfPlane, c_void_p, c_void_p,
                                         ctypes.c_char_p, c_size_t]),
     "nf_kalman_state_read": (c_int, [c_void_p, _FP, _FP, _FP, c_size_t]),
+    "nf_batch_create": (c_int, [ctypes.POINTER(NfBatchItem), c_int, ctypes.POINTER(c_void_p), ctypes.c_char_p,
+                                c_size_t]),
+    "nf_batch_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_batch_graph_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_batch_destroy": (None, [c_void_p]),
     "nf_kernel_info": (c_int, [ctypes.c_char_p, c_size_t, ctypes.c_char_p, c_size_t, ctypes.c_char_p,
                                c_size_t, _IP]),
 }

@@ -6,11 +6,14 @@
 #include <cuda_runtime.h>
 
 namespace nfd {
-struct TileShape;
+struct StripShape;
+struct PlaneJob;
+struct BatchWork;
 #define NF_DECLARE_SPATIAL(BH, BW)                                                                              \
-  cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const TileShape& s, dim3 grid, size_t smem,          \
-                                         const void* src, ptrdiff_t ss, void* dst, ptrdiff_t ds, const cf* L,   \
-                                         cudaStream_t st);
+  cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const StripShape& s, dim3 grid, size_t smem,         \
+                                         const PlaneJob& job, cudaStream_t st);                                 \
+  cudaError_t launch_spatial_batch_##BH##x##BW(int storage, const BatchWork& w, int ctas, size_t smem,           \
+                                               cudaStream_t st);
 NF_DECLARE_SPATIAL(8, 8)
 NF_DECLARE_SPATIAL(16, 16)
 NF_DECLARE_SPATIAL(32, 32)

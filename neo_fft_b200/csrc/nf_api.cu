@@ -49,6 +49,30 @@ struct nf_kalman_state {
   }
 };
 
+// One persistent launch group: planes of one block shape and storage.
+struct BatchGroup {
+  int bh = 0, bw = 0, storage = 0, ctas = 0;
+  size_t smem = 0;
+  void* dev = nullptr;  // plans | shapes | jobs | tile_base | tiles_x
+  nfd::BatchWork work{};
+};
+
+struct nf_batch {
+  std::vector<BatchGroup> groups;
+  int* counters = nullptr;  // one queue head per group
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t capture_stream = nullptr;
+  ~nf_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    for (auto& g : groups)
+      if (g.dev) cudaFree(g.dev);
+    if (counters) cudaFree(counters);
+  }
+};
+
 namespace {
 
 nf_status fail(char* err, size_t len, const std::string& msg, nf_status code) {
@@ -251,37 +275,53 @@ Checked validate_call(const nf_plan& p, const nf_const_plane* sources, int n, co
   return c;
 }
 
-nfd::TileShape pick_tile(const nfd::DevPlan& d) {
-  nfd::TileShape S;
-  S.threads = 256;
+// Strip geometry: width by block size (the horizontal halo costs (bw-step)/tw of
+// recomputed blocks), height chosen so one plane yields about `target_ctas` CTAs
+// (two resident CTAs per SM on 148 SMs) in the plain launch; batches use tall
+// strips because many planes already fill the GPU.
+nfd::StripShape pick_strip(const nfd::DevPlan& d, int target_ctas) {
+  nfd::StripShape S;
   const int b = std::max(d.bh, d.bw);
-  int tile = b <= 8 ? 32 : b <= 16 ? 64 : b <= 32 ? 64 : 48;
+  int tw = b <= 16 ? 64 : b <= 32 ? 64 : 48;
   for (;;) {
-    S.tw = std::min(tile, d.gx.length);
-    S.th = std::min(b <= 16 ? tile / 2 : tile, d.gy.length);
+    S.tw = std::min(tw, d.gx.length);
     S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
-    if (nfd::tile_smem_bytes(d.bh, d.bw, S) <= 200 * 1024 || tile <= 8) break;
-    tile /= 2;
+    S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
+    S.th = d.gy.length;
+    if (nfd::strip_smem_bytes(d.bh, d.bw, S) <= 110 * 1024 || tw <= 8) break;
+    tw /= 2;
   }
+  const int strips = (d.gx.length + S.tw - 1) / S.tw;
+  const int segs = std::max(1, std::min((target_ctas + strips - 1) / strips, d.gy.length / std::max(1, 2 * d.bh)));
+  S.th = std::max(1, (d.gy.length + segs - 1) / segs);
   return S;
+}
+
+constexpr int kPlainCtas = 2 * 148;
+
+cudaError_t launch_spatial_shape(const nfd::DevPlan& d, const nfd::StripShape& S, dim3 grid, size_t smem,
+                                 const nfd::PlaneJob& job, cudaStream_t st) {
+  if (d.bh == d.bw) {
+    switch (d.bw) {
+      case 8: return nfd::launch_spatial_8x8(d, S, grid, smem, job, st);
+      case 16: return nfd::launch_spatial_16x16(d, S, grid, smem, job, st);
+      case 32: return nfd::launch_spatial_32x32(d, S, grid, smem, job, st);
+      case 12: return nfd::launch_spatial_12x12(d, S, grid, smem, job, st);
+      case 48: return nfd::launch_spatial_48x48(d, S, grid, smem, job, st);
+      default: break;
+    }
+  }
+  return nfd::launch_spatial_0x0(d, S, grid, smem, job, st);
 }
 
 cudaError_t run_spatial(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, void* dst, ptrdiff_t ds, const cf* L,
                         cudaStream_t st) {
-  const nfd::TileShape S = pick_tile(d);
-  const size_t smem = nfd::tile_smem_bytes(d.bh, d.bw, S);
+  const nfd::StripShape S = pick_strip(d, kPlainCtas);
+  const size_t smem = nfd::strip_smem_bytes(d.bh, d.bw, S);
   const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th);
-  if (d.bh == d.bw) {
-    switch (d.bw) {
-      case 8: return nfd::launch_spatial_8x8(d, S, grid, smem, src, ss, dst, ds, L, st);
-      case 16: return nfd::launch_spatial_16x16(d, S, grid, smem, src, ss, dst, ds, L, st);
-      case 32: return nfd::launch_spatial_32x32(d, S, grid, smem, src, ss, dst, ds, L, st);
-      case 12: return nfd::launch_spatial_12x12(d, S, grid, smem, src, ss, dst, ds, L, st);
-      case 48: return nfd::launch_spatial_48x48(d, S, grid, smem, src, ss, dst, ds, L, st);
-      default: break;
-    }
-  }
-  return nfd::launch_spatial_0x0(d, S, grid, smem, src, ss, dst, ds, L, st);
+  const nfd::PlaneJob job{static_cast<const unsigned char*>(src), (long long)ss, static_cast<unsigned char*>(dst),
+                          (long long)ds, L, 0};
+  return launch_spatial_shape(d, S, grid, smem, job, st);
 }
 
 cudaError_t run_volume(const nfd::DevPlan& d, const nfd::VolumeSources& v, void* dst, ptrdiff_t ds, cudaStream_t st) {
@@ -382,6 +422,20 @@ void check_kalman_source(const nf_plan& p, const nf_const_plane& s) {
   const size_t elem = size_t(storage_of(p.t.format));
   plane_extent(s.width, s.height, s.stride_bytes, elem);
   check_pointer(s.data, elem);
+}
+
+cudaError_t launch_batch_group(const BatchGroup& g, cudaStream_t st) {
+  if (g.bh == g.bw) {
+    switch (g.bw) {
+      case 8: return nfd::launch_spatial_batch_8x8(g.storage, g.work, g.ctas, g.smem, st);
+      case 16: return nfd::launch_spatial_batch_16x16(g.storage, g.work, g.ctas, g.smem, st);
+      case 32: return nfd::launch_spatial_batch_32x32(g.storage, g.work, g.ctas, g.smem, st);
+      case 12: return nfd::launch_spatial_batch_12x12(g.storage, g.work, g.ctas, g.smem, st);
+      case 48: return nfd::launch_spatial_batch_48x48(g.storage, g.work, g.ctas, g.smem, st);
+      default: break;
+    }
+  }
+  return nfd::launch_spatial_batch_0x0(g.storage, g.work, g.ctas, g.smem, st);
 }
 
 } // namespace
@@ -604,6 +658,149 @@ nf_status nf_kalman_state_read(const nf_kalman_state* s, float* last, float* cov
   for (size_t i = 0; i < count; ++i) proc[i] = float(tmp[i]);
   return NF_OK;
 }
+
+nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(out && (count == 0 || items), "null batch output or items");
+    auto b = std::make_unique<nf_batch>();
+    struct Entry {
+      int group, plan;
+      nfd::PlaneJob job;
+      int tiles_x, tiles;
+      long long cost;
+    };
+    std::vector<Entry> entries;
+    std::vector<std::vector<const nf_plan*>> group_plans;
+    for (int i = 0; i < count; ++i) {
+      const nf_batch_item& it = items[i];
+      nfb::require(it.plan != nullptr, "null plan in batch");
+      const nf_plan& p = *it.plan;
+      nfb::require(!p.t.kalman && (p.t.temporal_size == 1 || p.t.algo == nfb::Algo::FFT3D) && !p.t.temporal_ola,
+                   "batch items must be single-frame plans");
+      validate_call(p, &it.source, 1, nullptr, 0, it.dst);
+      const int storage = storage_of(p.t.format);
+      int gi = -1;
+      for (size_t g = 0; g < b->groups.size(); ++g)
+        if (b->groups[g].bh == p.t.bh && b->groups[g].bw == p.t.bw && b->groups[g].storage == storage) gi = int(g);
+      if (gi < 0) {
+        gi = int(b->groups.size());
+        BatchGroup g;
+        g.bh = p.t.bh;
+        g.bw = p.t.bw;
+        g.storage = storage;
+        b->groups.push_back(g);
+        group_plans.emplace_back();
+      }
+      auto& plans = group_plans[size_t(gi)];
+      int pi = -1;
+      for (size_t j = 0; j < plans.size(); ++j)
+        if (plans[j] == &p) pi = int(j);
+      if (pi < 0) {
+        pi = int(plans.size());
+        plans.push_back(&p);
+      }
+      Entry e{gi, pi,
+              {static_cast<const unsigned char*>(it.source.data), (long long)it.source.stride_bytes,
+               static_cast<unsigned char*>(it.dst.data), (long long)it.dst.stride_bytes, nullptr, pi},
+              0, 0, (long long)p.t.gx.count * p.t.gy.count};
+      entries.push_back(e);
+    }
+    cudaError_t ce;
+    if (!b->groups.empty() &&
+        (ce = cudaMalloc(&b->counters, sizeof(int) * b->groups.size())) != cudaSuccess)
+      return cuda_fail(err, len, ce, "device allocation failed");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+      BatchGroup& g = b->groups[gi];
+      const auto& plans = group_plans[gi];
+      std::vector<nfd::DevPlan> dplans;
+      std::vector<nfd::StripShape> shapes;
+      for (const nf_plan* p : plans) {
+        dplans.push_back(p->dev);
+        // Tall strips: the batch already supplies parallelism; segments of about
+        // 256 rows keep the dynamic queue balanced.
+        nfd::StripShape S = pick_strip(p->dev, 1);
+        const int segs = std::max(1, (p->t.gy.length + 255) / 256);
+        S.th = (p->t.gy.length + segs - 1) / segs;
+        shapes.push_back(S);
+        g.smem = std::max(g.smem, nfd::strip_smem_bytes(g.bh, g.bw, S));
+      }
+      std::vector<Entry> mine;
+      for (auto& e : entries)
+        if (e.group == int(gi)) mine.push_back(e);
+      // Largest planes first: shortens the tail of the dynamic queue.
+      std::stable_sort(mine.begin(), mine.end(), [](const Entry& a, const Entry& c) { return a.cost > c.cost; });
+      std::vector<nfd::PlaneJob> jobs;
+      std::vector<int> base(1, 0), tiles_x;
+      for (auto& e : mine) {
+        const nfd::StripShape& S = shapes[size_t(e.plan)];
+        const nf_plan* p = plans[size_t(e.plan)];
+        const int tx = (p->t.gx.length + S.tw - 1) / S.tw, ty = (p->t.gy.length + S.th - 1) / S.th;
+        jobs.push_back(e.job);
+        tiles_x.push_back(tx);
+        base.push_back(base.back() + tx * ty);
+      }
+      Blob blob;
+      const size_t o_p = blob.add(dplans), o_s = blob.add(shapes), o_j = blob.add(jobs), o_b = blob.add(base),
+                   o_t = blob.add(tiles_x);
+      if ((ce = cudaMalloc(&g.dev, blob.bytes.size())) != cudaSuccess)
+        return cuda_fail(err, len, ce, "device allocation failed");
+      if ((ce = cudaMemcpy(g.dev, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail(err, len, ce, "batch upload failed");
+      auto* base_ptr = static_cast<unsigned char*>(g.dev);
+      g.work.plans = reinterpret_cast<const nfd::DevPlan*>(base_ptr + o_p);
+      g.work.shapes = reinterpret_cast<const nfd::StripShape*>(base_ptr + o_s);
+      g.work.jobs = reinterpret_cast<const nfd::PlaneJob*>(base_ptr + o_j);
+      g.work.job_tile_base = reinterpret_cast<const int*>(base_ptr + o_b);
+      g.work.job_tiles_x = reinterpret_cast<const int*>(base_ptr + o_t);
+      g.work.njobs = int(jobs.size());
+      g.work.counter = b->counters + gi;
+      g.ctas = std::max(1, std::min(base.back(), 2 * sms));
+    }
+    *out = b.release();
+    return NF_OK;
+  });
+}
+
+nf_status nf_batch_launch(nf_batch* b, void* stream, char* err, size_t len) {
+  if (!b) return fail(err, len, "null batch", NF_INVALID_ARGUMENT);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (b->groups.empty()) return NF_OK;
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, sizeof(int) * b->groups.size(), st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
+  for (const auto& g : b->groups)
+    if ((e = launch_batch_group(g, st)) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  return NF_OK;
+}
+
+nf_status nf_batch_graph_launch(nf_batch* b, void* stream, char* err, size_t len) {
+  if (!b) return fail(err, len, "null batch", NF_INVALID_ARGUMENT);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e;
+  if (!b->exec) {
+    // Capture needs a non-legacy stream; capture on a private one and replay on `st`.
+    if (!b->capture_stream && (e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
+      return cuda_fail(err, len, e, "stream creation failed");
+    if ((e = cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return cuda_fail(err, len, e, "graph capture failed");
+    const nf_status s = nf_batch_launch(b, b->capture_stream, err, len);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->capture_stream, &g);
+    if (s != NF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "graph capture failed");
+    b->graph = g;
+    if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess)
+      return cuda_fail(err, len, e, "graph instantiation failed");
+  }
+  if ((e = cudaGraphLaunch(b->exec, st)) != cudaSuccess) return cuda_fail(err, len, e, "graph launch failed");
+  return NF_OK;
+}
+
+void nf_batch_destroy(nf_batch* b) { delete b; }
 
 nf_status nf_kernel_info(char* fft_backend, size_t fb_len, char* target, size_t t_len, char* fft, size_t f_len,
                          int* lanes) {

@@ -10,21 +10,34 @@
 
 namespace nfd {
 namespace {
-template <int ST>
-cudaError_t launch_one(const DevPlan& d, const TileShape& S, dim3 grid, size_t smem, const void* src, ptrdiff_t ss,
-                       void* dst, ptrdiff_t ds, const cf* L, cudaStream_t st) {
-  auto k = spatial_tile_kernel<NF_BH, NF_BW, ST>;
+template <class K>
+cudaError_t prepare(K k, size_t smem) {
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  return e;
+}
+template <int ST>
+cudaError_t launch_one(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem, const PlaneJob& job,
+                       cudaStream_t st) {
+  auto k = spatial_strip_kernel<NF_BH, NF_BW, ST>;
+  cudaError_t e = prepare(k, smem);
   if (e != cudaSuccess) return e;
-  k<<<grid, S.threads, smem, st>>>(d, S, static_cast<const unsigned char*>(src), ss, static_cast<unsigned char*>(dst),
-                                   ds, L);
+  k<<<grid, 256, smem, st>>>(d, S, job);
+  return cudaGetLastError();
+}
+template <int ST>
+cudaError_t launch_batch(const BatchWork& w, int ctas, size_t smem, cudaStream_t st) {
+  auto k = spatial_batch_kernel<NF_BH, NF_BW, ST>;
+  cudaError_t e = prepare(k, smem);
+  if (e != cudaSuccess) return e;
+  k<<<ctas, 256, smem, st>>>(w);
   return cudaGetLastError();
 }
 template <int ST>
 cudaError_t launch_kalman_one(const DevPlan& d, int nb, dim3 grid, size_t smem, const void* src, ptrdiff_t ss,
                               const KalmanArgs& a, cudaStream_t st) {
   auto k = kalman_advance_kernel<NF_BH, NF_BW, ST>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  cudaError_t e = prepare(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, 256, smem, st>>>(d, nb, static_cast<const unsigned char*>(src), ss, a);
   return cudaGetLastError();
@@ -33,22 +46,23 @@ cudaError_t launch_kalman_one(const DevPlan& d, int nb, dim3 grid, size_t smem, 
 
 #define NF_DEFINE(BH, BW) NF_DEFINE_(BH, BW)
 #define NF_DEFINE_(BH, BW)                                                                                        \
-  cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const TileShape& S, dim3 grid, size_t smem,           \
-                                         const void* src, ptrdiff_t ss, void* dst, ptrdiff_t ds, const cf* L,    \
-                                         cudaStream_t st) {                                                      \
-    if (d.storage == kStoreU8) return launch_one<kStoreU8>(d, S, grid, smem, src, ss, dst, ds, L, st);          \
-    if (d.storage == kStoreU16) return launch_one<kStoreU16>(d, S, grid, smem, src, ss, dst, ds, L, st);        \
-    return launch_one<kStoreF32>(d, S, grid, smem, src, ss, dst, ds, L, st);                                     \
-  }
-NF_DEFINE(NF_BH, NF_BW)
-
-#define NF_DEFINE_KALMAN(BH, BW) NF_DEFINE_KALMAN_(BH, BW)
-#define NF_DEFINE_KALMAN_(BH, BW)                                                                                \
+  cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem,          \
+                                         const PlaneJob& job, cudaStream_t st) {                                 \
+    if (d.storage == kStoreU8) return launch_one<kStoreU8>(d, S, grid, smem, job, st);                          \
+    if (d.storage == kStoreU16) return launch_one<kStoreU16>(d, S, grid, smem, job, st);                        \
+    return launch_one<kStoreF32>(d, S, grid, smem, job, st);                                                     \
+  }                                                                                                              \
+  cudaError_t launch_spatial_batch_##BH##x##BW(int storage, const BatchWork& w, int ctas, size_t smem,           \
+                                               cudaStream_t st) {                                                \
+    if (storage == kStoreU8) return launch_batch<kStoreU8>(w, ctas, smem, st);                                  \
+    if (storage == kStoreU16) return launch_batch<kStoreU16>(w, ctas, smem, st);                                \
+    return launch_batch<kStoreF32>(w, ctas, smem, st);                                                           \
+  }                                                                                                              \
   cudaError_t launch_kalman_##BH##x##BW(const DevPlan& d, int nb, dim3 grid, size_t smem, const void* src,       \
                                         ptrdiff_t ss, const KalmanArgs& a, cudaStream_t st) {                   \
     if (d.storage == kStoreU8) return launch_kalman_one<kStoreU8>(d, nb, grid, smem, src, ss, a, st);           \
     if (d.storage == kStoreU16) return launch_kalman_one<kStoreU16>(d, nb, grid, smem, src, ss, a, st);         \
     return launch_kalman_one<kStoreF32>(d, nb, grid, smem, src, ss, a, st);                                      \
   }
-NF_DEFINE_KALMAN(NF_BH, NF_BW)
+NF_DEFINE(NF_BH, NF_BW)
 } // namespace nfd

@@ -1,30 +1,32 @@
-// Single-frame tile kernel: FFT3D bt=1/-1 (and Kalman render) and DFTTest tbsize=1.
+// Single-frame strip kernel: FFT3D bt=1/-1 (and Kalman render) and DFTTest tbsize=1.
 //
-// One CTA owns an output tile of the visible plane and computes every block that
-// touches it, one block row at a time (rows of the reference's `by` loop,
-// src/algorithms/plan.cpp:432-537 and 553-605):
+// A CTA owns a column strip of the visible plane (TW columns, TH rows) and walks
+// down it one block row at a time (the reference's `by` loop,
+// src/algorithms/plan.cpp:432-537 and 553-605). Per block row:
 //
-//   A  row transforms   thread = (block, row): reflect+decode the source samples,
-//                       apply the analysis window, real forward transform of the
-//                       row into K = bw/2+1 bins (shared memory).
-//   B  column pass      thread = (block, column): forward transform along y in
-//                       registers; the DC of each block is exchanged through
-//                       shared memory; per-bin filter; inverse transform along y.
-//   C  row inverses     thread = (block, row): inverse real transform of the row,
-//                       non-finite check, synthesis weighting into a block buffer.
-//   D  overlap-add      thread = output pixel: contributions are added in the
-//                       reference's order (block row ascending, then block column
-//                       ascending; FFT3D sums a row strip first and applies the
-//                       vertical synthesis weight once per block row), so every
-//                       output is owner-written and deterministic without atomics.
+//   0  stage    the source rows the block row adds are reflected, decoded and
+//               checked once per sample into a shared ring of BH rows
+//   A  rows     thread = (block, row): analysis window, real forward transform of
+//               the row into K = bw/2+1 bins (shared memory)
+//   B  columns  thread = (block, column): forward transform along y in registers,
+//               the block's DC is exchanged through shared memory, per-bin filter,
+//               inverse transform along y
+//   C  rows     thread = (block, row): inverse real transform, non-finite check,
+//               synthesis weighting (written in place over the row's bins)
+//   D  overlap  thread = output pixel: contributions are added in the reference's
+//               order (block row ascending, then block column ascending; FFT3D sums
+//               the row strip first and applies the vertical synthesis weight once
+//               per block row), into a ring accumulator of BH rows
+//   E  retire   rows no later block row can touch are quantised and stored
 //
-// After the last block row the tile is quantised and stored.
+// Outputs are owner-written and deterministic without atomics. Blocks overlapping
+// two strips are computed by both (the horizontal halo); vertically the strip is
+// tall, so little work is repeated.
 #pragma once
 #include "device_plan.cuh"
 
 namespace nfd {
 
-// Sample loads (u8/u16 integer, or f32).
 template <int STORAGE>
 __device__ __forceinline__ float load_sample(const unsigned char* row, int x) {
   if (STORAGE == kStoreU8) return float(row[x]);
@@ -57,25 +59,34 @@ __device__ __forceinline__ void store_sample(unsigned char* row, int x, float ac
   else reinterpret_cast<unsigned short*>(row)[x] = (unsigned short)(c);
 }
 
-struct TileShape {
-  int tw, th;    // output tile (plane pixels)
-  int nbx_max;   // blocks per block row that can touch a tile
-  int threads;
+// One plane to filter: source/destination (device memory, signed byte strides) and
+// for Kalman render the state's estimate L ([block][bins]) instead of a source.
+struct PlaneJob {
+  const unsigned char* src;
+  long long src_stride;
+  unsigned char* dst;
+  long long dst_stride;
+  const cf* kalman_L;
+  int plan;  // index into the batch's plan table
 };
 
-// Shared-memory layout (floats): spec [nbx][bh][K] complex | obuf [nbx][bh][bw]
-// | acc [th][tw] | dc [2*nbx].
-__host__ __device__ inline size_t tile_smem_bytes(int bh, int bw, const TileShape& s) {
+struct StripShape {
+  int tw, th;    // strip width and segment height (plane pixels)
+  int nbx_max;   // block columns that can touch a strip
+  int win_max;   // staged input columns: (nbx_max-1)*step + bw
+};
+
+// Shared layout (floats): ring_in [bh][win] | spec [nbx][bh][K] complex (the
+// inverse rows overwrite it in place) | acc [bh][tw] | dc [2*nbx].
+__host__ __device__ inline size_t strip_smem_bytes(int bh, int bw, const StripShape& s) {
   const size_t K = size_t(bw / 2 + 1);
-  return sizeof(float) * (size_t(s.nbx_max) * bh * K * 2 + size_t(s.nbx_max) * bh * bw + size_t(s.th) * s.tw +
+  return sizeof(float) * (size_t(bh) * s.win_max + size_t(s.nbx_max) * bh * K * 2 + size_t(bh) * s.tw +
                           2 * size_t(s.nbx_max));
 }
 
 template <int BHC, int BWC, int STORAGE>
-__global__ void __launch_bounds__(256) spatial_tile_kernel(DevPlan P, TileShape S, const unsigned char* src,
-                                                           ptrdiff_t src_stride, unsigned char* dst,
-                                                           ptrdiff_t dst_stride, const cf* kalman_L) {
-  extern __shared__ float smem[];
+__device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, const StripShape& S, int px0, int py0,
+                                           float* smem) {
   const int BH = BHC > 0 ? BHC : P.bh;
   const int BW = BWC > 0 ? BWC : P.bw;
   const int K = BW / 2 + 1;
@@ -87,15 +98,8 @@ __global__ void __launch_bounds__(256) spatial_tile_kernel(DevPlan P, TileShape 
   constexpr bool kCodelet = BHC == BWC && (BWC == 8 || BWC == 16 || BWC == 32);
   const bool codelet = kCodelet || (BHC == 0 && P.codelet != 0);
   const DevAxis gx = P.gx, gy = P.gy;
+  const cf* kalman_L = J.kalman_L;
 
-  cf* spec = reinterpret_cast<cf*>(smem);
-  float* obuf = smem + size_t(S.nbx_max) * BH * K * 2;
-  float* acc = obuf + size_t(S.nbx_max) * BH * BW;
-  float* dc = acc + size_t(S.th) * S.tw;
-
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  // Tile in plane coordinates and in cover coordinates.
-  const int px0 = blockIdx.x * S.tw, py0 = blockIdx.y * S.th;
   const int tw = min(S.tw, gx.length - px0), th = min(S.th, gy.length - py0);
   const int X0 = px0 + gx.offset, Y0 = py0 + gy.offset;
   const int bx_lo = max(0, floor_div_i(X0 - BW, gx.step) + 1);
@@ -103,30 +107,45 @@ __global__ void __launch_bounds__(256) spatial_tile_kernel(DevPlan P, TileShape 
   const int by_lo = max(0, floor_div_i(Y0 - BH, gy.step) + 1);
   const int by_hi = min(gy.count - 1, floor_div_i(Y0 + th - 1, gy.step));
   const int nbx = bx_hi - bx_lo + 1;
+  const int cx0 = bx_lo * gx.step;           // first staged cover column
+  const int win = (nbx - 1) * gx.step + BW;  // staged columns
+
+  float* ring_in = smem;
+  cf* spec = reinterpret_cast<cf*>(smem + size_t(BH) * S.win_max);
+  float* acc = smem + size_t(BH) * S.win_max + size_t(S.nbx_max) * BH * K * 2;
+  float* dc = acc + size_t(BH) * S.tw;
+  const int tid = threadIdx.x, nthr = blockDim.x;
   bool bad = false;
 
-  for (int i = tid; i < S.th * S.tw; i += nthr) acc[i] = 0.0f;
-
+  __syncthreads();  // shared memory may still be read by a previous work item
+  for (int i = tid; i < BH * S.tw; i += nthr) acc[i] = 0.0f;
   const float fct = fdiv(1.0f, fmul(float(BW), float(BH)));
 
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
-    // ---- A: row transforms -------------------------------------------------
+    __syncthreads();
     if (!kalman_L) {
+      // ---- 0: stage the rows this block row adds ----------------------------
+      const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
+      const int nrows = oy + BH - r0;
+      for (int i = tid; i < nrows * win; i += nthr) {
+        const int rr = i / win, xx = i - rr * win;
+        const int cy = r0 + rr;
+        const unsigned char* srow = J.src + ptrdiff_t(reflect_axis(cy, gy)) * J.src_stride;
+        const float s = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
+        const float v = fmul(fsub(s, P.dec_base), P.dec_scale);
+        if (!isfin(v)) bad = true;
+        ring_in[size_t(cy % BH) * S.win_max + xx] = v;
+      }
+      __syncthreads();
+      // ---- A: row transforms ------------------------------------------------
       for (int task = tid; task < nbx * BH; task += nthr) {
         const int b = task / BH, y = task - b * BH;
-        const int ox = (bx_lo + b) * gx.step;
-        const unsigned char* srow = src + ptrdiff_t(reflect_axis(oy + y, gy)) * src_stride;
+        const float* in = ring_in + size_t((oy + y) % BH) * S.win_max + b * gx.step;
         float row[CAPW];
 #pragma unroll UW
-        for (int x = 0; x < CAPW; ++x) {
-          if (x < BW) {
-            const float s = load_sample<STORAGE>(srow, reflect_axis(ox + x, gx));
-            const float v = fmul(fsub(s, P.dec_base), P.dec_scale);
-            if (!isfin(v)) bad = true;
-            row[x] = P.algo == 0 ? fmul(fmul(v, P.wya[y]), P.wxa[x]) : fmul(v, P.h[y * BW + x]);
-          }
-        }
+        for (int x = 0; x < CAPW; ++x)
+          if (x < BW) row[x] = P.algo == 0 ? fmul(fmul(in[x], P.wya[y]), P.wxa[x]) : fmul(in[x], P.h[y * BW + x]);
         nf::row_forward<BWC>(row, BW, spec + (size_t(b) * BH + y) * K, P.tww, codelet);
       }
       __syncthreads();
@@ -184,13 +203,14 @@ __global__ void __launch_bounds__(256) spatial_tile_kernel(DevPlan P, TileShape 
       }
       __syncthreads();
     }
-    // ---- C: row inverses and synthesis weighting ----------------------------
+    // ---- C: row inverses, synthesis weighting (in place) --------------------
     for (int task = tid; task < nbx * BH; task += nthr) {
       const int b = task / BH, y = task - b * BH;
       if (P.center && y != BH / 2) continue;
+      cf* bins = spec + (size_t(b) * BH + y) * K;
       float row[CAPW];
-      nf::row_inverse<BWC>(spec + (size_t(b) * BH + y) * K, BW, fct, row, P.tww, codelet);
-      float* ob = obuf + (size_t(b) * BH + y) * BW;
+      nf::row_inverse<BWC>(bins, BW, fct, row, P.tww, codelet);
+      float* ob = reinterpret_cast<float*>(bins);
 #pragma unroll UW
       for (int x = 0; x < CAPW; ++x) {
         if (x < BW) {
@@ -200,43 +220,92 @@ __global__ void __launch_bounds__(256) spatial_tile_kernel(DevPlan P, TileShape 
       }
     }
     __syncthreads();
-    // ---- D: ordered overlap-add into the tile accumulator --------------------
+    // ---- D: ordered overlap-add into the ring accumulator --------------------
+    const float* obuf = reinterpret_cast<const float*>(spec);
+    const size_t ob_row = size_t(2 * K);  // floats per (block, row) slot
     const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
-    const int band = yhi - ylo;
-    if (band > 0) {
-      for (int i = tid; i < band * tw; i += nthr) {
-        const int yy = i / tw, xx = i - yy * tw;
-        const int Y = ylo + yy, X = X0 + xx;
-        const int ly = Y - oy;
-        float* a = acc + size_t(Y - Y0) * S.tw + xx;
-        if (P.center) {
-          const int bc = X - BW / 2;  // block whose centre is X (step 1)
-          if (ly == BH / 2 && bc >= bx_lo && bc <= bx_hi)
-            *a = obuf[(size_t(bc - bx_lo) * BH + ly) * BW + BW / 2];
-          continue;
-        }
-        const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
-        if (P.algo == 0) {
-          float r = 0.0f;
-          for (int bb = b0; bb <= b1; ++bb) r = fadd(r, obuf[(size_t(bb - bx_lo) * BH + ly) * BW + (X - bb * gx.step)]);
-          *a = fadd(*a, fmul(r, P.wys[ly]));
-        } else {
-          float s = *a;
-          for (int bb = b0; bb <= b1; ++bb) s = fadd(s, obuf[(size_t(bb - bx_lo) * BH + ly) * BW + (X - bb * gx.step)]);
-          *a = s;
-        }
+    for (int i = tid; yhi > ylo && i < (yhi - ylo) * tw; i += nthr) {
+      const int yy = i / tw, xx = i - yy * tw;
+      const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
+      float* a = acc + size_t(Y % BH) * S.tw + xx;
+      if (P.center) {
+        const int bc = X - BW / 2;  // block whose centre is X (step 1)
+        if (ly == BH / 2 && bc >= bx_lo && bc <= bx_hi) *a = obuf[(size_t(bc - bx_lo) * BH + ly) * ob_row + BW / 2];
+        continue;
+      }
+      const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
+      if (P.algo == 0) {
+        float r = 0.0f;
+        for (int bb = b0; bb <= b1; ++bb)
+          r = fadd(r, obuf[(size_t(bb - bx_lo) * BH + ly) * ob_row + (X - bb * gx.step)]);
+        *a = fadd(*a, fmul(r, P.wys[ly]));
+      } else {
+        float s = *a;
+        for (int bb = b0; bb <= b1; ++bb)
+          s = fadd(s, obuf[(size_t(bb - bx_lo) * BH + ly) * ob_row + (X - bb * gx.step)]);
+        *a = s;
       }
     }
     __syncthreads();
-  }
-  // ---- store -----------------------------------------------------------------
-  for (int i = tid; i < th * tw; i += nthr) {
-    const int yy = i / tw, xx = i - yy * tw;
-    const float v = acc[size_t(yy) * S.tw + xx];
-    if (!isfin(v)) bad = true;
-    store_sample<STORAGE>(dst + ptrdiff_t(py0 + yy) * dst_stride, px0 + xx, v, P);
+    // ---- E: retire rows that no later block row touches ---------------------
+    const int rlo = max(oy, Y0), rhi = min(by == by_hi ? Y0 + th : oy + gy.step, Y0 + th);
+    for (int i = tid; rhi > rlo && i < (rhi - rlo) * tw; i += nthr) {
+      const int yy = i / tw, xx = i - yy * tw;
+      const int Y = rlo + yy;
+      float* a = acc + size_t(Y % BH) * S.tw + xx;
+      const float v = *a;
+      if (!isfin(v)) bad = true;
+      store_sample<STORAGE>(J.dst + ptrdiff_t(Y - gy.offset) * J.dst_stride, px0 + xx, v, P);
+      *a = 0.0f;
+    }
   }
   if (bad) atomicOr(P.err, kErrNonFinite);
+}
+
+// Plain launch: grid (strips, segments) over one plane.
+template <int BHC, int BWC, int STORAGE>
+__global__ void __launch_bounds__(256, 2) spatial_strip_kernel(DevPlan P, StripShape S, PlaneJob J) {
+  extern __shared__ float smem[];
+  strip_tile<BHC, BWC, STORAGE>(P, J, S, blockIdx.x * S.tw, blockIdx.y * S.th, smem);
+}
+
+// Batched launch: a persistent grid pulls (plane, strip, segment) work items from
+// a device queue; planes may come from different plans of the same block shape
+// (luma and chroma, or clips of several resolutions).
+struct BatchWork {
+  const DevPlan* plans;
+  const StripShape* shapes;  // per plan
+  const PlaneJob* jobs;
+  const int* job_tile_base;  // prefix sums of tiles per job (njobs+1)
+  const int* job_tiles_x;    // strips per job
+  int njobs;
+  int* counter;              // work-queue head, reset by the host before launch
+};
+
+template <int BHC, int BWC, int STORAGE>
+__global__ void __launch_bounds__(256, 2) spatial_batch_kernel(BatchWork W) {
+  extern __shared__ float smem[];
+  __shared__ int item;
+  const int total = W.job_tile_base[W.njobs];
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) item = atomicAdd(W.counter, 1);
+    __syncthreads();
+    const int t = item;
+    if (t >= total) break;
+    int lo = 0, hi = W.njobs - 1;  // job containing tile t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (W.job_tile_base[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const PlaneJob J = W.jobs[lo];
+    const DevPlan P = W.plans[J.plan];
+    const StripShape S = W.shapes[J.plan];
+    const int local = t - W.job_tile_base[lo];
+    const int sx = local % W.job_tiles_x[lo], sy = local / W.job_tiles_x[lo];
+    strip_tile<BHC, BWC, STORAGE>(P, J, S, sx * S.tw, sy * S.th, smem);
+  }
 }
 
 } // namespace nfd

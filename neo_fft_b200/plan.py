@@ -309,6 +309,41 @@ class KalmanState:
             self._h = None
 
 
+class Batch:
+    """Batched/persistent form: many single-frame planes (CUDA tensors) filtered by one
+    persistent launch per block shape with a device work queue; `launch(graph=True)`
+    replays a captured CUDA graph. Outputs equal per-plane `Plan.process_at`."""
+
+    def __init__(self, items):
+        """items: iterable of (plan, source_tensor, dst_tensor)."""
+        self._lib = C.load()
+        items = list(items)
+        self._keep = items  # planes must stay alive while the batch exists
+        arr = (C.NfBatchItem * len(items))(*[C.NfBatchItem(p._h.value, _plane(s, True), _plane(d, False))
+                                             for p, s, d in items])
+        self._plans = [p for p, _, _ in items]
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_batch_create(arr, len(items), ctypes.byref(self._h), err, 512), err.value)
+
+    def launch(self, graph: bool = False, stream=None) -> None:
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        fn = self._lib.nf_batch_graph_launch if graph else self._lib.nf_batch_launch
+        C.raise_for(fn(self._h, ctypes.c_void_p(s), err, 512), err.value)
+
+    def sync_status(self) -> None:
+        for p in {id(p): p for p in self._plans}.values():
+            p.sync_status()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.nf_batch_destroy(h)
+            self._h = None
+
+
 def kernel_info() -> dict:
     """KernelInfo (docs/api/en/kernel-info.md): labels of the active implementation."""
     lib = C.load()

@@ -139,6 +139,12 @@ nf_status nf_kalman_advance_device(const nf_plan* plan, nf_const_plane source, n
                                    char* err, size_t err_len);
 nf_status nf_kalman_render_device(const nf_plan* plan, nf_const_plane source, nf_plane dst,
                                   const nf_kalman_state* state, void* stream, char* err, size_t err_len);
+/* Host-memory variants: the plane is staged through the plan's device buffers and
+ * the call synchronises `stream` (NF_NON_FINITE like the reference). */
+nf_status nf_kalman_advance_host(const nf_plan* plan, nf_const_plane source, nf_kalman_state* state, void* stream,
+                                 char* err, size_t err_len);
+nf_status nf_kalman_render_host(const nf_plan* plan, nf_const_plane source, nf_plane dst,
+                                const nf_kalman_state* state, void* stream, char* err, size_t err_len);
 /* Read back the state (host arrays of `count` bins; C/Q as float). */
 nf_status nf_kalman_state_read(const nf_kalman_state* state, float* last_interleaved, float* covariance,
                                float* process, size_t count);

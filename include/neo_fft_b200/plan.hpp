@@ -1,0 +1,261 @@
+// C++ drop-in facade: the class signature of neo-fft's core `Plan`
+// (src/algorithms/plan.hpp:18-140 in the reference) implemented over the C ABI in
+// neo_fft_b200.h, so the VapourSynth/AviSynth host layer (src/plugin/filter.hpp,
+// src/plugin/descriptors.hpp) can call the B200 path unchanged.
+//
+// Planes are the host's DualSynth2 `span2d` views in host memory; each call stages
+// them through the plan's device buffers (nf_plan_process_host). Errors are
+// rethrown with the reference's exception types and texts: std::invalid_argument
+// for configuration/geometry, std::runtime_error("non-finite sample or
+// intermediate") for data (src/base/checked.hpp:13-41).
+//
+// The sampled noise models (pfactor, nlocation) are not implemented on the B200
+// path; plans requesting them fail at creation with std::invalid_argument, so the
+// pattern-model members below report an inactive model.
+#pragma once
+#include "neo_fft_b200.h"
+
+#include <dualsynth/span2d.hpp>
+
+#include <array>
+#include <complex>
+#include <cstdint>
+#include <memory>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+namespace neo_fft {
+
+namespace runtime {
+class SpectraCache;     // host-side raw-spectrum cache: not used by the B200 path
+class Retention;
+}  // namespace runtime
+
+enum class Algorithm { FFT3D, DFTTest };
+struct SampleFormat {
+  int bits = 8;
+  bool floating = false, chroma = false;
+};
+struct EnhancementConfig {
+  float sharpen = 0, scutoff = .3f, svr = 1, smin = 4, smax = 20;
+  float dehalo = 0, hr = 2, ht = 50;
+};
+struct DFTCurves {
+  std::vector<float> shared, x, y, time;
+  int system = 0;
+  bool empty() const { return shared.empty() && x.empty() && y.empty() && time.empty(); }
+};
+struct NoiseLocation {
+  int frame, plane, y, x;
+};
+struct FFT3DConfig {
+  int bw = 32, bh = 32, ow = -1, oh = -1, wintype = 0, opt = 0, bt = 1;
+  float sigma = 2, beta = 1, degrid = 1, kratio = 2;
+  std::optional<float> sigma2, sigma3, sigma4;
+  EnhancementConfig enhancement;
+  float pfactor = 0, pcutoff = .1f;
+  int pframe = 0, px = 0, py = 0;
+  bool pshow = false;
+  int left = 0, top = 0, right = 0, bottom = 0;
+  bool interlaced = false;
+  int cache_frames = -1, cache_mb = 128;
+  int kalman_warmup = 8;
+};
+struct DFTConfig {
+  int block = 16, overlap = 12, mode = 1, swin = 0, twin = 7, ftype = 0, opt = 0, tbsize = 1;
+  float sbeta = 2.5f, tbeta = 2.5f, sigma = 8, sigma2 = 8, pmin = 0, pmax = 500, f0beta = 1;
+  bool zmean = true;
+  int temporal_mode = 0, temporal_overlap = 0;
+  int dither = 0, dither_seed = 0;
+  DFTCurves curves;
+  std::vector<NoiseLocation> locations;
+  std::optional<float> alpha;
+};
+struct Axis {
+  int length = 0, block = 0, overlap = 0, step = 0, count = 0, cover = 0, offset = 0;
+};
+struct Geometry {
+  Axis x, y;
+};
+
+namespace detail {
+inline void check(nf_status s, const char* err) {
+  if (s == NF_OK) return;
+  if (s == NF_INVALID_ARGUMENT) throw std::invalid_argument(err);
+  throw std::runtime_error(err);
+}
+template <class T>
+nf_const_plane cplane(const span2d::Plane<const T>& p) {
+  return {p.data(), p.width(), p.height(), p.stride_bytes()};
+}
+template <class T>
+nf_plane mplane(const span2d::Plane<T>& p) {
+  return {p.data(), p.width(), p.height(), p.stride_bytes()};
+}
+}  // namespace detail
+
+// Kalman state (kernels/kalman.hpp:5-14) held in device memory. Copies are deep
+// (the host layer copies checkpoints before replay, filter.hpp:171).
+class KalmanState {
+ public:
+  KalmanState() = default;
+  KalmanState(const KalmanState& o) { *this = o; }
+  KalmanState& operator=(const KalmanState& o) {
+    if (this == &o) return *this;
+    reset();
+    if (o.state_) {
+      char err[256] = {0};
+      nf_kalman_state* s = nullptr;
+      detail::check(nf_kalman_state_create(o.plan_, 0, &s, err, sizeof(err)), err);
+      state_ = s;
+      plan_ = o.plan_;
+      nf_kalman_state_copy(state_, o.state_, nullptr);
+    }
+    return *this;
+  }
+  KalmanState(KalmanState&& o) noexcept : plan_(o.plan_), state_(o.state_) { o.state_ = nullptr; }
+  KalmanState& operator=(KalmanState&& o) noexcept {
+    std::swap(plan_, o.plan_);
+    std::swap(state_, o.state_);
+    return *this;
+  }
+  ~KalmanState() { reset(); }
+  nf_kalman_state* handle() const { return state_; }
+
+ private:
+  friend class Plan;
+  void reset() {
+    if (state_) nf_kalman_state_destroy(state_);
+    state_ = nullptr;
+  }
+  const nf_plan* plan_ = nullptr;
+  nf_kalman_state* state_ = nullptr;
+};
+
+class Plan {
+ public:
+  // Plan(int, int, SampleFormat, const FFT3DConfig&) — plan.hpp:51.
+  Plan(int width, int height, SampleFormat format, const FFT3DConfig& c,
+       std::shared_ptr<runtime::Retention> = {})
+      : format(format), algorithm(Algorithm::FFT3D) {
+    nf_fft3d_config n{};
+    n.bw = c.bw; n.bh = c.bh; n.ow = c.ow; n.oh = c.oh; n.wintype = c.wintype; n.opt = c.opt; n.bt = c.bt;
+    n.sigma = c.sigma; n.beta = c.beta; n.degrid = c.degrid; n.kratio = c.kratio;
+    n.has_sigma2 = c.sigma2.has_value(); n.sigma2 = c.sigma2.value_or(0);
+    n.has_sigma3 = c.sigma3.has_value(); n.sigma3 = c.sigma3.value_or(0);
+    n.has_sigma4 = c.sigma4.has_value(); n.sigma4 = c.sigma4.value_or(0);
+    const auto& e = c.enhancement;
+    n.sharpen = e.sharpen; n.scutoff = e.scutoff; n.svr = e.svr; n.smin = e.smin; n.smax = e.smax;
+    n.dehalo = e.dehalo; n.hr = e.hr; n.ht = e.ht;
+    n.pfactor = c.pfactor; n.pcutoff = c.pcutoff; n.pframe = c.pframe; n.px = c.px; n.py = c.py;
+    n.pshow = c.pshow; n.left = c.left; n.top = c.top; n.right = c.right; n.bottom = c.bottom;
+    n.interlaced = c.interlaced; n.cache_frames = c.cache_frames; n.cache_mb = c.cache_mb;
+    n.kalman_warmup = c.kalman_warmup;
+    char err[512] = {0};
+    detail::check(nf_plan_create_fft3d(width, height, to_c(format), &n, &plan_, err, sizeof(err)), err);
+    kalman_ = c.bt == 0;
+    init();
+  }
+  // Plan(int, int, SampleFormat, const DFTConfig&, noise) — plan.hpp:52.
+  template <class Noise = void>
+  Plan(int width, int height, SampleFormat format, const DFTConfig& c, std::shared_ptr<const Noise> = {},
+       std::shared_ptr<runtime::Retention> = {})
+      : format(format), algorithm(Algorithm::DFTTest) {
+    nf_dft_config n{};
+    n.block = c.block; n.overlap = c.overlap; n.mode = c.mode; n.swin = c.swin; n.twin = c.twin;
+    n.ftype = c.ftype; n.opt = c.opt; n.tbsize = c.tbsize; n.sbeta = c.sbeta; n.tbeta = c.tbeta;
+    n.sigma = c.sigma; n.sigma2 = c.sigma2; n.pmin = c.pmin; n.pmax = c.pmax; n.f0beta = c.f0beta;
+    n.zmean = c.zmean; n.temporal_mode = c.temporal_mode; n.temporal_overlap = c.temporal_overlap;
+    n.dither = c.dither; n.dither_seed = c.dither_seed;
+    n.slocation = c.curves.shared.data(); n.n_slocation = int(c.curves.shared.size());
+    n.ssx = c.curves.x.data(); n.n_ssx = int(c.curves.x.size());
+    n.ssy = c.curves.y.data(); n.n_ssy = int(c.curves.y.size());
+    n.sst = c.curves.time.data(); n.n_sst = int(c.curves.time.size());
+    n.ssystem = c.curves.system;
+    std::vector<int> loc;
+    for (const auto& l : c.locations) loc.insert(loc.end(), {l.frame, l.plane, l.y, l.x});
+    n.nlocation = loc.data(); n.n_nlocation = int(c.locations.size());
+    n.has_alpha = c.alpha.has_value(); n.alpha = c.alpha.value_or(0);
+    char err[512] = {0};
+    detail::check(nf_plan_create_dft(width, height, to_c(format), &n, &plan_, err, sizeof(err)), err);
+    init();
+  }
+  Plan(const Plan&) = delete;
+  Plan& operator=(const Plan&) = delete;
+  ~Plan() { nf_plan_destroy(plan_); }
+
+  Geometry geometry;
+  const SampleFormat format;
+  const Algorithm algorithm;
+  int temporal_size = 1;
+  struct Fft {
+    std::size_t bins_ = 0;
+    std::size_t bins() const { return bins_; }
+  } fft;
+
+  template <class T>
+  void process(span2d::Plane<const T> src, span2d::Plane<T> dst) const {
+    process_at<T>({&src, 1}, dst, 0, 0);
+  }
+  template <class T>
+  void process(span2d::Span<const span2d::Plane<const T>> sources, span2d::Plane<T> dst) const {
+    process_at<T>(sources, dst, 0, 0);
+  }
+  // process_at (plan.hpp:77-80); the SpectraCache arguments are accepted and ignored.
+  template <class T, class Cache = runtime::SpectraCache, class Request = void>
+  void process_at(span2d::Span<const span2d::Plane<const T>> sources, span2d::Plane<T> dst, int frame, int plane,
+                  span2d::Span<const int> targets = {}, Cache* = nullptr, Request* = nullptr) const {
+    std::vector<nf_const_plane> s;
+    s.reserve(sources.size());
+    for (const auto& p : sources) s.push_back(detail::cplane(p));
+    char err[512] = {0};
+    detail::check(nf_plan_process_host(plan_, s.data(), int(s.size()), targets.data(), int(targets.size()),
+                                       detail::mplane(dst), frame, plane, nullptr, err, sizeof(err)),
+                  err);
+  }
+
+  bool kalman() const { return kalman_; }
+  bool preview() const { return false; }
+  bool needs_pattern_frame() const { return false; }
+  bool pattern_ready() const { return false; }
+  KalmanState initial_kalman() const {
+    KalmanState s;
+    char err[512] = {0};
+    detail::check(nf_kalman_state_create(plan_, 0, &s.state_, err, sizeof(err)), err);
+    s.plan_ = plan_;
+    return s;
+  }
+  template <class T>
+  void advance_kalman(span2d::Plane<const T> source, KalmanState& state) const {
+    char err[512] = {0};
+    detail::check(nf_kalman_advance_host(plan_, detail::cplane(source), state.state_, nullptr, err, sizeof(err)),
+                  err);
+  }
+  template <class T>
+  void render_kalman(span2d::Plane<const T> source, span2d::Plane<T> dst, const KalmanState& state) const {
+    char err[512] = {0};
+    detail::check(nf_kalman_render_host(plan_, detail::cplane(source), detail::mplane(dst), state.state_, nullptr,
+                                        err, sizeof(err)),
+                  err);
+  }
+  const nf_plan* handle() const { return plan_; }
+
+ private:
+  static nf_format to_c(SampleFormat f) { return {f.bits, f.floating ? 1 : 0, f.chroma ? 1 : 0}; }
+  void init() {
+    nf_axis x{}, y{};
+    int t = 1, b = 0;
+    nf_plan_geometry(plan_, &x, &y, &t, &b);
+    geometry.x = {x.length, x.block, x.overlap, x.step, x.count, x.cover, x.offset};
+    geometry.y = {y.length, y.block, y.overlap, y.step, y.count, y.cover, y.offset};
+    temporal_size = t;
+    fft.bins_ = std::size_t(b);
+  }
+  nf_plan* plan_ = nullptr;
+  bool kalman_ = false;
+};
+
+}  // namespace neo_fft

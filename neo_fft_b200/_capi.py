@@ -85,6 +85,9 @@ PROTOTYPES = {
     "nf_kalman_advance_device": (c_int, [c_void_p, NfConstPlane, c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_kalman_render_device": (c_int, [c_void_p, NfConstPlane, NfPlane, c_void_p, c_void_p,
                                         ctypes.c_char_p, c_size_t]),
+    "nf_kalman_advance_host": (c_int, [c_void_p, NfConstPlane, c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_kalman_render_host": (c_int, [c_void_p, NfConstPlane, NfPlane, c_void_p, c_void_p, ctypes.c_char_p,
+                                      c_size_t]),
     "nf_kalman_state_read": (c_int, [c_void_p, _FP, _FP, _FP, c_size_t]),
     "nf_batch_create": (c_int, [ctypes.POINTER(NfBatchItem), c_int, ctypes.POINTER(c_void_p), ctypes.c_char_p,
                                 c_size_t]),

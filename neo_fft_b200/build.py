@@ -43,7 +43,9 @@ def _run(cmd: list[str]) -> None:
 def _stale(obj: Path, src: Path) -> bool:
     if not obj.exists():
         return True
-    deps = [src] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list((ROOT / "include").glob("*.h"))
+    deps = [src] + list(CSRC.glob("*.cuh")) + [CSRC / "launch.hpp"]
+    if src.name in ("nf_api.cu", "plan_build.cpp"):  # kernel units do not see the C ABI or the table builder
+        deps += list(CSRC.glob("*.hpp")) + list((ROOT / "include").glob("*.h"))
     return any(d.stat().st_mtime > obj.stat().st_mtime for d in deps)
 
 

@@ -556,7 +556,7 @@ NF_HD bool is_codelet_length(int n) { return n == 8 || n == 16 || n == 32; }
 // bin's imaginary part as exactly 0 (fft16x16_avx2.cpp:268-271,
 // fft32x32_avx2.cpp:329-335); the project transform does the same for every even W.
 template <int WC>
-NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool codelet) {
+NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool codelet, int bin_stride = 1) {
   const int w = WC > 0 ? WC : w_rt;
   constexpr int CAP = WC > 0 ? WC : kMaxProject;
   constexpr int U = WC > 0 ? CAP : 1;
@@ -568,8 +568,8 @@ NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool
   const int K = w / 2 + 1;
 #pragma unroll U
   for (int k = 0; k < CAP / 2 + 1; ++k)
-    if (k < K) bins[k] = a[k];
-  if (w % 2 == 0 && !(codelet && w == 8)) bins[w / 2].i = 0.0f;
+    if (k < K) bins[k * bin_stride] = a[k];
+  if (w % 2 == 0 && !(codelet && w == 8)) bins[(w / 2) * bin_stride].i = 0.0f;
 }
 
 // Inverse of one row: K bins -> W real samples scaled by fct. Bins 1..(W-1)/2 are
@@ -578,7 +578,8 @@ NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool
 // their imaginary parts are cleared, because a half-complex inverse defines the
 // row from their real parts only.
 template <int WC>
-NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf* table, bool codelet) {
+NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf* table, bool codelet,
+                       int bin_stride = 1) {
   const int w = WC > 0 ? WC : w_rt;
   constexpr int CAP = WC > 0 ? WC : kMaxProject;
   constexpr int U = WC > 0 ? CAP : 1;
@@ -586,7 +587,7 @@ NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf
   cf a[CAP];
 #pragma unroll U
   for (int k = 0; k < CAP / 2 + 1; ++k)
-    if (k < K) a[k] = bins[k];
+    if (k < K) a[k] = bins[k * bin_stride];
 #pragma unroll U
   for (int k = 1; k < CAP; ++k)
     if (k < (w + 1) / 2) a[w - k] = cf{a[k].r, fsub(0.0f, a[k].i)};

@@ -283,21 +283,27 @@ nfd::StripShape pick_strip(const nfd::DevPlan& d, int target_ctas) {
   nfd::StripShape S;
   const int b = std::max(d.bh, d.bw);
   int tw = b <= 16 ? 64 : b <= 32 ? 64 : 48;
+  S.tab_floats = nfd::strip_table_floats(d);
   for (;;) {
     S.tw = std::min(tw, d.gx.length);
     S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
     S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
+    int q = (S.win_max + 3) / 4;
+    if (q % 2 == 0) ++q;  // odd float4 count: consecutive staged rows start in different banks
+    S.ring_pitch = 4 * q;
     S.th = d.gy.length;
     if (nfd::strip_smem_bytes(d.bh, d.bw, S) <= 110 * 1024 || tw <= 8) break;
     tw /= 2;
   }
   const int strips = (d.gx.length + S.tw - 1) / S.tw;
-  const int segs = std::max(1, std::min((target_ctas + strips - 1) / strips, d.gy.length / std::max(1, 2 * d.bh)));
+  // At most one wave in the plain launch (a partial second wave doubles the time).
+  const int segs = std::max(1, std::min(target_ctas / strips, d.gy.length / std::max(1, 2 * d.bh)));
   S.th = std::max(1, (d.gy.length + segs - 1) / segs);
   return S;
 }
 
-constexpr int kPlainCtas = 2 * 148;
+// Resident CTAs of the plain launch: two per SM for blocks up to 16x16, else one.
+int plain_ctas(const nfd::DevPlan& d) { return (d.bh * d.bw <= 256 ? 2 : 1) * 148; }
 
 cudaError_t launch_spatial_shape(const nfd::DevPlan& d, const nfd::StripShape& S, dim3 grid, size_t smem,
                                  const nfd::PlaneJob& job, cudaStream_t st) {
@@ -316,7 +322,7 @@ cudaError_t launch_spatial_shape(const nfd::DevPlan& d, const nfd::StripShape& S
 
 cudaError_t run_spatial(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, void* dst, ptrdiff_t ds, const cf* L,
                         cudaStream_t st) {
-  const nfd::StripShape S = pick_strip(d, kPlainCtas);
+  const nfd::StripShape S = pick_strip(d, plain_ctas(d));
   const size_t smem = nfd::strip_smem_bytes(d.bh, d.bw, S);
   const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th);
   const nfd::PlaneJob job{static_cast<const unsigned char*>(src), (long long)ss, static_cast<unsigned char*>(dst),
@@ -643,6 +649,74 @@ nf_status nf_kalman_render_device(const nf_plan* p, nf_const_plane source, nf_pl
     return NF_OK;
   });
 }
+namespace {
+// Copies a host plane into the plan's staging buffer (slot `slot` of `nslots`).
+nf_status stage_host_plane(const nf_plan& p, const nf_const_plane& s, int slot, int nslots, cudaStream_t st,
+                           nf_const_plane* out, nf_plane* dst_out, char* err, size_t len) {
+  const size_t elem = size_t(storage_of(p.t.format));
+  const size_t pitch = ((size_t(p.t.gx.length) * elem + 255) / 256) * 256;
+  const size_t plane_bytes = pitch * size_t(p.t.gy.length);
+  const size_t need = plane_bytes * size_t(nslots);
+  cudaError_t e;
+  if (p.staging_bytes < need) {
+    if (p.staging) cudaFree(p.staging);
+    p.staging = nullptr;
+    p.staging_bytes = 0;
+    if ((e = cudaMalloc(&p.staging, need)) != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
+    p.staging_bytes = need;
+  }
+  auto* base = static_cast<unsigned char*>(p.staging) + size_t(slot) * plane_bytes;
+  if (s.data) {
+    e = cudaMemcpy2DAsync(base, pitch, s.data, size_t(s.stride_bytes), size_t(s.width) * elem, size_t(s.height),
+                          cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "host to device copy failed");
+  }
+  if (out) *out = {base, s.width, s.height, ptrdiff_t(pitch)};
+  if (dst_out) *dst_out = {base, s.width, s.height, ptrdiff_t(pitch)};
+  return NF_OK;
+}
+} // namespace
+
+nf_status nf_kalman_advance_host(const nf_plan* p, nf_const_plane source, nf_kalman_state* state, void* stream,
+                                 char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && state, "null plan or state");
+    check_kalman_source(*p, source);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(p->staging_mu);
+    nf_const_plane d{};
+    nf_status s = stage_host_plane(*p, source, 0, 1, st, &d, nullptr, err, len);
+    if (s != NF_OK) return s;
+    s = nf_kalman_advance_device(p, d, state, stream, err, len);
+    if (s != NF_OK) return s;
+    return read_error_word(*p, st, err, len);
+  });
+}
+
+nf_status nf_kalman_render_host(const nf_plan* p, nf_const_plane source, nf_plane dst, const nf_kalman_state* state,
+                                void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && state, "null plan or state");
+    check_kalman_source(*p, source);
+    nfb::require(dst.width == p->t.gx.length && dst.height == p->t.gy.length, "frame dimensions differ from plan");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(p->staging_mu);
+    nf_const_plane d{};
+    nf_plane o{};
+    nf_status s = stage_host_plane(*p, source, 0, 2, st, &d, nullptr, err, len);
+    if (s == NF_OK) s = stage_host_plane(*p, nf_const_plane{nullptr, dst.width, dst.height, dst.stride_bytes}, 1, 2, st,
+                                         nullptr, &o, err, len);
+    if (s != NF_OK) return s;
+    s = nf_kalman_render_device(p, d, o, state, stream, err, len);
+    if (s != NF_OK) return s;
+    const size_t elem = size_t(storage_of(p->t.format));
+    const cudaError_t e = cudaMemcpy2DAsync(dst.data, size_t(dst.stride_bytes), o.data, size_t(o.stride_bytes),
+                                            size_t(dst.width) * elem, size_t(dst.height), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "device to host copy failed");
+    return read_error_word(*p, st, err, len);
+  });
+}
+
 nf_status nf_kalman_state_read(const nf_kalman_state* s, float* last, float* cov, float* proc, size_t count) {
   if (!s || count != s->count) return NF_INVALID_ARGUMENT;
   if (cudaMemcpy(last, s->last, count * sizeof(cf), cudaMemcpyDeviceToHost) != cudaSuccess) return NF_DEVICE_ERROR;

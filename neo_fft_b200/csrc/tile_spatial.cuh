@@ -71,17 +71,32 @@ struct PlaneJob {
 };
 
 struct StripShape {
-  int tw, th;    // strip width and segment height (plane pixels)
-  int nbx_max;   // block columns that can touch a strip
-  int win_max;   // staged input columns: (nbx_max-1)*step + bw
+  int tw, th;     // strip width and segment height (plane pixels)
+  int nbx_max;    // block columns that can touch a strip (spectrum/overlap stride)
+  int win_max;    // staged input columns: (nbx_max-1)*step + bw
+  int ring_pitch; // floats per staged row: a multiple of 4 with an odd float4 count
+  int tab_floats; // per-plan tables staged in shared memory
 };
 
-// Shared layout (floats): ring_in [bh][win] | spec [nbx][bh][K] complex (the
-// inverse rows overwrite it in place) | acc [bh][tw] | dc [2*nbx].
+// Floats of the per-plan tables a strip stages in shared memory (strip_tile).
+__host__ __device__ inline int strip_table_floats(const DevPlan& P) {
+  const int K = P.bw / 2 + 1, bins = P.bh * K;
+  int n = P.algo == 0 ? 2 * (P.bw + P.bh) : 2 * P.bh * P.bw;
+  if (P.grid) n += 2 * bins;
+  if (P.filt.primary) n += bins;
+  if (P.enh.sharpen_w) n += bins;
+  if (P.enh.halo_w) n += bins;
+  return (n + 3) & ~3;
+}
+
+// Shared layout (floats): tables | ring_in [bh][ring_pitch] | spec [bh][K][nbx]
+// complex (block fastest) | ob [bh][nbx][bw+4] (synthesised rows, x fastest) |
+// acc [bh][tw] | dc [2*nbx].
 __host__ __device__ inline size_t strip_smem_bytes(int bh, int bw, const StripShape& s) {
   const size_t K = size_t(bw / 2 + 1);
-  return sizeof(float) * (size_t(bh) * s.win_max + size_t(s.nbx_max) * bh * K * 2 + size_t(bh) * s.tw +
-                          2 * size_t(s.nbx_max));
+  const size_t spec_cf = (size_t(s.nbx_max) * bh * K + 1) & ~size_t(1);  // keeps ob 16-byte aligned
+  return sizeof(float) * (size_t(s.tab_floats) + size_t(bh) * s.ring_pitch + spec_cf * 2 +
+                          size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max));
 }
 
 template <int BHC, int BWC, int STORAGE>
@@ -99,6 +114,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const bool codelet = kCodelet || (BHC == 0 && P.codelet != 0);
   const DevAxis gx = P.gx, gy = P.gy;
   const cf* kalman_L = J.kalman_L;
+  const int NB = S.nbx_max;   // block stride of spec and ob
+  const int OBW = BW + 4;     // ob row pitch (conflict-free float4 stores and overlap reads)
 
   const int tw = min(S.tw, gx.length - px0), th = min(S.th, gy.length - py0);
   const int X0 = px0 + gx.offset, Y0 = py0 + gy.offset;
@@ -110,16 +127,47 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const int cx0 = bx_lo * gx.step;           // first staged cover column
   const int win = (nbx - 1) * gx.step + BW;  // staged columns
 
-  float* ring_in = smem;
-  cf* spec = reinterpret_cast<cf*>(smem + size_t(BH) * S.win_max);
-  float* acc = smem + size_t(BH) * S.win_max + size_t(S.nbx_max) * BH * K * 2;
+  float* tab = smem;
+  float* ring_in = tab + S.tab_floats;
+  cf* spec = reinterpret_cast<cf*>(ring_in + size_t(BH) * S.ring_pitch);
+  float* ob = reinterpret_cast<float*>(spec + ((size_t(BH) * K * NB + 1) & ~size_t(1)));
+  float* acc = ob + size_t(BH) * NB * OBW;
   float* dc = acc + size_t(BH) * S.tw;
   const int tid = threadIdx.x, nthr = blockDim.x;
   bool bad = false;
 
   __syncthreads();  // shared memory may still be read by a previous work item
+  // ---- per-plan tables into shared memory --------------------------------------
+  const int bins = BH * K;
+  float* t_wa = tab;  // FFT3D: wxa[BW] wya[BH] wxs[BW] wys[BH]; DFTTest: h[BH*BW] hsyn[BH*BW]
+  int off = 0;
+  auto stage = [&](const float* src, int n) {
+    float* d = tab + off;
+    for (int i = tid; i < n; i += nthr) d[i] = src[i];
+    off += n;
+    return d;
+  };
+  const float *wxa = nullptr, *wya = nullptr, *wxs = nullptr, *wys = nullptr, *h = nullptr, *hsyn = nullptr;
+  if (P.algo == 0) {
+    wxa = stage(P.wxa, BW);
+    wya = stage(P.wya, BH);
+    wxs = stage(P.wxs, BW);
+    wys = stage(P.wys, BH);
+  } else {
+    h = stage(P.h, BH * BW);
+    hsyn = stage(P.hsyn, BH * BW);
+  }
+  (void)t_wa;
+  const cf* grid = P.grid ? reinterpret_cast<const cf*>(stage(reinterpret_cast<const float*>(P.grid), 2 * bins)) : nullptr;
+  DevSpectral filt = P.filt, enh = P.enh;
+  if (P.filt.primary) filt.primary = stage(P.filt.primary, bins);
+  if (P.enh.sharpen_w) filt.sharpen_w = enh.sharpen_w = stage(P.enh.sharpen_w, bins);
+  if (P.enh.halo_w) filt.halo_w = enh.halo_w = stage(P.enh.halo_w, bins);
   for (int i = tid; i < BH * S.tw; i += nthr) acc[i] = 0.0f;
+  __syncthreads();
+  const float grid0 = grid ? grid[0].r : 1.0f;
   const float fct = fdiv(1.0f, fmul(float(BW), float(BH)));
+  const bool vec4 = (gx.step & 3) == 0 && (BW & 3) == 0;
 
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
@@ -132,21 +180,37 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         const int rr = i / win, xx = i - rr * win;
         const int cy = r0 + rr;
         const unsigned char* srow = J.src + ptrdiff_t(reflect_axis(cy, gy)) * J.src_stride;
-        const float s = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
-        const float v = fmul(fsub(s, P.dec_base), P.dec_scale);
+        const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
+        const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
         if (!isfin(v)) bad = true;
-        ring_in[size_t(cy % BH) * S.win_max + xx] = v;
+        ring_in[size_t(cy % BH) * S.ring_pitch + xx] = v;
       }
       __syncthreads();
-      // ---- A: row transforms ------------------------------------------------
+      // ---- A: row transforms (block index fastest) --------------------------
       for (int task = tid; task < nbx * BH; task += nthr) {
-        const int b = task / BH, y = task - b * BH;
-        const float* in = ring_in + size_t((oy + y) % BH) * S.win_max + b * gx.step;
+        const int y = task / nbx, b = task - y * nbx;
+        const float* in = ring_in + size_t((oy + y) % BH) * S.ring_pitch + b * gx.step;
         float row[CAPW];
+        if (vec4) {
+#pragma unroll UW
+          for (int x = 0; x < CAPW; x += 4) {
+            if (x < BW) {
+              const float4 q = *reinterpret_cast<const float4*>(in + x);
+              row[x] = q.x;
+              row[x + 1] = q.y;
+              row[x + 2] = q.z;
+              row[x + 3] = q.w;
+            }
+          }
+        } else {
+#pragma unroll UW
+          for (int x = 0; x < CAPW; ++x)
+            if (x < BW) row[x] = in[x];
+        }
 #pragma unroll UW
         for (int x = 0; x < CAPW; ++x)
-          if (x < BW) row[x] = P.algo == 0 ? fmul(fmul(in[x], P.wya[y]), P.wxa[x]) : fmul(in[x], P.h[y * BW + x]);
-        nf::row_forward<BWC>(row, BW, spec + (size_t(b) * BH + y) * K, P.tww, codelet);
+          if (x < BW) row[x] = P.algo == 0 ? fmul(fmul(row[x], wya[y]), wxa[x]) : fmul(row[x], h[y * BW + x]);
+        nf::row_forward<BWC>(row, BW, spec + size_t(y) * K * NB + b, P.tww, codelet, NB);
       }
       __syncthreads();
     }
@@ -155,10 +219,10 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     for (int base = 0; base < ncol; base += nthr) {
       const int task = base + tid;
       const bool active = task < ncol;
-      const int b = active ? task / K : 0, k = active ? task - b * K : 0;
+      const int k = active ? task / nbx : 0, b = active ? task - k * nbx : 0;
       cf col[CAPH];
+      cf* sp = spec + size_t(k) * NB + b;  // + y*K*NB
       if (active) {
-        cf* sp = spec + size_t(b) * BH * K + k;
         if (kalman_L) {
           const cf* L = kalman_L + (size_t(by) * gx.count + (bx_lo + b)) * P.bins + k;
 #pragma unroll UH
@@ -167,83 +231,87 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         } else {
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = sp[size_t(y) * K];
+            if (y < BH) col[y] = sp[size_t(y) * K * NB];
           nf::fft_1d<true, BHC>(col, BH, P.twh, codelet);
         }
         if (k == 0) dc[b] = col[0].r;
       }
       __syncthreads();
       if (active) {
-        const float g = P.grid ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
+        const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
         if (P.algo == 1 || P.fft3d_mode != kEnhanceOnly) {
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = spectral_bin(col[y], P.grid, y * K + k, g, P.filt, bad);
+            if (y < BH) col[y] = spectral_bin(col[y], grid, y * K + k, g, filt, bad);
         }
-        if (P.algo == 0 && P.fft3d_mode == kWienerThenEnh && k == 0) dc[nbx + b] = col[0].r;
+        if (P.algo == 0 && P.fft3d_mode == kWienerThenEnh && k == 0) dc[NB + b] = col[0].r;
       }
-      if (P.algo == 0 && P.fft3d_mode != kWienerFused && P.enh.enh) {
+      if (P.algo == 0 && P.fft3d_mode != kWienerFused && enh.enh) {
         // enhance(): template ratio recomputed from the spectrum being enhanced
         // (plan.cpp:325-329).
         if (P.fft3d_mode == kWienerThenEnh) __syncthreads();
         if (active) {
-          const float dcv = P.fft3d_mode == kWienerThenEnh ? dc[nbx + b] : dc[b];
-          const float g2 = P.grid ? fdiv(fmul(P.mean_scale, dcv), P.grid[0].r) : 0.0f;
+          const float dcv = P.fft3d_mode == kWienerThenEnh ? dc[NB + b] : dc[b];
+          const float g2 = grid ? fdiv(fmul(P.mean_scale, dcv), grid0) : 0.0f;
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = spectral_bin(col[y], P.grid, y * K + k, g2, P.enh, bad);
+            if (y < BH) col[y] = spectral_bin(col[y], grid, y * K + k, g2, enh, bad);
         }
       }
       if (active) {
         nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
-        cf* sp = spec + size_t(b) * BH * K + k;
 #pragma unroll UH
         for (int y = 0; y < CAPH; ++y)
-          if (y < BH) sp[size_t(y) * K] = col[y];
+          if (y < BH) sp[size_t(y) * K * NB] = col[y];
       }
       __syncthreads();
     }
-    // ---- C: row inverses, synthesis weighting (in place) --------------------
+    // ---- C: row inverses and synthesis weighting -----------------------------
     for (int task = tid; task < nbx * BH; task += nthr) {
-      const int b = task / BH, y = task - b * BH;
+      const int y = task / nbx, b = task - y * nbx;
       if (P.center && y != BH / 2) continue;
-      cf* bins = spec + (size_t(b) * BH + y) * K;
       float row[CAPW];
-      nf::row_inverse<BWC>(bins, BW, fct, row, P.tww, codelet);
-      float* ob = reinterpret_cast<float*>(bins);
+      nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, fct, row, P.tww, codelet, NB);
+      float* o = ob + (size_t(y) * NB + b) * OBW;
 #pragma unroll UW
       for (int x = 0; x < CAPW; ++x) {
         if (x < BW) {
           if (!isfin(row[x])) bad = true;
-          ob[x] = P.algo == 0 ? fmul(row[x], P.wxs[x]) : fmul(row[x], P.hsyn[y * BW + x]);
+          row[x] = P.algo == 0 ? fmul(row[x], wxs[x]) : fmul(row[x], hsyn[y * BW + x]);
         }
+      }
+      if ((BW & 3) == 0) {
+#pragma unroll UW
+        for (int x = 0; x < CAPW; x += 4)
+          if (x < BW) *reinterpret_cast<float4*>(o + x) = make_float4(row[x], row[x + 1], row[x + 2], row[x + 3]);
+      } else {
+#pragma unroll UW
+        for (int x = 0; x < CAPW; ++x)
+          if (x < BW) o[x] = row[x];
       }
     }
     __syncthreads();
     // ---- D: ordered overlap-add into the ring accumulator --------------------
-    const float* obuf = reinterpret_cast<const float*>(spec);
-    const size_t ob_row = size_t(2 * K);  // floats per (block, row) slot
     const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
     for (int i = tid; yhi > ylo && i < (yhi - ylo) * tw; i += nthr) {
       const int yy = i / tw, xx = i - yy * tw;
       const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;
+      const float* orow = ob + size_t(ly) * NB * OBW;
       if (P.center) {
         const int bc = X - BW / 2;  // block whose centre is X (step 1)
-        if (ly == BH / 2 && bc >= bx_lo && bc <= bx_hi) *a = obuf[(size_t(bc - bx_lo) * BH + ly) * ob_row + BW / 2];
+        if (ly == BH / 2 && bc >= bx_lo && bc <= bx_hi) *a = orow[size_t(bc - bx_lo) * OBW + BW / 2];
         continue;
       }
       const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
       if (P.algo == 0) {
         float r = 0.0f;
-        for (int bb = b0; bb <= b1; ++bb)
-          r = fadd(r, obuf[(size_t(bb - bx_lo) * BH + ly) * ob_row + (X - bb * gx.step)]);
-        *a = fadd(*a, fmul(r, P.wys[ly]));
+        for (int bb = b0; bb <= b1; ++bb) r = fadd(r, orow[size_t(bb - bx_lo) * OBW + (X - bb * gx.step)]);
+        *a = fadd(*a, fmul(r, wys[ly]));
       } else {
-        float s = *a;
-        for (int bb = b0; bb <= b1; ++bb)
-          s = fadd(s, obuf[(size_t(bb - bx_lo) * BH + ly) * ob_row + (X - bb * gx.step)]);
-        *a = s;
+        float sacc = *a;
+        for (int bb = b0; bb <= b1; ++bb) sacc = fadd(sacc, orow[size_t(bb - bx_lo) * OBW + (X - bb * gx.step)]);
+        *a = sacc;
       }
     }
     __syncthreads();
@@ -262,9 +330,17 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   if (bad) atomicOr(P.err, kErrNonFinite);
 }
 
+// Resident CTAs per SM the register budget allows: blocks up to 16x16 keep two
+// 256-thread CTAs per SM (128 registers per thread); larger transforms need the
+// full 255-register budget.
+template <int BHC, int BWC>
+struct StripOccupancy {
+  static constexpr int value = (BHC > 0 && BHC * BWC <= 256) ? 2 : 1;
+};
+
 // Plain launch: grid (strips, segments) over one plane.
 template <int BHC, int BWC, int STORAGE>
-__global__ void __launch_bounds__(256, 2) spatial_strip_kernel(DevPlan P, StripShape S, PlaneJob J) {
+__global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_strip_kernel(DevPlan P, StripShape S, PlaneJob J) {
   extern __shared__ float smem[];
   strip_tile<BHC, BWC, STORAGE>(P, J, S, blockIdx.x * S.tw, blockIdx.y * S.th, smem);
 }
@@ -283,7 +359,7 @@ struct BatchWork {
 };
 
 template <int BHC, int BWC, int STORAGE>
-__global__ void __launch_bounds__(256, 2) spatial_batch_kernel(BatchWork W) {
+__global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_batch_kernel(BatchWork W) {
   extern __shared__ float smem[];
   __shared__ int item;
   const int total = W.job_tile_base[W.njobs];

@@ -1,0 +1,52 @@
+// Test-only: exercises include/neo_fft_b200/plan.hpp the way the reference's host
+// layer does (src/plugin/filter.hpp:349-360: process_at with sources, frame, plane,
+// targets and cache arguments; Kalman initial/advance/render with copied states).
+// Prints FNV-1a checksums of the outputs for comparison with the Python path.
+#include "neo_fft_b200/plan.hpp"
+
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+static std::uint64_t fnv(const void* p, std::size_t n) {
+  std::uint64_t h = 1469598103934665603ull;
+  const auto* b = static_cast<const unsigned char*>(p);
+  for (std::size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
+}
+
+int main() {
+  using namespace neo_fft;
+  const int w = 96, h = 64;
+  std::vector<std::uint16_t> src(std::size_t(w) * h), dst(src.size());
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) src[std::size_t(y) * w + x] = std::uint16_t((x * 37 + y * 101 + (x * y) % 17) * 29 % 60000);
+  DFTConfig c;
+  c.block = 16; c.overlap = 12; c.sigma = 8; c.curves.shared = {0, 8, 1, 8};
+  Plan plan(w, h, SampleFormat{16, false, false}, c);
+  span2d::Plane<const std::uint16_t> s(src.data(), w, h, w * 2);
+  span2d::Plane<std::uint16_t> d(dst.data(), w, h, w * 2);
+  plan.process_at<std::uint16_t>({&s, 1}, d, 0, 0, {}, static_cast<runtime::SpectraCache*>(nullptr));
+  std::printf("dft %llu\n", (unsigned long long)fnv(dst.data(), dst.size() * 2));
+
+  FFT3DConfig k;
+  k.bt = 0; k.sigma = 2.5f; k.kratio = 2.0f; k.bw = k.bh = 16;
+  std::vector<float> fsrc(std::size_t(w) * h), fdst(fsrc.size());
+  for (std::size_t i = 0; i < fsrc.size(); ++i) fsrc[i] = float((i * 7919) % 1000) / 1000.0f;
+  Plan kp(w, h, SampleFormat{32, true, false}, k);
+  span2d::Plane<const float> fs(fsrc.data(), w, h, w * 4);
+  span2d::Plane<float> fd(fdst.data(), w, h, w * 4);
+  KalmanState st = kp.initial_kalman();
+  for (int f = 0; f < 3; ++f) kp.advance_kalman<float>(fs, st);
+  KalmanState copy = st;  // checkpoint copy (filter.hpp:171)
+  kp.render_kalman<float>(fs, fd, copy);
+  std::printf("kalman %llu\n", (unsigned long long)fnv(fdst.data(), fdst.size() * 4));
+  try {
+    FFT3DConfig bad;
+    bad.bt = 7;
+    Plan p2(w, h, SampleFormat{8, false, false}, bad);
+  } catch (const std::invalid_argument& e) {
+    std::printf("error %s\n", e.what());
+  }
+  return 0;
+}

@@ -51,3 +51,50 @@ def test_invalid_config_rejected_on_host():
         Plan(64, 64, SampleFormat(8), DFTConfig(ftype=7))
     with pytest.raises(ValueError, match="unsupported sample format"):
         Plan(64, 64, SampleFormat(9), DFTConfig())
+
+
+def _build_facade_check():
+    import subprocess
+    exe = ROOT / "tests" / "_build" / "facade_check"
+    exe.parent.mkdir(exist_ok=True)
+    src = ROOT / "tests" / "native" / "facade_check.cpp"
+    subprocess.run(["g++", "-std=c++17", "-O1", f"-I{ROOT / 'include'}", f"-I{ROOT / 'oracle' / 'shim'}", str(src),
+                    "-o", str(exe), f"-L{ROOT / 'neo_fft_b200'}", "-lneofft_b200",
+                    f"-Wl,-rpath,{ROOT / 'neo_fft_b200'}"], check=True)
+    return exe
+
+
+def test_cpp_facade_compiles_and_links():
+    """include/neo_fft_b200/plan.hpp (the reference Plan's class signature over the
+    C ABI) compiles against a span2d provider and links to the library."""
+    assert _build_facade_check().exists()
+
+
+@pytest.mark.gpu
+def test_cpp_facade_matches_python_path(cuda):
+    import subprocess
+    import numpy as np
+    from neo_fft_b200.plan import DFTConfig, FFT3DConfig, Plan, SampleFormat
+    out = subprocess.run([str(_build_facade_check())], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = dict(line.split(" ", 1) for line in out if line)
+    w, h = 96, 64
+    y, x = np.mgrid[0:h, 0:w]
+    src = ((x * 37 + y * 101 + (x * y) % 17) * 29 % 60000).astype(np.uint16)
+    dst = Plan(w, h, SampleFormat(16), DFTConfig(block=16, overlap=12, sigma=8, slocation=[0, 8, 1, 8])).process(src)
+
+    def fnv(b):
+        v = 1469598103934665603
+        for c in b:
+            v = ((v ^ c) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+        return v
+    assert int(got["dft"]) == fnv(dst.tobytes())
+    assert got["error"] == "FFT3D bt outside -1..5"
+    fsrc = ((np.arange(w * h) * 7919) % 1000 / 1000.0).astype(np.float32).reshape(h, w)
+    kp = Plan(w, h, SampleFormat(32, True), FFT3DConfig(bw=16, bh=16, bt=0, sigma=2.5, kratio=2.0))
+    st = kp.initial_kalman()
+    d = cuda.from_numpy(fsrc).cuda()
+    for _ in range(3):
+        kp.advance_kalman(d, st)
+    out_t = cuda.empty_like(d)
+    kp.render_kalman(d, out_t, st)
+    assert int(got["kalman"]) == fnv(out_t.cpu().numpy().tobytes())

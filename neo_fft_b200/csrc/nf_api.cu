@@ -281,23 +281,27 @@ Checked validate_call(const nf_plan& p, const nf_const_plane* sources, int n, co
 // strips because many planes already fill the GPU.
 nfd::StripShape pick_strip(const nfd::DevPlan& d, int target_ctas) {
   nfd::StripShape S;
-  const int b = std::max(d.bh, d.bw);
-  int tw = b <= 16 ? 64 : b <= 32 ? 64 : 48;
   S.tab_floats = nfd::strip_table_floats(d);
+  // Block columns per strip: the row phases run nbx*bh tasks on 256 threads, so
+  // aim for a multiple of 256 (two rounds for blocks up to 16x16, one above).
+  const int rounds = d.bh * d.bw <= 256 ? 2 : 1;
+  int nbx = std::max(2, (256 * rounds) / std::max(1, d.bh));
+  const int edge = (d.bw + d.gx.step - 1) / d.gx.step - 1;  // blocks beyond the owned columns
   for (;;) {
-    S.tw = std::min(tw, d.gx.length);
+    S.tw = std::min(std::max(d.gx.step, (nbx - edge) * d.gx.step), d.gx.length);
     S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
     S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
     int q = (S.win_max + 3) / 4;
     if (q % 2 == 0) ++q;  // odd float4 count: consecutive staged rows start in different banks
     S.ring_pitch = 4 * q;
     S.th = d.gy.length;
-    if (nfd::strip_smem_bytes(d.bh, d.bw, S) <= 110 * 1024 || tw <= 8) break;
-    tw /= 2;
+    if (nfd::strip_smem_bytes(d.bh, d.bw, S) <= (rounds == 2 ? 110 : 200) * 1024 || nbx <= edge + 2) break;
+    nbx = std::max(edge + 2, nbx * 3 / 4);
   }
   const int strips = (d.gx.length + S.tw - 1) / S.tw;
   // At most one wave in the plain launch (a partial second wave doubles the time).
-  const int segs = std::max(1, std::min(target_ctas / strips, d.gy.length / std::max(1, 2 * d.bh)));
+  // Segments shorter than 3 block heights recompute too many vertical neighbours.
+  const int segs = std::max(1, std::min(target_ctas / strips, d.gy.length / std::max(1, 3 * d.bh)));
   S.th = std::max(1, (d.gy.length + segs - 1) / segs);
   return S;
 }

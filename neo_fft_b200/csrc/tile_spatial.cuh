@@ -159,10 +159,21 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   }
   (void)t_wa;
   const cf* grid = P.grid ? reinterpret_cast<const cf*>(stage(reinterpret_cast<const float*>(P.grid), 2 * bins)) : nullptr;
-  DevSpectral filt = P.filt, enh = P.enh;
-  if (P.filt.primary) filt.primary = stage(P.filt.primary, bins);
-  if (P.enh.sharpen_w) filt.sharpen_w = enh.sharpen_w = stage(P.enh.sharpen_w, bins);
-  if (P.enh.halo_w) filt.halo_w = enh.halo_w = stage(P.enh.halo_w, bins);
+  // Filter parameters with their tables redirected to shared memory. They live in
+  // shared memory too (a per-thread copy would sit on the local-memory stack).
+  __shared__ DevSpectral s_filt, s_enh;
+  const float* prim = P.filt.primary ? stage(P.filt.primary, bins) : nullptr;
+  const float* shw = P.enh.sharpen_w ? stage(P.enh.sharpen_w, bins) : nullptr;
+  const float* hlw = P.enh.halo_w ? stage(P.enh.halo_w, bins) : nullptr;
+  if (tid == 0) {
+    s_filt = P.filt;
+    s_enh = P.enh;
+    if (prim) s_filt.primary = prim;
+    if (shw) s_filt.sharpen_w = s_enh.sharpen_w = shw;
+    if (hlw) s_filt.halo_w = s_enh.halo_w = hlw;
+  }
+  const DevSpectral& filt = s_filt;
+  const DevSpectral& enh = s_enh;
   for (int i = tid; i < BH * S.tw; i += nthr) acc[i] = 0.0f;
   __syncthreads();
   const float grid0 = grid ? grid[0].r : 1.0f;
@@ -375,12 +386,20 @@ __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_
       if (W.job_tile_base[mid] <= t) lo = mid;
       else hi = mid - 1;
     }
-    const PlaneJob J = W.jobs[lo];
-    const DevPlan P = W.plans[J.plan];
-    const StripShape S = W.shapes[J.plan];
+    // The work item's plan, job and shape are read once into shared memory (a
+    // per-thread copy of the plan would live on the local-memory stack).
+    __shared__ DevPlan sP;
+    __shared__ PlaneJob sJ;
+    __shared__ StripShape sS;
+    if (threadIdx.x == 0) {
+      sJ = W.jobs[lo];
+      sP = W.plans[sJ.plan];
+      sS = W.shapes[sJ.plan];
+    }
+    __syncthreads();
     const int local = t - W.job_tile_base[lo];
     const int sx = local % W.job_tiles_x[lo], sy = local / W.job_tiles_x[lo];
-    strip_tile<BHC, BWC, STORAGE>(P, J, S, sx * S.tw, sy * S.th, smem);
+    strip_tile<BHC, BWC, STORAGE>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
   }
 }
 

@@ -4,6 +4,8 @@
 
 Workloads (one plane per launch, seeded synthetic content):
   dft16    DFTTest sbsize 16 / sosize 12, ftype 0, sigma 8 flat curve, u16 1920x1080
+  dft16_batch the same configuration as one batched launch over 4 YUV420 frames
+           (4 x 1920x1080 + 8 x 960x540 planes)
   dft16_4k the same on a u16 3840x2160 plane (input+output larger than L2)
   fft3d32  FFT3D bw=bh=32, ow=oh=16, sigma 2, u8 640x360
   fft3d48  FFT3D bt=3 bw=bh=48, ow=oh=24, sigma 3, sharpen 0.3, u16 (10-bit) 3840x2160
@@ -40,6 +42,21 @@ def main():
         plan = Plan(w, h, SampleFormat(16), DFTConfig(block=16, overlap=12, ftype=0, sigma=8.0, slocation=[0, 8, 1, 8]))
         srcs = [torch.from_numpy(_plane(h, w, np.uint16, 4096, 60000, 1)).to(dev)]
         targets = ()
+    elif wl == "dft16_batch":
+        from . import Batch
+        cfg = DFTConfig(block=16, overlap=12, ftype=0, sigma=8.0, slocation=[0, 8, 1, 8])
+        luma, chroma = Plan(1920, 1080, SampleFormat(16), cfg), Plan(960, 540, SampleFormat(16), cfg)
+        items = []
+        for f in range(4):
+            for p, (w, h) in ((luma, (1920, 1080)), (chroma, (960, 540)), (chroma, (960, 540))):
+                s_ = torch.from_numpy(_plane(h, w, np.uint16, 4096, 60000, f)).to(dev)
+                items.append((p, s_, torch.empty_like(s_)))
+        batch = Batch(items)
+        for _ in range(a.launches):
+            batch.launch()
+        torch.cuda.synchronize()
+        batch.sync_status()
+        return
     elif wl == "fft3d32":
         w, h = 640, 360
         plan = Plan(w, h, SampleFormat(8), FFT3DConfig(bw=32, bh=32, ow=16, oh=16, sigma=2.0))

@@ -286,6 +286,7 @@ def run_ours(args):
         chroma.process([pin_in[f][2].numpy()], pin_out[f][2].numpy())
     host_plane_value = FRAMES * W * H / (time.perf_counter() - t0) / 1e6
 
+    train = differentiable_pass(args, dev)
     cpu = cpu_baseline() if (rank == 0 and world == 1) else None
     if world > 1:
         dist.barrier()
@@ -315,8 +316,61 @@ def run_ours(args):
                               "peak_source": "148 SMs x 128 FP32 lanes x 2 x max SM clock (nominal)"}},
         "clocks": clocks.summary() if clocks else None,
         "cpu_baseline": cpu,
+        "fwd_bwd": train,
     }
     print(json.dumps(line))
+
+
+def differentiable_pass(args, dev):
+    """Differentiable DFTTest: 16 float32 256x256 noisy patches, sbsize 16 / sosize 8, ftype 0,
+    learnable 16x9 table; loss = MSE to the clean patches. Times the forward alone and
+    forward+backward (gradients w.r.t. pixels and table) with CUDA events around each
+    step and the L2 flushed (a 256 MB write) before every step."""
+    import torch
+
+    from neo_fft_b200 import DFTConfig
+    from neo_fft_b200.autograd import SigmaTableDenoiser
+    sys.path.insert(0, str(ROOT))
+    from tests.synth import noisy_patches
+    n, s = 16, 256
+    noisy, clean = noisy_patches(n, s, 41)
+    x0 = torch.from_numpy(noisy).to(dev)
+    cl = torch.from_numpy(clean).to(dev)
+    m = SigmaTableDenoiser(s, s, DFTConfig(block=16, overlap=8, ftype=0, sigma=4.0))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def fwd():
+        with torch.no_grad():
+            m(x0)
+
+    def fwd_bwd():
+        x = x0.detach().requires_grad_()
+        m.table.grad = None
+        ((m(x) - cl) ** 2).mean().backward()
+
+    def measure(fn, steps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        total = 0.0
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            total += e0.elapsed_time(e1)
+        m.plan.sync_status()
+        return total / steps
+
+    steps = max(5, args.steps)
+    f_ms, fb_ms = measure(fwd, steps), measure(fwd_bwd, steps)
+    px = n * s * s
+    return {"value": px / (fb_ms / 1e3) / 1e6, "unit": "Mpx/s", "ms_per_step": fb_ms,
+            "forward_value": px / (f_ms / 1e3) / 1e6, "forward_ms": f_ms, "ratio_to_forward": f_ms / fb_ms,
+            "workload": "16 float32 256x256 patches, sbsize 16 / sosize 8, ftype 0, learnable 16x9 table, "
+                        "MSE loss; gradients w.r.t. pixels and table (autograd over the C ABI adjoint kernels)",
+            "l2": "flushed before every step (256 MB write)"}
 
 
 def ctypes_stream(stream):

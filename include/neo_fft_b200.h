@@ -123,6 +123,12 @@ nf_status nf_plan_process_device(const nf_plan* plan, const nf_const_plane* sour
 nf_status nf_plan_process_host(const nf_plan* plan, const nf_const_plane* sources, int nsources,
                                const int* targets, int ntargets, nf_plane dst, int frame, int plane,
                                void* stream, char* err, size_t err_len);
+/* Several planes of one single-frame plan (FFT3D bt=1, DFTTest tbsize=1) in one launch,
+ * for callers that hold many small planes at once (patch batches). Same results as one
+ * nf_plan_process_device call per plane; at most 32 planes per call. The reference has
+ * no counterpart: its host calls Plan::process_at once per plane (filter.hpp:349-360). */
+nf_status nf_plan_process_planes_device(const nf_plan* plan, const nf_const_plane* sources, const nf_plane* dsts,
+                                        int nplanes, void* stream, char* err, size_t err_len);
 /* Synchronises `stream` and returns NF_NON_FINITE if any launch since the last call
  * met a non-finite sample or intermediate (then clears the flag). */
 nf_status nf_plan_sync_status(const nf_plan* plan, void* stream, char* err, size_t err_len);
@@ -170,6 +176,28 @@ nf_status nf_batch_launch(nf_batch* batch, void* stream, char* err, size_t err_l
 /* Captures nf_batch_launch into a CUDA graph on first use, then replays the graph. */
 nf_status nf_batch_graph_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
 void nf_batch_destroy(nf_batch* batch);
+
+/* Differentiable form (no reference counterpart; the reference has no gradients).
+ * DFTTest plans keep their per-bin primary table A ([tbsize][sbsize][sbsize/2+1],
+ * already calibrated: the threshold the Wiener gain compares with) in device memory.
+ * nf_plan_set_primary replaces it from device memory on `stream`, so a training loop
+ * can learn it; a plan without sigma curves starts from its uniform value, which
+ * nf_plan_get_primary copies out. Replacing the table changes the plan: calls on
+ * other streams that use the plan must be ordered with the replacement. */
+nf_status nf_plan_set_primary(nf_plan* plan, const float* table_device, int count, void* stream, char* err,
+                              size_t err_len);
+nf_status nf_plan_get_primary(const nf_plan* plan, float* table_device, int count, void* stream, char* err,
+                              size_t err_len);
+/* Backward of nf_plan_process_device for float DFTTest plans (tbsize=1, smode=1,
+ * ftype 0, 1 or 2): given the forward inputs and the gradient of the outputs,
+ * writes the gradient of the inputs and the summed gradient of the primary table
+ * over all planes. Forward spectra are recomputed, not stored. `scratch` is caller-
+ * provided device memory of nf_dft_backward_scratch_bytes bytes. Sums run in a fixed
+ * order, so gradients are deterministic. At most 32 planes per call. */
+nf_status nf_dft_backward_scratch_bytes(const nf_plan* plan, int nplanes, size_t* bytes);
+nf_status nf_dft_backward_device(const nf_plan* plan, const nf_const_plane* sources, const nf_const_plane* grad_out,
+                                 const nf_plane* grad_sources, int nplanes, float* grad_primary, void* scratch,
+                                 size_t scratch_bytes, void* stream, char* err, size_t err_len);
 
 /* KernelInfo (docs/api/en/kernel-info.md; vapoursynth.cpp:64-69): labels of the
  * active implementation. Each string buffer receives at most len bytes. */

@@ -94,6 +94,14 @@ PROTOTYPES = {
     "nf_batch_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_batch_graph_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_batch_destroy": (None, [c_void_p]),
+    "nf_plan_process_planes_device": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfPlane), c_int,
+                                              c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_plan_set_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_plan_get_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_dft_backward_scratch_bytes": (c_int, [c_void_p, c_int, ctypes.POINTER(c_size_t)]),
+    "nf_dft_backward_device": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfConstPlane),
+                                       ctypes.POINTER(NfPlane), c_int, c_void_p, c_void_p, c_size_t, c_void_p,
+                                       ctypes.c_char_p, c_size_t]),
     "nf_kernel_info": (c_int, [ctypes.c_char_p, c_size_t, ctypes.c_char_p, c_size_t, ctypes.c_char_p,
                                c_size_t, _IP]),
 }

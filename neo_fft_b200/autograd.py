@@ -1,0 +1,104 @@
+"""Differentiable DFTTest (tbsize=1, smode=1, float planes, ftype 0/1/2) for PyTorch.
+
+`DFTTestFunction.apply(x, table, plan)` filters a batch of float32 CUDA planes
+x[B, H, W] with the primary table `table` (the per-bin threshold the Wiener gain
+compares with, [sbsize * (sbsize//2+1)], already calibrated) and differentiates with
+respect to both. Forward runs the sm_100a strip kernel over up to 32 planes per launch (results
+identical to `Plan.process`); backward runs the hand-written adjoint kernels through the C ABI
+(nf_dft_backward_device), recomputing block spectra instead of storing them.
+
+`SigmaTableDenoiser` wraps it as a module with a learnable table; in data-parallel
+training its table gradient is all-reduced once per step (`allreduce_table_grad`).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _capi as C
+from .plan import DFTConfig, Plan, SampleFormat, _plane
+
+
+def _set_primary(plan: Plan, table: torch.Tensor, stream) -> None:
+    t = table.detach().contiguous().to(torch.float32)
+    err = ctypes.create_string_buffer(256)
+    C.raise_for(plan._lib.nf_plan_set_primary(plan._h, ctypes.c_void_p(t.data_ptr()), t.numel(), stream, err, 256),
+                err.value)
+    return t
+
+
+class DFTTestFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x: torch.Tensor, table: torch.Tensor, plan: Plan):
+        if x.dim() != 3 or x.dtype != torch.float32 or not x.is_cuda:
+            raise ValueError("x must be a float32 CUDA tensor [batch, height, width]")
+        x = x.contiguous()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        keep = _set_primary(plan, table, stream)
+        out = torch.empty_like(x)
+        plan.process_planes(list(x), list(out), stream=stream.value)
+        ctx.save_for_backward(x, keep)
+        ctx.plan = plan
+        return out
+
+    @staticmethod
+    def backward(ctx, gout: torch.Tensor):
+        x, table = ctx.saved_tensors
+        plan: Plan = ctx.plan
+        gout = gout.contiguous()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        keep = _set_primary(plan, table, stream)  # noqa: F841 (kept alive until the launch is enqueued)
+        gx = torch.empty_like(x)
+        gtab = torch.zeros_like(table, dtype=torch.float32)
+        lib = plan._lib
+        err = ctypes.create_string_buffer(256)
+        for start in range(0, x.shape[0], 32):
+            n = min(32, x.shape[0] - start)
+            need = ctypes.c_size_t()
+            lib.nf_dft_backward_scratch_bytes(plan._h, n, ctypes.byref(need))
+            scratch = torch.empty(max(1, need.value), dtype=torch.uint8, device=x.device)
+            part = torch.empty_like(gtab)
+            srcs = (C.NfConstPlane * n)(*[_plane(x[start + i], True) for i in range(n)])
+            gouts = (C.NfConstPlane * n)(*[_plane(gout[start + i], True) for i in range(n)])
+            gsrcs = (C.NfPlane * n)(*[_plane(gx[start + i], False) for i in range(n)])
+            st = lib.nf_dft_backward_device(plan._h, srcs, gouts, gsrcs, n, ctypes.c_void_p(part.data_ptr()),
+                                            ctypes.c_void_p(scratch.data_ptr()), need.value, stream, err, 256)
+            C.raise_for(st, err.value)
+            gtab += part
+        return gx, gtab.to(table.dtype), None
+
+
+class SigmaTableDenoiser(torch.nn.Module):
+    """DFTTest with a learnable per-frequency table (sbsize x (sbsize//2+1))."""
+
+    def __init__(self, width: int, height: int, config: DFTConfig, initial: torch.Tensor | None = None):
+        super().__init__()
+        if config.tbsize != 1 or config.mode != 1 or config.ftype not in (0, 1, 2):
+            raise ValueError("differentiable DFTTest needs tbsize=1, smode=1 and ftype 0, 1 or 2")
+        self.plan = Plan(width, height, SampleFormat(32, True), config)
+        k = config.block * (config.block // 2 + 1)
+        if initial is None:
+            initial = torch.empty(k, dtype=torch.float32, device="cuda")
+            err = ctypes.create_string_buffer(256)
+            stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+            C.raise_for(self.plan._lib.nf_plan_get_primary(self.plan._h, ctypes.c_void_p(initial.data_ptr()), k,
+                                                           stream, err, 256), err.value)
+        self.table = torch.nn.Parameter(initial.clone().float().cuda())
+
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        return DFTTestFunction.apply(x, self.table, self.plan)
+
+
+def shard(n: int, rank: int, world: int) -> range:
+    """Contiguous shard of n patches for data-parallel training."""
+    per = (n + world - 1) // world
+    return range(min(n, rank * per), min(n, (rank + 1) * per))
+
+
+def allreduce_table_grad(module: SigmaTableDenoiser, group=None) -> None:
+    """Sum the table gradient over data-parallel ranks (one NCCL all-reduce of
+    sbsize*(sbsize//2+1) floats per step); pixel gradients stay local."""
+    import torch.distributed as dist
+    if module.table.grad is not None and dist.is_initialized():
+        dist.all_reduce(module.table.grad, op=dist.ReduceOp.SUM, group=group)

@@ -1,0 +1,346 @@
+// Adjoint (backward) of the single-frame DFTTest pipeline for float planes
+// (tbsize=1, smode=1, ftype 0/1/2, zmean on or off), with respect to the source
+// pixels and to the per-bin primary table A (the learnable sigma table).
+//
+// Forward per block (src/algorithms/plan.cpp:538-607, kernels/scalar/spectral.cpp):
+//   v = 255*s (decode), b = v*h, X = r2c(b), g = mean*Re X0 / Re G0, M = g*G,
+//   R = X - M, p = |R|^2, gain(p, A), Y = gain*R + M, y = c2r(Y)/N, acc += y*hsyn,
+//   out = acc/255.
+// Backward per block, with the forward spectra recomputed (nothing is stored):
+//   d_acc = d_out/255 -> dy = d_acc*hsyn (transposed overlap-add, gathered)
+//   dY = (m_kx/N) * r2c(dy)          adjoint of the half-complex inverse
+//                                     (m_kx = 1 for the DC/Nyquist columns, else 2)
+//   per bin: dR = gain*dY + 2*dgain/dp*<dY,R>*R, dM = dY - dR, dX = dR,
+//            dA += <dY,R>*dgain/dA; dg = sum_k <dM_k, G_k>; dX0.re += dg*mean/Re G0
+//   db = c2r_unnormalised(dX')        adjoint of r2c (dX' halves interior columns)
+//   dv = db*h -> d_cover (ordered gather, like the forward overlap-add)
+// A second kernel folds the cover gradient onto the source through the single
+// reflection and multiplies by 255; a third reduces the per-tile table gradients
+// in a fixed order. Every sum has a fixed order, so gradients are deterministic.
+#pragma once
+#include "tile_spatial.cuh"
+
+namespace nfd {
+
+struct AdjointShape {
+  int tw, th;       // tile of the cover plane
+  int nbx_max, win_max, ring_pitch, tab_floats;
+  int tiles_x, tiles_y;
+};
+
+struct AdjointJob {
+  const float* src;     // forward input plane (float samples)
+  long long src_stride; // bytes
+  const float* gout;    // gradient of the output plane
+  long long gout_stride;
+  float* dcov;          // scratch: cover-plane gradient [cover_h][cover_w]
+  float* partial;       // scratch: per-tile table gradients [tiles][bins]
+};
+
+__host__ __device__ inline size_t adjoint_smem_bytes(int bh, int bw, const AdjointShape& s) {
+  const size_t K = size_t(bw / 2 + 1), bins = size_t(bh) * K;
+  const size_t spec_cf = (size_t(s.nbx_max) * bh * K + 1) & ~size_t(1);
+  return sizeof(float) * (size_t(s.tab_floats) + 2 * size_t(bh) * s.ring_pitch + 2 * spec_cf * 2 +
+                          size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max) +
+                          size_t(s.nbx_max) * bins + bins + 2 * size_t(s.nbx_max) * K);
+}
+
+// Per-bin backward of spectral_bin for ftype 0 (Wiener, any exponent), 1 (hard
+// threshold) and 2 (constant gain). x: forward spectrum bin; dy: incoming complex
+// gradient. Returns dX; adds the template gradient to dg and the table gradient to da.
+__device__ __forceinline__ cf spectral_bin_adjoint(cf x, cf dy, const cf* grid, int k, float g, const DevSpectral& p,
+                                                   float& dg, float& da) {
+  const float a = p.primary ? p.primary[k] : p.a;
+  const float mr = grid ? g * grid[k].r : 0.0f;
+  const float mi = grid ? g * grid[k].i : 0.0f;
+  const float re = x.r - mr, im = x.i - mi;
+  const float power = re * re + im * im;
+  float gain = 0.0f, dgain_dp = 0.0f, dgain_da = 0.0f;
+  if (p.type == 0) {
+    const float q = power + 1e-15f;
+    const float r = (power - a) / q;
+    if (r > 0.0f) {
+      float dw;  // d gain / d r
+      const float e1 = p.exponent - 1.0f, e5 = p.exponent - 0.5f;
+      if (fabsf(e1) < 0.00005f) {
+        gain = r;
+        dw = 1.0f;
+      } else if (fabsf(e5) < 0.00005f) {
+        gain = sqrtf(r);
+        dw = 0.5f / gain;
+      } else {
+        gain = powf(r, p.exponent);
+        dw = p.exponent * gain / r;
+      }
+      dgain_dp = dw * (a + 1e-15f) / (q * q);
+      dgain_da = -dw / q;
+    }
+  } else if (p.type == 1) {
+    gain = power < a ? 0.0f : 1.0f;
+  } else {
+    gain = a;
+    dgain_da = 1.0f;
+  }
+  const float dgain = dy.r * re + dy.i * im;  // <dY, R>
+  da += dgain * dgain_da;
+  const float dp = dgain * dgain_dp;
+  const cf dr = {gain * dy.r + 2.0f * dp * re, gain * dy.i + 2.0f * dp * im};
+  if (grid) dg += (dy.r - dr.r) * grid[k].r + (dy.i - dr.i) * grid[k].i;
+  return dr;
+}
+
+template <int BHC, int BWC>
+__device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob& J, const AdjointShape& S, int tile,
+                                             float* smem) {
+  const int BH = BHC > 0 ? BHC : P.bh;
+  const int BW = BWC > 0 ? BWC : P.bw;
+  const int K = BW / 2 + 1;
+  constexpr int CAPH = BHC > 0 ? BHC : nf::kMaxProject;
+  constexpr int CAPW = BWC > 0 ? BWC : nf::kMaxProject;
+  constexpr int UH = BHC > 0 ? CAPH : 1, UW = BWC > 0 ? CAPW : 1;
+  constexpr bool kCodelet = BHC == BWC && (BWC == 8 || BWC == 16 || BWC == 32);
+  const bool codelet = kCodelet || (BHC == 0 && P.codelet != 0);
+  const DevAxis gx = P.gx, gy = P.gy;
+  const int NB = S.nbx_max, OBW = BW + 4, bins = BH * K;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+
+  // Tile of the cover plane (cover coordinates).
+  const int X0 = (tile % S.tiles_x) * S.tw, Y0 = (tile / S.tiles_x) * S.th;
+  const int tw = min(S.tw, gx.cover - X0), th = min(S.th, gy.cover - Y0);
+  const int bx_lo = max(0, floor_div_i(X0 - BW, gx.step) + 1);
+  const int bx_hi = min(gx.count - 1, floor_div_i(X0 + tw - 1, gx.step));
+  const int by_lo = max(0, floor_div_i(Y0 - BH, gy.step) + 1);
+  const int by_hi = min(gy.count - 1, floor_div_i(Y0 + th - 1, gy.step));
+  const int nbx = bx_hi - bx_lo + 1;
+  const int cx0 = bx_lo * gx.step;
+  const int win = (nbx - 1) * gx.step + BW;
+
+  float* tab = smem;
+  float* ring = tab + S.tab_floats;
+  float* gring = ring + size_t(BH) * S.ring_pitch;
+  const size_t spec_cf = (size_t(NB) * BH * K + 1) & ~size_t(1);
+  cf* spec = reinterpret_cast<cf*>(gring + size_t(BH) * S.ring_pitch);
+  cf* gspec = spec + spec_cf;
+  float* ob = reinterpret_cast<float*>(gspec + spec_cf);
+  float* acc = ob + size_t(BH) * NB * OBW;
+  float* dc = acc + size_t(BH) * S.tw;
+  float* da_blk = dc + 2 * size_t(NB);
+  float* da_tile = da_blk + size_t(NB) * bins;
+  float* dg_part = da_tile + bins;  // [NB][K]
+
+  // tables
+  int off = 0;
+  auto stage = [&](const float* src, int n) {
+    float* d = tab + off;
+    for (int i = tid; i < n; i += nthr) d[i] = src[i];
+    off += n;
+    return d;
+  };
+  const float* h = stage(P.h, BH * BW);
+  const float* hsyn = stage(P.hsyn, BH * BW);
+  const cf* grid = P.grid ? reinterpret_cast<const cf*>(stage(reinterpret_cast<const float*>(P.grid), 2 * bins)) : nullptr;
+  __shared__ DevSpectral s_filt;
+  const float* prim = P.filt.primary ? stage(P.filt.primary, bins) : nullptr;
+  if (tid == 0) {
+    s_filt = P.filt;
+    if (prim) s_filt.primary = prim;
+  }
+  for (int i = tid; i < BH * S.tw; i += nthr) acc[i] = 0.0f;
+  for (int i = tid; i < bins; i += nthr) da_tile[i] = 0.0f;
+  __syncthreads();
+  const DevSpectral& filt = s_filt;
+  const float grid0 = grid ? grid[0].r : 1.0f;
+  const float invN = 1.0f / (float(BW) * float(BH));
+  const float out_scale = P.out_scale;
+
+  for (int by = by_lo; by <= by_hi; ++by) {
+    const int oy = by * gy.step;
+    __syncthreads();
+    // ---- stage source rows (decoded) and upstream-gradient rows -------------
+    const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
+    const int nrows = oy + BH - r0;
+    for (int i = tid; i < nrows * win; i += nthr) {
+      const int rr = i / win, xx = i - rr * win;
+      const int cy = r0 + rr, cx = cx0 + xx;
+      const float* srow = reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(J.src) +
+                                                         ptrdiff_t(reflect_axis(cy, gy)) * J.src_stride);
+      ring[size_t(cy % BH) * S.ring_pitch + xx] = srow[reflect_axis(cx, gx)] * P.dec_scale;
+      const int py = cy - gy.offset, px = cx - gx.offset;
+      float gv = 0.0f;
+      if (py >= 0 && py < gy.length && px >= 0 && px < gx.length)
+        gv = reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(J.gout) +
+                                            ptrdiff_t(py) * J.gout_stride)[px] * out_scale;
+      gring[size_t(cy % BH) * S.ring_pitch + xx] = gv;
+    }
+    __syncthreads();
+    // ---- rows: forward spectrum rows and gradient rows ----------------------
+    for (int task = tid; task < 2 * nbx * BH; task += nthr) {
+      const int which = task / (nbx * BH), t2 = task - which * nbx * BH;
+      const int y = t2 / nbx, b = t2 - y * nbx;
+      const float* in = (which ? gring : ring) + size_t((oy + y) % BH) * S.ring_pitch + b * gx.step;
+      float row[CAPW];
+#pragma unroll UW
+      for (int x = 0; x < CAPW; ++x)
+        if (x < BW) row[x] = which ? in[x] * hsyn[y * BW + x] : fmul(in[x], h[y * BW + x]);
+      nf::row_forward<BWC>(row, BW, (which ? gspec : spec) + size_t(y) * K * NB + b, P.tww, codelet, NB);
+    }
+    __syncthreads();
+    // ---- columns: forward transforms, DC exchange, per-bin adjoint -----------
+    // (k = 0 tasks come first, so every block's DC is exchanged in the first pass)
+    const int ncol = nbx * K;
+    for (int base = 0; base < ncol; base += nthr) {
+      const int task = base + tid;
+      const bool active = task < ncol;
+      const int k = active ? task / nbx : 0, b = active ? task - k * nbx : 0;
+      cf x[CAPH], gcol[CAPH];
+      cf* sp = spec + size_t(k) * NB + b;
+      cf* gp = gspec + size_t(k) * NB + b;
+      float dg = 0.0f;
+      if (active) {
+#pragma unroll UH
+        for (int y = 0; y < CAPH; ++y)
+          if (y < BH) {
+            x[y] = sp[size_t(y) * K * NB];
+            gcol[y] = gp[size_t(y) * K * NB];
+          }
+        nf::fft_1d<true, BHC>(x, BH, P.twh, codelet);
+        nf::fft_1d<true, BHC>(gcol, BH, P.twh, codelet);
+        if (k == 0) dc[b] = x[0].r;
+      }
+      __syncthreads();
+      if (active) {
+        const float g = grid ? fmul(P.mean_scale, dc[b]) / grid0 : 0.0f;
+        const float mk = (k == 0 || (BW % 2 == 0 && k == BW / 2)) ? invN : 2.0f * invN;
+        const bool own = (bx_lo + b) * gx.step >= X0 && (bx_lo + b) * gx.step < X0 + tw && oy >= Y0 && oy < Y0 + th;
+#pragma unroll UH
+        for (int y = 0; y < CAPH; ++y)
+          if (y < BH) {
+            float da = 0.0f;
+            const cf dY = {gcol[y].r * mk, gcol[y].i * mk};
+            sp[size_t(y) * K * NB] = spectral_bin_adjoint(x[y], dY, grid, y * K + k, g, filt, dg, da);
+            da_blk[size_t(b) * bins + y * K + k] = own ? da : 0.0f;
+          }
+        dg_part[size_t(b) * K + k] = dg;
+      }
+    }
+    __syncthreads();
+    // ---- columns: template-ratio gradient, adjoint of r2c, inverse -----------
+    for (int task = tid; task < ncol; task += nthr) {
+      const int k = task / nbx, b = task - k * nbx;
+      cf x[CAPH];
+      cf* sp = spec + size_t(k) * NB + b;
+#pragma unroll UH
+      for (int y = 0; y < CAPH; ++y)
+        if (y < BH) x[y] = sp[size_t(y) * K * NB];
+      if (k == 0 && grid) {  // g = mean * Re X0 / Re G0
+        float dgs = 0.0f;
+        for (int kk = 0; kk < K; ++kk) dgs += dg_part[size_t(b) * K + kk];
+        x[0].r += dgs * P.mean_scale / grid0;
+      }
+      // adjoint of r2c: halve interior columns, unnormalised inverse
+      const float half = (k == 0 || (BW % 2 == 0 && k == BW / 2)) ? 1.0f : 0.5f;
+#pragma unroll UH
+      for (int y = 0; y < CAPH; ++y)
+        if (y < BH) x[y] = {x[y].r * half, x[y].i * half};
+      nf::fft_1d<false, BHC>(x, BH, P.twh, codelet);
+#pragma unroll UH
+      for (int y = 0; y < CAPH; ++y)
+        if (y < BH) sp[size_t(y) * K * NB] = x[y];
+    }
+    __syncthreads();
+    // ---- table gradient of owned blocks, in block order ----------------------
+    for (int i = tid; i < bins; i += nthr) {
+      float s = da_tile[i];
+      for (int b = 0; b < nbx; ++b) s += da_blk[size_t(b) * bins + i];
+      da_tile[i] = s;
+    }
+    // ---- rows: unnormalised inverse, analysis-window weighting ---------------
+    for (int task = tid; task < nbx * BH; task += nthr) {
+      const int y = task / nbx, b = task - y * nbx;
+      float row[CAPW];
+      nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, 1.0f, row, P.tww, codelet, NB);
+      float* o = ob + (size_t(y) * NB + b) * OBW;
+#pragma unroll UW
+      for (int x = 0; x < CAPW; ++x)
+        if (x < BW) o[x] = row[x] * h[y * BW + x];
+    }
+    __syncthreads();
+    // ---- ordered gather into the cover-gradient ring; retire rows -------------
+    const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
+    for (int i = tid; yhi > ylo && i < (yhi - ylo) * tw; i += nthr) {
+      const int yy = i / tw, xx = i - yy * tw;
+      const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
+      float* a = acc + size_t(Y % BH) * S.tw + xx;
+      const float* orow = ob + size_t(ly) * NB * OBW;
+      const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
+      float sacc = *a;
+      for (int bb = b0; bb <= b1; ++bb) sacc += orow[size_t(bb - bx_lo) * OBW + (X - bb * gx.step)];
+      *a = sacc;
+    }
+    __syncthreads();
+    const int rlo = max(oy, Y0), rhi = min(by == by_hi ? Y0 + th : oy + gy.step, Y0 + th);
+    for (int i = tid; rhi > rlo && i < (rhi - rlo) * tw; i += nthr) {
+      const int yy = i / tw, xx = i - yy * tw;
+      const int Y = rlo + yy;
+      float* a = acc + size_t(Y % BH) * S.tw + xx;
+      J.dcov[size_t(Y) * gx.cover + X0 + xx] = *a;
+      *a = 0.0f;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < bins; i += nthr) J.partial[size_t(tile) * bins + i] = da_tile[i];
+}
+
+constexpr int kAdjointMaxPlanes = 32;
+struct AdjointBatch {  // passed by value: no per-call uploads, capturable in graphs
+  AdjointJob job[kAdjointMaxPlanes];
+  float* gsrc[kAdjointMaxPlanes];
+  long long gsrc_stride[kAdjointMaxPlanes];
+  int n;
+};
+
+template <int BHC, int BWC>
+__global__ void __launch_bounds__(256, 1) dft_adjoint_kernel(DevPlan P, AdjointShape S, AdjointBatch B) {
+  extern __shared__ float smem[];
+  const int tiles = S.tiles_x * S.tiles_y;
+  adjoint_tile<BHC, BWC>(P, B.job[blockIdx.x / tiles], S, blockIdx.x % tiles, smem);
+}
+
+#ifdef NF_ADJOINT_AUX_KERNELS  // defined by the one unit that launches them (nf_api.cu)
+// Source gradient: each source pixel gathers the cover positions that reflect onto
+// it (single reflection per axis, ascending cover row then column) times 255.
+__global__ void dft_adjoint_fold_kernel(DevPlan P, AdjointBatch B) {
+  const AdjointJob& J = B.job[blockIdx.z];
+  const DevAxis gx = P.gx, gy = P.gy;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= gx.length || y >= gy.length) return;
+  int cxs[3], cys[3], nx = 0, ny = 0;
+  // cover c reflects to source j: c = off + j, or c = off - j (j >= 1), or
+  // c = off + 2L - 2 - j (j <= L - 2); keep those inside the cover, ascending.
+  auto axis = [](int j, const DevAxis& a, int* out, int& n) {
+    const int c1 = a.offset - j, c0 = a.offset + j, c2 = a.offset + 2 * a.length - 2 - j;
+    if (j >= 1 && c1 >= 0) out[n++] = c1;
+    out[n++] = c0;
+    if (j <= a.length - 2 && c2 < a.cover && c2 - a.offset >= a.length) out[n++] = c2;
+  };
+  axis(x, gx, cxs, nx);
+  axis(y, gy, cys, ny);
+  float s = 0.0f;
+  for (int i = 0; i < ny; ++i)
+    for (int j = 0; j < nx; ++j) s += J.dcov[size_t(cys[i]) * gx.cover + cxs[j]];
+  float* row = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(B.gsrc[blockIdx.z]) +
+                                        ptrdiff_t(y) * B.gsrc_stride[blockIdx.z]);
+  row[x] = s * P.dec_scale;
+}
+
+// Table gradient: sum of all tiles' partials of all planes, in tile order.
+__global__ void dft_adjoint_reduce_kernel(const float* partial, int ntiles, int bins, float* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= bins) return;
+  float s = 0.0f;
+  for (int t = 0; t < ntiles; ++t) s += partial[size_t(t) * bins + k];
+  out[k] = s;
+}
+#endif
+
+} // namespace nfd

@@ -7,11 +7,11 @@
 
 namespace nfd {
 struct StripShape;
-struct PlaneJob;
+struct PlaneJobs;
 struct BatchWork;
 #define NF_DECLARE_SPATIAL(BH, BW)                                                                              \
   cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const StripShape& s, dim3 grid, size_t smem,         \
-                                         const PlaneJob& job, cudaStream_t st);                                 \
+                                         const PlaneJobs& job, cudaStream_t st);                                \
   cudaError_t launch_spatial_batch_##BH##x##BW(int storage, const BatchWork& w, int ctas, size_t smem,           \
                                                cudaStream_t st);
 NF_DECLARE_SPATIAL(8, 8)
@@ -22,6 +22,12 @@ NF_DECLARE_SPATIAL(48, 48)
 NF_DECLARE_SPATIAL(0, 0)
 #undef NF_DECLARE_SPATIAL
 struct KalmanArgs;
+struct AdjointShape;
+struct AdjointBatch;
+cudaError_t launch_adjoint_16x16(const DevPlan& d, const AdjointShape& S, const AdjointBatch& b, size_t smem,
+                                 cudaStream_t st);
+cudaError_t launch_adjoint_0x0(const DevPlan& d, const AdjointShape& S, const AdjointBatch& b, size_t smem,
+                               cudaStream_t st);
 struct VolumeShape;
 struct VolumeSources;
 #define NF_DECLARE_VOLUME(BH, BW)                                                                               \

@@ -7,6 +7,8 @@
 #include "tile_volume.cuh"
 #include "launch.hpp"
 #include "kalman.cuh"
+#define NF_ADJOINT_AUX_KERNELS
+#include "adjoint.cuh"
 
 #include <cuda_runtime.h>
 
@@ -137,6 +139,14 @@ void temporal_twiddles(int T, int c, std::vector<cf>& fwd, std::vector<cf>& inv)
   }
 }
 
+// DFTTest plans always carry a device primary table so it can be replaced
+// (nf_plan_set_primary); without sigma curves it holds the uniform value a, which
+// gives the same per-bin arithmetic as the uniform path.
+std::vector<float> primary_table(const nfb::PlanTables& t) {
+  if (t.algo != nfb::Algo::DFTTest || !t.spectral.primary.empty()) return t.spectral.primary;
+  return std::vector<float>(size_t(t.temporal_size) * size_t(t.bins), t.spectral.a);
+}
+
 nf_status finalize_plan(std::unique_ptr<nf_plan>& p, char* err, size_t len) {
   const nfb::PlanTables& t = p->t;
   cudaError_t e = cudaGetDevice(&p->device);
@@ -147,7 +157,7 @@ nf_status finalize_plan(std::unique_ptr<nf_plan>& p, char* err, size_t len) {
   temporal_twiddles(std::max(1, t.temporal_size), t.temporal_size / 2, tfwd, tinv);
   const size_t o_wxa = blob.add(t.wx.analysis), o_wya = blob.add(t.wy.analysis), o_wxs = blob.add(t.wx.synthesis),
                o_wys = blob.add(t.wy.synthesis), o_h = blob.add(t.h), o_hs = blob.add(t.h_synthesis),
-               o_grid = blob.add(t.grid), o_prim = blob.add(t.spectral.primary),
+               o_grid = blob.add(t.grid), o_prim = blob.add(primary_table(t)),
                o_sw = blob.add(t.enhancement.sharpen_window), o_hw = blob.add(t.enhancement.halo_window),
                o_twh = blob.add(twh), o_tww = blob.add(tww), o_twt = blob.add(twt), o_tf = blob.add(tfwd),
                o_ti = blob.add(tinv);
@@ -310,7 +320,7 @@ nfd::StripShape pick_strip(const nfd::DevPlan& d, int target_ctas) {
 int plain_ctas(const nfd::DevPlan& d) { return (d.bh * d.bw <= 256 ? 2 : 1) * 148; }
 
 cudaError_t launch_spatial_shape(const nfd::DevPlan& d, const nfd::StripShape& S, dim3 grid, size_t smem,
-                                 const nfd::PlaneJob& job, cudaStream_t st) {
+                                 const nfd::PlaneJobs& job, cudaStream_t st) {
   if (d.bh == d.bw) {
     switch (d.bw) {
       case 8: return nfd::launch_spatial_8x8(d, S, grid, smem, job, st);
@@ -324,14 +334,22 @@ cudaError_t launch_spatial_shape(const nfd::DevPlan& d, const nfd::StripShape& S
   return nfd::launch_spatial_0x0(d, S, grid, smem, job, st);
 }
 
+// One launch over J.n planes of one plan; the strip shape aims the whole grid at one
+// wave of resident CTAs.
+cudaError_t run_spatial_planes(const nfd::DevPlan& d, const nfd::PlaneJobs& J, cudaStream_t st) {
+  const nfd::StripShape S = pick_strip(d, std::max(1, plain_ctas(d) / J.n));
+  const size_t smem = nfd::strip_smem_bytes(d.bh, d.bw, S);
+  const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th, J.n);
+  return launch_spatial_shape(d, S, grid, smem, J, st);
+}
+
 cudaError_t run_spatial(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, void* dst, ptrdiff_t ds, const cf* L,
                         cudaStream_t st) {
-  const nfd::StripShape S = pick_strip(d, plain_ctas(d));
-  const size_t smem = nfd::strip_smem_bytes(d.bh, d.bw, S);
-  const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th);
-  const nfd::PlaneJob job{static_cast<const unsigned char*>(src), (long long)ss, static_cast<unsigned char*>(dst),
-                          (long long)ds, L, 0};
-  return launch_spatial_shape(d, S, grid, smem, job, st);
+  nfd::PlaneJobs J{};
+  J.n = 1;
+  J.job[0] = {static_cast<const unsigned char*>(src), (long long)ss, static_cast<unsigned char*>(dst), (long long)ds,
+              L, 0};
+  return run_spatial_planes(d, J, st);
 }
 
 cudaError_t run_volume(const nfd::DevPlan& d, const nfd::VolumeSources& v, void* dst, ptrdiff_t ds, cudaStream_t st) {
@@ -514,6 +532,27 @@ nf_status nf_plan_process_device(const nf_plan* p, const nf_const_plane* sources
     nfb::require(p != nullptr, "null plan");
     return process_device(*p, sources, nsources, targets, ntargets, dst, frame, plane,
                           static_cast<cudaStream_t>(stream), err, err_len);
+  });
+}
+
+nf_status nf_plan_process_planes_device(const nf_plan* p, const nf_const_plane* sources, const nf_plane* dsts,
+                                        int nplanes, void* stream, char* err, size_t err_len) {
+  return guarded(err, err_len, [&]() -> nf_status {
+    nfb::require(p && sources && dsts, "null argument");
+    nfb::require(nplanes > 0 && nplanes <= nfd::kMaxPlaneJobs, "multi-plane calls take 1..32 planes");
+    nfb::require(!(p->t.algo == nfb::Algo::FFT3D && p->t.kalman), "Kalman plans render through nf_kalman_render_device");
+    nfb::require(p->t.temporal_size == 1 && !p->t.temporal_ola,
+                 "multi-plane calls take single-frame plans (FFT3D bt=1, DFTTest tbsize=1)");
+    nfd::PlaneJobs J{};
+    J.n = nplanes;
+    for (int i = 0; i < nplanes; ++i) {
+      validate_call(*p, &sources[i], 1, nullptr, 0, dsts[i]);
+      J.job[i] = {static_cast<const unsigned char*>(sources[i].data), (long long)sources[i].stride_bytes,
+                  static_cast<unsigned char*>(dsts[i].data), (long long)dsts[i].stride_bytes, nullptr, 0};
+    }
+    const cudaError_t e = run_spatial_planes(p->dev, J, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(err, err_len, e, "kernel launch failed");
+    return NF_OK;
   });
 }
 
@@ -879,6 +918,113 @@ nf_status nf_batch_graph_launch(nf_batch* b, void* stream, char* err, size_t len
 }
 
 void nf_batch_destroy(nf_batch* b) { delete b; }
+
+nf_status nf_plan_set_primary(nf_plan* p, const float* table, int count, void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && table, "null plan or table");
+    nfb::require(p->t.algo == nfb::Algo::DFTTest, "primary tables are replaceable on DFTTest plans only");
+    nfb::require(count == p->t.temporal_size * p->t.bins, "primary table shape mismatch");
+    const cudaError_t e = cudaMemcpyAsync(const_cast<float*>(p->dev.filt.primary), table, size_t(count) * sizeof(float),
+                                          cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "table copy failed");
+    return NF_OK;
+  });
+}
+
+nf_status nf_plan_get_primary(const nf_plan* p, float* table, int count, void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && table, "null plan or table");
+    nfb::require(p->t.algo == nfb::Algo::DFTTest, "primary tables are replaceable on DFTTest plans only");
+    nfb::require(count == p->t.temporal_size * p->t.bins, "primary table shape mismatch");
+    const cudaError_t e = cudaMemcpyAsync(table, p->dev.filt.primary, size_t(count) * sizeof(float),
+                                          cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "table copy failed");
+    return NF_OK;
+  });
+}
+
+namespace {
+void check_adjoint_plan(const nf_plan& p) {
+  const auto& t = p.t;
+  nfb::require(t.algo == nfb::Algo::DFTTest && t.temporal_size == 1 && !t.center && t.format.floating &&
+                   (t.spectral.type >= 0 && t.spectral.type <= 2),
+               "backward requires a float DFTTest plan with tbsize=1, smode=1 and ftype 0, 1 or 2");
+}
+nfd::AdjointShape adjoint_shape(const nfd::DevPlan& d) {
+  nfd::AdjointShape S{};
+  S.tab_floats = 2 * d.bh * d.bw + (d.grid ? 2 * d.bins : 0) + d.bins;
+  S.tab_floats = (S.tab_floats + 3) & ~3;
+  S.tw = std::min(d.gx.cover, std::max(d.gx.step, 64 / d.gx.step * d.gx.step));
+  S.th = std::min(d.gy.cover, std::max(2 * d.bh, 64));
+  S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
+  S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
+  int q = (S.win_max + 3) / 4;
+  if (q % 2 == 0) ++q;
+  S.ring_pitch = 4 * q;
+  S.tiles_x = (d.gx.cover + S.tw - 1) / S.tw;
+  S.tiles_y = (d.gy.cover + S.th - 1) / S.th;
+  return S;
+}
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+} // namespace
+
+nf_status nf_dft_backward_scratch_bytes(const nf_plan* p, int nplanes, size_t* bytes) {
+  if (!p || !bytes || nplanes < 0) return NF_INVALID_ARGUMENT;
+  const nfd::AdjointShape S = adjoint_shape(p->dev);
+  const size_t tiles = size_t(S.tiles_x) * S.tiles_y;
+  *bytes = size_t(nplanes) * align256(size_t(p->t.gx.cover) * p->t.gy.cover * 4) +
+           align256(size_t(nplanes) * tiles * p->t.bins * 4);
+  return NF_OK;
+}
+
+nf_status nf_dft_backward_device(const nf_plan* p, const nf_const_plane* sources, const nf_const_plane* grad_out,
+                                 const nf_plane* grad_src, int nplanes, float* grad_primary, void* scratch,
+                                 size_t scratch_bytes, void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && sources && grad_out && grad_src && grad_primary, "null argument");
+    check_adjoint_plan(*p);
+    nfb::require(nplanes > 0 && nplanes <= nfd::kAdjointMaxPlanes, "backward takes 1..32 planes per call");
+    size_t need = 0;
+    nf_dft_backward_scratch_bytes(p, nplanes, &need);
+    nfb::require(scratch && scratch_bytes >= need, "backward scratch too small");
+    for (int i = 0; i < nplanes; ++i) {
+      nf_plane gs = grad_src[i];
+      validate_call(*p, &sources[i], 1, nullptr, 0, gs);
+      nfb::require(grad_out[i].width == p->t.gx.length && grad_out[i].height == p->t.gy.length,
+                   "frame dimensions differ from plan");
+      plane_extent(grad_out[i].width, grad_out[i].height, grad_out[i].stride_bytes, 4);
+      check_pointer(grad_out[i].data, 4);
+    }
+    const nfd::DevPlan& d = p->dev;
+    const nfd::AdjointShape S = adjoint_shape(d);
+    const size_t tiles = size_t(S.tiles_x) * S.tiles_y;
+    const size_t cov = align256(size_t(p->t.gx.cover) * p->t.gy.cover * 4), part = tiles * p->t.bins * 4;
+    auto* base = static_cast<unsigned char*>(scratch);
+    nfd::AdjointBatch B{};
+    B.n = nplanes;
+    for (int i = 0; i < nplanes; ++i) {
+      B.job[i] = {static_cast<const float*>(sources[i].data), (long long)sources[i].stride_bytes,
+                  static_cast<const float*>(grad_out[i].data), (long long)grad_out[i].stride_bytes,
+                  reinterpret_cast<float*>(base + size_t(i) * cov),
+                  reinterpret_cast<float*>(base + size_t(nplanes) * cov + size_t(i) * part)};
+      B.gsrc[i] = static_cast<float*>(grad_src[i].data);
+      B.gsrc_stride[i] = grad_src[i].stride_bytes;
+    }
+    const size_t smem = nfd::adjoint_smem_bytes(d.bh, d.bw, S);
+    nfb::require(smem <= 227 * 1024, "block size too large for the backward tile");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = (d.bh == 16 && d.bw == 16) ? nfd::launch_adjoint_16x16(d, S, B, smem, st)
+                                                : nfd::launch_adjoint_0x0(d, S, B, smem, st);
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+    const dim3 fb(32, 8), fg((p->t.gx.length + 31) / 32, (p->t.gy.length + 7) / 8, nplanes);
+    nfd::dft_adjoint_fold_kernel<<<fg, fb, 0, st>>>(d, B);
+    // partials of all planes are contiguous: tiles*nplanes rows of `bins`
+    nfd::dft_adjoint_reduce_kernel<<<(p->t.bins + 127) / 128, 128, 0, st>>>(
+        reinterpret_cast<const float*>(base + size_t(nplanes) * cov), int(tiles) * nplanes, p->t.bins, grad_primary);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+    return NF_OK;
+  });
+}
 
 nf_status nf_kernel_info(char* fft_backend, size_t fb_len, char* target, size_t t_len, char* fft, size_t f_len,
                          int* lanes) {

@@ -17,7 +17,7 @@ cudaError_t prepare(K k, size_t smem) {
   return e;
 }
 template <int ST>
-cudaError_t launch_one(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem, const PlaneJob& job,
+cudaError_t launch_one(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem, const PlaneJobs& job,
                        cudaStream_t st) {
   auto k = spatial_strip_kernel<NF_BH, NF_BW, ST>;
   cudaError_t e = prepare(k, smem);
@@ -47,7 +47,7 @@ cudaError_t launch_kalman_one(const DevPlan& d, int nb, dim3 grid, size_t smem, 
 #define NF_DEFINE(BH, BW) NF_DEFINE_(BH, BW)
 #define NF_DEFINE_(BH, BW)                                                                                        \
   cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem,          \
-                                         const PlaneJob& job, cudaStream_t st) {                                 \
+                                         const PlaneJobs& job, cudaStream_t st) {                                \
     if (d.storage == kStoreU8) return launch_one<kStoreU8>(d, S, grid, smem, job, st);                          \
     if (d.storage == kStoreU16) return launch_one<kStoreU16>(d, S, grid, smem, job, st);                        \
     return launch_one<kStoreF32>(d, S, grid, smem, job, st);                                                     \

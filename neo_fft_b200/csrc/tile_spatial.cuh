@@ -349,11 +349,19 @@ struct StripOccupancy {
   static constexpr int value = (BHC > 0 && BHC * BWC <= 256) ? 2 : 1;
 };
 
-// Plain launch: grid (strips, segments) over one plane.
+// Plain launch: grid (strips, segments, planes) over up to kMaxPlaneJobs planes of
+// one plan (one plane for the drop-in call; several for multi-plane calls).
+constexpr int kMaxPlaneJobs = 32;
+struct PlaneJobs {
+  PlaneJob job[kMaxPlaneJobs];
+  int n;
+};
+
 template <int BHC, int BWC, int STORAGE>
-__global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_strip_kernel(DevPlan P, StripShape S, PlaneJob J) {
+__global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value)
+    spatial_strip_kernel(DevPlan P, StripShape S, const __grid_constant__ PlaneJobs J) {
   extern __shared__ float smem[];
-  strip_tile<BHC, BWC, STORAGE>(P, J, S, blockIdx.x * S.tw, blockIdx.y * S.th, smem);
+  strip_tile<BHC, BWC, STORAGE>(P, J.job[blockIdx.z], S, blockIdx.x * S.tw, blockIdx.y * S.th, smem);
 }
 
 // Batched launch: a persistent grid pulls (plane, strip, segment) work items from

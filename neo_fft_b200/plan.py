@@ -238,6 +238,22 @@ class Plan:
         C.raise_for(st, err.value)
         return dst
 
+    def process_planes(self, sources, dsts, stream=None):
+        """Several single-frame planes (device tensors) in one launch per 32 planes;
+        equal to process_at per plane."""
+        import torch
+        if len(sources) != len(dsts):
+            raise ValueError("sources and dsts differ in length")
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        for start in range(0, len(sources), 32):
+            chunk = range(start, min(start + 32, len(sources)))
+            srcs = (C.NfConstPlane * len(chunk))(*[_plane(sources[i], True) for i in chunk])
+            ds = (C.NfPlane * len(chunk))(*[_plane(dsts[i], False) for i in chunk])
+            C.raise_for(self._lib.nf_plan_process_planes_device(self._h, srcs, ds, len(chunk), ctypes.c_void_p(s),
+                                                                err, 512), err.value)
+        return dsts
+
     def process(self, sources, dst=None):
         """Plan::process (plan.hpp:58-75); allocates dst like the first source when omitted."""
         if dst is None:

@@ -1,0 +1,106 @@
+"""Test infrastructure (oracle only): a binary64, differentiable PyTorch restatement of
+the reference DFTTest spatial path (tbsize 1, smode 1, float planes, ftype 0/1/2), used
+as the gradient oracle for the sm_100a adjoint kernels. Never used by the product.
+
+Steps, each following the reference core:
+  * decode and reflect-pad: padded = 255 * src[reflect(y - offset_y), reflect(x - offset_x)]
+    over cover_h x cover_w (src/algorithms/pad.hpp:41-45 and :65-80);
+  * per block at (by*step, bx*step): analysis window h (src/algorithms/windows.cpp, taken from
+    the reference's own dft_window_3d), forward r2c (unnormalised), spectrum layout
+    [row][bin] with bin = 0..sbsize/2 (src/algorithms/plan.cpp:563-570);
+  * zmean: scale = spectrum[0].re / grid[0].re with grid = r2c(255 * h) (plan.cpp:213-224, :575);
+  * spectral gain per bin k with threshold a = table[k] (src/kernels/scalar/spectral.cpp:7-52):
+    ftype 0: max((p - a) / (p + 1e-15), 0); ftype 1: p < a ? 0 : 1; ftype 2: a,
+    applied to the mean-removed bin and the mean added back;
+  * normalised c2r, times h * sbsize^2 (h_synthesis, plan.cpp:616-617), summed into the
+    accumulator (scatter_dfttest, plan.cpp:596-598);
+  * output = accum[offset_y + y][offset_x + x] / 255 (plan.cpp:604-609).
+
+Parity of this restatement is pinned by `forward` agreeing with the reference plan's own
+float32 output (tests/test_gpu_adjoint.py checks it on each configuration it uses).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+
+def reference_tables(config):
+    """(h [b, b] float32, wscale) from the reference's own window builder."""
+    from . import ref
+    b = config.block
+    h = np.zeros(b * b, np.float32)
+    w1 = np.zeros(1, np.float32)
+    err = ctypes.create_string_buffer(256)
+    rc = ref.load().ref_dft_window_3d(1, b, config.overlap, 1, config.swin, config.twin, config.sbeta,
+                                      config.tbeta, config.temporal_mode, config.temporal_overlap,
+                                      ref.fp(h), ref.fp(w1), err, 256)
+    if rc:
+        raise ValueError(err.value.decode())
+    return h.reshape(b, b), float(w1[0])
+
+
+def _reflect_index(length: int, offset: int, cover: int):
+    j = np.arange(cover) - offset
+    j = np.where(j < 0, -j, np.where(j < length, j, 2 * length - 2 - j))
+    return j
+
+
+class DFTTestFP64:
+    """forward(x [B, H, W] float64 tensor, table [b*(b/2+1)] float64 tensor) -> [B, H, W]."""
+
+    def __init__(self, width: int, height: int, config):
+        from . import ref
+        from neo_fft_b200.plan import SampleFormat
+        if config.tbsize != 1 or config.mode != 1 or config.ftype not in (0, 1, 2):
+            raise ValueError("restatement covers tbsize 1, smode 1, ftype 0..2")
+        rp = ref.RefPlan(width, height, SampleFormat(32, True), config)
+        self.gx, self.gy = rp.x, rp.y
+        self.width, self.height, self.config = width, height, config
+        self.h, self.wscale = reference_tables(config)
+        self.iy = _reflect_index(height, self.gy["offset"], self.gy["cover"])
+        self.ix = _reflect_index(width, self.gx["offset"], self.gx["cover"])
+
+    def forward(self, x, table):
+        import torch
+        import torch.nn.functional as F
+        b = self.config.block
+        step = b - self.config.overlap
+        dev = x.device
+        h = torch.from_numpy(self.h.astype(np.float64)).to(dev)
+        iy = torch.from_numpy(self.iy).to(dev)
+        ix = torch.from_numpy(self.ix).to(dev)
+        padded = 255.0 * x[:, iy][:, :, ix]                           # [B, Ch, Cw]
+        B, ch, cw = padded.shape
+        ny, nx = self.gy["count"], self.gx["count"]
+        blocks = padded.unfold(1, b, step).unfold(2, b, step)       # [B, ny, nx, b, b]
+        blocks = blocks[:, :ny, :nx] * h
+        spec = torch.fft.rfft2(blocks)                              # [B, ny, nx, b, b/2+1]
+        a = table.reshape(b, b // 2 + 1)
+        if self.config.zmean:
+            grid = torch.fft.rfft2(255.0 * h)
+            mean = (spec[..., 0, 0].real / grid[0, 0].real)[..., None, None] * grid
+        else:
+            mean = torch.zeros_like(spec)
+        re = spec - mean
+        power = re.real ** 2 + re.imag ** 2
+        if self.config.ftype == 0:
+            gain = torch.clamp((power - a) / (power + 1e-15), min=0.0)
+        elif self.config.ftype == 1:
+            gain = (power >= a).to(power.dtype)
+        else:
+            gain = a.expand_as(power)
+        filtered = gain * re + mean
+        out_blocks = torch.fft.irfft2(filtered, s=(b, b)) * (h * float(b * b))
+        cols = out_blocks.permute(0, 3, 4, 1, 2).reshape(B, b * b, ny * nx)
+        acc = F.fold(cols, output_size=(ch, cw), kernel_size=b, stride=step)[:, 0]
+        oy, ox = self.gy["offset"], self.gx["offset"]
+        return acc[:, oy:oy + self.height, ox:ox + self.width] / 255.0
+
+    def uniform_table(self):
+        """The table a DFTTest plan without curves uses: sigma / wscale for ftype 0/1, sigma for 2."""
+        c = self.config
+        b = c.block
+        v = np.float32(c.sigma) / np.float32(self.wscale) if c.ftype < 2 else np.float32(c.sigma)
+        return np.full(b * (b // 2 + 1), v, np.float32)

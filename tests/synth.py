@@ -47,3 +47,24 @@ def plane(h, w, bits=8, floating=False, seed=(0, 0, 0), kind="texture"):
     else:
         base = textured(h, w, seed, 0.06 * peak, 0.92 * peak)
     return to_format(base, bits, False, 0.02 * peak, (*seed, 1))
+
+
+def noisy_patches(n: int, size: int, seed):
+    """Differentiable-training workload: clean = band-limited texture in [0, 1]; noisy =
+    clean + coloured Gaussian noise whose amplitude spectrum follows a seeded random radial
+    curve, with the noise sd drawn from U[0.01, 0.05] per patch. Returns (noisy, clean),
+    float32 [n, size, size]."""
+    rng = np.random.default_rng(seed)
+    clean = np.stack([textured(size, size, (*np.atleast_1d(seed), 100, i), 0.0, 1.0) for i in range(n)])
+    fy = np.fft.fftfreq(size)[:, None]
+    fx = np.fft.rfftfreq(size)[None, :]
+    r = np.sqrt(fx * fx + fy * fy) / np.sqrt(0.5)
+    noisy = np.empty_like(clean)
+    for i in range(n):
+        knots = rng.uniform(0.2, 1.0, 6)
+        curve = np.interp(r, np.linspace(0, 1, 6), knots)
+        spec = np.fft.rfft2(rng.standard_normal((size, size))) * curve
+        noise = np.fft.irfft2(spec, s=(size, size))
+        noise *= rng.uniform(0.01, 0.05) / max(noise.std(), 1e-12)
+        noisy[i] = clean[i] + noise
+    return noisy.astype(np.float32), clean.astype(np.float32)

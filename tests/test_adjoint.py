@@ -1,0 +1,224 @@
+"""Differentiable DFTTest (tbsize 1, float planes, ftype 0/1/2).
+
+CPU: the binary64 restatement (oracle/dft_fp64.py) is pinned to the reference core's own
+float32 output, and its autograd gradient to central finite differences.
+GPU: the sm_100a forward (through the autograd function) equals `Plan.process` bit for bit,
+and the adjoint kernels (nf_dft_backward_device) match the binary64 autograd gradient.
+
+Tolerances: forward with the plan's own table is bit-exact; gradients are compared with the
+binary64 gradient by relative L2 error <= 2e-5 and max error <= 1e-4 of the largest
+component (binary32 accumulation over ~sbsize^2 / step^2 overlapping blocks).
+"""
+import numpy as np
+import pytest
+
+from neo_fft_b200.plan import DFTConfig, SampleFormat
+from tests.synth import plane
+
+CONFIGS = [
+    DFTConfig(block=16, overlap=8, ftype=0, sigma=20.0),
+    DFTConfig(block=16, overlap=12, ftype=0, sigma=12.0, zmean=0),
+    DFTConfig(block=16, overlap=8, ftype=2, sigma=0.8),
+    DFTConfig(block=16, overlap=8, ftype=1, sigma=30.0),
+    DFTConfig(block=12, overlap=6, ftype=0, sigma=20.0),
+    DFTConfig(block=8, overlap=4, ftype=0, sigma=20.0, swin=1),
+]
+IDS = ["b16o8w", "b16o12nz", "b16o8gain", "b16o8hard", "b12o6", "b8o4hamming"]
+GRAD_L2 = 2e-5
+GRAD_MAX = 1e-4
+
+
+def perturbed_table(o, seed):
+    rng = np.random.default_rng(seed)
+    return (o.uniform_table().astype(np.float64) * rng.uniform(0.6, 1.4, o.uniform_table().size)).astype(np.float32)
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=IDS)
+def test_fp64_restatement_matches_reference(ref, cfg):
+    import torch
+    from oracle.dft_fp64 import DFTTestFP64
+    w, h = 150, 98
+    x = plane(h, w, 32, True, seed=(31, 0, 0))
+    o = DFTTestFP64(w, h, cfg)
+    exp = ref.RefPlan(w, h, SampleFormat(32, True), cfg).process(x)
+    got = o.forward(torch.from_numpy(x).double()[None], torch.from_numpy(o.uniform_table()).double())[0].numpy()
+    assert np.abs(got - exp).max() <= 1e-6
+
+
+def central_difference(f, x, idx, h):
+    """(f(x + h e_idx) - f(x - h e_idx)) / 2h in binary64."""
+    import torch
+    d = torch.zeros_like(x)
+    d[idx] = h
+    with torch.no_grad():
+        return float((f(x + d) - f(x - d)) / (2 * h))
+
+
+class FDCheck:
+    """Central differences at h and h/4. Where the two disagree by more than the
+    tolerance, the interval straddles a kink of the gain (the Wiener clamp at power = a),
+    the function is not differentiable there at that step, and the coordinate is
+    counted as skipped; every other coordinate must match the gradient."""
+
+    def __init__(self, tol):
+        self.tol, self.skipped, self.checked = tol, 0, 0
+
+    def __call__(self, f, x, idx, h, grad):
+        fd = central_difference(f, x, idx, h)
+        if abs(fd - grad) <= self.tol:
+            self.checked += 1
+            return
+        fd4 = central_difference(f, x, idx, h / 4)
+        if abs(fd - fd4) > self.tol:
+            self.skipped += 1
+            return
+        raise AssertionError(f"coordinate {idx}: central difference {fd:.9g}, gradient {grad:.9g}")
+
+
+@pytest.mark.parametrize("cfg", [CONFIGS[0], CONFIGS[2], CONFIGS[4]], ids=["wiener", "gain", "b12"])
+def test_fp64_gradient_matches_finite_differences(ref, cfg):
+    """Binary64 autograd of the restatement against central differences (h = 1e-6) on
+    64 random coordinates (48 pixels, 16 table entries); agreement <= 1e-6 relative to the
+    largest gradient component."""
+    import torch
+    from oracle.dft_fp64 import DFTTestFP64
+    w, h = 44, 40
+    o = DFTTestFP64(w, h, cfg)
+    x = torch.from_numpy(plane(h, w, 32, True, seed=(32, 0, 0))).double()[None].requires_grad_()
+    t = torch.from_numpy(perturbed_table(o, 3)).double().requires_grad_()
+    g = torch.from_numpy(np.random.default_rng(4).standard_normal((1, h, w)))
+    (o.forward(x, t) * g).sum().backward()
+    rng = np.random.default_rng(5)
+    xs, ts = x.detach(), t.detach()
+    px, tb = FDCheck(1e-6 * float(x.grad.abs().max())), FDCheck(1e-6 * max(float(t.grad.abs().max()), 1e-12))
+    for _ in range(48):
+        idx = (0, int(rng.integers(h)), int(rng.integers(w)))
+        px(lambda v: (o.forward(v, ts) * g).sum(), xs, idx, 1e-6, float(x.grad[idx]))
+    for _ in range(16):
+        k = int(rng.integers(t.numel()))
+        tb(lambda v: (o.forward(xs, v) * g).sum(), ts, k, 1e-6 * max(1.0, float(ts[k])), float(t.grad[k]))
+    assert px.skipped + tb.skipped <= 2, (px.skipped, tb.skipped)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    scale = max(np.abs(b).max(), 1e-30)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30), np.abs(a - b).max() / scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg", CONFIGS, ids=IDS)
+def test_forward_matches_plan_process(cuda, cfg):
+    import torch
+    from neo_fft_b200.autograd import SigmaTableDenoiser
+    from neo_fft_b200.plan import Plan
+    w, h = 150, 98
+    xs = np.stack([plane(h, w, 32, True, seed=(33, 0, f)) for f in range(3)])
+    m = SigmaTableDenoiser(w, h, cfg)
+    out = m(torch.from_numpy(xs).cuda()).detach().cpu().numpy()
+    p = Plan(w, h, SampleFormat(32, True), cfg)
+    for f in range(3):
+        assert np.array_equal(out[f], p.process(xs[f]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg", CONFIGS, ids=IDS)
+def test_gradients_match_fp64_autograd(cuda, ref, cfg):
+    import torch
+    from neo_fft_b200.autograd import SigmaTableDenoiser
+    from oracle.dft_fp64 import DFTTestFP64
+    w, h, n = 150, 98, 3
+    o = DFTTestFP64(w, h, cfg)
+    tab = perturbed_table(o, 6)
+    xs = np.stack([plane(h, w, 32, True, seed=(34, 0, f)) for f in range(n)])
+    g = np.random.default_rng(7).standard_normal((n, h, w)).astype(np.float32)
+
+    m = SigmaTableDenoiser(w, h, cfg, initial=torch.from_numpy(tab))
+    x = torch.from_numpy(xs).cuda().requires_grad_()
+    y = m(x)
+    (y * torch.from_numpy(g).cuda()).sum().backward()
+
+    xd = torch.from_numpy(xs).double().requires_grad_()
+    td = torch.from_numpy(tab).double().requires_grad_()
+    yd = o.forward(xd, td)
+    (yd * torch.from_numpy(g).double()).sum().backward()
+
+    assert np.abs(y.detach().cpu().numpy() - yd.detach().numpy()).max() <= 2e-5
+    l2, mx = _rel(x.grad.cpu().numpy(), xd.grad.numpy())
+    assert l2 <= GRAD_L2 and mx <= GRAD_MAX, (l2, mx)
+    if cfg.ftype == 1:
+        assert not m.table.grad.abs().any()
+    else:
+        l2, mx = _rel(m.table.grad.cpu().numpy(), td.grad.numpy())
+        assert l2 <= GRAD_L2 and mx <= GRAD_MAX, (l2, mx)
+
+
+@pytest.mark.gpu
+def test_backward_is_deterministic_and_chunks_past_32_planes(cuda):
+    import torch
+    from neo_fft_b200.autograd import SigmaTableDenoiser
+    cfg = CONFIGS[0]
+    w, h, n = 64, 48, 35
+    m = SigmaTableDenoiser(w, h, cfg)
+    xs = torch.from_numpy(np.stack([plane(h, w, 32, True, seed=(35, 0, f)) for f in range(n)])).cuda()
+    g = torch.from_numpy(np.random.default_rng(8).standard_normal((n, h, w)).astype(np.float32)).cuda()
+    grads = []
+    for _ in range(2):
+        m.table.grad = None
+        x = xs.clone().requires_grad_()
+        (m(x) * g).sum().backward()
+        grads.append((x.grad.clone(), m.table.grad.clone()))
+    assert torch.equal(grads[0][0], grads[1][0]) and torch.equal(grads[0][1], grads[1][1])
+    # pixel gradients do not depend on the other planes of the call
+    x1 = xs[:1].clone().requires_grad_()
+    m.table.grad = None
+    (m(x1) * g[:1]).sum().backward()
+    assert torch.equal(x1.grad[0], grads[0][0][0])
+
+
+@pytest.mark.gpu
+def test_backward_rejects_unsupported_plans(cuda):
+    import torch
+    from neo_fft_b200.autograd import DFTTestFunction
+    from neo_fft_b200.plan import Plan
+    p = Plan(64, 48, SampleFormat(32, True), DFTConfig(block=16, overlap=8, ftype=3, sigma=2.0))
+    x = torch.zeros((1, 48, 64), device="cuda", requires_grad=True)
+    t = torch.ones(16 * 9, device="cuda", requires_grad=True)
+    y = DFTTestFunction.apply(x, t, p)
+    with pytest.raises(ValueError, match="backward requires a float DFTTest plan"):
+        y.sum().backward()
+
+
+@pytest.mark.gpu
+def test_training_workload_gradients_match_fp64_finite_differences(cuda, ref):
+    """16 float32 256x256 noisy patches, sbsize 16 / sosize 8, learnable 16x9 table, ftype 0,
+    loss = mean squared error to the clean patches: the GPU gradient agrees with binary64
+    central differences (h = 1e-4) of the restatement on 64 random coordinates (48 pixels,
+    16 table entries) within 1e-4 of the largest gradient component."""
+    import torch
+    from neo_fft_b200.autograd import SigmaTableDenoiser
+    from oracle.dft_fp64 import DFTTestFP64
+    from tests.synth import noisy_patches
+    n, s = 16, 256
+    cfg = DFTConfig(block=16, overlap=8, ftype=0, sigma=4.0)
+    noisy, clean = noisy_patches(n, s, 41)
+    m = SigmaTableDenoiser(s, s, cfg)
+    x = torch.from_numpy(noisy).cuda().requires_grad_()
+    cl = torch.from_numpy(clean).cuda()
+    ((m(x) - cl) ** 2).mean().backward()
+    gx, gt = x.grad.cpu().double(), m.table.grad.cpu().double()
+    tab = m.table.detach().cpu().double()
+
+    o = DFTTestFP64(s, s, cfg)
+    xd, cd = torch.from_numpy(noisy).double(), torch.from_numpy(clean).double()
+    rng = np.random.default_rng(42)
+    px, tb = FDCheck(1e-4 * float(gx.abs().max())), FDCheck(1e-4 * float(gt.abs().max()))
+    for _ in range(48):
+        i, yy, xx = int(rng.integers(n)), int(rng.integers(s)), int(rng.integers(s))
+        # one pixel only moves its own patch: difference the loss of that patch
+        px(lambda v: ((o.forward(v, tab) - cd[i:i + 1]) ** 2).sum() / cd.numel(), xd[i:i + 1], (0, yy, xx), 1e-4,
+           float(gx[i, yy, xx]))
+    for _ in range(16):
+        k = int(rng.integers(tab.numel()))
+        tb(lambda v: ((o.forward(xd, v) - cd) ** 2).mean(), tab, k, 1e-4, float(gt[k]))
+    assert px.skipped + tb.skipped <= 6, (px.skipped, tb.skipped)

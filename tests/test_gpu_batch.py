@@ -47,3 +47,38 @@ def test_batch_rejects_multi_frame_plans(cuda):
     s = cuda.zeros((48, 64), dtype=cuda.uint8, device="cuda")
     with pytest.raises(ValueError, match="batch items must be single-frame plans"):
         Batch([(p, s, cuda.empty_like(s))])
+
+
+@pytest.mark.parametrize("fmt,cfg,size", [
+    (SampleFormat(32, True), DFTConfig(block=16, overlap=8, ftype=0, sigma=4.0), (256, 256)),
+    (SampleFormat(16), DFTConfig(block=16, overlap=12, ftype=0, sigma=8.0, slocation=[0, 8, 1, 8]), (320, 180)),
+    (SampleFormat(8), FFT3DConfig(bw=32, bh=32, ow=16, oh=16, sigma=2.0, sharpen=0.3), (200, 120)),
+    (SampleFormat(10), DFTConfig(block=12, overlap=9, ftype=1, sigma=6.0), (150, 98)),
+], ids=["f32-dft16", "u16-dft16", "u8-fft3d32", "u10-dft12"])
+def test_multi_plane_launch_equals_per_plane(cuda, fmt, cfg, size):
+    """nf_plan_process_planes_device over 35 planes (two launches: 32 + 3), some of them
+    strided views, equals one nf_plan_process_device call per plane bit for bit."""
+    w, h = size
+    p = Plan(w, h, fmt, cfg)
+    srcs = []
+    for i in range(35):
+        a = cuda.from_numpy(plane(h, w, fmt.bits, fmt.floating, seed=(9, 0, i))).cuda()
+        if i % 4 == 1:  # padded rows: stride larger than the width
+            big = cuda.zeros((h, w + 24), dtype=a.dtype, device=a.device)
+            big[:, :w] = a
+            a = big[:, :w]
+        srcs.append(a)
+    outs = [cuda.empty((h, w), dtype=s.dtype, device=s.device) for s in srcs]
+    p.process_planes(srcs, outs)
+    for s, o in zip(srcs, outs):
+        r = cuda.empty_like(o)
+        p.process_at([s], r)
+        assert cuda.equal(o, r)
+    p.sync_status()
+
+
+def test_multi_plane_launch_rejects_temporal_plans(cuda):
+    p = Plan(64, 48, SampleFormat(8), FFT3DConfig(bw=16, bh=16, bt=3))
+    a = cuda.zeros((48, 64), dtype=cuda.uint8, device="cuda")
+    with pytest.raises(ValueError, match="single-frame plans"):
+        p.process_planes([a], [cuda.empty_like(a)])

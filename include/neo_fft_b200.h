@@ -199,6 +199,22 @@ nf_status nf_dft_backward_device(const nf_plan* plan, const nf_const_plane* sour
                                  const nf_plane* grad_sources, int nplanes, float* grad_primary, void* scratch,
                                  size_t scratch_bytes, void* stream, char* err, size_t err_len);
 
+/* Allocation-free backward: nf_dft_backward_device with its scratch in a fixed
+ * 16 MiB device buffer inside the library (one per device) instead of a caller
+ * buffer. No counterpart in the reference (it has no gradients). For hosts that
+ * must not allocate device memory per call: a plain C host has no caching
+ * allocator to borrow from, and cudaMalloc/cudaFree synchronise the device, which
+ * stalls every other stream such a host keeps busy. Calls whose scratch need
+ * (nf_dft_backward_scratch_bytes) exceeds nf_dft_backward_static_capacity() fail
+ * with NF_INVALID_ARGUMENT. The first call on each device looks the buffer's
+ * address up (cudaGetSymbolAddress) and should come before any stream capture;
+ * later calls only launch kernels. The buffer is shared: calls that overlap in
+ * time (other threads or unordered streams) race on it and must be serialised. */
+size_t nf_dft_backward_static_capacity(void);
+nf_status nf_dft_backward_device_static(const nf_plan* plan, const nf_const_plane* sources,
+                                        const nf_const_plane* grad_out, const nf_plane* grad_sources, int nplanes,
+                                        float* grad_primary, void* stream, char* err, size_t err_len);
+
 /* KernelInfo (docs/api/en/kernel-info.md; vapoursynth.cpp:64-69): labels of the
  * active implementation. Each string buffer receives at most len bytes. */
 nf_status nf_kernel_info(char* fft_backend, size_t fft_backend_len, char* target, size_t target_len, char* fft,

@@ -30,7 +30,7 @@ NVCCFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-f
 HOST_SOURCES = ["plan_build.cpp"]
 # (source, object stem, extra defines): the tile kernel is compiled once per block shape.
 SPATIAL_SHAPES = [(8, 8), (16, 16), (32, 32), (12, 12), (48, 48), (0, 0)]
-CUDA_UNITS = [("nf_api.cu", "nf_api", [])] + \
+CUDA_UNITS = [("nf_api.cu", "nf_api", []), ("nf_noalloc.cu", "nf_noalloc", [])] + \
     [("spatial_inst.cu", f"spatial_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \
     [("volume_inst.cu", f"volume_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \
     [("adjoint_inst.cu", f"adjoint_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in [(16, 16), (0, 0)]]
@@ -45,7 +45,7 @@ def _stale(obj: Path, src: Path) -> bool:
     if not obj.exists():
         return True
     deps = [src] + list(CSRC.glob("*.cuh")) + [CSRC / "launch.hpp"]
-    if src.name in ("nf_api.cu", "plan_build.cpp"):  # kernel units do not see the C ABI or the table builder
+    if src.name in ("nf_api.cu", "nf_noalloc.cu", "plan_build.cpp"):  # kernel units do not see the C ABI
         deps += list(CSRC.glob("*.hpp")) + list((ROOT / "include").glob("*.h"))
     return any(d.stat().st_mtime > obj.stat().st_mtime for d in deps)
 

@@ -17,15 +17,27 @@ import ctypes
 import torch
 
 from . import _capi as C
-from .plan import DFTConfig, Plan, SampleFormat, _plane
+from .plan import DFTConfig, Plan, SampleFormat
 
 
-def _set_primary(plan: Plan, table: torch.Tensor, stream) -> None:
-    t = table.detach().contiguous().to(torch.float32)
+def _set_primary(plan: Plan, table: torch.Tensor, stream) -> torch.Tensor:
+    t = table.detach()
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        t = t.contiguous().to(torch.float32)
     err = ctypes.create_string_buffer(256)
     C.raise_for(plan._lib.nf_plan_set_primary(plan._h, ctypes.c_void_p(t.data_ptr()), t.numel(), stream, err, 256),
                 err.value)
     return t
+
+
+def _plane_array(t: torch.Tensor, start: int, n: int, const: bool):
+    """ctypes array of n planes t[start:start+n] of a contiguous [B, H, W] float32 tensor,
+    built from the base pointer (no per-plane tensor views)."""
+    cls = C.NfConstPlane if const else C.NfPlane
+    _, h, w = t.shape
+    step = h * w * 4
+    base = t.data_ptr() + start * step
+    return (cls * n)(*[cls(base + i * step, w, h, w * 4) for i in range(n)])
 
 
 class DFTTestFunction(torch.autograd.Function):
@@ -37,7 +49,12 @@ class DFTTestFunction(torch.autograd.Function):
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         keep = _set_primary(plan, table, stream)
         out = torch.empty_like(x)
-        plan.process_planes(list(x), list(out), stream=stream.value)
+        err = ctypes.create_string_buffer(256)
+        for start in range(0, x.shape[0], 32):
+            n = min(32, x.shape[0] - start)
+            C.raise_for(plan._lib.nf_plan_process_planes_device(plan._h, _plane_array(x, start, n, True),
+                                                                _plane_array(out, start, n, False), n, stream,
+                                                                err, 256), err.value)
         ctx.save_for_backward(x, keep)
         ctx.plan = plan
         return out
@@ -50,23 +67,22 @@ class DFTTestFunction(torch.autograd.Function):
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         keep = _set_primary(plan, table, stream)  # noqa: F841 (kept alive until the launch is enqueued)
         gx = torch.empty_like(x)
-        gtab = torch.zeros_like(table, dtype=torch.float32)
         lib = plan._lib
         err = ctypes.create_string_buffer(256)
-        for start in range(0, x.shape[0], 32):
-            n = min(32, x.shape[0] - start)
-            need = ctypes.c_size_t()
-            lib.nf_dft_backward_scratch_bytes(plan._h, n, ctypes.byref(need))
-            scratch = torch.empty(max(1, need.value), dtype=torch.uint8, device=x.device)
-            part = torch.empty_like(gtab)
-            srcs = (C.NfConstPlane * n)(*[_plane(x[start + i], True) for i in range(n)])
-            gouts = (C.NfConstPlane * n)(*[_plane(gout[start + i], True) for i in range(n)])
-            gsrcs = (C.NfPlane * n)(*[_plane(gx[start + i], False) for i in range(n)])
-            st = lib.nf_dft_backward_device(plan._h, srcs, gouts, gsrcs, n, ctypes.c_void_p(part.data_ptr()),
-                                            ctypes.c_void_p(scratch.data_ptr()), need.value, stream, err, 256)
+        nb = x.shape[0]
+        chunks = [(s0, min(32, nb - s0)) for s0 in range(0, nb, 32)]
+        parts = torch.empty((len(chunks), table.numel()), dtype=torch.float32, device=x.device)
+        need = ctypes.c_size_t()
+        lib.nf_dft_backward_scratch_bytes(plan._h, chunks[0][1], ctypes.byref(need))
+        scratch = torch.empty(max(1, need.value), dtype=torch.uint8, device=x.device)
+        for c, (start, n) in enumerate(chunks):
+            st = lib.nf_dft_backward_device(plan._h, _plane_array(x, start, n, True), _plane_array(gout, start, n, True),
+                                            _plane_array(gx, start, n, False), n,
+                                            ctypes.c_void_p(parts[c].data_ptr()), ctypes.c_void_p(scratch.data_ptr()),
+                                            need.value, stream, err, 256)
             C.raise_for(st, err.value)
-            gtab += part
-        return gx, gtab.to(table.dtype), None
+        gtab = parts[0] if len(chunks) == 1 else parts.sum(0)
+        return gx, gtab.to(table.dtype).view_as(table), None
 
 
 class SigmaTableDenoiser(torch.nn.Module):

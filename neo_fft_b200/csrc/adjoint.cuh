@@ -300,7 +300,7 @@ struct AdjointBatch {  // passed by value: no per-call uploads, capturable in gr
 };
 
 template <int BHC, int BWC>
-__global__ void __launch_bounds__(256, 1) dft_adjoint_kernel(DevPlan P, AdjointShape S, AdjointBatch B) {
+__global__ void __launch_bounds__(256, 2) dft_adjoint_kernel(DevPlan P, AdjointShape S, AdjointBatch B) {
   extern __shared__ float smem[];
   const int tiles = S.tiles_x * S.tiles_y;
   adjoint_tile<BHC, BWC>(P, B.job[blockIdx.x / tiles], S, blockIdx.x % tiles, smem);
@@ -333,13 +333,24 @@ __global__ void dft_adjoint_fold_kernel(DevPlan P, AdjointBatch B) {
   row[x] = s * P.dec_scale;
 }
 
-// Table gradient: sum of all tiles' partials of all planes, in tile order.
-__global__ void dft_adjoint_reduce_kernel(const float* partial, int ntiles, int bins, float* out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= bins) return;
+// Table gradient: sum of all tiles' partials of all planes. Block (32, 32): x = bin
+// within a chunk of 32, y = residue class of the tile index; each thread sums its
+// class in ascending tile order, then the 32 class sums are added in a fixed tree.
+// The order never depends on timing, so the result is deterministic.
+__global__ void __launch_bounds__(1024) dft_adjoint_reduce_kernel(const float* partial, int ntiles, int bins,
+                                                                  float* out) {
+  __shared__ float part[32][33];
+  const int k = blockIdx.x * 32 + threadIdx.x;
   float s = 0.0f;
-  for (int t = 0; t < ntiles; ++t) s += partial[size_t(t) * bins + k];
-  out[k] = s;
+  if (k < bins)
+    for (int t = threadIdx.y; t < ntiles; t += 32) s += partial[size_t(t) * bins + k];
+  part[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 16; w > 0; w >>= 1) {
+    if (threadIdx.y < w) part[threadIdx.y][threadIdx.x] += part[threadIdx.y + w][threadIdx.x];
+    __syncthreads();
+  }
+  if (threadIdx.y == 0 && k < bins) out[k] = part[0][threadIdx.x];
 }
 #endif
 

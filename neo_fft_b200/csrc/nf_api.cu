@@ -1019,7 +1019,7 @@ nf_status nf_dft_backward_device(const nf_plan* p, const nf_const_plane* sources
     const dim3 fb(32, 8), fg((p->t.gx.length + 31) / 32, (p->t.gy.length + 7) / 8, nplanes);
     nfd::dft_adjoint_fold_kernel<<<fg, fb, 0, st>>>(d, B);
     // partials of all planes are contiguous: tiles*nplanes rows of `bins`
-    nfd::dft_adjoint_reduce_kernel<<<(p->t.bins + 127) / 128, 128, 0, st>>>(
+    nfd::dft_adjoint_reduce_kernel<<<(p->t.bins + 31) / 32, dim3(32, 32), 0, st>>>(
         reinterpret_cast<const float*>(base + size_t(nplanes) * cov), int(tiles) * nplanes, p->t.bins, grad_primary);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
     return NF_OK;

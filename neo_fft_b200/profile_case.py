@@ -11,6 +11,8 @@ Workloads (one plane per launch, seeded synthetic content):
   fft3d48  FFT3D bt=3 bw=bh=48, ow=oh=24, sigma 3, sharpen 0.3, u16 (10-bit) 3840x2160
   kalman32 FFT3D bt=0 (Kalman advance), bw=bh=32, float 1920x1080
   dft12t5  DFTTest tbsize 5 tmode 1, sbsize 12 / sosize 9, ftype 1, float 1920x1080
+  adjoint16 differentiable DFTTest: 16 float 256x256 noisy patches, sbsize 16 / sosize 8,
+           ftype 0, learnable table, MSE loss; one forward+backward per launch
 """
 from __future__ import annotations
 
@@ -85,6 +87,22 @@ def main():
         blocks = temporal_blocks(4, 9, 5, 0)
         srcs = [clip[s] for b in blocks for s in b["slots"]]
         targets = [b["target"] for b in blocks]
+    elif wl == "adjoint16":
+        import sys
+        from pathlib import Path
+        sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+        from tests.synth import noisy_patches
+
+        from .autograd import SigmaTableDenoiser
+        noisy, clean = noisy_patches(16, 256, 41)
+        x0, cl = torch.from_numpy(noisy).to(dev), torch.from_numpy(clean).to(dev)
+        m = SigmaTableDenoiser(256, 256, DFTConfig(block=16, overlap=8, ftype=0, sigma=4.0))
+        for _ in range(a.launches):
+            x = x0.detach().requires_grad_()
+            ((m(x) - cl) ** 2).mean().backward()
+        torch.cuda.synchronize()
+        m.plan.sync_status()
+        return
     else:
         raise SystemExit(f"unknown workload {wl}")
     out = torch.empty_like(srcs[0])

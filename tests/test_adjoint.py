@@ -222,3 +222,38 @@ def test_training_workload_gradients_match_fp64_finite_differences(cuda, ref):
         k = int(rng.integers(tab.numel()))
         tb(lambda v: ((o.forward(xd, v) - cd) ** 2).mean(), tab, k, 1e-4, float(gt[k]))
     assert px.skipped + tb.skipped <= 6, (px.skipped, tb.skipped)
+
+
+@pytest.mark.gpu
+def test_training_step_replays_from_a_cuda_graph(cuda):
+    """Forward + backward captured into one CUDA graph and replayed gives the eager
+    gradients bit for bit (the path bench.py times as graph_value)."""
+    import torch
+    from neo_fft_b200.autograd import SigmaTableDenoiser
+    from tests.synth import noisy_patches
+    noisy, clean = noisy_patches(4, 128, 43)
+    m = SigmaTableDenoiser(128, 128, DFTConfig(block=16, overlap=8, ftype=0, sigma=4.0))
+    cl = torch.from_numpy(clean).cuda()
+    x = torch.from_numpy(noisy).cuda().requires_grad_()
+    ((m(x) - cl) ** 2).mean().backward()
+    eager = (x.grad.clone(), m.table.grad.clone())
+
+    static_x = torch.from_numpy(noisy).cuda().requires_grad_()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            m.table.grad = None
+            static_x.grad = None
+            ((m(static_x) - cl) ** 2).mean().backward()
+    torch.cuda.current_stream().wait_stream(side)
+    m.table.grad = None
+    static_x.grad = None
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        ((m(static_x) - cl) ** 2).mean().backward()
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(static_x.grad, eager[0]) and torch.equal(m.table.grad, eager[1])
+    m.plan.sync_status()

@@ -287,6 +287,7 @@ def run_ours(args):
     host_plane_value = FRAMES * W * H / (time.perf_counter() - t0) / 1e6
 
     train = differentiable_pass(args, dev)
+    configs = other_configs(args, dev) if world == 1 else None
     cpu = cpu_baseline() if (rank == 0 and world == 1) else None
     if world > 1:
         dist.barrier()
@@ -317,6 +318,7 @@ def run_ours(args):
         "clocks": clocks.summary() if clocks else None,
         "cpu_baseline": cpu,
         "fwd_bwd": train,
+        "other_configs": configs,
     }
     print(json.dumps(line))
 
@@ -391,6 +393,130 @@ def differentiable_pass(args, dev):
             "workload": "16 float32 256x256 patches, sbsize 16 / sosize 8, ftype 0, learnable 16x9 table, "
                         "MSE loss; gradients w.r.t. pixels and table (autograd over the C ABI adjoint kernels)",
             "l2": "flushed before every step (256 MB write)"}
+
+
+def _texture(h, w, seed, lo, hi, noise_sd, dtype, peak=None):
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    t = gaussian_filter(rng.standard_normal((h, w)), 3.0)
+    t = lo + (hi - lo) * (t - t.min()) / max(np.ptp(t), 1e-12) + rng.standard_normal((h, w)) * noise_sd
+    if peak is not None:
+        t = np.clip(np.round(t), 0, peak)
+    return t.astype(dtype)
+
+
+def _event_timer(dev, flush):
+    import torch
+
+    def measure(fn, steps, warmup):
+        for _ in range(max(3, warmup)):
+            fn()
+        total = 0.0
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            total += e0.elapsed_time(e1)
+        return total / steps
+    return measure
+
+
+def other_configs(args, dev):
+    """The remaining configurations, each timed with CUDA events per step and the L2
+    flushed (256 MB write) before every step. Mpx counts luma pixels per output frame."""
+    import torch
+
+    from neo_fft_b200 import Batch, ClipBatch, DFTConfig, FFT3DConfig, Plan, SampleFormat
+    from neo_fft_b200.temporal import temporal_blocks
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    measure = _event_timer(dev, flush)
+    steps = max(3, min(args.steps, 10))
+    out = {}
+
+    # A: FFT3D bt=1, 640x360 GRAY8, 24 frames, 32x32 blocks, overlap 16, sigma 2.
+    w, h, n = 640, 360, 24
+    plan = Plan(w, h, SampleFormat(8), FFT3DConfig(bw=32, bh=32, ow=16, oh=16, sigma=2.0))
+    frames = [torch.from_numpy(_texture(h, w, [1, 0, f], 16, 235, 5, np.uint8, 255)).to(dev) for f in range(n)]
+    outs = [torch.empty_like(f) for f in frames]
+    batch = Batch([(plan, frames[f], outs[f]) for f in range(n)])
+    plain_ms = measure(lambda: [plan.process_at([frames[f]], outs[f]) for f in range(n)], steps, args.warmup)
+    batch_ms = measure(lambda: batch.launch(graph=True), steps, args.warmup)
+    plan.sync_status()
+    out["A"] = {"workload": "FFT3D bt=1 32x32 ow=oh=16 sigma 2, 640x360 GRAY8, 24 frames",
+                "plain": n * w * h / (plain_ms / 1e3) / 1e6, "batched": n * w * h / (batch_ms / 1e3) / 1e6,
+                "unit": "Mpx/s", "plain_ms": plain_ms, "batched_ms": batch_ms}
+    del batch, frames, outs
+
+    # C: FFT3D bt=3 48x48 ow=oh=24 sigma 3 sharpen 0.3, 3840x2160 YUV420P10; a 10-frame
+    # clip drifting 2 px per frame. Plain: the 8 interior output frames, one volume launch
+    # per plane; batched: all 10 outputs through the clip batch under a CUDA graph.
+    W4, H4, nf = 3840, 2160, 10
+    cfg = FFT3DConfig(bw=48, bh=48, ow=24, oh=24, bt=3, sigma=3.0, sharpen=0.3)
+    pl = [Plan(W4, H4, SampleFormat(10), cfg), Plan(W4 // 2, H4 // 2, SampleFormat(10, chroma=True), cfg)]
+    base = [_texture(H4, W4, [3, 0, 0, 0], 64, 940, 8, np.uint16, 1023),
+            _texture(H4 // 2, W4 // 2, [3, 0, 0, 1], 64, 960, 8, np.uint16, 1023),
+            _texture(H4 // 2, W4 // 2, [3, 0, 0, 2], 64, 960, 8, np.uint16, 1023)]
+    dclip = [[torch.from_numpy(np.ascontiguousarray(np.roll(b, 2 * f, axis=1))).to(dev) for b in base]
+             for f in range(nf)]
+    douts = [[torch.empty_like(p) for p in fr] for fr in dclip]
+
+    def c_plain():
+        for t in range(1, nf - 1):
+            for p in range(3):
+                pl[min(p, 1)].process_at([dclip[t - 1][p], dclip[t][p], dclip[t + 1][p]], douts[t][p])
+    c_ms = measure(c_plain, steps, args.warmup)
+    cb = ClipBatch([(pl[min(p, 1)], [dclip[f][p] for f in range(nf)], [douts[f][p] for f in range(nf)])
+                    for p in range(3)])
+    cb_ms = measure(lambda: cb.launch(graph=True), steps, args.warmup)
+    for p in pl:
+        p.sync_status()
+    del cb
+    out["C"] = {"workload": "FFT3D bt=3 48x48 ow=oh=24 sigma 3 sharpen 0.3, 3840x2160 YUV420P10, 10-frame clip",
+                "plain": (nf - 2) * W4 * H4 / (c_ms / 1e3) / 1e6, "plain_ms": c_ms,
+                "plain_form": "8 interior output frames, one volume launch per plane",
+                "batched": nf * W4 * H4 / (cb_ms / 1e3) / 1e6, "batched_ms": cb_ms,
+                "batched_form": "all 10 output frames: clip batch (spectra once per frame, temporal strips), graph",
+                "unit": "Mpx/s"}
+    del dclip, douts
+
+    # D1: FFT3D bt=0 Kalman 32x32 sigma 2.5 kratio 2, 1920x1080 float, 16 sequential
+    # frames: advance + render per frame, state resident in HBM.
+    w, h, n = 1920, 1080, 16
+    kp = Plan(w, h, SampleFormat(32, True), FFT3DConfig(bw=32, bh=32, bt=0, sigma=2.5, kratio=2.0))
+    kf = [torch.from_numpy(_texture(h, w, [4, 0, f], 0, 1, 0.02, np.float32)).to(dev) for f in range(4)]
+    kout = torch.empty_like(kf[0])
+    state = kp.initial_kalman()
+
+    def d1():
+        for f in range(n):
+            kp.advance_kalman(kf[f % 4], state)
+            kp.render_kalman(kf[f % 4], kout, state)
+    d1_ms = measure(d1, steps, args.warmup)
+    kp.sync_status()
+    out["D1"] = {"workload": "FFT3D bt=0 Kalman 32x32 sigma 2.5 kratio 2, 1920x1080 float32, 16 sequential frames",
+                 "plain": n * w * h / (d1_ms / 1e3) / 1e6, "unit": "Mpx/s", "plain_ms": d1_ms}
+    del kf, state
+
+    # D2: DFTTest tbsize 5 tmode 1 (tosize 0), sbsize 12 sosize 9 ftype 1 sigma 8,
+    # 1920x1080 float32; 8 output frames of a 12-frame clip.
+    nclip, nout = 12, 8
+    dp = Plan(w, h, SampleFormat(32, True), DFTConfig(block=12, overlap=9, tbsize=5, temporal_mode=1, ftype=1,
+                                                      sigma=8.0))
+    df = [torch.from_numpy(_texture(h, w, [4, 0, f], 0, 1, 0.02, np.float32)).to(dev) for f in range(nclip)]
+    dout = torch.empty_like(df[0])
+    jobs = []
+    for t in range(2, 2 + nout):
+        blocks = temporal_blocks(t, nclip, 5, 0)
+        jobs.append(([df[s] for b in blocks for s in b["slots"]], [b["target"] for b in blocks]))
+    d2_ms = measure(lambda: [dp.process_at(srcs, dout, targets=tg) for srcs, tg in jobs], steps, args.warmup)
+    dp.sync_status()
+    out["D2"] = {"workload": "DFTTest tbsize 5 tmode 1 sbsize 12 sosize 9 ftype 1 sigma 8, 1920x1080 float32, "
+                             "8 output frames", "plain": nout * w * h / (d2_ms / 1e3) / 1e6, "unit": "Mpx/s",
+                 "plain_ms": d2_ms}
+    return out
 
 
 def ctypes_stream(stream):

@@ -177,6 +177,30 @@ nf_status nf_batch_launch(nf_batch* batch, void* stream, char* err, size_t err_l
 nf_status nf_batch_graph_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
 void nf_batch_destroy(nf_batch* batch);
 
+/* FFT3D temporal clips (bt 2..5) in batched form: every output frame of every clip,
+ * frame n filtered from frames n-bt/2 .. n+(bt-1)/2, or from frame n alone where that
+ * window leaves the clip (the host layer's rule, filter.hpp:407-421). Each frame's
+ * spatial spectra are computed once into a device ring of bt frame spectra per clip
+ * plane (the reference caches them in SpectraCache, plan.cpp:437-447); results equal
+ * one nf_plan_process_device call per output frame bit for bit. Items must share the
+ * block shape and sample storage; planes must stay allocated while the batch is used,
+ * and outputs must not overlap any frame of their clip. No reference counterpart: the
+ * reference filters one frame per call. */
+typedef struct nf_clip_batch nf_clip_batch;
+typedef struct nf_clip_item {
+  const nf_plan* plan;
+  const nf_const_plane* frames; /* nframes source planes (device memory) */
+  const nf_plane* dsts;         /* nframes output planes (device memory) */
+  int nframes;
+} nf_clip_item;
+nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_batch** batch, char* err,
+                               size_t err_len);
+/* Enqueues all frame steps on `stream` (no allocation or synchronisation). */
+nf_status nf_clip_batch_launch(nf_clip_batch* batch, void* stream, char* err, size_t err_len);
+/* Captures nf_clip_batch_launch into a CUDA graph on first use, then replays it. */
+nf_status nf_clip_batch_graph_launch(nf_clip_batch* batch, void* stream, char* err, size_t err_len);
+void nf_clip_batch_destroy(nf_clip_batch* batch);
+
 /* Differentiable form (no reference counterpart; the reference has no gradients).
  * DFTTest plans keep their per-bin primary table A ([tbsize][sbsize][sbsize/2+1],
  * already calibrated: the threshold the Wiener gain compares with) in device memory.

@@ -63,6 +63,11 @@ class NfBatchItem(ctypes.Structure):
     _fields_ = [("plan", c_void_p), ("source", NfConstPlane), ("dst", NfPlane)]
 
 
+class NfClipItem(ctypes.Structure):
+    _fields_ = [("plan", c_void_p), ("frames", ctypes.POINTER(NfConstPlane)), ("dsts", ctypes.POINTER(NfPlane)),
+                ("nframes", c_int)]
+
+
 # Every symbol the header declares, with its prototype: (restype, argtypes).
 PROTOTYPES = {
     "nf_abi_version": (c_int, []),
@@ -96,6 +101,11 @@ PROTOTYPES = {
     "nf_batch_destroy": (None, [c_void_p]),
     "nf_plan_process_planes_device": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfPlane), c_int,
                                               c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_clip_batch_create": (c_int, [ctypes.POINTER(NfClipItem), c_int, ctypes.POINTER(c_void_p), ctypes.c_char_p,
+                                     c_size_t]),
+    "nf_clip_batch_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_clip_batch_graph_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_clip_batch_destroy": (None, [c_void_p]),
     "nf_plan_set_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_plan_get_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_dft_backward_scratch_bytes": (c_int, [c_void_p, c_int, ctypes.POINTER(c_size_t)]),

@@ -33,6 +33,7 @@ SPATIAL_SHAPES = [(8, 8), (16, 16), (32, 32), (12, 12), (48, 48), (0, 0)]
 CUDA_UNITS = [("nf_api.cu", "nf_api", []), ("nf_noalloc.cu", "nf_noalloc", [])] + \
     [("spatial_inst.cu", f"spatial_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \
     [("volume_inst.cu", f"volume_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \
+    [("temporal_inst.cu", f"temporal_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \
     [("adjoint_inst.cu", f"adjoint_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in [(16, 16), (0, 0)]]
 
 

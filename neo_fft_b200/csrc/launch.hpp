@@ -21,6 +21,19 @@ NF_DECLARE_SPATIAL(12, 12)
 NF_DECLARE_SPATIAL(48, 48)
 NF_DECLARE_SPATIAL(0, 0)
 #undef NF_DECLARE_SPATIAL
+struct SpectraWork;
+#define NF_DECLARE_TEMPORAL(BH, BW)                                                                             \
+  cudaError_t launch_spectra_batch_##BH##x##BW(int storage, const SpectraWork& w, int items, size_t smem,        \
+                                               cudaStream_t st);                                                \
+  cudaError_t launch_temporal_batch_##BH##x##BW(int storage, const BatchWork& w, int ctas, size_t smem,          \
+                                                cudaStream_t st);
+NF_DECLARE_TEMPORAL(8, 8)
+NF_DECLARE_TEMPORAL(16, 16)
+NF_DECLARE_TEMPORAL(32, 32)
+NF_DECLARE_TEMPORAL(12, 12)
+NF_DECLARE_TEMPORAL(48, 48)
+NF_DECLARE_TEMPORAL(0, 0)
+#undef NF_DECLARE_TEMPORAL
 struct KalmanArgs;
 struct AdjointShape;
 struct AdjointBatch;

@@ -9,6 +9,7 @@
 #include "kalman.cuh"
 #define NF_ADJOINT_AUX_KERNELS
 #include "adjoint.cuh"
+#include "tile_temporal.cuh"
 
 #include <cuda_runtime.h>
 
@@ -72,6 +73,36 @@ struct nf_batch {
     for (auto& g : groups)
       if (g.dev) cudaFree(g.dev);
     if (counters) cudaFree(counters);
+  }
+};
+
+// FFT3D temporal clips: per frame step, pass 1 (spectra of the newest frame of every
+// clip into its ring of T frame spectra) then pass 2 (the outputs whose windows are
+// complete). Work lists of every step are built and uploaded once at creation.
+struct nf_clip_batch {
+  int bh = 0, bw = 0, storage = 0;
+  size_t smem1 = 0, smem2 = 0;
+  int nbc = 1, ctas2 = 1;
+  struct Step {
+    nfd::SpectraWork w1{};
+    int items1 = 0;
+    nfd::BatchWork w2{};
+    int tiles2 = 0;
+  };
+  std::vector<Step> steps;
+  void* dev = nullptr;      // plans | shapes | per-step job tables
+  void* rings = nullptr;    // frame spectra, T per clip plane
+  void* tspec = nullptr;    // slot pointer arrays of the temporal jobs
+  int* counters = nullptr;  // one work-queue head per step
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t capture_stream = nullptr;
+  ~nf_clip_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    for (void* q : {dev, rings, tspec, static_cast<void*>(counters)})
+      if (q) cudaFree(q);
   }
 };
 
@@ -464,6 +495,36 @@ cudaError_t launch_batch_group(const BatchGroup& g, cudaStream_t st) {
     }
   }
   return nfd::launch_spatial_batch_0x0(g.storage, g.work, g.ctas, g.smem, st);
+}
+
+cudaError_t launch_spectra_shape(int bh, int bw, int storage, const nfd::SpectraWork& w, int items, size_t smem,
+                                 cudaStream_t st) {
+  if (bh == bw) {
+    switch (bw) {
+      case 8: return nfd::launch_spectra_batch_8x8(storage, w, items, smem, st);
+      case 16: return nfd::launch_spectra_batch_16x16(storage, w, items, smem, st);
+      case 32: return nfd::launch_spectra_batch_32x32(storage, w, items, smem, st);
+      case 12: return nfd::launch_spectra_batch_12x12(storage, w, items, smem, st);
+      case 48: return nfd::launch_spectra_batch_48x48(storage, w, items, smem, st);
+      default: break;
+    }
+  }
+  return nfd::launch_spectra_batch_0x0(storage, w, items, smem, st);
+}
+
+cudaError_t launch_temporal_shape(int bh, int bw, int storage, const nfd::BatchWork& w, int ctas, size_t smem,
+                                  cudaStream_t st) {
+  if (bh == bw) {
+    switch (bw) {
+      case 8: return nfd::launch_temporal_batch_8x8(storage, w, ctas, smem, st);
+      case 16: return nfd::launch_temporal_batch_16x16(storage, w, ctas, smem, st);
+      case 32: return nfd::launch_temporal_batch_32x32(storage, w, ctas, smem, st);
+      case 12: return nfd::launch_temporal_batch_12x12(storage, w, ctas, smem, st);
+      case 48: return nfd::launch_temporal_batch_48x48(storage, w, ctas, smem, st);
+      default: break;
+    }
+  }
+  return nfd::launch_temporal_batch_0x0(storage, w, ctas, smem, st);
 }
 
 } // namespace
@@ -919,6 +980,245 @@ nf_status nf_batch_graph_launch(nf_batch* b, void* stream, char* err, size_t len
 
 void nf_batch_destroy(nf_batch* b) { delete b; }
 
+nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_batch** out, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(out && count > 0 && items, "null clip batch output or items");
+    auto b = std::make_unique<nf_clip_batch>();
+    std::vector<const nf_plan*> plans;
+    std::vector<int> plan_of(static_cast<size_t>(count));
+    for (int i = 0; i < count; ++i) {
+      const nf_clip_item& it = items[i];
+      nfb::require(it.plan != nullptr && it.frames && it.dsts && it.nframes > 0, "invalid clip item");
+      const nf_plan& p = *it.plan;
+      nfb::require(p.t.algo == nfb::Algo::FFT3D && !p.t.kalman && p.t.temporal_size >= 2 && p.t.temporal_size <= 5,
+                   "clip batches take FFT3D plans with bt 2..5");
+      const int storage = storage_of(p.t.format);
+      if (i == 0) {
+        b->bh = p.t.bh;
+        b->bw = p.t.bw;
+        b->storage = storage;
+      }
+      nfb::require(p.t.bh == b->bh && p.t.bw == b->bw && storage == b->storage,
+                   "clip batch items must share block shape and sample storage");
+      const size_t elem = size_t(storage);
+      for (int f = 0; f < it.nframes; ++f) {
+        validate_call(p, &it.frames[f], 1, nullptr, 0, it.dsts[f]);
+        // outputs are written while other outputs still read the clip's frames
+        const size_t de = plane_extent(it.dsts[f].width, it.dsts[f].height, it.dsts[f].stride_bytes, elem);
+        for (int g = 0; g < it.nframes; ++g)
+          disjoint(it.frames[g].data,
+                   plane_extent(it.frames[g].width, it.frames[g].height, it.frames[g].stride_bytes, elem),
+                   it.dsts[f].data, de);
+      }
+      int pi = -1;
+      for (size_t j = 0; j < plans.size(); ++j)
+        if (plans[j] == &p) pi = int(j);
+      if (pi < 0) {
+        pi = int(plans.size());
+        plans.push_back(&p);
+      }
+      plan_of[size_t(i)] = pi;
+    }
+    // strips of pass 2 (tall segments: the batch supplies the parallelism) and the
+    // block-column chunk of pass 1
+    std::vector<nfd::DevPlan> dplans;
+    std::vector<nfd::StripShape> shapes;
+    for (const nf_plan* p : plans) {
+      dplans.push_back(p->dev);
+      nfd::StripShape S = pick_strip(p->dev, 1);
+      const int segs = std::max(1, (p->t.gy.length + 255) / 256);
+      S.th = (p->t.gy.length + segs - 1) / segs;
+      shapes.push_back(S);
+      b->smem2 = std::max(b->smem2, nfd::strip_smem_bytes(b->bh, b->bw, S));
+    }
+    int max_count = 1, step = plans[0]->t.gx.step;
+    for (const nf_plan* p : plans) max_count = std::max(max_count, p->t.gx.count);
+    for (const nf_plan* p : plans) step = std::min(step, p->t.gx.step);
+    b->nbc = 1;
+    for (int n = 2; n <= std::min(16, max_count); ++n)
+      if (nfd::spectra_smem_bytes(b->bh, b->bw, step, n) <= 100 * 1024) b->nbc = n;
+    b->smem1 = 0;
+    for (const nf_plan* p : plans)
+      b->smem1 = std::max(b->smem1, nfd::spectra_smem_bytes(b->bh, b->bw, p->t.gx.step, b->nbc));
+    nfb::require(b->smem1 <= 200 * 1024, "block size too large for the spectra pass");
+    // rings: T frame spectra per clip plane that has interior outputs
+    std::vector<size_t> ring_off(static_cast<size_t>(count), SIZE_MAX);
+    size_t ring_bytes = 0;
+    for (int i = 0; i < count; ++i) {
+      const nf_plan& p = *items[i].plan;
+      if (items[i].nframes < p.t.temporal_size) continue;
+      ring_off[size_t(i)] = ring_bytes;
+      const size_t frame = size_t(p.t.gy.count) * p.t.bins * p.t.gx.count * sizeof(cf);
+      ring_bytes += ((frame * p.t.temporal_size) + 255) & ~size_t(255);
+    }
+    cudaError_t ce;
+    if (ring_bytes && (ce = cudaMalloc(&b->rings, ring_bytes)) != cudaSuccess)
+      return cuda_fail(err, len, ce, "device allocation failed");
+    auto frame_spec = [&](int i, int f) {
+      const nf_plan& p = *items[i].plan;
+      const size_t frame = size_t(p.t.gy.count) * p.t.bins * p.t.gx.count;
+      return reinterpret_cast<cf*>(static_cast<unsigned char*>(b->rings) + ring_off[size_t(i)]) +
+             size_t(f % p.t.temporal_size) * frame;
+    };
+    int nsteps = 0;
+    for (int i = 0; i < count; ++i)
+      nsteps = std::max(nsteps, items[i].nframes + (items[i].plan->t.temporal_size - 1) / 2);
+    // slot pointer arrays of all temporal jobs
+    std::vector<const cf*> slot_ptrs;
+    struct Pass2 {
+      std::vector<nfd::PlaneJob> jobs;
+      std::vector<size_t> tspec_index;  // SIZE_MAX for pixel jobs
+      std::vector<int> base{0}, tiles_x;
+    };
+    std::vector<std::vector<nfd::SpectraJob>> pass1(static_cast<size_t>(nsteps));
+    std::vector<std::vector<int>> pass1_base(static_cast<size_t>(nsteps), std::vector<int>(1, 0));
+    std::vector<Pass2> pass2(static_cast<size_t>(nsteps));
+    for (int s = 0; s < nsteps; ++s) {
+      for (int i = 0; i < count; ++i) {
+        const nf_clip_item& it = items[i];
+        const nf_plan& p = *it.plan;
+        const int bt = p.t.temporal_size, left = bt / 2, right = (bt - 1) / 2;
+        const int pi = plan_of[size_t(i)];
+        if (ring_off[size_t(i)] != SIZE_MAX && s < it.nframes) {
+          const int chunks = (p.t.gx.count + b->nbc - 1) / b->nbc;
+          pass1[size_t(s)].push_back({static_cast<const unsigned char*>(it.frames[s].data),
+                                      (long long)it.frames[s].stride_bytes, frame_spec(i, s), pi, chunks});
+          pass1_base[size_t(s)].push_back(pass1_base[size_t(s)].back() + chunks * p.t.gy.count);
+        }
+        const int t = s - right;
+        if (t < 0 || t >= it.nframes) continue;
+        const bool fallback = it.nframes < bt || t < left || it.nframes - 1 - t < right;
+        nfd::PlaneJob job{fallback ? static_cast<const unsigned char*>(it.frames[t].data) : nullptr,
+                          (long long)it.frames[t].stride_bytes, static_cast<unsigned char*>(it.dsts[t].data),
+                          (long long)it.dsts[t].stride_bytes, nullptr, pi, nullptr};
+        Pass2& q = pass2[size_t(s)];
+        q.jobs.push_back(job);
+        if (fallback) {
+          q.tspec_index.push_back(SIZE_MAX);
+        } else {
+          q.tspec_index.push_back(slot_ptrs.size());
+          for (int j = 0; j < bt; ++j) slot_ptrs.push_back(frame_spec(i, t - left + j));
+        }
+        const nfd::StripShape& S = shapes[size_t(pi)];
+        const int tx = (p.t.gx.length + S.tw - 1) / S.tw, ty = (p.t.gy.length + S.th - 1) / S.th;
+        q.tiles_x.push_back(tx);
+        q.base.push_back(q.base.back() + tx * ty);
+      }
+    }
+    if (!slot_ptrs.empty()) {
+      if ((ce = cudaMalloc(&b->tspec, slot_ptrs.size() * sizeof(cf*))) != cudaSuccess)
+        return cuda_fail(err, len, ce, "device allocation failed");
+      if ((ce = cudaMemcpy(b->tspec, slot_ptrs.data(), slot_ptrs.size() * sizeof(cf*), cudaMemcpyHostToDevice)) !=
+          cudaSuccess)
+        return cuda_fail(err, len, ce, "clip batch upload failed");
+    }
+    const auto* slots_dev = static_cast<const cf* const*>(b->tspec);
+    Blob blob;
+    const size_t o_p = blob.add(dplans), o_s = blob.add(shapes);
+    struct Offsets {
+      size_t j1 = SIZE_MAX, b1 = SIZE_MAX, j2 = SIZE_MAX, b2 = SIZE_MAX, t2 = SIZE_MAX;
+    };
+    std::vector<Offsets> offs(static_cast<size_t>(nsteps));
+    for (int s = 0; s < nsteps; ++s) {
+      Offsets& o = offs[size_t(s)];
+      if (!pass1[size_t(s)].empty()) {
+        o.j1 = blob.add(pass1[size_t(s)]);
+        o.b1 = blob.add(pass1_base[size_t(s)]);
+      }
+      Pass2& q = pass2[size_t(s)];
+      for (size_t j = 0; j < q.jobs.size(); ++j)
+        if (q.tspec_index[j] != SIZE_MAX) q.jobs[j].tspec = slots_dev + q.tspec_index[j];
+      if (!q.jobs.empty()) {
+        o.j2 = blob.add(q.jobs);
+        o.b2 = blob.add(q.base);
+        o.t2 = blob.add(q.tiles_x);
+      }
+    }
+    if ((ce = cudaMalloc(&b->dev, blob.bytes.size())) != cudaSuccess)
+      return cuda_fail(err, len, ce, "device allocation failed");
+    if ((ce = cudaMemcpy(b->dev, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cuda_fail(err, len, ce, "clip batch upload failed");
+    if ((ce = cudaMalloc(&b->counters, sizeof(int) * size_t(nsteps))) != cudaSuccess)
+      return cuda_fail(err, len, ce, "device allocation failed");
+    auto* base = static_cast<unsigned char*>(b->dev);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    const int per_sm = b->bh * b->bw <= 256 ? 2 : 1;
+    b->steps.resize(size_t(nsteps));
+    for (int s = 0; s < nsteps; ++s) {
+      auto& st = b->steps[size_t(s)];
+      const Offsets& o = offs[size_t(s)];
+      if (o.j1 != SIZE_MAX) {
+        st.w1.plans = reinterpret_cast<const nfd::DevPlan*>(base + o_p);
+        st.w1.jobs = reinterpret_cast<const nfd::SpectraJob*>(base + o.j1);
+        st.w1.item_base = reinterpret_cast<const int*>(base + o.b1);
+        st.w1.njobs = int(pass1[size_t(s)].size());
+        st.w1.nbc = b->nbc;
+        st.items1 = pass1_base[size_t(s)].back();
+      }
+      if (o.j2 != SIZE_MAX) {
+        st.w2.plans = reinterpret_cast<const nfd::DevPlan*>(base + o_p);
+        st.w2.shapes = reinterpret_cast<const nfd::StripShape*>(base + o_s);
+        st.w2.jobs = reinterpret_cast<const nfd::PlaneJob*>(base + o.j2);
+        st.w2.job_tile_base = reinterpret_cast<const int*>(base + o.b2);
+        st.w2.job_tiles_x = reinterpret_cast<const int*>(base + o.t2);
+        st.w2.njobs = int(pass2[size_t(s)].jobs.size());
+        st.w2.counter = b->counters + s;
+        st.tiles2 = pass2[size_t(s)].base.back();
+      }
+    }
+    b->ctas2 = per_sm * sms;
+    *out = b.release();
+    return NF_OK;
+  });
+}
+
+nf_status nf_clip_batch_launch(nf_clip_batch* b, void* stream, char* err, size_t len) {
+  if (!b) return fail(err, len, "null clip batch", NF_INVALID_ARGUMENT);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (b->steps.empty()) return NF_OK;
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, sizeof(int) * b->steps.size(), st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
+  for (const auto& s : b->steps) {
+    if (s.items1 > 0 && (e = launch_spectra_shape(b->bh, b->bw, b->storage, s.w1, s.items1, b->smem1, st)) !=
+                            cudaSuccess)
+      return cuda_fail(err, len, e, "kernel launch failed");
+    if (s.w2.njobs > 0) {
+      const int ctas = std::max(1, std::min(b->ctas2, s.tiles2));
+      if ((e = launch_temporal_shape(b->bh, b->bw, b->storage, s.w2, ctas, b->smem2, st)) != cudaSuccess)
+        return cuda_fail(err, len, e, "kernel launch failed");
+    }
+  }
+  return NF_OK;
+}
+
+nf_status nf_clip_batch_graph_launch(nf_clip_batch* b, void* stream, char* err, size_t len) {
+  if (!b) return fail(err, len, "null clip batch", NF_INVALID_ARGUMENT);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e;
+  if (!b->exec) {
+    if (!b->capture_stream && (e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
+      return cuda_fail(err, len, e, "stream creation failed");
+    if ((e = cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return cuda_fail(err, len, e, "graph capture failed");
+    const nf_status s = nf_clip_batch_launch(b, b->capture_stream, err, len);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->capture_stream, &g);
+    if (s != NF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "graph capture failed");
+    b->graph = g;
+    if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess)
+      return cuda_fail(err, len, e, "graph instantiation failed");
+  }
+  if ((e = cudaGraphLaunch(b->exec, st)) != cudaSuccess) return cuda_fail(err, len, e, "graph launch failed");
+  return NF_OK;
+}
+
+void nf_clip_batch_destroy(nf_clip_batch* b) { delete b; }
+
 nf_status nf_plan_set_primary(nf_plan* p, const float* table, int count, void* stream, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(p && table, "null plan or table");
@@ -950,18 +1250,34 @@ void check_adjoint_plan(const nf_plan& p) {
                    (t.spectral.type >= 0 && t.spectral.type <= 2),
                "backward requires a float DFTTest plan with tbsize=1, smode=1 and ftype 0, 1 or 2");
 }
-nfd::AdjointShape adjoint_shape(const nfd::DevPlan& d) {
+// Cover tiles of the backward: 64-pixel-wide strips (a whole number of block steps);
+// the tile height is chosen for the whole call so that the CTAs of all planes fill
+// whole waves of resident CTAs (two per SM), weighing each CTA by the rows it
+// transforms (tile height plus the block-height halo).
+nfd::AdjointShape adjoint_shape(const nfd::DevPlan& d, int nplanes) {
   nfd::AdjointShape S{};
   S.tab_floats = 2 * d.bh * d.bw + (d.grid ? 2 * d.bins : 0) + d.bins;
   S.tab_floats = (S.tab_floats + 3) & ~3;
   S.tw = std::min(d.gx.cover, std::max(d.gx.step, 64 / d.gx.step * d.gx.step));
-  S.th = std::min(d.gy.cover, std::max(2 * d.bh, 64));
   S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
   S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
   int q = (S.win_max + 3) / 4;
   if (q % 2 == 0) ++q;
   S.ring_pitch = 4 * q;
   S.tiles_x = (d.gx.cover + S.tw - 1) / S.tw;
+  const long long slots = 2LL * 148;
+  const int lo = std::min(d.gy.cover, std::max(2 * d.bh, 32));
+  long long best = -1;
+  for (int th = lo; th <= d.gy.cover; th += std::max(1, d.gy.step)) {
+    const long long tiles_y = (d.gy.cover + th - 1) / th;
+    const long long ctas = (long long)std::max(1, nplanes) * S.tiles_x * tiles_y;
+    const long long cost = ((ctas + slots - 1) / slots) * (th + d.bh);
+    if (best < 0 || cost < best) {
+      best = cost;
+      S.th = th;
+    }
+    if (tiles_y == 1) break;
+  }
   S.tiles_y = (d.gy.cover + S.th - 1) / S.th;
   return S;
 }
@@ -970,7 +1286,7 @@ size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
 nf_status nf_dft_backward_scratch_bytes(const nf_plan* p, int nplanes, size_t* bytes) {
   if (!p || !bytes || nplanes < 0) return NF_INVALID_ARGUMENT;
-  const nfd::AdjointShape S = adjoint_shape(p->dev);
+  const nfd::AdjointShape S = adjoint_shape(p->dev, nplanes);
   const size_t tiles = size_t(S.tiles_x) * S.tiles_y;
   *bytes = size_t(nplanes) * align256(size_t(p->t.gx.cover) * p->t.gy.cover * 4) +
            align256(size_t(nplanes) * tiles * p->t.bins * 4);
@@ -996,7 +1312,7 @@ nf_status nf_dft_backward_device(const nf_plan* p, const nf_const_plane* sources
       check_pointer(grad_out[i].data, 4);
     }
     const nfd::DevPlan& d = p->dev;
-    const nfd::AdjointShape S = adjoint_shape(d);
+    const nfd::AdjointShape S = adjoint_shape(d, nplanes);
     const size_t tiles = size_t(S.tiles_x) * S.tiles_y;
     const size_t cov = align256(size_t(p->t.gx.cover) * p->t.gy.cover * 4), part = tiles * p->t.bins * 4;
     auto* base = static_cast<unsigned char*>(scratch);

@@ -1,0 +1,157 @@
+// FFT3D temporal clips (bt=2..5) in two passes over HBM:
+//   pass 1 (spectra_batch_kernel): windowed spatial r2c of every block of a frame,
+//     computed once per frame and written to a per-plane ring of T frame spectra —
+//     the device counterpart of the reference's raw-spectrum cache (SpectraCache,
+//     src/algorithms/plan.cpp:437-447);
+//   pass 2 (temporal_batch_kernel): the streaming strip (strip_tile in temporal mode)
+//     reads the T spectra of each block, filters across time and reconstructs.
+// Clip edges, where the host layer falls back to a single frame (filter.hpp:407-421),
+// run as pixel-mode strips in the same pass-2 launch.
+#pragma once
+#include "tile_spatial.cuh"
+
+namespace nfd {
+
+// Spectrum layout of one frame: [block row][bin][block column] complex, so the
+// threads of a warp (consecutive block columns) read and write consecutive words.
+struct SpectraJob {
+  const unsigned char* src;
+  long long src_stride;
+  cf* out;
+  int plan;
+  int chunks_x;  // block-column chunks per block row
+};
+
+struct SpectraWork {
+  const DevPlan* plans;
+  const SpectraJob* jobs;
+  const int* item_base;  // prefix sums of (block rows x chunks) per job (njobs+1)
+  int njobs;
+  int nbc;               // block columns per chunk
+};
+
+// Shared layout (floats): wxa[bw] wya[bh] | ring [bh][pitch] | spec [bh][K][nbc] complex.
+__host__ __device__ inline size_t spectra_smem_bytes(int bh, int bw, int step, int nbc) {
+  const size_t K = size_t(bw / 2 + 1);
+  const size_t win = size_t(nbc - 1) * step + bw;
+  const size_t pitch = (win + 3) & ~size_t(3);
+  return sizeof(float) * (((size_t(bw + bh) + 3) & ~size_t(3)) + size_t(bh) * pitch + 2 * size_t(bh) * K * nbc);
+}
+
+template <int BHC, int BWC, int STORAGE>
+__global__ void __launch_bounds__(256) spectra_batch_kernel(SpectraWork W) {
+  extern __shared__ float smem[];
+  const int BH = BHC > 0 ? BHC : W.plans[0].bh;
+  const int BW = BWC > 0 ? BWC : W.plans[0].bw;
+  const int K = BW / 2 + 1;
+  constexpr int CAPH = BHC > 0 ? BHC : nf::kMaxProject;
+  constexpr int CAPW = BWC > 0 ? BWC : nf::kMaxProject;
+  constexpr int UH = BHC > 0 ? CAPH : 1, UW = BWC > 0 ? CAPW : 1;
+  constexpr bool kCodelet = BHC == BWC && (BWC == 8 || BWC == 16 || BWC == 32);
+
+  const int item = blockIdx.x;
+  int lo = 0, hi = W.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (W.item_base[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  __shared__ SpectraJob sJ;
+  __shared__ DevPlan sP;
+  if (threadIdx.x == 0) {
+    sJ = W.jobs[lo];
+    sP = W.plans[sJ.plan];
+  }
+  __syncthreads();
+  const DevPlan& P = sP;
+  const bool codelet = kCodelet || (BHC == 0 && P.codelet != 0);
+  const DevAxis gx = P.gx, gy = P.gy;
+  const int local = item - W.item_base[lo];
+  const int by = local / sJ.chunks_x, chunk = local - by * sJ.chunks_x;
+  const int nbc = W.nbc;
+  const int bx0 = chunk * nbc, nb = min(nbc, gx.count - bx0);
+  const int oy = by * gy.step, cx0 = bx0 * gx.step;
+  const int win = (nb - 1) * gx.step + BW;
+  const int pitch = ((nbc - 1) * gx.step + BW + 3) & ~3;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+
+  float* wxa = smem;
+  float* wya = wxa + BW;
+  float* ring = smem + ((BW + BH + 3) & ~3);
+  cf* spec = reinterpret_cast<cf*>(ring + size_t(BH) * pitch);
+  for (int i = tid; i < BW; i += nthr) wxa[i] = P.wxa[i];
+  for (int i = tid; i < BH; i += nthr) wya[i] = P.wya[i];
+  bool bad = false;
+  // stage the block row's samples (decoded, reflected) with coalesced loads
+  for (int i = tid; i < BH * win; i += nthr) {
+    const int y = i / win, xx = i - y * win;
+    const unsigned char* srow = sJ.src + ptrdiff_t(reflect_axis(oy + y, gy)) * sJ.src_stride;
+    const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
+    const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
+    if (!isfin(v)) bad = true;
+    ring[size_t(y) * pitch + xx] = v;
+  }
+  __syncthreads();
+  for (int task = tid; task < nb * BH; task += nthr) {
+    const int y = task / nb, b = task - y * nb;
+    const float* in = ring + size_t(y) * pitch + b * gx.step;
+    float row[CAPW];
+#pragma unroll UW
+    for (int x = 0; x < CAPW; ++x)
+      if (x < BW) row[x] = fmul(fmul(in[x], wya[y]), wxa[x]);
+    nf::row_forward<BWC>(row, BW, spec + size_t(y) * K * nbc + b, P.tww, codelet, nbc);
+  }
+  __syncthreads();
+  const size_t cnt = size_t(gx.count);
+  cf* out = sJ.out + size_t(by) * P.bins * cnt + bx0;
+  for (int task = tid; task < nb * K; task += nthr) {
+    const int k = task / nb, b = task - k * nb;
+    cf col[CAPH];
+    const cf* sp = spec + size_t(k) * nbc + b;
+#pragma unroll UH
+    for (int y = 0; y < CAPH; ++y)
+      if (y < BH) col[y] = sp[size_t(y) * K * nbc];
+    nf::fft_1d<true, BHC>(col, BH, P.twh, codelet);
+#pragma unroll UH
+    for (int y = 0; y < CAPH; ++y)
+      if (y < BH) out[size_t(y * K + k) * cnt + b] = col[y];
+  }
+  if (bad) atomicOr(P.err, kErrNonFinite);
+}
+
+// Pass 2: persistent strips over the step's jobs (temporal jobs carry tspec; clip-edge
+// jobs filter their single source frame in pixel mode).
+template <int BHC, int BWC, int STORAGE>
+__global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) temporal_batch_kernel(BatchWork W) {
+  extern __shared__ float smem[];
+  __shared__ int item;
+  const int total = W.job_tile_base[W.njobs];
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) item = atomicAdd(W.counter, 1);
+    __syncthreads();
+    const int t = item;
+    if (t >= total) break;
+    int lo = 0, hi = W.njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (W.job_tile_base[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    __shared__ DevPlan sP;
+    __shared__ PlaneJob sJ;
+    __shared__ StripShape sS;
+    if (threadIdx.x == 0) {
+      sJ = W.jobs[lo];
+      sP = W.plans[sJ.plan];
+      sS = W.shapes[sJ.plan];
+    }
+    __syncthreads();
+    const int local = t - W.job_tile_base[lo];
+    const int sx = local % W.job_tiles_x[lo], sy = local / W.job_tiles_x[lo];
+    if (sJ.tspec) strip_tile<BHC, BWC, STORAGE, true>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+    else strip_tile<BHC, BWC, STORAGE, false>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+  }
+}
+
+} // namespace nfd

@@ -360,6 +360,41 @@ class Batch:
             self._h = None
 
 
+class ClipBatch:
+    """FFT3D temporal clips (bt 2..5) in batched form: `clips` is a list of
+    (plan, frames, dsts) with device tensors; every output frame is filtered with the
+    host layer's frame window (temporal.fft3d_slots). Equal to per-frame process_at."""
+
+    def __init__(self, clips):
+        self._lib = C.load()
+        self._keep = []
+        items = []
+        for plan, frames, dsts in clips:
+            if len(frames) != len(dsts):
+                raise ValueError("frames and dsts differ in length")
+            fa = (C.NfConstPlane * len(frames))(*[_plane(f, True) for f in frames])
+            da = (C.NfPlane * len(dsts))(*[_plane(d, False) for d in dsts])
+            self._keep.append((plan, list(frames), list(dsts), fa, da))
+            items.append(C.NfClipItem(plan._h.value, fa, da, len(frames)))
+        arr = (C.NfClipItem * len(items))(*items)
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_clip_batch_create(arr, len(items), ctypes.byref(self._h), err, 512), err.value)
+
+    def launch(self, graph: bool = False, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        fn = self._lib.nf_clip_batch_graph_launch if graph else self._lib.nf_clip_batch_launch
+        C.raise_for(fn(self._h, ctypes.c_void_p(s), err, 512), err.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.nf_clip_batch_destroy(h)
+            self._h = None
+
+
 def kernel_info() -> dict:
     """KernelInfo (docs/api/en/kernel-info.md): labels of the active implementation."""
     lib = C.load()

@@ -233,70 +233,69 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     if constexpr (TEMPORAL) {
       // FFT3D bt=2..5 (spectral.cpp:90-160): per bin, T-point DFT across the slots'
       // spatial spectra, Wiener per temporal frequency, inverse DFT at the centre
-      // slot; then enhancement with the recovered spectrum's template ratio.
+      // slot; then enhancement with the recovered spectrum's template ratio. The
+      // filter runs element-parallel over (bin, block) so the slots' loads overlap;
+      // the column inverses follow as in pixel mode.
       const int T = P.T, c = T / 2;
       const size_t cnt = size_t(gx.count);
-      const size_t row_base = size_t(by) * bins * cnt;
+      const size_t row_base = size_t(by) * bins * cnt + size_t(bx_lo);
       const float invT = fdiv(1.0f, float(T));
-      for (int base = 0; base < ncol; base += nthr) {
-        const int task = base + tid;
-        const bool active = task < ncol;
-        const int k = active ? task / nbx : 0, b = active ? task - k * nbx : 0;
-        const size_t colp = row_base + size_t(bx_lo + b);
-        cf col[CAPH];
-        if (active && k == 0) dc[b] = J.tspec[c][colp].r;
+      for (int b = tid; b < nbx; b += nthr) dc[b] = J.tspec[c][row_base + b].r;
+      __syncthreads();
+      const int nel = bins * nbx;
+#pragma unroll 2
+      for (int e = tid; e < nel; e += nthr) {
+        const int kk = e / nbx, b = e - kk * nbx;
+        const size_t at = row_base + size_t(kk) * cnt + b;
+        cf v[5];
+        for (int j = 0; j < T; ++j) v[j] = J.tspec[j][at];
+        const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
+        if (grid && !isfin(g)) bad = true;
+        const cf M = grid ? cf{fmul(g, grid[kk].r), fmul(g, grid[kk].i)} : cf{0.0f, 0.0f};
+        const cf gT = {fmul(M.r, float(T)), fmul(M.i, float(T))};
+        const float noise = filt.primary ? fmul(filt.primary[kk], P.noise_mult) : P.noise_uniform;
+        if (!isfin(noise)) bad = true;
+        cf yv = {0.0f, 0.0f};
+        for (int m = 0; m < T; ++m) {
+          cf F = {0.0f, 0.0f};
+          for (int j = 0; j < T; ++j) F = nf::cadd(F, nf::cmul_plain(v[j], P.tfwd[m * T + j]));
+          const cf R = m == 0 ? nf::csub(F, gT) : F;
+          const float power = fadd(fmul(R.r, R.r), fmul(R.i, R.i));
+          if (!isfin(power)) bad = true;
+          const float q = fadd(power, 1e-15f);
+          const float gr = fdiv(fsub(q, noise), q);
+          const float gain = gr < P.lower ? P.lower : gr;
+          cf Rf = {fmul(gain, R.r), fmul(gain, R.i)};
+          if (m == 0) Rf = nf::cadd(Rf, gT);
+          yv = nf::cadd(yv, nf::cmul_plain(Rf, P.tinv[m]));
+        }
+        spec[size_t(kk) * NB + b] = {fmul(yv.r, invT), fmul(yv.i, invT)};
+      }
+      __syncthreads();
+      if (enh.enh) {
+        for (int b = tid; b < nbx; b += nthr) dc[NB + b] = spec[b].r;  // recovered DC
         __syncthreads();
-        if (active) {
-          const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
-          if (grid && !isfin(g)) bad = true;
-#pragma unroll UH
-          for (int y = 0; y < CAPH; ++y) {
-            if (y < BH) {
-              const int kk = y * K + k;
-              const size_t at = colp + size_t(kk) * cnt;
-              cf v[5];
-              for (int j = 0; j < T; ++j) v[j] = J.tspec[j][at];
-              const cf M = grid ? cf{fmul(g, grid[kk].r), fmul(g, grid[kk].i)} : cf{0.0f, 0.0f};
-              const cf gT = {fmul(M.r, float(T)), fmul(M.i, float(T))};
-              const float noise = filt.primary ? fmul(filt.primary[kk], P.noise_mult) : P.noise_uniform;
-              if (!isfin(noise)) bad = true;
-              cf yv = {0.0f, 0.0f};
-              for (int m = 0; m < T; ++m) {
-                cf F = {0.0f, 0.0f};
-                for (int j = 0; j < T; ++j) F = nf::cadd(F, nf::cmul_plain(v[j], P.tfwd[m * T + j]));
-                const cf R = m == 0 ? nf::csub(F, gT) : F;
-                const float power = fadd(fmul(R.r, R.r), fmul(R.i, R.i));
-                if (!isfin(power)) bad = true;
-                const float q = fadd(power, 1e-15f);
-                const float gr = fdiv(fsub(q, noise), q);
-                const float gain = gr < P.lower ? P.lower : gr;
-                cf Rf = {fmul(gain, R.r), fmul(gain, R.i)};
-                if (m == 0) Rf = nf::cadd(Rf, gT);
-                yv = nf::cadd(yv, nf::cmul_plain(Rf, P.tinv[m]));
-              }
-              col[y] = {fmul(yv.r, invT), fmul(yv.i, invT)};
-            }
-          }
-          if (k == 0) dc[NB + b] = col[0].r;
-        }
-        if (enh.enh) {
-          __syncthreads();
-          if (active) {
-            const float g2 = grid ? fdiv(fmul(P.mean_scale, dc[NB + b]), grid0) : 0.0f;
-#pragma unroll UH
-            for (int y = 0; y < CAPH; ++y)
-              if (y < BH) col[y] = spectral_bin(col[y], grid, y * K + k, g2, enh, bad);
-          }
-        }
-        if (active) {
-          nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
-          cf* sp = spec + size_t(k) * NB + b;
-#pragma unroll UH
-          for (int y = 0; y < CAPH; ++y)
-            if (y < BH) sp[size_t(y) * K * NB] = col[y];
+        for (int e = tid; e < nel; e += nthr) {
+          const int kk = e / nbx, b = e - kk * nbx;
+          const float g2 = grid ? fdiv(fmul(P.mean_scale, dc[NB + b]), grid0) : 0.0f;
+          cf* sp = spec + size_t(kk) * NB + b;
+          *sp = spectral_bin(*sp, grid, kk, g2, enh, bad);
         }
         __syncthreads();
       }
+      for (int task = tid; task < ncol; task += nthr) {
+        const int k = task / nbx, b = task - k * nbx;
+        cf col[CAPH];
+        cf* sp = spec + size_t(k) * NB + b;
+#pragma unroll UH
+        for (int y = 0; y < CAPH; ++y)
+          if (y < BH) col[y] = sp[size_t(y) * K * NB];
+        nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
+#pragma unroll UH
+        for (int y = 0; y < CAPH; ++y)
+          if (y < BH) sp[size_t(y) * K * NB] = col[y];
+      }
+      __syncthreads();
     } else {
     for (int base = 0; base < ncol; base += nthr) {
       const int task = base + tid;

@@ -4,13 +4,15 @@
 
 Workloads (one plane per launch, seeded synthetic content):
   dft16    DFTTest sbsize 16 / sosize 12, ftype 0, sigma 8 flat curve, u16 1920x1080
-  dft16_batch the same configuration as one batched launch over 4 YUV420 frames
-           (4 x 1920x1080 + 8 x 960x540 planes)
+  dft16_batch the same configuration as one batched launch over --frames YUV420 frames
+           (default 4: 4 x 1920x1080 + 8 x 960x540 planes)
   dft16_4k the same on a u16 3840x2160 plane (input+output larger than L2)
   fft3d32  FFT3D bw=bh=32, ow=oh=16, sigma 2, u8 640x360
   fft3d48  FFT3D bt=3 bw=bh=48, ow=oh=24, sigma 3, sharpen 0.3, u16 (10-bit) 3840x2160
   kalman32 FFT3D bt=0 (Kalman advance), bw=bh=32, float 1920x1080
   dft12t5  DFTTest tbsize 5 tmode 1, sbsize 12 / sosize 9, ftype 1, float 1920x1080
+  clip48   FFT3D bt=3 48x48 ow=oh=24 sigma 3 sharpen 0.3, 1920x1080 YUV420P10 clip of 6
+           frames as one clip batch (spectra pass + temporal strips) per launch
   adjoint16 differentiable DFTTest: 16 float 256x256 noisy patches, sbsize 16 / sosize 8,
            ftype 0, learnable table, MSE loss; one forward+backward per launch
 """
@@ -36,6 +38,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="dft16")
     ap.add_argument("--launches", type=int, default=3)
+    ap.add_argument("--frames", type=int, default=4, help="frames of the dft16_batch workload")
     a = ap.parse_args()
     dev = torch.device("cuda", 0)
     wl = a.workload
@@ -49,7 +52,7 @@ def main():
         cfg = DFTConfig(block=16, overlap=12, ftype=0, sigma=8.0, slocation=[0, 8, 1, 8])
         luma, chroma = Plan(1920, 1080, SampleFormat(16), cfg), Plan(960, 540, SampleFormat(16), cfg)
         items = []
-        for f in range(4):
+        for f in range(a.frames):
             for p, (w, h) in ((luma, (1920, 1080)), (chroma, (960, 540)), (chroma, (960, 540))):
                 s_ = torch.from_numpy(_plane(h, w, np.uint16, 4096, 60000, f)).to(dev)
                 items.append((p, s_, torch.empty_like(s_)))
@@ -87,6 +90,22 @@ def main():
         blocks = temporal_blocks(4, 9, 5, 0)
         srcs = [clip[s] for b in blocks for s in b["slots"]]
         targets = [b["target"] for b in blocks]
+    elif wl == "clip48":
+        from . import ClipBatch
+        cfg = FFT3DConfig(bw=48, bh=48, ow=24, oh=24, bt=3, sigma=3.0, sharpen=0.3)
+        pls = [Plan(1920, 1080, SampleFormat(10), cfg), Plan(960, 540, SampleFormat(10, chroma=True), cfg)]
+        clips = []
+        for p in range(3):
+            pw, ph = (1920, 1080) if p == 0 else (960, 540)
+            fr = [torch.from_numpy(_plane(ph, pw, np.uint16, 64, 940, 10 * p + f)).to(dev) for f in range(6)]
+            clips.append((pls[min(p, 1)], fr, [torch.empty_like(x) for x in fr]))
+        cb = ClipBatch(clips)
+        for _ in range(a.launches):
+            cb.launch()
+        torch.cuda.synchronize()
+        for p in pls:
+            p.sync_status()
+        return
     elif wl == "adjoint16":
         import sys
         from pathlib import Path

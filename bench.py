@@ -289,7 +289,7 @@ def run_ours(args):
         chroma.process([pin_in[f][2].numpy()], pin_out[f][2].numpy())
     host_plane_value = FRAMES * W * H / (time.perf_counter() - t0) / 1e6
 
-    train = differentiable_pass(args, dev)
+    train = differentiable_pass(args, dev, world)
     configs = other_configs(args, dev) if world == 1 else None
     cpu = cpu_baseline() if (rank == 0 and world == 1) else None
     if world > 1:
@@ -328,7 +328,7 @@ def run_ours(args):
     print(json.dumps(line))
 
 
-def differentiable_pass(args, dev):
+def differentiable_pass(args, dev, world=1):
     """Differentiable DFTTest: 16 float32 256x256 noisy patches, sbsize 16 / sosize 8, ftype 0,
     learnable 16x9 table; loss = MSE to the clean patches. Times the forward alone and
     forward+backward (gradients w.r.t. pixels and table) with CUDA events around each
@@ -336,7 +336,7 @@ def differentiable_pass(args, dev):
     import torch
 
     from neo_fft_b200 import DFTConfig
-    from neo_fft_b200.autograd import SigmaTableDenoiser
+    from neo_fft_b200.autograd import SigmaTableDenoiser, allreduce_table_grad
     sys.path.insert(0, str(ROOT))
     from tests.synth import noisy_patches
     n, s = 16, 256
@@ -354,6 +354,8 @@ def differentiable_pass(args, dev):
         x = x0.detach().requires_grad_()
         m.table.grad = None
         ((m(x) - cl) ** 2).mean().backward()
+        if world > 1:  # data-parallel step: one all-reduce of the 144-float table gradient
+            allreduce_table_grad(m)
 
     def measure(fn, steps):
         for _ in range(max(3, args.warmup)):

@@ -112,9 +112,18 @@ def shard(n: int, rank: int, world: int) -> range:
     return range(min(n, rank * per), min(n, (rank + 1) * per))
 
 
-def allreduce_table_grad(module: SigmaTableDenoiser, group=None) -> None:
-    """Sum the table gradient over data-parallel ranks (one NCCL all-reduce of
-    sbsize*(sbsize//2+1) floats per step); pixel gradients stay local."""
+def allreduce_grad(grad: torch.Tensor, group=None) -> torch.Tensor:
+    """Sum a gradient tensor over the ranks of `group` in place (NCCL for CUDA tensors,
+    gloo for CPU ones); a no-op outside torch.distributed."""
     import torch.distributed as dist
-    if module.table.grad is not None and dist.is_initialized():
-        dist.all_reduce(module.table.grad, op=dist.ReduceOp.SUM, group=group)
+    if dist.is_available() and dist.is_initialized():
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+    return grad
+
+
+def allreduce_table_grad(module: SigmaTableDenoiser, group=None) -> None:
+    """Data-parallel step: sum the table gradient over the ranks (one all-reduce of
+    sbsize*(sbsize//2+1) floats per step); pixel gradients stay local. Each rank's loss
+    must be normalised by the global batch, so that the sum is the full-batch gradient."""
+    if module.table.grad is not None:
+        allreduce_grad(module.table.grad, group)

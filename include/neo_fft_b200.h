@@ -177,15 +177,18 @@ nf_status nf_batch_launch(nf_batch* batch, void* stream, char* err, size_t err_l
 nf_status nf_batch_graph_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
 void nf_batch_destroy(nf_batch* batch);
 
-/* FFT3D temporal clips (bt 2..5) in batched form: every output frame of every clip,
- * frame n filtered from frames n-bt/2 .. n+(bt-1)/2, or from frame n alone where that
- * window leaves the clip (the host layer's rule, filter.hpp:407-421). Each frame's
- * spatial spectra are computed once into a device ring of bt frame spectra per clip
- * plane (the reference caches them in SpectraCache, plan.cpp:437-447); results equal
- * one nf_plan_process_device call per output frame bit for bit. Items must share the
- * block shape and sample storage; planes must stay allocated while the batch is used,
- * and outputs must not overlap any frame of their clip. No reference counterpart: the
- * reference filters one frame per call. */
+/* Temporal clips in batched form: every output frame of every clip, with the host
+ * layer's frame selection, equal bit for bit to one nf_plan_process_device call per
+ * output frame. No reference counterpart: the reference filters one frame per call.
+ *  - FFT3D bt 2..5: frame n from frames n-bt/2 .. n+(bt-1)/2, or from frame n alone
+ *    where that window leaves the clip (filter.hpp:407-421). Each frame's spatial
+ *    spectra are computed once into a device ring of bt frame spectra per clip plane
+ *    (the reference caches them in SpectraCache, plan.cpp:437-447).
+ *  - DFTTest tmode 1 with tosize 0 and smode 1 (clips of at least tbsize frames): the
+ *    temporal blocks of temporal_grid.hpp:5-40 each serve tbsize output frames, so each
+ *    block's volume is transformed and filtered once for all of them.
+ * Items must share the algorithm, block shape and sample storage; planes must stay
+ * allocated while the batch is used, and outputs must not overlap any frame of their clip. */
 typedef struct nf_clip_batch nf_clip_batch;
 typedef struct nf_clip_item {
   const nf_plan* plan;

@@ -22,11 +22,14 @@ NF_DECLARE_SPATIAL(48, 48)
 NF_DECLARE_SPATIAL(0, 0)
 #undef NF_DECLARE_SPATIAL
 struct SpectraWork;
+struct VolumeSpectraWork;
 #define NF_DECLARE_TEMPORAL(BH, BW)                                                                             \
   cudaError_t launch_spectra_batch_##BH##x##BW(int storage, const SpectraWork& w, int items, size_t smem,        \
                                                cudaStream_t st);                                                \
-  cudaError_t launch_temporal_batch_##BH##x##BW(int storage, const BatchWork& w, int ctas, size_t smem,          \
-                                                cudaStream_t st);
+  cudaError_t launch_volume_spectra_batch_##BH##x##BW(int storage, const VolumeSpectraWork& w, int items,       \
+                                                      size_t smem, cudaStream_t st);                            \
+  cudaError_t launch_temporal_batch_##BH##x##BW(int storage, int slice, const BatchWork& w, int ctas,            \
+                                                size_t smem, cudaStream_t st);
 NF_DECLARE_TEMPORAL(8, 8)
 NF_DECLARE_TEMPORAL(16, 16)
 NF_DECLARE_TEMPORAL(32, 32)

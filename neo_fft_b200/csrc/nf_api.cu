@@ -81,10 +81,12 @@ struct nf_batch {
 // complete). Work lists of every step are built and uploaded once at creation.
 struct nf_clip_batch {
   int bh = 0, bw = 0, storage = 0;
+  int slice = 0;  // 0: FFT3D temporal clips; 1: DFTTest tmode 1 slice form
   size_t smem1 = 0, smem2 = 0;
   int nbc = 1, ctas2 = 1;
   struct Step {
     nfd::SpectraWork w1{};
+    nfd::VolumeSpectraWork w1v{};
     int items1 = 0;
     nfd::BatchWork w2{};
     int tiles2 = 0;
@@ -512,19 +514,34 @@ cudaError_t launch_spectra_shape(int bh, int bw, int storage, const nfd::Spectra
   return nfd::launch_spectra_batch_0x0(storage, w, items, smem, st);
 }
 
-cudaError_t launch_temporal_shape(int bh, int bw, int storage, const nfd::BatchWork& w, int ctas, size_t smem,
-                                  cudaStream_t st) {
+cudaError_t launch_volume_spectra_shape(int bh, int bw, int storage, const nfd::VolumeSpectraWork& w, int items,
+                                        size_t smem, cudaStream_t st) {
   if (bh == bw) {
     switch (bw) {
-      case 8: return nfd::launch_temporal_batch_8x8(storage, w, ctas, smem, st);
-      case 16: return nfd::launch_temporal_batch_16x16(storage, w, ctas, smem, st);
-      case 32: return nfd::launch_temporal_batch_32x32(storage, w, ctas, smem, st);
-      case 12: return nfd::launch_temporal_batch_12x12(storage, w, ctas, smem, st);
-      case 48: return nfd::launch_temporal_batch_48x48(storage, w, ctas, smem, st);
+      case 8: return nfd::launch_volume_spectra_batch_8x8(storage, w, items, smem, st);
+      case 16: return nfd::launch_volume_spectra_batch_16x16(storage, w, items, smem, st);
+      case 32: return nfd::launch_volume_spectra_batch_32x32(storage, w, items, smem, st);
+      case 12: return nfd::launch_volume_spectra_batch_12x12(storage, w, items, smem, st);
+      case 48: return nfd::launch_volume_spectra_batch_48x48(storage, w, items, smem, st);
       default: break;
     }
   }
-  return nfd::launch_temporal_batch_0x0(storage, w, ctas, smem, st);
+  return nfd::launch_volume_spectra_batch_0x0(storage, w, items, smem, st);
+}
+
+cudaError_t launch_temporal_shape(int bh, int bw, int storage, int slice, const nfd::BatchWork& w, int ctas,
+                                  size_t smem, cudaStream_t st) {
+  if (bh == bw) {
+    switch (bw) {
+      case 8: return nfd::launch_temporal_batch_8x8(storage, slice, w, ctas, smem, st);
+      case 16: return nfd::launch_temporal_batch_16x16(storage, slice, w, ctas, smem, st);
+      case 32: return nfd::launch_temporal_batch_32x32(storage, slice, w, ctas, smem, st);
+      case 12: return nfd::launch_temporal_batch_12x12(storage, slice, w, ctas, smem, st);
+      case 48: return nfd::launch_temporal_batch_48x48(storage, slice, w, ctas, smem, st);
+      default: break;
+    }
+  }
+  return nfd::launch_temporal_batch_0x0(storage, slice, w, ctas, smem, st);
 }
 
 } // namespace
@@ -990,19 +1007,31 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       const nf_clip_item& it = items[i];
       nfb::require(it.plan != nullptr && it.frames && it.dsts && it.nframes > 0, "invalid clip item");
       const nf_plan& p = *it.plan;
-      nfb::require(p.t.algo == nfb::Algo::FFT3D && !p.t.kalman && p.t.temporal_size >= 2 && p.t.temporal_size <= 5,
-                   "clip batches take FFT3D plans with bt 2..5");
+      const bool fft3d = p.t.algo == nfb::Algo::FFT3D && !p.t.kalman && p.t.temporal_size >= 2 &&
+                         p.t.temporal_size <= 5;
+      const bool dft = p.t.algo == nfb::Algo::DFTTest && p.t.temporal_ola && p.t.temporal_overlap == 0 &&
+                       !p.t.center && p.t.temporal_size >= 2 && p.t.temporal_size <= nfd::kMaxVolumeSlots;
+      nfb::require(fft3d || dft,
+                   "clip batches take FFT3D plans with bt 2..5 or DFTTest plans with tmode 1, tosize 0 and smode 1");
       const int storage = storage_of(p.t.format);
       if (i == 0) {
         b->bh = p.t.bh;
         b->bw = p.t.bw;
         b->storage = storage;
+        b->slice = dft ? 1 : 0;
       }
-      nfb::require(p.t.bh == b->bh && p.t.bw == b->bw && storage == b->storage,
-                   "clip batch items must share block shape and sample storage");
+      nfb::require(p.t.bh == b->bh && p.t.bw == b->bw && storage == b->storage && (dft ? 1 : 0) == b->slice,
+                   "clip batch items must share algorithm, block shape and sample storage");
+      nfb::require(!dft || it.nframes >= p.t.temporal_size, "DFTTest clips must hold at least tbsize frames");
       const size_t elem = size_t(storage);
       for (int f = 0; f < it.nframes; ++f) {
-        validate_call(p, &it.frames[f], 1, nullptr, 0, it.dsts[f]);
+        if (dft) {
+          std::vector<nf_const_plane> block(size_t(p.t.temporal_size), it.frames[f]);
+          const int target = 0;
+          validate_call(p, block.data(), p.t.temporal_size, &target, 1, it.dsts[f]);
+        } else {
+          validate_call(p, &it.frames[f], 1, nullptr, 0, it.dsts[f]);
+        }
         // outputs are written while other outputs still read the clip's frames
         const size_t de = plane_extent(it.dsts[f].width, it.dsts[f].height, it.dsts[f].stride_bytes, elem);
         for (int g = 0; g < it.nframes; ++g)
@@ -1034,19 +1063,25 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
     int max_count = 1, step = plans[0]->t.gx.step;
     for (const nf_plan* p : plans) max_count = std::max(max_count, p->t.gx.count);
     for (const nf_plan* p : plans) step = std::min(step, p->t.gx.step);
+    int tmax = 1;
+    for (const nf_plan* p : plans) tmax = std::max(tmax, p->t.temporal_size);
+    auto pass1_smem = [&](int st, int n) {
+      return b->slice ? nfd::volume_spectra_smem_bytes(b->bh, b->bw, tmax, st, n)
+                      : nfd::spectra_smem_bytes(b->bh, b->bw, st, n);
+    };
     b->nbc = 1;
-    for (int n = 2; n <= std::min(16, max_count); ++n)
-      if (nfd::spectra_smem_bytes(b->bh, b->bw, step, n) <= 100 * 1024) b->nbc = n;
+    for (int n = 2; n <= std::min(b->slice ? 32 : 16, max_count); ++n)
+      if (pass1_smem(step, n) <= 100 * 1024) b->nbc = n;
     b->smem1 = 0;
-    for (const nf_plan* p : plans)
-      b->smem1 = std::max(b->smem1, nfd::spectra_smem_bytes(b->bh, b->bw, p->t.gx.step, b->nbc));
+    for (const nf_plan* p : plans) b->smem1 = std::max(b->smem1, pass1_smem(p->t.gx.step, b->nbc));
     nfb::require(b->smem1 <= 200 * 1024, "block size too large for the spectra pass");
-    // rings: T frame spectra per clip plane that has interior outputs
+    // rings: FFT3D, T frame spectra per clip plane that has interior outputs; DFTTest,
+    // the T filtered slice spectra of one temporal block
     std::vector<size_t> ring_off(static_cast<size_t>(count), SIZE_MAX);
     size_t ring_bytes = 0;
     for (int i = 0; i < count; ++i) {
       const nf_plan& p = *items[i].plan;
-      if (items[i].nframes < p.t.temporal_size) continue;
+      if (!b->slice && items[i].nframes < p.t.temporal_size) continue;
       ring_off[size_t(i)] = ring_bytes;
       const size_t frame = size_t(p.t.gy.count) * p.t.bins * p.t.gx.count * sizeof(cf);
       ring_bytes += ((frame * p.t.temporal_size) + 255) & ~size_t(255);
@@ -1061,8 +1096,10 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
              size_t(f % p.t.temporal_size) * frame;
     };
     int nsteps = 0;
-    for (int i = 0; i < count; ++i)
-      nsteps = std::max(nsteps, items[i].nframes + (items[i].plan->t.temporal_size - 1) / 2);
+    for (int i = 0; i < count; ++i) {
+      const int T = items[i].plan->t.temporal_size;
+      nsteps = std::max(nsteps, b->slice ? (items[i].nframes + T - 1) / T : items[i].nframes + (T - 1) / 2);
+    }
     // slot pointer arrays of all temporal jobs
     std::vector<const cf*> slot_ptrs;
     struct Pass2 {
@@ -1071,10 +1108,43 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       std::vector<int> base{0}, tiles_x;
     };
     std::vector<std::vector<nfd::SpectraJob>> pass1(static_cast<size_t>(nsteps));
+    std::vector<std::vector<nfd::VolumeSpectraJob>> pass1v(static_cast<size_t>(nsteps));
     std::vector<std::vector<int>> pass1_base(static_cast<size_t>(nsteps), std::vector<int>(1, 0));
     std::vector<Pass2> pass2(static_cast<size_t>(nsteps));
     for (int s = 0; s < nsteps; ++s) {
-      for (int i = 0; i < count; ++i) {
+      for (int i = 0; b->slice && i < count; ++i) {
+        // DFTTest: step s is temporal block s, frames T*s .. T*s+T-1 clamped to the clip
+        // (temporal_grid.hpp:5-40 with tosize 0); its outputs are the frames it starts.
+        const nf_clip_item& it = items[i];
+        const nf_plan& p = *it.plan;
+        const int T = p.t.temporal_size, start = T * s;
+        if (start >= it.nframes) continue;
+        const int pi = plan_of[size_t(i)];
+        nfd::VolumeSpectraJob vj{};
+        for (int z = 0; z < T; ++z) {
+          const int f = std::min(std::max(start + z, 0), it.nframes - 1);
+          vj.src[z] = static_cast<const unsigned char*>(it.frames[f].data);
+          vj.src_stride[z] = it.frames[f].stride_bytes;
+          vj.out[z] = frame_spec(i, z);
+        }
+        vj.plan = pi;
+        vj.chunks_x = (p.t.gx.count + b->nbc - 1) / b->nbc;
+        pass1v[size_t(s)].push_back(vj);
+        pass1_base[size_t(s)].push_back(pass1_base[size_t(s)].back() + vj.chunks_x * p.t.gy.count);
+        Pass2& q = pass2[size_t(s)];
+        const nfd::StripShape& S = shapes[size_t(pi)];
+        const int tx = (p.t.gx.length + S.tw - 1) / S.tw, ty = (p.t.gy.length + S.th - 1) / S.th;
+        for (int z = 0; z < T && start + z < it.nframes; ++z) {
+          const int n = start + z;
+          q.jobs.push_back({nullptr, 0, static_cast<unsigned char*>(it.dsts[n].data),
+                            (long long)it.dsts[n].stride_bytes, nullptr, pi, z, nullptr});
+          q.tspec_index.push_back(slot_ptrs.size());
+          slot_ptrs.push_back(frame_spec(i, z));
+          q.tiles_x.push_back(tx);
+          q.base.push_back(q.base.back() + tx * ty);
+        }
+      }
+      for (int i = 0; !b->slice && i < count; ++i) {
         const nf_clip_item& it = items[i];
         const nf_plan& p = *it.plan;
         const int bt = p.t.temporal_size, left = bt / 2, right = (bt - 1) / 2;
@@ -1090,7 +1160,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
         const bool fallback = it.nframes < bt || t < left || it.nframes - 1 - t < right;
         nfd::PlaneJob job{fallback ? static_cast<const unsigned char*>(it.frames[t].data) : nullptr,
                           (long long)it.frames[t].stride_bytes, static_cast<unsigned char*>(it.dsts[t].data),
-                          (long long)it.dsts[t].stride_bytes, nullptr, pi, nullptr};
+                          (long long)it.dsts[t].stride_bytes, nullptr, pi, 0, nullptr};
         Pass2& q = pass2[size_t(s)];
         q.jobs.push_back(job);
         if (fallback) {
@@ -1124,6 +1194,9 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       if (!pass1[size_t(s)].empty()) {
         o.j1 = blob.add(pass1[size_t(s)]);
         o.b1 = blob.add(pass1_base[size_t(s)]);
+      } else if (!pass1v[size_t(s)].empty()) {
+        o.j1 = blob.add(pass1v[size_t(s)]);
+        o.b1 = blob.add(pass1_base[size_t(s)]);
       }
       Pass2& q = pass2[size_t(s)];
       for (size_t j = 0; j < q.jobs.size(); ++j)
@@ -1148,12 +1221,19 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
     for (int s = 0; s < nsteps; ++s) {
       auto& st = b->steps[size_t(s)];
       const Offsets& o = offs[size_t(s)];
-      if (o.j1 != SIZE_MAX) {
+      if (o.j1 != SIZE_MAX && !b->slice) {
         st.w1.plans = reinterpret_cast<const nfd::DevPlan*>(base + o_p);
         st.w1.jobs = reinterpret_cast<const nfd::SpectraJob*>(base + o.j1);
         st.w1.item_base = reinterpret_cast<const int*>(base + o.b1);
         st.w1.njobs = int(pass1[size_t(s)].size());
         st.w1.nbc = b->nbc;
+        st.items1 = pass1_base[size_t(s)].back();
+      } else if (o.j1 != SIZE_MAX) {
+        st.w1v.plans = reinterpret_cast<const nfd::DevPlan*>(base + o_p);
+        st.w1v.jobs = reinterpret_cast<const nfd::VolumeSpectraJob*>(base + o.j1);
+        st.w1v.item_base = reinterpret_cast<const int*>(base + o.b1);
+        st.w1v.njobs = int(pass1v[size_t(s)].size());
+        st.w1v.nbc = b->nbc;
         st.items1 = pass1_base[size_t(s)].back();
       }
       if (o.j2 != SIZE_MAX) {
@@ -1180,12 +1260,14 @@ nf_status nf_clip_batch_launch(nf_clip_batch* b, void* stream, char* err, size_t
   cudaError_t e = cudaMemsetAsync(b->counters, 0, sizeof(int) * b->steps.size(), st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
   for (const auto& s : b->steps) {
-    if (s.items1 > 0 && (e = launch_spectra_shape(b->bh, b->bw, b->storage, s.w1, s.items1, b->smem1, st)) !=
-                            cudaSuccess)
-      return cuda_fail(err, len, e, "kernel launch failed");
+    if (s.items1 > 0) {
+      e = b->slice ? launch_volume_spectra_shape(b->bh, b->bw, b->storage, s.w1v, s.items1, b->smem1, st)
+                   : launch_spectra_shape(b->bh, b->bw, b->storage, s.w1, s.items1, b->smem1, st);
+      if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+    }
     if (s.w2.njobs > 0) {
       const int ctas = std::max(1, std::min(b->ctas2, s.tiles2));
-      if ((e = launch_temporal_shape(b->bh, b->bw, b->storage, s.w2, ctas, b->smem2, st)) != cudaSuccess)
+      if ((e = launch_temporal_shape(b->bh, b->bw, b->storage, b->slice, s.w2, ctas, b->smem2, st)) != cudaSuccess)
         return cuda_fail(err, len, e, "kernel launch failed");
     }
   }

@@ -24,8 +24,16 @@ cudaError_t spectra(const SpectraWork& w, int items, size_t smem, cudaStream_t s
   return cudaGetLastError();
 }
 template <int ST>
+cudaError_t volume_spectra(const VolumeSpectraWork& w, int items, size_t smem, cudaStream_t st) {
+  auto k = volume_spectra_batch_kernel<NF_BH, NF_BW, ST>;
+  cudaError_t e = prepare(k, smem);
+  if (e != cudaSuccess) return e;
+  k<<<items, 256, smem, st>>>(w);
+  return cudaGetLastError();
+}
+template <int ST, int SRC>
 cudaError_t temporal(const BatchWork& w, int ctas, size_t smem, cudaStream_t st) {
-  auto k = temporal_batch_kernel<NF_BH, NF_BW, ST>;
+  auto k = temporal_batch_kernel<NF_BH, NF_BW, ST, SRC>;
   cudaError_t e = prepare(k, smem);
   if (e != cudaSuccess) return e;
   k<<<ctas, 256, smem, st>>>(w);
@@ -41,11 +49,22 @@ cudaError_t temporal(const BatchWork& w, int ctas, size_t smem, cudaStream_t st)
     if (storage == kStoreU16) return spectra<kStoreU16>(w, items, smem, st);                                     \
     return spectra<kStoreF32>(w, items, smem, st);                                                                \
   }                                                                                                              \
-  cudaError_t launch_temporal_batch_##BH##x##BW(int storage, const BatchWork& w, int ctas, size_t smem,          \
-                                                cudaStream_t st) {                                               \
-    if (storage == kStoreU8) return temporal<kStoreU8>(w, ctas, smem, st);                                       \
-    if (storage == kStoreU16) return temporal<kStoreU16>(w, ctas, smem, st);                                     \
-    return temporal<kStoreF32>(w, ctas, smem, st);                                                                \
+  cudaError_t launch_volume_spectra_batch_##BH##x##BW(int storage, const VolumeSpectraWork& w, int items,       \
+                                                      size_t smem, cudaStream_t st) {                            \
+    if (storage == kStoreU8) return volume_spectra<kStoreU8>(w, items, smem, st);                                \
+    if (storage == kStoreU16) return volume_spectra<kStoreU16>(w, items, smem, st);                              \
+    return volume_spectra<kStoreF32>(w, items, smem, st);                                                         \
+  }                                                                                                              \
+  cudaError_t launch_temporal_batch_##BH##x##BW(int storage, int slice, const BatchWork& w, int ctas,            \
+                                                size_t smem, cudaStream_t st) {                                  \
+    if (slice) {                                                                                                 \
+      if (storage == kStoreU8) return temporal<kStoreU8, kSrcSlice>(w, ctas, smem, st);                          \
+      if (storage == kStoreU16) return temporal<kStoreU16, kSrcSlice>(w, ctas, smem, st);                        \
+      return temporal<kStoreF32, kSrcSlice>(w, ctas, smem, st);                                                   \
+    }                                                                                                            \
+    if (storage == kStoreU8) return temporal<kStoreU8, kSrcTemporal>(w, ctas, smem, st);                         \
+    if (storage == kStoreU16) return temporal<kStoreU16, kSrcTemporal>(w, ctas, smem, st);                       \
+    return temporal<kStoreF32, kSrcTemporal>(w, ctas, smem, st);                                                  \
   }
 NF_DEFINE(NF_BH, NF_BW)
 } // namespace nfd

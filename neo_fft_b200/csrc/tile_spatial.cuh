@@ -68,10 +68,17 @@ struct PlaneJob {
   long long dst_stride;
   const cf* kalman_L;
   int plan;  // index into the batch's plan table
-  // FFT3D temporal form: T spatial spectra (slot order, layout [block row][bin][block
-  // column]) computed beforehand; the strip filters across them instead of reading pixels.
+  int zt;    // DFTTest slice form: the output's slice of its temporal block
+  // Spectra computed beforehand, layout [block row][bin][block column]: FFT3D temporal
+  // form, the T slots' spatial spectra (the strip filters across them); DFTTest slice
+  // form, tspec[0] = the filtered spatial spectrum of slice zt (the strip reconstructs it).
   const cf* const* tspec;
 };
+
+// Source of a strip's block spectra.
+constexpr int kSrcPixels = 0;    // source pixels (or a Kalman estimate)
+constexpr int kSrcTemporal = 1;  // FFT3D bt=2..5 slot spectra, filtered across time here
+constexpr int kSrcSlice = 2;     // DFTTest tmode 1 filtered slice spectra
 
 struct StripShape {
   int tw, th;     // strip width and segment height (plane pixels)
@@ -102,7 +109,7 @@ __host__ __device__ inline size_t strip_smem_bytes(int bh, int bw, const StripSh
                           size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max));
 }
 
-template <int BHC, int BWC, int STORAGE, bool TEMPORAL = false>
+template <int BHC, int BWC, int STORAGE, int SRC = kSrcPixels>
 __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, const StripShape& S, int px0, int py0,
                                            float* smem) {
   const int BH = BHC > 0 ? BHC : P.bh;
@@ -157,7 +164,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     wxs = stage(P.wxs, BW);
     wys = stage(P.wys, BH);
   } else {
-    h = stage(P.h, BH * BW);
+    h = stage(P.h + (SRC == kSrcSlice ? size_t(J.zt) * BH * BW : 0), BH * BW);
     hsyn = stage(P.hsyn, BH * BW);
   }
   (void)t_wa;
@@ -181,12 +188,16 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   __syncthreads();
   const float grid0 = grid ? grid[0].r : 1.0f;
   const float fct = fdiv(1.0f, fmul(float(BW), float(BH)));
+  // DFTTest slice form: 3-D normalisation and the temporal-OLA synthesis weight
+  // volume * h[zt] (plan.cpp:594-601).
+  const float fct3 = fdiv(1.0f, fmul(fmul(float(P.T), float(BH)), float(BW)));
+  const float volume = fmul(fmul(float(P.T), float(BW)), float(BH));
   const bool vec4 = (gx.step & 3) == 0 && (BW & 3) == 0;
 
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
     __syncthreads();
-    if (!TEMPORAL && !kalman_L) {
+    if (SRC == kSrcPixels && !kalman_L) {
       // ---- 0: stage the rows this block row adds ----------------------------
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
       const int nrows = oy + BH - r0;
@@ -230,7 +241,24 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     }
     // ---- B: column forward, filter, column inverse --------------------------
     const int ncol = nbx * K;
-    if constexpr (TEMPORAL) {
+    if constexpr (SRC == kSrcSlice) {
+      // DFTTest tmode 1 (plan.cpp:544-601): the slice's spectrum was filtered in 3-D by
+      // the volume pass; only the column inverses remain.
+      const cf* S = J.tspec[0] + size_t(by) * bins * size_t(gx.count) + size_t(bx_lo);
+      for (int task = tid; task < ncol; task += nthr) {
+        const int k = task / nbx, b = task - k * nbx;
+        cf col[CAPH];
+#pragma unroll UH
+        for (int y = 0; y < CAPH; ++y)
+          if (y < BH) col[y] = S[size_t(y * K + k) * gx.count + b];
+        nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
+        cf* sp = spec + size_t(k) * NB + b;
+#pragma unroll UH
+        for (int y = 0; y < CAPH; ++y)
+          if (y < BH) sp[size_t(y) * K * NB] = col[y];
+      }
+      __syncthreads();
+    } else if constexpr (SRC == kSrcTemporal) {
       // FFT3D bt=2..5 (spectral.cpp:90-160): per bin, T-point DFT across the slots'
       // spatial spectra, Wiener per temporal frequency, inverse DFT at the centre
       // slot; then enhancement with the recovered spectrum's template ratio. The
@@ -353,13 +381,15 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const int y = task / nbx, b = task - y * nbx;
       if (P.center && y != BH / 2) continue;
       float row[CAPW];
-      nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, fct, row, P.tww, codelet, NB);
+      nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, SRC == kSrcSlice ? fct3 : fct, row, P.tww, codelet,
+                           NB);
       float* o = ob + (size_t(y) * NB + b) * OBW;
 #pragma unroll UW
       for (int x = 0; x < CAPW; ++x) {
         if (x < BW) {
           if (!isfin(row[x])) bad = true;
-          row[x] = P.algo == 0 ? fmul(row[x], wxs[x]) : fmul(row[x], hsyn[y * BW + x]);
+          if constexpr (SRC == kSrcSlice) row[x] = fmul(fmul(volume, row[x]), h[y * BW + x]);
+          else row[x] = P.algo == 0 ? fmul(row[x], wxs[x]) : fmul(row[x], hsyn[y * BW + x]);
         }
       }
       if ((BW & 3) == 0) {

@@ -119,9 +119,152 @@ __global__ void __launch_bounds__(256) spectra_batch_kernel(SpectraWork W) {
   if (bad) atomicOr(P.err, kErrNonFinite);
 }
 
-// Pass 2: persistent strips over the step's jobs (temporal jobs carry tspec; clip-edge
-// jobs filter their single source frame in pixel mode).
+// DFTTest tmode 1 with tosize 0 (temporal_grid.hpp:5-40): every output frame lies in
+// exactly one temporal block, so a block's volume is transformed, filtered and inverted
+// along time once, and all T filtered slice spectra are kept for the T outputs.
+constexpr int kMaxVolumeSlots = 15;
+struct VolumeSpectraJob {
+  const unsigned char* src[kMaxVolumeSlots];
+  long long src_stride[kMaxVolumeSlots];
+  cf* out[kMaxVolumeSlots];
+  int plan;
+  int chunks_x;
+};
+
+struct VolumeSpectraWork {
+  const DevPlan* plans;
+  const VolumeSpectraJob* jobs;
+  const int* item_base;  // prefix sums of (block rows x chunks) per job (njobs+1)
+  int njobs;
+  int nbc;
+};
+
+// Shared layout (floats): h [T][bh][bw] | ring [bh][pitch] | spec [T][bh][K][nbc] complex
+// | dc [nbc].
+__host__ __device__ inline size_t volume_spectra_smem_bytes(int bh, int bw, int T, int step, int nbc) {
+  const size_t K = size_t(bw / 2 + 1);
+  const size_t win = size_t(nbc - 1) * step + bw;
+  const size_t pitch = (win + 3) & ~size_t(3);
+  const size_t h = (size_t(T) * bh * bw + 3) & ~size_t(3);
+  return sizeof(float) * (h + size_t(bh) * pitch + 2 * size_t(T) * bh * K * nbc + nbc);
+}
+
+// Pass 1 of the DFTTest slice form: per block row chunk, the 3-D forward transform of
+// each volume (spatial per slice, then time; the volume tile's phases A, B1 and T),
+// the spectral filter and the inverse along time; all T slices written out.
 template <int BHC, int BWC, int STORAGE>
+__global__ void __launch_bounds__(256) volume_spectra_batch_kernel(VolumeSpectraWork W) {
+  extern __shared__ float smem[];
+  const int BH = BHC > 0 ? BHC : W.plans[0].bh;
+  const int BW = BWC > 0 ? BWC : W.plans[0].bw;
+  const int K = BW / 2 + 1;
+  constexpr int CAPH = BHC > 0 ? BHC : nf::kMaxProject;
+  constexpr int CAPW = BWC > 0 ? BWC : nf::kMaxProject;
+  constexpr int UH = BHC > 0 ? CAPH : 1, UW = BWC > 0 ? CAPW : 1;
+  constexpr bool kCodelet = BHC == BWC && (BWC == 8 || BWC == 16 || BWC == 32);
+
+  const int item = blockIdx.x;
+  int lo = 0, hi = W.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (W.item_base[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  __shared__ DevPlan sP;
+  __shared__ int s_chunks, s_plan;
+  if (threadIdx.x == 0) {
+    s_plan = W.jobs[lo].plan;
+    s_chunks = W.jobs[lo].chunks_x;
+    sP = W.plans[s_plan];
+  }
+  __syncthreads();
+  const VolumeSpectraJob& J = W.jobs[lo];
+  const DevPlan& P = sP;
+  const bool codelet = kCodelet || (BHC == 0 && P.codelet != 0);
+  const DevAxis gx = P.gx, gy = P.gy;
+  const int T = P.T;
+  const int local = item - W.item_base[lo];
+  const int by = local / s_chunks, chunk = local - by * s_chunks;
+  const int nbc = W.nbc;
+  const int bx0 = chunk * nbc, nb = min(nbc, gx.count - bx0);
+  const int oy = by * gy.step, cx0 = bx0 * gx.step;
+  const int win = (nb - 1) * gx.step + BW;
+  const int pitch = ((nbc - 1) * gx.step + BW + 3) & ~3;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int bins = BH * K;
+  const size_t slot = size_t(bins) * nbc;  // complex per slice in spec
+
+  float* h = smem;
+  float* ring = smem + ((size_t(T) * BH * BW + 3) & ~size_t(3));
+  cf* spec = reinterpret_cast<cf*>(ring + size_t(BH) * pitch);
+  float* dc = reinterpret_cast<float*>(spec + size_t(T) * slot);
+  for (int i = tid; i < T * BH * BW; i += nthr) h[i] = P.h[i];
+  bool bad = false;
+  for (int z = 0; z < T; ++z) {
+    __syncthreads();
+    for (int i = tid; i < BH * win; i += nthr) {
+      const int y = i / win, xx = i - y * win;
+      const unsigned char* srow = J.src[z] + ptrdiff_t(reflect_axis(oy + y, gy)) * J.src_stride[z];
+      const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
+      const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
+      if (!isfin(v)) bad = true;
+      ring[size_t(y) * pitch + xx] = v;
+    }
+    __syncthreads();
+    for (int task = tid; task < nb * BH; task += nthr) {
+      const int y = task / nb, b = task - y * nb;
+      const float* in = ring + size_t(y) * pitch + b * gx.step;
+      float row[CAPW];
+#pragma unroll UW
+      for (int x = 0; x < CAPW; ++x)
+        if (x < BW) row[x] = fmul(in[x], h[(z * BH + y) * BW + x]);
+      nf::row_forward<BWC>(row, BW, spec + size_t(z) * slot + size_t(y) * K * nbc + b, P.tww, codelet, nbc);
+    }
+  }
+  __syncthreads();
+  for (int task = tid; task < T * nb * K; task += nthr) {
+    const int z = task / (nb * K), r = task - z * nb * K, k = r / nb, b = r - k * nb;
+    cf col[CAPH];
+    cf* sp = spec + size_t(z) * slot + size_t(k) * nbc + b;
+#pragma unroll UH
+    for (int y = 0; y < CAPH; ++y)
+      if (y < BH) col[y] = sp[size_t(y) * K * nbc];
+    nf::fft_1d<true, BHC>(col, BH, P.twh, codelet);
+#pragma unroll UH
+    for (int y = 0; y < CAPH; ++y)
+      if (y < BH) sp[size_t(y) * K * nbc] = col[y];
+  }
+  __syncthreads();
+  // forward along time; the volume DC is bin 0 of slice 0 afterwards
+  for (int task = tid; task < bins * nb; task += nthr) {
+    const int kk = task / nb, b = task - kk * nb;
+    cf* bp = spec + size_t(kk) * nbc + b;
+    cf line[kMaxVolumeSlots];
+    for (int z = 0; z < T; ++z) line[z] = bp[size_t(z) * slot];
+    nf::fft_project<true, 0, 16>(line, T, P.twt);
+    for (int z = 0; z < T; ++z) bp[size_t(z) * slot] = line[z];
+    if (kk == 0) dc[b] = line[0].r;
+  }
+  __syncthreads();
+  const size_t cnt = size_t(gx.count);
+  const size_t row_base = size_t(by) * bins * cnt + size_t(bx0);
+  for (int task = tid; task < bins * nb; task += nthr) {
+    const int kk = task / nb, b = task - kk * nb;
+    const cf* bp = spec + size_t(kk) * nbc + b;
+    const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
+                        ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
+    cf line[kMaxVolumeSlots];
+    for (int z = 0; z < T; ++z) line[z] = spectral_bin(bp[size_t(z) * slot], P.grid, z * bins + kk, g, P.filt, bad);
+    nf::fft_project<false, 0, 16>(line, T, P.twt);
+    for (int z = 0; z < T; ++z) J.out[z][row_base + size_t(kk) * cnt + b] = line[z];
+  }
+  if (bad) atomicOr(P.err, kErrNonFinite);
+}
+
+// Pass 2: persistent strips over the step's jobs. FFT3D (SRC = kSrcTemporal): temporal
+// jobs carry tspec, clip-edge jobs filter their single source frame in pixel mode.
+// DFTTest (SRC = kSrcSlice): every job reconstructs one slice spectrum.
+template <int BHC, int BWC, int STORAGE, int SRC>
 __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) temporal_batch_kernel(BatchWork W) {
   extern __shared__ float smem[];
   __shared__ int item;
@@ -149,8 +292,12 @@ __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) temporal
     __syncthreads();
     const int local = t - W.job_tile_base[lo];
     const int sx = local % W.job_tiles_x[lo], sy = local / W.job_tiles_x[lo];
-    if (sJ.tspec) strip_tile<BHC, BWC, STORAGE, true>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
-    else strip_tile<BHC, BWC, STORAGE, false>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+    if constexpr (SRC == kSrcSlice) {
+      strip_tile<BHC, BWC, STORAGE, kSrcSlice>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+    } else {
+      if (sJ.tspec) strip_tile<BHC, BWC, STORAGE, kSrcTemporal>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+      else strip_tile<BHC, BWC, STORAGE, kSrcPixels>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+    }
   }
 }
 

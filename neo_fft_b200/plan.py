@@ -361,9 +361,10 @@ class Batch:
 
 
 class ClipBatch:
-    """FFT3D temporal clips (bt 2..5) in batched form: `clips` is a list of
-    (plan, frames, dsts) with device tensors; every output frame is filtered with the
-    host layer's frame window (temporal.fft3d_slots). Equal to per-frame process_at."""
+    """Temporal clips in batched form: `clips` is a list of (plan, frames, dsts) with
+    device tensors; every output frame is filtered with the host layer's frame selection
+    (FFT3D bt 2..5: temporal.fft3d_slots; DFTTest tmode 1 with tosize 0:
+    temporal.temporal_blocks). Equal to per-frame process_at."""
 
     def __init__(self, clips):
         self._lib = C.load()

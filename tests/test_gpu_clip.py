@@ -1,12 +1,12 @@
-"""FFT3D temporal clips in batched form (nf_clip_batch): every output frame equals one
-nf_plan_process_device call with the host layer's frame window (temporal.fft3d_slots:
-frames n-bt/2 .. n+(bt-1)/2, single frame at the clip edges) bit for bit, and the
-reference core on a sample of frames."""
+"""Temporal clips in batched form (nf_clip_batch): every output frame equals one
+nf_plan_process_device call with the host layer's frame selection bit for bit — FFT3D
+bt 2..5 with temporal.fft3d_slots (frames n-bt/2 .. n+(bt-1)/2, single frame at the clip
+edges), DFTTest tmode 1 with temporal.temporal_blocks — and the reference core."""
 import numpy as np
 import pytest
 
 from neo_fft_b200.plan import ClipBatch, DFTConfig, FFT3DConfig, Plan, SampleFormat
-from neo_fft_b200.temporal import fft3d_slots
+from neo_fft_b200.temporal import fft3d_slots, temporal_blocks
 from tests.synth import plane
 
 pytestmark = pytest.mark.gpu
@@ -77,17 +77,69 @@ def test_clip_batch_matches_reference(cuda, ref):
         assert np.array_equal(dsts[t].cpu().numpy(), exp)
 
 
+def _per_frame_dft(cuda, plan, frames):
+    outs = []
+    for t in range(len(frames)):
+        blocks = temporal_blocks(t, len(frames), plan.temporal_size, 0)
+        o = cuda.empty_like(frames[t])
+        plan.process_at([frames[j] for b in blocks for j in b["slots"]], o, targets=[b["target"] for b in blocks])
+        outs.append(o)
+    return outs
+
+
+@pytest.mark.parametrize("fmt,cfg,n", [
+    (SampleFormat(32, True), DFTConfig(block=12, overlap=9, tbsize=5, temporal_mode=1, ftype=1, sigma=8.0), 12),
+    (SampleFormat(16), DFTConfig(block=16, overlap=8, tbsize=3, temporal_mode=1, ftype=0, sigma=6.0,
+                                 slocation=[0, 4, 0.5, 8, 1, 12]), 7),
+    (SampleFormat(8), DFTConfig(block=8, overlap=4, tbsize=2, temporal_mode=1, ftype=2, sigma=0.7, zmean=0), 5),
+    (SampleFormat(10), DFTConfig(block=10, overlap=5, tbsize=4, temporal_mode=1, ftype=0, sigma=5.0), 6),
+], ids=["f32-t5-b12", "u16-t3-b16-curve", "u8-t2-b8", "u10-t4-b10"])
+def test_dfttest_clip_batch_equals_per_frame(cuda, fmt, cfg, n):
+    w, h = 150, 98
+    plan = Plan(w, h, fmt, cfg)
+    frames = _clip(cuda, n, h, w, fmt, 95)
+    dsts = [cuda.empty_like(f) for f in frames]
+    batch = ClipBatch([(plan, frames, dsts)])
+    for graph in (False, True):
+        for d in dsts:
+            d.fill_(0)
+        batch.launch(graph=graph)
+        for got, exp in zip(dsts, _per_frame_dft(cuda, plan, frames)):
+            assert cuda.equal(got, exp)
+    plan.sync_status()
+
+
+def test_dfttest_clip_batch_matches_reference(cuda, ref):
+    fmt = SampleFormat(32, True)
+    cfg = DFTConfig(block=12, overlap=9, tbsize=5, temporal_mode=1, ftype=1, sigma=8.0)
+    w, h, n = 64, 48, 7
+    plan = Plan(w, h, fmt, cfg)
+    host = [plane(h, w, 32, True, seed=(96, 0, f)) for f in range(n)]
+    frames = [cuda.from_numpy(x).cuda() for x in host]
+    dsts = [cuda.empty_like(f) for f in frames]
+    ClipBatch([(plan, frames, dsts)]).launch()
+    rp = ref.RefPlan(w, h, fmt, cfg)
+    for t in range(n):
+        blocks = temporal_blocks(t, n, 5, 0)
+        exp = rp.process([host[j] for b in blocks for j in b["slots"]], targets=[b["target"] for b in blocks])
+        assert np.array_equal(dsts[t].cpu().numpy(), exp)
+
+
 def test_clip_batch_rejects_invalid_items(cuda):
     fmt = SampleFormat(8)
     fr = _clip(cuda, 4, 64, 96, fmt, 90)
     d = [cuda.empty_like(f) for f in fr]
     with pytest.raises(ValueError, match="bt 2..5"):
         ClipBatch([(Plan(96, 64, fmt, FFT3DConfig(bw=16, bh=16, bt=1)), fr, d)])
-    with pytest.raises(ValueError, match="bt 2..5"):
-        ClipBatch([(Plan(96, 64, fmt, DFTConfig(tbsize=3)), fr, d)])
+    with pytest.raises(ValueError, match="tmode 1, tosize 0"):
+        ClipBatch([(Plan(96, 64, fmt, DFTConfig(tbsize=3)), fr, d)])  # tmode 0
+    with pytest.raises(ValueError, match="tmode 1, tosize 0"):
+        ClipBatch([(Plan(96, 64, fmt, DFTConfig(tbsize=3, temporal_mode=1, temporal_overlap=1)), fr, d)])
+    with pytest.raises(ValueError, match="at least tbsize"):
+        ClipBatch([(Plan(96, 64, fmt, DFTConfig(tbsize=5, temporal_mode=1)), fr, d)])
     p16 = Plan(96, 64, fmt, FFT3DConfig(bw=16, bh=16, bt=3))
     p32 = Plan(96, 64, fmt, FFT3DConfig(bw=32, bh=32, bt=3))
-    with pytest.raises(ValueError, match="share block shape"):
+    with pytest.raises(ValueError, match="share algorithm, block shape"):
         ClipBatch([(p16, fr, d), (p32, fr, [cuda.empty_like(f) for f in fr])])
     with pytest.raises(ValueError):
         ClipBatch([(p16, fr, [fr[1], d[1], d[2], d[3]])])  # an output overlaps a frame of the clip

@@ -141,6 +141,14 @@ nf_status nf_kalman_state_create(const nf_plan* plan, int fp64_variance, nf_kalm
                                  size_t err_len);
 void nf_kalman_state_destroy(nf_kalman_state* state);
 nf_status nf_kalman_state_copy(nf_kalman_state* dst, const nf_kalman_state* src, void* stream);
+/* A new state of the same plan and variance precision holding a copy of `src`
+ * (KalmanState's copy constructor, kernels/kalman.hpp:5-14; checkpoints copy states,
+ * filter.hpp:171). */
+nf_status nf_kalman_state_clone(const nf_kalman_state* src, nf_kalman_state** out, void* stream, char* err,
+                                size_t err_len);
+/* Device bytes held by a state (KalmanState::bytes, used by the checkpoint budget,
+ * runtime/checkpoints.hpp:10-16). */
+size_t nf_kalman_state_bytes(const nf_kalman_state* state);
 nf_status nf_kalman_advance_device(const nf_plan* plan, nf_const_plane source, nf_kalman_state* state, void* stream,
                                    char* err, size_t err_len);
 nf_status nf_kalman_render_device(const nf_plan* plan, nf_const_plane source, nf_plane dst,

@@ -109,10 +109,9 @@ class KalmanState {
     if (o.state_) {
       char err[256] = {0};
       nf_kalman_state* s = nullptr;
-      detail::check(nf_kalman_state_create(o.plan_, 0, &s, err, sizeof(err)), err);
+      detail::check(nf_kalman_state_clone(o.state_, &s, nullptr, err, sizeof(err)), err);
       state_ = s;
       plan_ = o.plan_;
-      nf_kalman_state_copy(state_, o.state_, nullptr);
     }
     return *this;
   }
@@ -124,6 +123,8 @@ class KalmanState {
   }
   ~KalmanState() { reset(); }
   nf_kalman_state* handle() const { return state_; }
+  // KalmanState::bytes (runtime/checkpoints.hpp:13-14 sums them per checkpoint).
+  std::size_t bytes() const { return sizeof(*this) + (state_ ? nf_kalman_state_bytes(state_) : 0); }
 
  private:
   friend class Plan;

@@ -87,6 +87,8 @@ PROTOTYPES = {
     "nf_kalman_state_create": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p), ctypes.c_char_p, c_size_t]),
     "nf_kalman_state_destroy": (None, [c_void_p]),
     "nf_kalman_state_copy": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "nf_kalman_state_clone": (c_int, [c_void_p, ctypes.POINTER(c_void_p), c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_kalman_state_bytes": (c_size_t, [c_void_p]),
     "nf_kalman_advance_device": (c_int, [c_void_p, NfConstPlane, c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_kalman_render_device": (c_int, [c_void_p, NfConstPlane, NfPlane, c_void_p, c_void_p,
                                         ctypes.c_char_p, c_size_t]),

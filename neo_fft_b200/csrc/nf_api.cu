@@ -734,6 +734,23 @@ nf_status nf_kalman_state_copy(nf_kalman_state* dst, const nf_kalman_state* src,
   if (e == cudaSuccess) e = cudaMemcpyAsync(dst->process, src->process, src->count * var, cudaMemcpyDeviceToDevice, st);
   return e == cudaSuccess ? NF_OK : NF_DEVICE_ERROR;
 }
+nf_status nf_kalman_state_clone(const nf_kalman_state* src, nf_kalman_state** out, void* stream, char* err,
+                                size_t len) {
+  if (!src || !out) return fail(err, len, "null state or output pointer", NF_INVALID_ARGUMENT);
+  nf_kalman_state* s = nullptr;
+  nf_status st = nf_kalman_state_create(src->plan, src->fp64, &s, err, len);
+  if (st != NF_OK) return st;
+  if ((st = nf_kalman_state_copy(s, src, stream)) != NF_OK) {
+    nf_kalman_state_destroy(s);
+    return fail(err, len, "state copy failed", st);
+  }
+  *out = s;
+  return NF_OK;
+}
+size_t nf_kalman_state_bytes(const nf_kalman_state* s) {
+  if (!s) return 0;
+  return s->count * (sizeof(cf) + 2 * (s->fp64 ? sizeof(double) : sizeof(float)));
+}
 nf_status nf_kalman_advance_device(const nf_plan* p, nf_const_plane source, nf_kalman_state* state, void* stream,
                                    char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {

@@ -318,6 +318,21 @@ class KalmanState:
         C.raise_for(self._lib.nf_kalman_state_copy(self._h, other._h, ctypes.c_void_p(stream or 0)),
                     b"state copy failed")
 
+    def clone(self, stream=None) -> "KalmanState":
+        """A new device state with the same plan, precision and contents (the copy a
+        checkpoint takes, filter.hpp:171)."""
+        out = KalmanState.__new__(KalmanState)
+        out._lib, out.count = self._lib, self.count
+        out._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_kalman_state_clone(self._h, ctypes.byref(out._h), ctypes.c_void_p(stream or 0),
+                                                    err, 512), err.value)
+        return out
+
+    @property
+    def nbytes(self) -> int:
+        return int(self._lib.nf_kalman_state_bytes(self._h))
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

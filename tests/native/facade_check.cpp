@@ -2,6 +2,7 @@
 // layer does (src/plugin/filter.hpp:349-360: process_at with sources, frame, plane,
 // targets and cache arguments; Kalman initial/advance/render with copied states).
 // Prints FNV-1a checksums of the outputs for comparison with the Python path.
+#include "neo_fft_b200/checkpoints.hpp"
 #include "neo_fft_b200/plan.hpp"
 
 #include <cstdint>
@@ -41,6 +42,20 @@ int main() {
   KalmanState copy = st;  // checkpoint copy (filter.hpp:171)
   kp.render_kalman<float>(fs, fd, copy);
   std::printf("kalman %llu\n", (unsigned long long)fnv(fdst.data(), fdst.size() * 4));
+  // random-access Kalman frames through the checkpoint policy (filter.hpp:152-250)
+  std::vector<std::vector<float>> frames(24, std::vector<float>(fsrc.size()));
+  for (int f = 0; f < 24; ++f)
+    for (std::size_t i = 0; i < fsrc.size(); ++i) frames[f][i] = float((i * 7919 + std::size_t(f) * 104729) % 1000) / 1000.0f;
+  KalmanSeek seek({&kp, nullptr, nullptr, nullptr}, 4);
+  for (int n : {5, 6, 7, 20, 3, 21}) {
+    auto source = [&](int f) { return span2d::Plane<const float>(frames[f].data(), w, h, w * 4); };
+    seek.frame(
+        n, [&](const Plan& p, int, int f, KalmanState& s) { p.advance_kalman<float>(source(f), s); },
+        [&](const Plan* p, int, const KalmanState* s) {
+          if (p && s) p->render_kalman<float>(source(n), fd, *s);
+        });
+    std::printf("seek%d %llu\n", n, (unsigned long long)fnv(fdst.data(), fdst.size() * 4));
+  }
   try {
     FFT3DConfig bad;
     bad.bt = 7;

@@ -98,3 +98,12 @@ def test_cpp_facade_matches_python_path(cuda):
     out_t = cuda.empty_like(d)
     kp.render_kalman(d, out_t, st)
     assert int(got["kalman"]) == fnv(out_t.cpu().numpy().tobytes())
+    # the C++ checkpoint/seek policy equals the Python mirror
+    from neo_fft_b200.checkpoints import KalmanSeek
+    frames = [cuda.from_numpy(((np.arange(w * h, dtype=np.int64) * 7919 + f * 104729) % 1000 / 1000.0)
+                              .astype(np.float32).reshape(h, w)).cuda() for f in range(24)]
+    seek = KalmanSeek([kp], warmup=4)
+    for n in (5, 6, 7, 20, 3, 21):
+        o = cuda.empty_like(frames[0])
+        seek.frame(n, lambda f, p: frames[f], [o])
+        assert int(got[f"seek{n}"]) == fnv(o.cpu().numpy().tobytes()), n

@@ -212,6 +212,20 @@ nf_status nf_clip_batch_launch(nf_clip_batch* batch, void* stream, char* err, si
 nf_status nf_clip_batch_graph_launch(nf_clip_batch* batch, void* stream, char* err, size_t err_len);
 void nf_clip_batch_destroy(nf_clip_batch* batch);
 
+/* Sampled noise models. DFTTest with nlocation (ftype 0/1): DFTNoise
+ * (src/algorithms/dft_noise.cpp:5-41) builds the per-bin primary table from windowed
+ * 3-D power spectra of sample volumes the host layer gathers (filter.hpp:476-490):
+ * `slices` holds nlocations x tbsize x sbsize x sbsize floats in 8-bit amplitude units.
+ * nf_dft_noise_power computes the table (tbsize * bins floats) on the host, as the
+ * reference does once per filter; nf_plan_set_noise_model publishes it to a plan (every
+ * plan of the filter shares one model). Processing before publication fails with the
+ * reference's "DFTTest sample model not initialized".
+ * nf_plan_model_state: 0 = plan has no sampled model, 1 = waiting for it, 2 = ready. */
+nf_status nf_dft_noise_power(const nf_dft_config* config, const float* slices, int nlocations, float* power,
+                             int count, char* err, size_t err_len);
+nf_status nf_plan_set_noise_model(nf_plan* plan, const float* power, int count, char* err, size_t err_len);
+int nf_plan_model_state(const nf_plan* plan);
+
 /* Differentiable form (no reference counterpart; the reference has no gradients).
  * DFTTest plans keep their per-bin primary table A ([tbsize][sbsize][sbsize/2+1],
  * already calibrated: the threshold the Wiener gain compares with) in device memory.

@@ -20,7 +20,9 @@
 #include <array>
 #include <complex>
 #include <cstdint>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <optional>
 #include <stdexcept>
 #include <string>
@@ -82,6 +84,24 @@ struct Geometry {
 };
 
 namespace detail {
+inline nf_dft_config to_c(const DFTConfig& c, std::vector<int>& loc) {
+  nf_dft_config n{};
+  n.block = c.block; n.overlap = c.overlap; n.mode = c.mode; n.swin = c.swin; n.twin = c.twin;
+  n.ftype = c.ftype; n.opt = c.opt; n.tbsize = c.tbsize; n.sbeta = c.sbeta; n.tbeta = c.tbeta;
+  n.sigma = c.sigma; n.sigma2 = c.sigma2; n.pmin = c.pmin; n.pmax = c.pmax; n.f0beta = c.f0beta;
+  n.zmean = c.zmean; n.temporal_mode = c.temporal_mode; n.temporal_overlap = c.temporal_overlap;
+  n.dither = c.dither; n.dither_seed = c.dither_seed;
+  n.slocation = c.curves.shared.data(); n.n_slocation = int(c.curves.shared.size());
+  n.ssx = c.curves.x.data(); n.n_ssx = int(c.curves.x.size());
+  n.ssy = c.curves.y.data(); n.n_ssy = int(c.curves.y.size());
+  n.sst = c.curves.time.data(); n.n_sst = int(c.curves.time.size());
+  n.ssystem = c.curves.system;
+  loc.clear();
+  for (const auto& l : c.locations) loc.insert(loc.end(), {l.frame, l.plane, l.y, l.x});
+  n.nlocation = loc.data(); n.n_nlocation = int(c.locations.size());
+  n.has_alpha = c.alpha.has_value(); n.alpha = c.alpha.value_or(0);
+  return n;
+}
 inline void check(nf_status s, const char* err) {
   if (s == NF_OK) return;
   if (s == NF_INVALID_ARGUMENT) throw std::invalid_argument(err);
@@ -136,6 +156,45 @@ class KalmanState {
   nf_kalman_state* state_ = nullptr;
 };
 
+// DFTNoise (src/algorithms/dft_noise.hpp:9-30): the sampled noise model shared by the
+// DFTTest plans of one filter. prepare() gathers tbsize slices per location through the
+// host layer's callback and builds the per-bin table once; plans upload the published
+// table before their next call.
+class DFTNoise {
+ public:
+  explicit DFTNoise(const DFTConfig& c)
+      : locations(c.locations), temporal_size(c.tbsize), block_size(c.block), config_(c) {}
+  using Gather = std::function<void(const NoiseLocation&, int, span2d::Span<float>)>;
+  void prepare(const Gather& gather) const {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (power_) return;
+    const std::size_t slice = std::size_t(block_size) * block_size;
+    std::vector<float> slices(locations.size() * std::size_t(temporal_size) * slice);
+    for (std::size_t l = 0; l < locations.size(); ++l)
+      for (int z = 0; z < temporal_size; ++z)
+        gather(locations[l], z, span2d::Span<float>(slices.data() + (l * temporal_size + std::size_t(z)) * slice, slice));
+    auto out = std::make_shared<std::vector<float>>(std::size_t(temporal_size) * block_size * (block_size / 2 + 1));
+    std::vector<int> loc;
+    nf_dft_config n = detail::to_c(config_, loc);
+    char err[512] = {0};
+    detail::check(nf_dft_noise_power(&n, slices.data(), int(locations.size()), out->data(), int(out->size()), err,
+                                     sizeof(err)),
+                  err);
+    power_ = std::move(out);
+  }
+  std::shared_ptr<const std::vector<float>> power() const {
+    std::lock_guard<std::mutex> lock(mu_);
+    return power_;
+  }
+  const std::vector<NoiseLocation> locations;
+  const int temporal_size, block_size;
+
+ private:
+  DFTConfig config_;
+  mutable std::mutex mu_;
+  mutable std::shared_ptr<const std::vector<float>> power_;
+};
+
 class Plan {
  public:
   // Plan(int, int, SampleFormat, const FFT3DConfig&) — plan.hpp:51.
@@ -160,30 +219,19 @@ class Plan {
     kalman_ = c.bt == 0;
     init();
   }
-  // Plan(int, int, SampleFormat, const DFTConfig&, noise) — plan.hpp:52.
-  template <class Noise = void>
-  Plan(int width, int height, SampleFormat format, const DFTConfig& c, std::shared_ptr<const Noise> = {},
+  // Plan(int, int, SampleFormat, const DFTConfig&, noise) — plan.hpp:52; plans of one
+  // filter share the sampled noise model (filter.hpp:81-82).
+  Plan(int width, int height, SampleFormat format, const DFTConfig& c, std::shared_ptr<const DFTNoise> noise = {},
        std::shared_ptr<runtime::Retention> = {})
       : format(format), algorithm(Algorithm::DFTTest) {
-    nf_dft_config n{};
-    n.block = c.block; n.overlap = c.overlap; n.mode = c.mode; n.swin = c.swin; n.twin = c.twin;
-    n.ftype = c.ftype; n.opt = c.opt; n.tbsize = c.tbsize; n.sbeta = c.sbeta; n.tbeta = c.tbeta;
-    n.sigma = c.sigma; n.sigma2 = c.sigma2; n.pmin = c.pmin; n.pmax = c.pmax; n.f0beta = c.f0beta;
-    n.zmean = c.zmean; n.temporal_mode = c.temporal_mode; n.temporal_overlap = c.temporal_overlap;
-    n.dither = c.dither; n.dither_seed = c.dither_seed;
-    n.slocation = c.curves.shared.data(); n.n_slocation = int(c.curves.shared.size());
-    n.ssx = c.curves.x.data(); n.n_ssx = int(c.curves.x.size());
-    n.ssy = c.curves.y.data(); n.n_ssy = int(c.curves.y.size());
-    n.sst = c.curves.time.data(); n.n_sst = int(c.curves.time.size());
-    n.ssystem = c.curves.system;
     std::vector<int> loc;
-    for (const auto& l : c.locations) loc.insert(loc.end(), {l.frame, l.plane, l.y, l.x});
-    n.nlocation = loc.data(); n.n_nlocation = int(c.locations.size());
-    n.has_alpha = c.alpha.has_value(); n.alpha = c.alpha.value_or(0);
+    nf_dft_config n = detail::to_c(c, loc);
     char err[512] = {0};
     detail::check(nf_plan_create_dft(width, height, to_c(format), &n, &plan_, err, sizeof(err)), err);
     init();
+    if (nf_plan_model_state(plan_) != 0) noise_ = noise ? std::move(noise) : std::make_shared<DFTNoise>(c);
   }
+  std::shared_ptr<const DFTNoise> dft_noise() const { return noise_; }
   Plan(const Plan&) = delete;
   Plan& operator=(const Plan&) = delete;
   ~Plan() { nf_plan_destroy(plan_); }
@@ -209,6 +257,7 @@ class Plan {
   template <class T, class Cache = runtime::SpectraCache, class Request = void>
   void process_at(span2d::Span<const span2d::Plane<const T>> sources, span2d::Plane<T> dst, int frame, int plane,
                   span2d::Span<const int> targets = {}, Cache* = nullptr, Request* = nullptr) const {
+    if (noise_) upload_noise();
     std::vector<nf_const_plane> s;
     s.reserve(sources.size());
     for (const auto& p : sources) s.push_back(detail::cplane(p));
@@ -245,6 +294,18 @@ class Plan {
   const nf_plan* handle() const { return plan_; }
 
  private:
+  // Publishes the shared noise model's table to this plan once it exists.
+  void upload_noise() const {
+    auto power = noise_->power();
+    std::lock_guard<std::mutex> lock(noise_mu_);
+    if (!power || power.get() == uploaded_) return;
+    char err[512] = {0};
+    detail::check(nf_plan_set_noise_model(plan_, power->data(), int(power->size()), err, sizeof(err)), err);
+    uploaded_ = power.get();
+  }
+  std::shared_ptr<const DFTNoise> noise_;
+  mutable std::mutex noise_mu_;
+  mutable const std::vector<float>* uploaded_ = nullptr;
   static nf_format to_c(SampleFormat f) { return {f.bits, f.floating ? 1 : 0, f.chroma ? 1 : 0}; }
   void init() {
     nf_axis x{}, y{};

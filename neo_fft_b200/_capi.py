@@ -108,6 +108,10 @@ PROTOTYPES = {
     "nf_clip_batch_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_clip_batch_graph_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_clip_batch_destroy": (None, [c_void_p]),
+    "nf_dft_noise_power": (c_int, [ctypes.POINTER(NfDftConfig), c_void_p, c_int, c_void_p, c_int, ctypes.c_char_p,
+                                   c_size_t]),
+    "nf_plan_set_noise_model": (c_int, [c_void_p, c_void_p, c_int, ctypes.c_char_p, c_size_t]),
+    "nf_plan_model_state": (c_int, [c_void_p]),
     "nf_plan_set_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_plan_get_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_dft_backward_scratch_bytes": (c_int, [c_void_p, c_int, ctypes.POINTER(c_size_t)]),

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -30,6 +31,7 @@ struct nf_plan {
   int device = 0;
   mutable std::mutex staging_mu;
   mutable void* staging = nullptr;  // device staging for the host-memory path
+  std::atomic<bool> model_ready{false};  // sampled noise model published (primary table filled)
   mutable size_t staging_bytes = 0;
   ~nf_plan() {
     if (tables) cudaFree(tables);
@@ -435,6 +437,8 @@ nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n,
   cudaError_t e;
   if (p.t.algo == nfb::Algo::FFT3D && p.t.kalman)
     return fail(err, len, "Kalman plans render through nf_kalman_render_device", NF_INVALID_ARGUMENT);
+  if (p.t.noise_model && !p.model_ready.load(std::memory_order_acquire))
+    return fail(err, len, "DFTTest sample model not initialized", NF_INVALID_ARGUMENT);
   if (c.tslots == 1 && !p.t.temporal_ola) {
     e = run_spatial(p.dev, sources[0].data, sources[0].stride_bytes, dst.data, dst.stride_bytes, nullptr, st);
   } else {
@@ -1317,6 +1321,37 @@ nf_status nf_clip_batch_graph_launch(nf_clip_batch* b, void* stream, char* err, 
 }
 
 void nf_clip_batch_destroy(nf_clip_batch* b) { delete b; }
+
+nf_status nf_dft_noise_power(const nf_dft_config* c, const float* slices, int nlocations, float* power, int count,
+                             char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(c && power, "null config or output");
+    const std::vector<float> v = nfb::dft_noise_power(*c, slices, nlocations);
+    nfb::require(count == int(v.size()), "noise model size mismatch");
+    std::memcpy(power, v.data(), v.size() * sizeof(float));
+    return NF_OK;
+  });
+}
+
+nf_status nf_plan_set_noise_model(nf_plan* p, const float* power, int count, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && power, "null plan or model");
+    nfb::require(p->t.noise_model, "plan has no sampled noise model");
+    nfb::require(count == p->t.temporal_size * p->t.bins, "noise model size mismatch");
+    for (int i = 0; i < count; ++i) nfb::finite(power[i]);
+    cudaError_t e = cudaMemcpy(const_cast<float*>(p->dev.filt.primary), power, size_t(count) * sizeof(float),
+                               cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "model upload failed");
+    p->model_ready.store(true, std::memory_order_release);
+    return NF_OK;
+  });
+}
+
+int nf_plan_model_state(const nf_plan* p) {
+  if (!p) return -1;
+  const bool needs = p->t.noise_model;
+  return needs ? (p->model_ready.load(std::memory_order_acquire) ? 2 : 1) : 0;
+}
 
 nf_status nf_plan_set_primary(nf_plan* p, const float* table, int count, void* stream, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {

@@ -616,18 +616,20 @@ PlanTables build_dft(int w, int h, nf_format f, const nf_dft_config& c) {
   const float volume = float(c.tbsize) * float(c.block) * float(c.block);
   for (std::size_t i = 0; i < p.h.size(); ++i) p.h_synthesis[i] = p.h[i] * volume;
   const bool sampled = c.ftype < 2 && c.n_nlocation > 0;
-  if (sampled)
-    throw std::invalid_argument("DFTTest sampled noise model (nlocation) is not implemented on the GPU path");
+  if (sampled) {
+    (void)dft_noise_setup(c);  // the reference builds its DFTNoise inside Plan (plan.cpp:193-198)
+    p.noise_model = true;
+  }
   const Curves curves = curves_of(c);
   const float scale = c.ftype < 2 ? p.wscale : 1.0f;
   p.spectral.type = c.ftype;
-  p.spectral.a = curves.empty() ? finite(c.sigma / scale) : 0;
+  p.spectral.a = !sampled && curves.empty() ? finite(c.sigma / scale) : 0;
   p.spectral.b = finite(c.sigma2 / scale);
   p.spectral.low = finite(c.pmin / p.wscale);
   p.spectral.high = finite(c.pmax / p.wscale);
   p.spectral.exponent = c.f0beta;
   p.spectral.floor = 0;
-  if (!curves.empty()) p.spectral.primary = dft_profile(curves, c.tbsize, c.block, c.sigma, scale);
+  if (!sampled && !curves.empty()) p.spectral.primary = dft_profile(curves, c.tbsize, c.block, c.sigma, scale);
   if (c.zmean) {
     auto block = p.h;
     for (float& v : block) v = finite(255.0f * v);
@@ -636,6 +638,62 @@ PlanTables build_dft(int w, int h, nf_format f, const nf_dft_config& c) {
     require(p.grid[0].r != 0, "DFTTest zmean requires nonzero template DC");
   }
   return p;
+}
+
+} // namespace nfb
+
+namespace nfb {
+
+// --- DFTNoise (src/algorithms/dft_noise.cpp:5-41) ---
+DftNoiseSetup dft_noise_setup(const nf_dft_config& c) {
+  validate_dft(c);
+  require(c.ftype < 2 && c.n_nlocation > 0, "inactive DFTTest sample model");
+  DftNoiseSetup s;
+  s.temporal_size = c.tbsize;
+  s.block = c.block;
+  s.bins3 = c.tbsize * c.block * (c.block / 2 + 1);
+  s.zmean = c.zmean != 0;
+  const DftWindow sample = dft_window_3d(c.tbsize, c.block, 0, 0, c.swin, c.twin, c.sbeta, c.tbeta, 0, 0);
+  const DftWindow output = dft_window_3d(c.tbsize, c.block, c.mode == 0 ? 0 : c.overlap, c.mode, c.swin, c.twin,
+                                         c.sbeta, c.tbeta, c.temporal_mode, c.temporal_overlap);
+  const float alpha = c.has_alpha ? c.alpha : (c.ftype == 0 ? 5.0f : 7.0f);
+  s.calibration = finite(finite((1.0f / float(c.n_nlocation)) * finite(sample.wscale / output.wscale)) * alpha);
+  s.window = sample.h;
+  std::vector<float> input(s.window.size());
+  for (std::size_t i = 0; i < input.size(); ++i) input[i] = 255.0f * s.window[i];
+  s.grid.resize(std::size_t(s.bins3));
+  host_r2c_3d(input.data(), s.grid.data(), c.tbsize, c.block, c.block);
+  for (const cf& g : s.grid) {
+    finite(g.r);
+    finite(g.i);
+  }
+  require(!s.zmean || s.grid[0].r != 0, "DFTTest sample template DC must be nonzero");
+  return s;
+}
+
+std::vector<float> dft_noise_power(const nf_dft_config& c, const float* slices, int nlocations) {
+  const DftNoiseSetup s = dft_noise_setup(c);
+  require(slices != nullptr && nlocations == c.n_nlocation, "DFTTest noise slices differ from nlocation");
+  const std::size_t samples = s.window.size();
+  std::vector<float> input(samples), sum(std::size_t(s.bins3), 0.0f);
+  std::vector<cf> spectrum(std::size_t(s.bins3));
+  for (int l = 0; l < nlocations; ++l) {
+    const float* in = slices + std::size_t(l) * samples;
+    for (std::size_t i = 0; i < samples; ++i) input[i] = finite((in[i] * 1.0f) * s.window[i]);
+    host_r2c_3d(input.data(), spectrum.data(), s.temporal_size, s.block, s.block);
+    const float ratio = s.zmean ? finite(spectrum[0].r / s.grid[0].r) : 0.0f;
+    for (int k = 0; k < s.bins3; ++k) {
+      const float re = spectrum[k].r - (s.zmean ? ratio * s.grid[k].r : 0.0f);
+      const float im = spectrum[k].i - (s.zmean ? ratio * s.grid[k].i : 0.0f);
+      const float q = finite((re * re) + (im * im));
+      sum[k] = finite(sum[k] + q);
+    }
+  }
+  for (float& v : sum) {
+    v = s.calibration * v;
+    finite(1.0f * v);
+  }
+  return sum;
 }
 
 } // namespace nfb

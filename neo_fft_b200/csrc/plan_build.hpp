@@ -110,6 +110,7 @@ struct PlanTables {
   std::vector<float> h, h_synthesis;
   float wscale = 0;
   bool center = false, temporal_ola = false;
+  bool noise_model = false;  // primary table comes from the sampled noise model (nlocation)
   int temporal_overlap = 0, dither = 0, dither_seed = 0;
   // both
   Spectral spectral;
@@ -118,6 +119,20 @@ struct PlanTables {
 };
 
 PlanTables build_fft3d(int width, int height, nf_format format, const nf_fft3d_config& c);
+
+// DFTTest sampled noise model (DFTNoise, src/algorithms/dft_noise.cpp:5-41): sample
+// window, template spectrum of 255*window and calibration, checked at plan creation;
+// dft_noise_power averages the windowed 3-D power spectra of the gathered slices
+// ([location][tbsize][sbsize][sbsize], 8-bit amplitude units) into the primary table.
+struct DftNoiseSetup {
+  std::vector<float> window;
+  std::vector<cf> grid;
+  float calibration = 0;
+  int temporal_size = 1, block = 0, bins3 = 0;
+  bool zmean = false;
+};
+DftNoiseSetup dft_noise_setup(const nf_dft_config& c);
+std::vector<float> dft_noise_power(const nf_dft_config& c, const float* slices, int nlocations);
 PlanTables build_dft(int width, int height, nf_format format, const nf_dft_config& c);
 
 } // namespace nfb

@@ -265,6 +265,17 @@ class Plan:
                 dst = np.empty_like(np.asarray(first))
         return self.process_at(sources, dst)
 
+    @property
+    def model_state(self) -> int:
+        """0: no sampled noise model; 1: waiting for one; 2: ready."""
+        return int(self._lib.nf_plan_model_state(self._h))
+
+    def set_noise_model(self, power) -> None:
+        p = np.ascontiguousarray(power, np.float32)
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_plan_set_noise_model(self._h, ctypes.c_void_p(p.ctypes.data), p.size, err, 512),
+                    err.value)
+
     def sync_status(self, stream=None) -> None:
         """Raise NonFiniteError if any device launch met a non-finite value."""
         import torch
@@ -373,6 +384,59 @@ class Batch:
         if h is not None and h.value:
             self._lib.nf_batch_destroy(h)
             self._h = None
+
+
+def gather_noise(frames, location, z, block: int, fmt: SampleFormat) -> np.ndarray:
+    """The host layer's sample gather (src/plugin/filter.hpp:381-389): rows
+    y..y+block, columns x..x+block of plane `location[1]` of frame location[0] + z,
+    decoded to 8-bit amplitude units. `frames(frame, plane)` returns a 2-D array."""
+    frame, plane, y, x = location
+    src = np.asarray(frames(frame + z, plane))
+    if x > src.shape[1] - block or y > src.shape[0] - block:
+        raise ValueError("sample frame rectangle differs from plan")
+    scale = np.float32(255.0) if fmt.floating else np.float32(1.0 / float(1 << (fmt.bits - 8)))
+    return (src[y:y + block, x:x + block].astype(np.float32) - np.float32(0)) * scale
+
+
+class DFTNoise:
+    """DFTNoise (src/algorithms/dft_noise.hpp:9-30): the sampled noise model shared by
+    the DFTTest plans of one filter (nlocation, ftype 0/1). prepare(gather) builds the
+    per-bin table from gathered sample volumes — gather(location, z) returns the
+    block x block slice z of a location in 8-bit amplitude units (see gather_noise) —
+    and publish(*plans) hands it to the plans."""
+
+    def __init__(self, config: DFTConfig):
+        loc = list(config.nlocation)
+        if len(loc) % 4:
+            raise ValueError("DFTTest nlocation requires quadruples")
+        self.config = config
+        self.locations = [tuple(loc[i:i + 4]) for i in range(0, len(loc), 4)]
+        self.temporal_size, self.block_size = config.tbsize, config.block
+        self.power = None
+
+    def prepare(self, gather) -> np.ndarray:
+        if self.power is not None:
+            return self.power
+        T, S = self.temporal_size, self.block_size
+        slices = np.zeros((len(self.locations), T, S, S), np.float32)
+        for i, location in enumerate(self.locations):
+            for z in range(T):
+                slices[i, z] = gather(location, z)
+        lib = C.load()
+        cfg, keep = self.config.to_c()
+        out = np.zeros(T * S * (S // 2 + 1), np.float32)
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(lib.nf_dft_noise_power(ctypes.byref(cfg), ctypes.c_void_p(slices.ctypes.data), len(self.locations),
+                                           ctypes.c_void_p(out.ctypes.data), out.size, err, 512), err.value)
+        del keep
+        self.power = out
+        return out
+
+    def publish(self, *plans) -> None:
+        if self.power is None:
+            raise ValueError("DFTTest sample model not initialized")
+        for p in plans:
+            p.set_noise_model(self.power)
 
 
 class ClipBatch:

@@ -71,6 +71,7 @@ def load() -> ctypes.CDLL:
             "ref_dft_window_3d": (ci, [ci, ci, ci, ci, ci, ci, ctypes.c_float, ctypes.c_float, ci, ci, FP, FP, cp, cs]),
             "ref_dft_profile": (ci, [ctypes.POINTER(C.NfDftConfig), ctypes.c_float, FP, cp, cs]),
             "ref_fft3d_profile": (ci, [ci, ci, FP, FP, cp, cs]),
+            "ref_plan_prepare_noise": (ci, [vp, FP, ci, FP, ci, cp, cs]),
             "ref_dither": (ci, [FP, ci, ci, ci, ctypes.POINTER(ctypes.c_ubyte), ci, ci, ci, ci, ci, cp, cs]),
             "ref_dither_hash": (ctypes.c_uint, [ctypes.c_uint] * 5),
         }
@@ -159,6 +160,16 @@ class RefPlan:
         rc = self.lib.ref_plan_process_many(self.h, _storage(srcs[0]), arr, nslots, darr, len(outs), threads, err, 512)
         _raise(rc, err)
         return outs
+
+    def prepare_noise(self, slices: np.ndarray) -> np.ndarray:
+        """DFTNoise::prepare of this plan's sampled model from gathered slices
+        [location][tbsize][sbsize][sbsize]; returns the published power table."""
+        slices = np.ascontiguousarray(slices, np.float32)
+        out = np.zeros(self.temporal_size * self.bins, np.float32)
+        err = ctypes.create_string_buffer(512)
+        _raise(self.lib.ref_plan_prepare_noise(self.h, fp(slices), int(slices.shape[0]), fp(out), out.size, err, 512),
+               err)
+        return out
 
     # Kalman
     def kalman_state(self):

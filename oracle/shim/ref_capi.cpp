@@ -6,6 +6,7 @@
 //
 // Nothing here is linked into the product library.
 #include "algorithms/plan.hpp"
+#include "algorithms/dft_noise.hpp"
 #include "kernels/dither.hpp"
 #include "neo_fft_b200.h"
 #include "fft_core.cuh"
@@ -110,6 +111,28 @@ int ref_plan_create_dft(int w, int h, nf_format f, const nf_dft_config* c, void*
   });
 }
 void ref_plan_destroy(void* p) { delete static_cast<RefPlan*>(p); }
+
+// DFTNoise::prepare (dft_noise.cpp:26-41) of the plan's shared model, fed from
+// `slices` ([location][tbsize][sbsize][sbsize], 8-bit amplitude units), then the
+// published model copied to `power`.
+int ref_plan_prepare_noise(void* p, const float* slices, int nloc, float* power, int count, char* err, size_t len) {
+  return guarded(err, len, [&] {
+    const Plan& pl = *static_cast<RefPlan*>(p)->plan;
+    auto noise = pl.dft_noise();
+    if (!noise) throw std::invalid_argument("plan has no sampled noise model");
+    if (nloc != int(noise->locations.size())) throw std::invalid_argument("slice count differs from nlocation");
+    const std::size_t slice = std::size_t(noise->block_size) * noise->block_size;
+    noise->prepare([&](const NoiseLocation& location, int z, span2d::Span<float> out) {
+      std::size_t l = 0;
+      while (l < noise->locations.size() && &noise->locations[l] != &location) ++l;
+      const float* src = slices + (l * std::size_t(noise->temporal_size) + std::size_t(z)) * slice;
+      std::memcpy(out.data(), src, slice * sizeof(float));
+    });
+    auto model = noise->power();
+    if (!model || int(model->size()) != count) throw std::invalid_argument("noise model size mismatch");
+    std::memcpy(power, model->data(), model->size() * sizeof(float));
+  });
+}
 
 int ref_plan_geometry(void* p, nf_axis* x, nf_axis* y, int* temporal, int* bins) {
   const Plan& pl = *static_cast<RefPlan*>(p)->plan;

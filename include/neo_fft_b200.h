@@ -212,7 +212,8 @@ nf_status nf_clip_batch_launch(nf_clip_batch* batch, void* stream, char* err, si
 nf_status nf_clip_batch_graph_launch(nf_clip_batch* batch, void* stream, char* err, size_t err_len);
 void nf_clip_batch_destroy(nf_clip_batch* batch);
 
-/* Sampled noise models. DFTTest with nlocation (ftype 0/1): DFTNoise
+/* Sampled noise models (the published table is the plan's per-bin primary table:
+ * tbsize*bins floats for DFTTest, bins for FFT3D). DFTTest with nlocation (ftype 0/1): DFTNoise
  * (src/algorithms/dft_noise.cpp:5-41) builds the per-bin primary table from windowed
  * 3-D power spectra of sample volumes the host layer gathers (filter.hpp:476-490):
  * `slices` holds nlocations x tbsize x sbsize x sbsize floats in 8-bit amplitude units.
@@ -225,6 +226,24 @@ nf_status nf_dft_noise_power(const nf_dft_config* config, const float* slices, i
                              int count, char* err, size_t err_len);
 nf_status nf_plan_set_noise_model(nf_plan* plan, const float* power, int count, char* err, size_t err_len);
 int nf_plan_model_state(const nf_plan* plan);
+/* FFT3D with pfactor > 0: the pattern search of plan.cpp:227-288 on a device plane of
+ * the pattern frame (filter.hpp:175-194, 455-471). nf_plan_pattern_candidate scores
+ * every candidate block (the px/py block, or all blocks two or more inside the grid),
+ * takes the first minimum and returns its power scaled by pfactor (1 for Kalman) and
+ * the sampling weights (`count` = bins floats, host memory; synchronises `stream`);
+ * publish it with nf_plan_set_noise_model (pattern_candidate + publish_pattern,
+ * plan.hpp:93-94). nf_plan_prepare_pattern does both unless a model is already
+ * published (prepare_pattern, plan.hpp:95-97). Processing before publication fails
+ * with "FFT3D sampled model not initialized". With pshow, nf_plan_process_device
+ * renders the chosen block of the first source on a zero plane instead of filtering. */
+nf_status nf_plan_pattern_candidate(const nf_plan* plan, nf_const_plane source, float* power, int count, void* stream,
+                                    char* err, size_t err_len);
+nf_status nf_plan_prepare_pattern(nf_plan* plan, nf_const_plane source, void* stream, char* err, size_t err_len);
+/* The same with the source plane in host memory (staged through the plan). */
+nf_status nf_plan_pattern_candidate_host(const nf_plan* plan, nf_const_plane source, float* power, int count,
+                                         void* stream, char* err, size_t err_len);
+nf_status nf_plan_prepare_pattern_host(nf_plan* plan, nf_const_plane source, void* stream, char* err,
+                                       size_t err_len);
 
 /* Differentiable form (no reference counterpart; the reference has no gradients).
  * DFTTest plans keep their per-bin primary table A ([tbsize][sbsize][sbsize/2+1],

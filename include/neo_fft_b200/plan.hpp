@@ -216,7 +216,10 @@ class Plan {
     n.kalman_warmup = c.kalman_warmup;
     char err[512] = {0};
     detail::check(nf_plan_create_fft3d(width, height, to_c(format), &n, &plan_, err, sizeof(err)), err);
-    kalman_ = c.bt == 0;
+    // plan.cpp:110-115: preview when pshow samples a pattern or shows a varying-sigma plan
+    const auto differs = [&](const std::optional<float>& v) { return v.has_value() && *v != c.sigma; };
+    preview_ = c.pshow && (c.pfactor > 0 || differs(c.sigma2) || differs(c.sigma3) || differs(c.sigma4));
+    kalman_ = c.bt == 0 && !preview_;
     init();
   }
   // Plan(int, int, SampleFormat, const DFTConfig&, noise) — plan.hpp:52; plans of one
@@ -268,9 +271,29 @@ class Plan {
   }
 
   bool kalman() const { return kalman_; }
-  bool preview() const { return false; }
-  bool needs_pattern_frame() const { return false; }
-  bool pattern_ready() const { return false; }
+  bool preview() const { return preview_; }
+  // FFT3D sampled model (plan.hpp:90-97): the pattern candidate of a host plane, its
+  // publication, and prepare_pattern (search + publish unless already published).
+  bool needs_pattern_frame() const { return algorithm == Algorithm::FFT3D && nf_plan_model_state(plan_) != 0; }
+  bool pattern_ready() const { return nf_plan_model_state(plan_) == 2; }
+  template <class T>
+  std::shared_ptr<const std::vector<float>> pattern_candidate(span2d::Plane<const T> source) const {
+    auto out = std::make_shared<std::vector<float>>(fft.bins());
+    char err[512] = {0};
+    detail::check(nf_plan_pattern_candidate_host(plan_, detail::cplane(source), out->data(), int(out->size()), nullptr,
+                                                 err, sizeof(err)),
+                  err);
+    return out;
+  }
+  void publish_pattern(std::shared_ptr<const std::vector<float>> model) const {
+    char err[512] = {0};
+    detail::check(nf_plan_set_noise_model(plan_, model->data(), int(model->size()), err, sizeof(err)), err);
+  }
+  template <class T>
+  void prepare_pattern(span2d::Plane<const T> source) const {
+    char err[512] = {0};
+    detail::check(nf_plan_prepare_pattern_host(plan_, detail::cplane(source), nullptr, err, sizeof(err)), err);
+  }
   KalmanState initial_kalman() const {
     KalmanState s;
     char err[512] = {0};
@@ -318,6 +341,7 @@ class Plan {
   }
   nf_plan* plan_ = nullptr;
   bool kalman_ = false;
+  bool preview_ = false;
 };
 
 }  // namespace neo_fft

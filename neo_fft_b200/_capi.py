@@ -112,6 +112,12 @@ PROTOTYPES = {
                                    c_size_t]),
     "nf_plan_set_noise_model": (c_int, [c_void_p, c_void_p, c_int, ctypes.c_char_p, c_size_t]),
     "nf_plan_model_state": (c_int, [c_void_p]),
+    "nf_plan_pattern_candidate": (c_int, [c_void_p, NfConstPlane, c_void_p, c_int, c_void_p, ctypes.c_char_p,
+                                          c_size_t]),
+    "nf_plan_prepare_pattern": (c_int, [c_void_p, NfConstPlane, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_plan_pattern_candidate_host": (c_int, [c_void_p, NfConstPlane, c_void_p, c_int, c_void_p, ctypes.c_char_p,
+                                               c_size_t]),
+    "nf_plan_prepare_pattern_host": (c_int, [c_void_p, NfConstPlane, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_plan_set_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_plan_get_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_dft_backward_scratch_bytes": (c_int, [c_void_p, c_int, ctypes.POINTER(c_size_t)]),

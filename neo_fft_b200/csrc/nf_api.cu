@@ -10,6 +10,7 @@
 #define NF_ADJOINT_AUX_KERNELS
 #include "adjoint.cuh"
 #include "tile_temporal.cuh"
+#include "pattern.cuh"
 
 #include <cuda_runtime.h>
 
@@ -31,9 +32,28 @@ struct nf_plan {
   int device = 0;
   mutable std::mutex staging_mu;
   mutable void* staging = nullptr;  // device staging for the host-memory path
-  std::atomic<bool> model_ready{false};  // sampled noise model published (primary table filled)
   mutable size_t staging_bytes = 0;
+  std::atomic<bool> model_ready{false};  // sampled noise model published (primary table filled)
+  // FFT3D pattern search (pfactor / pshow): device scratch for the plane's block spectra,
+  // candidate scores, the chosen block's power and the preview block.
+  struct Pattern {
+    void* dev = nullptr;
+    nfd::DevPlan* plan = nullptr;
+    nfd::SpectraJob* job = nullptr;
+    int* item_base = nullptr;
+    float* weights = nullptr;
+    cf* spectra = nullptr;
+    float* scores = nullptr;
+    float* power = nullptr;
+    float* block = nullptr;
+    cf* work = nullptr;  // preview block spectrum
+    int nbc = 1, items = 0, cand_x0 = 0, cand_y0 = 0, cand_nx = 0, cand_ny = 0;
+    size_t smem = 0;
+  };
+  mutable Pattern pattern;
+  mutable std::mutex pattern_mu;
   ~nf_plan() {
+    if (pattern.dev) cudaFree(pattern.dev);
     if (tables) cudaFree(tables);
     if (err) cudaFree(err);
     if (staging) cudaFree(staging);
@@ -178,6 +198,7 @@ void temporal_twiddles(int T, int c, std::vector<cf>& fwd, std::vector<cf>& inv)
 // (nf_plan_set_primary); without sigma curves it holds the uniform value a, which
 // gives the same per-bin arithmetic as the uniform path.
 std::vector<float> primary_table(const nfb::PlanTables& t) {
+  if (t.algo == nfb::Algo::FFT3D && t.needs_pattern) return std::vector<float>(size_t(t.bins), 0.0f);
   if (t.algo != nfb::Algo::DFTTest || !t.spectral.primary.empty()) return t.spectral.primary;
   return std::vector<float>(size_t(t.temporal_size) * size_t(t.bins), t.spectral.a);
 }
@@ -245,7 +266,8 @@ nf_status finalize_plan(std::unique_ptr<nf_plan>& p, char* err, size_t len) {
   d.enh = {-2, 0, 0, 0, 0, 1, 0, nullptr, en.active() ? 1 : 0, en.sharpen, en.dehalo, en.a, en.b, en.c,
            static_cast<const float*>(ptr(o_sw)), static_cast<const float*>(ptr(o_hw))};
   if (d.algo == 0)
-    d.fft3d_mode = !t.denoise ? nfd::kEnhanceOnly : (!s.primary.empty() ? nfd::kWienerThenEnh : nfd::kWienerFused);
+    d.fft3d_mode = !t.denoise ? nfd::kEnhanceOnly
+                              : (!s.primary.empty() || t.needs_pattern ? nfd::kWienerThenEnh : nfd::kWienerFused);
   d.codelet = (t.bh == t.bw && (t.bw == 8 || t.bw == 16 || t.bw == 32)) ? 1 : 0;
   d.twh = static_cast<const cf*>(ptr(o_twh));
   d.tww = static_cast<const cf*>(ptr(o_tww));
@@ -429,6 +451,156 @@ nf_status read_error_word(const nf_plan& p, cudaStream_t st, char* err, size_t l
   return NF_OK;
 }
 
+// --- FFT3D pattern search (plan.cpp:227-288) ---
+cudaError_t launch_spectra_shape(int bh, int bw, int storage, const nfd::SpectraWork& w, int items, size_t smem,
+                                 cudaStream_t st);
+nf_status alloc_pattern(nf_plan& p, char* err, size_t len) {
+  const auto& t = p.t;
+  auto& pt = p.pattern;
+  int nbc = 1;
+  for (int n = 2; n <= std::min(16, t.gx.count); ++n)
+    if (nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, n) <= 100 * 1024) nbc = n;
+  pt.nbc = nbc;
+  pt.smem = nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, nbc);
+  const int chunks = (t.gx.count + nbc - 1) / nbc;
+  pt.items = chunks * t.gy.count;
+  const bool automatic = t.px == 0 && t.py == 0;
+  pt.cand_x0 = automatic ? 2 : t.px;
+  pt.cand_y0 = automatic ? 2 : t.py;
+  pt.cand_nx = automatic ? t.gx.count - 4 : 1;
+  pt.cand_ny = automatic ? t.gy.count - 4 : 1;
+  const size_t nblocks = size_t(t.gx.count) * t.gy.count;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t o_plan = take(sizeof(nfd::DevPlan)), o_job = take(sizeof(nfd::SpectraJob)), o_base = take(2 * sizeof(int)),
+               o_w = take(t.sample_weights.size() * sizeof(float)), o_spec = take(nblocks * t.bins * sizeof(cf)),
+               o_sc = take(size_t(pt.cand_nx) * pt.cand_ny * sizeof(float)), o_pw = take(size_t(t.bins) * sizeof(float)),
+               o_blk = take(size_t(t.bh) * t.bw * sizeof(float)), o_work = take(size_t(t.bins) * sizeof(cf));
+  cudaError_t e = cudaMalloc(&pt.dev, off);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
+  auto* b = static_cast<unsigned char*>(pt.dev);
+  pt.plan = reinterpret_cast<nfd::DevPlan*>(b + o_plan);
+  pt.job = reinterpret_cast<nfd::SpectraJob*>(b + o_job);
+  pt.item_base = reinterpret_cast<int*>(b + o_base);
+  pt.weights = reinterpret_cast<float*>(b + o_w);
+  pt.spectra = reinterpret_cast<cf*>(b + o_spec);
+  pt.scores = reinterpret_cast<float*>(b + o_sc);
+  pt.power = reinterpret_cast<float*>(b + o_pw);
+  pt.block = reinterpret_cast<float*>(b + o_blk);
+  pt.work = reinterpret_cast<cf*>(b + o_work);
+  const int base[2] = {0, pt.items};
+  if ((e = cudaMemcpy(pt.plan, &p.dev, sizeof(nfd::DevPlan), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(pt.item_base, base, sizeof(base), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(pt.weights, t.sample_weights.data(), t.sample_weights.size() * sizeof(float),
+                      cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail(err, len, e, "pattern upload failed");
+  return NF_OK;
+}
+
+void check_pattern_source(const nf_plan& p, const nf_const_plane& s) {
+  nfb::require(s.width == p.t.gx.length && s.height == p.t.gy.length, "pattern plane dimensions differ from plan");
+  const size_t elem = size_t(storage_of(p.t.format));
+  plane_extent(s.width, s.height, s.stride_bytes, elem);
+  check_pointer(s.data, elem);
+}
+
+// Scores every candidate block of `src` and returns the first minimum (row-major order);
+// with `power`, also the chosen block's unscaled power. Synchronises `st`.
+nf_status select_pattern(const nf_plan& p, const nf_const_plane& src, cudaStream_t st, int& bx, int& by,
+                         std::vector<float>* power, char* err, size_t len) {
+  check_pattern_source(p, src);
+  auto& pt = p.pattern;
+  const auto& t = p.t;
+  const nfd::SpectraJob job{static_cast<const unsigned char*>(src.data), (long long)src.stride_bytes, pt.spectra, 0,
+                            (t.gx.count + pt.nbc - 1) / pt.nbc};
+  cudaError_t e = cudaMemcpyAsync(pt.job, &job, sizeof(job), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "pattern upload failed");
+  const nfd::SpectraWork w{pt.plan, pt.job, pt.item_base, 1, pt.nbc};
+  if ((e = launch_spectra_shape(t.bh, t.bw, storage_of(t.format), w, pt.items, pt.smem, st)) != cudaSuccess)
+    return cuda_fail(err, len, e, "kernel launch failed");
+  const int ncand = pt.cand_nx * pt.cand_ny;
+  nfd::pattern_score_kernel<<<(ncand + 127) / 128, 128, 0, st>>>(pt.plan, pt.spectra, pt.weights, pt.cand_x0,
+                                                                 pt.cand_y0, pt.cand_nx, pt.cand_ny, pt.scores);
+  std::vector<float> scores(static_cast<size_t>(ncand));
+  if ((e = cudaGetLastError()) != cudaSuccess ||
+      (e = cudaMemcpyAsync(scores.data(), pt.scores, scores.size() * sizeof(float), cudaMemcpyDeviceToHost, st)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_fail(err, len, e, "pattern search failed");
+  const nf_status s = read_error_word(p, st, err, len);
+  if (s != NF_OK) return s;
+  int best = -1;
+  for (int c = 0; c < ncand; ++c) {
+    if (!std::isfinite(scores[size_t(c)])) return fail(err, len, "non-finite sample or intermediate", NF_NON_FINITE);
+    if (best < 0 || scores[size_t(c)] < scores[size_t(best)]) best = c;
+  }
+  nfb::require(best >= 0, "FFT3D no pattern candidate");
+  bx = pt.cand_x0 + best % pt.cand_nx;
+  by = pt.cand_y0 + best / pt.cand_nx;
+  if (power) {
+    nfd::pattern_power_kernel<<<1, 256, 0, st>>>(pt.plan, pt.spectra, bx, by, pt.power);
+    power->resize(size_t(t.bins));
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cudaMemcpyAsync(power->data(), pt.power, power->size() * sizeof(float), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return cuda_fail(err, len, e, "pattern search failed");
+  }
+  return NF_OK;
+}
+
+// pattern_candidate (plan.cpp:271-277): the chosen block's power scaled by pfactor (1 for
+// Kalman) and the sampling weights; the scaled table must survive the temporal multiplier.
+nf_status pattern_candidate(const nf_plan& p, const nf_const_plane& src, cudaStream_t st, std::vector<float>& power,
+                            char* err, size_t len) {
+  int bx = 0, by = 0;
+  const nf_status s = select_pattern(p, src, st, bx, by, &power, err, len);
+  if (s != NF_OK) return s;
+  const auto& t = p.t;
+  const float factor = t.kalman ? 1.0f : t.pfactor, maximum = float(t.temporal_size);
+  for (size_t k = 0; k < power.size(); ++k) {
+    float v = factor * power[k];
+    v = v * t.sample_weights[k];
+    nfb::finite(maximum * v);
+    power[k] = v;
+  }
+  if (t.kalman)
+    for (float r : power) nfb::finite(std::max(r, 1e-15f) * t.kalman_ratio2);
+  return NF_OK;
+}
+
+template <int ST>
+cudaError_t preview_launch(const nf_plan& p, const nf_const_plane& src, const nf_plane& dst, int ox, int oy,
+                           cudaStream_t st) {
+  auto& pt = p.pattern;
+  nfd::pattern_block_kernel<ST><<<1, 32, 0, st>>>(pt.plan, static_cast<const unsigned char*>(src.data),
+                                                  (long long)src.stride_bytes, ox, oy, pt.work, pt.block);
+  const dim3 b(32, 8), g((p.t.gx.length + 31) / 32, (p.t.gy.length + 7) / 8);
+  nfd::pattern_fill_kernel<ST><<<g, b, 0, st>>>(pt.plan, static_cast<unsigned char*>(dst.data),
+                                                (long long)dst.stride_bytes, ox, oy, pt.block);
+  return cudaGetLastError();
+}
+
+// pshow: the chosen pattern block of the first source, everything else zero (plan.cpp:409-418).
+nf_status preview_pattern(const nf_plan& p, const nf_const_plane& src, const nf_plane& dst, cudaStream_t st,
+                          char* err, size_t len) {
+  std::lock_guard<std::mutex> lock(p.pattern_mu);
+  int bx = 0, by = 0;
+  const nf_status s = select_pattern(p, src, st, bx, by, nullptr, err, len);
+  if (s != NF_OK) return s;
+  const int ox = bx * p.t.gx.step, oy = by * p.t.gy.step;
+  const int storage = storage_of(p.t.format);
+  const cudaError_t e = storage == nfd::kStoreU8    ? preview_launch<nfd::kStoreU8>(p, src, dst, ox, oy, st)
+                        : storage == nfd::kStoreU16 ? preview_launch<nfd::kStoreU16>(p, src, dst, ox, oy, st)
+                                                    : preview_launch<nfd::kStoreF32>(p, src, dst, ox, oy, st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  return NF_OK;
+}
+
 nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n, const int* targets, int nt,
                           nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len) {
   (void)frame;
@@ -439,6 +611,9 @@ nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n,
     return fail(err, len, "Kalman plans render through nf_kalman_render_device", NF_INVALID_ARGUMENT);
   if (p.t.noise_model && !p.model_ready.load(std::memory_order_acquire))
     return fail(err, len, "DFTTest sample model not initialized", NF_INVALID_ARGUMENT);
+  if (p.t.needs_pattern && !p.model_ready.load(std::memory_order_acquire))
+    return fail(err, len, "FFT3D sampled model not initialized", NF_INVALID_ARGUMENT);
+  if (p.t.preview) return preview_pattern(p, sources[0], dst, st, err, len);
   if (c.tslots == 1 && !p.t.temporal_ola) {
     e = run_spatial(p.dev, sources[0].data, sources[0].stride_bytes, dst.data, dst.stride_bytes, nullptr, st);
   } else {
@@ -575,8 +750,9 @@ nf_status nf_plan_create_fft3d(int width, int height, nf_format format, const nf
     nfb::require(config && plan, "missing configuration or output pointer");
     auto p = std::make_unique<nf_plan>();
     p->t = nfb::build_fft3d(width, height, format, *config);
-    const nf_status s = finalize_plan(p, err, err_len);
+    nf_status s = finalize_plan(p, err, err_len);
     if (s != NF_OK) return s;
+    if ((p->t.preview || p->t.needs_pattern) && (s = alloc_pattern(*p, err, err_len)) != NF_OK) return s;
     *plan = p.release();
     return NF_OK;
   });
@@ -761,12 +937,15 @@ nf_status nf_kalman_advance_device(const nf_plan* p, nf_const_plane source, nf_k
     nfb::require(p && state, "null plan or state");
     check_kalman_source(*p, source);
     nfb::require(state->count == size_t(p->t.gx.count) * p->t.gy.count * p->t.bins, "Kalman state shape differs");
+    nfb::require(!p->t.needs_pattern || p->model_ready.load(std::memory_order_acquire),
+                 "Kalman sampled model not initialized");
     nfd::KalmanArgs a{state->last,
                       state->fp64 ? nullptr : static_cast<float*>(state->covariance),
                       state->fp64 ? nullptr : static_cast<float*>(state->process),
                       state->fp64 ? static_cast<double*>(state->covariance) : nullptr,
                       state->fp64 ? static_cast<double*>(state->process) : nullptr,
-                      p->t.spectral.primary.empty() ? nullptr : p->dev.filt.primary, state->fp64};
+                      p->t.spectral.primary.empty() && !p->t.needs_pattern ? nullptr : p->dev.filt.primary,
+                      state->fp64};
     const cudaError_t e = run_kalman_advance(p->dev, source.data, source.stride_bytes, a, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
     return NF_OK;
@@ -818,6 +997,32 @@ nf_status stage_host_plane(const nf_plan& p, const nf_const_plane& s, int slot, 
   return NF_OK;
 }
 } // namespace
+
+nf_status nf_plan_pattern_candidate_host(const nf_plan* p, nf_const_plane source, float* power, int count,
+                                         void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p != nullptr, "null plan");
+    check_pattern_source(*p, source);
+    std::lock_guard<std::mutex> lock(p->staging_mu);
+    nf_const_plane staged{};
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    nf_status s = stage_host_plane(*p, source, 0, 1, st, &staged, nullptr, err, len);
+    if (s != NF_OK) return s;
+    return nf_plan_pattern_candidate(p, staged, power, count, stream, err, len);
+  });
+}
+
+nf_status nf_plan_prepare_pattern_host(nf_plan* p, nf_const_plane source, void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p != nullptr, "null plan");
+    nfb::require(p->t.needs_pattern, "FFT3D sampling is inactive");
+    if (p->model_ready.load(std::memory_order_acquire)) return NF_OK;
+    std::vector<float> v(size_t(p->t.bins));
+    nf_status s = nf_plan_pattern_candidate_host(p, source, v.data(), int(v.size()), stream, err, len);
+    if (s != NF_OK) return s;
+    return nf_plan_set_noise_model(p, v.data(), int(v.size()), err, len);
+  });
+}
 
 nf_status nf_kalman_advance_host(const nf_plan* p, nf_const_plane source, nf_kalman_state* state, void* stream,
                                  char* err, size_t len) {
@@ -1336,8 +1541,8 @@ nf_status nf_dft_noise_power(const nf_dft_config* c, const float* slices, int nl
 nf_status nf_plan_set_noise_model(nf_plan* p, const float* power, int count, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(p && power, "null plan or model");
-    nfb::require(p->t.noise_model, "plan has no sampled noise model");
-    nfb::require(count == p->t.temporal_size * p->t.bins, "noise model size mismatch");
+    nfb::require(p->t.noise_model || p->t.needs_pattern, "plan has no sampled noise model");
+    nfb::require(count == (p->t.noise_model ? p->t.temporal_size : 1) * p->t.bins, "noise model size mismatch");
     for (int i = 0; i < count; ++i) nfb::finite(power[i]);
     cudaError_t e = cudaMemcpy(const_cast<float*>(p->dev.filt.primary), power, size_t(count) * sizeof(float),
                                cudaMemcpyHostToDevice);
@@ -1347,9 +1552,36 @@ nf_status nf_plan_set_noise_model(nf_plan* p, const float* power, int count, cha
   });
 }
 
+nf_status nf_plan_pattern_candidate(const nf_plan* p, nf_const_plane source, float* power, int count, void* stream,
+                                    char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && power, "null plan or output");
+    nfb::require(p->t.needs_pattern, "FFT3D sampling is inactive");
+    nfb::require(count == p->t.bins, "noise model size mismatch");
+    std::lock_guard<std::mutex> lock(p->pattern_mu);
+    std::vector<float> v;
+    const nf_status s = pattern_candidate(*p, source, static_cast<cudaStream_t>(stream), v, err, len);
+    if (s != NF_OK) return s;
+    std::memcpy(power, v.data(), v.size() * sizeof(float));
+    return NF_OK;
+  });
+}
+
+nf_status nf_plan_prepare_pattern(nf_plan* p, nf_const_plane source, void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p != nullptr, "null plan");
+    nfb::require(p->t.needs_pattern, "FFT3D sampling is inactive");
+    if (p->model_ready.load(std::memory_order_acquire)) return NF_OK;
+    std::vector<float> v(size_t(p->t.bins));
+    nf_status s = nf_plan_pattern_candidate(p, source, v.data(), int(v.size()), stream, err, len);
+    if (s != NF_OK) return s;
+    return nf_plan_set_noise_model(p, v.data(), int(v.size()), err, len);
+  });
+}
+
 int nf_plan_model_state(const nf_plan* p) {
   if (!p) return -1;
-  const bool needs = p->t.noise_model;
+  const bool needs = p->t.noise_model || p->t.needs_pattern;
   return needs ? (p->model_ready.load(std::memory_order_acquire) ? 2 : 1) : 0;
 }
 

@@ -573,9 +573,32 @@ PlanTables build_fft3d(int w, int h, nf_format f, const nf_fft3d_config& c) {
   if (!p.preview) p.enhancement = enhancement_tables(c.bw, c.bh, factor, c);
   if (!p.preview && !p.enhancement.active()) p.enhancement = Enhancement{};
   p.spectral.fused_enhancement = !p.varying && !p.sampled && p.denoise && p.enhancement.active();
-  if (p.preview || (p.sampled && p.denoise))
-    throw std::invalid_argument(
-        "FFT3D sampled noise model (pfactor>0) and pshow preview are not implemented on the GPU path");
+  p.pfactor = c.pfactor;
+  p.px = c.px;
+  p.py = c.py;
+  p.needs_pattern = p.sampled && p.denoise;
+  if (p.preview || p.needs_pattern) {
+    // plan.cpp:142-158: candidate grid and the scoring weights q/(q+cutoff^2) with
+    // q = fx^2 + fy^2 on normalised frequencies.
+    if (c.px == 0 && c.py == 0)
+      require(p.gx.count >= 5 && p.gy.count >= 5, "FFT3D automatic pattern search requires a 5x5 grid");
+    else
+      require(c.px < p.gx.count && c.py < p.gy.count, "FFT3D pattern coordinates outside grid");
+    const float cutoff2 = finite(c.pcutoff * c.pcutoff);
+    require(cutoff2 > 0, "FFT3D pattern cutoff underflow");
+    const int K = c.bw / 2 + 1;
+    std::vector<float> fx(static_cast<std::size_t>(K));
+    for (int x = 0; x <= c.bw / 2; ++x) fx[std::size_t(x)] = 2 * float(x) / float(c.bw);
+    p.sample_weights.resize(std::size_t(c.bh) * K);
+    for (int y = 0; y < c.bh; ++y) {
+      const float fy = 2 * float(std::min(y, c.bh - y)) / float(c.bh);
+      const float other = fy * fy;
+      for (int x = 0; x < K; ++x) {
+        const float q = finite(other + finite(fx[std::size_t(x)] * fx[std::size_t(x)]));
+        p.sample_weights[std::size_t(y) * K + x] = finite(q / finite(q + cutoff2));
+      }
+    }
+  }
   if (c.degrid != 0) {
     std::vector<float> block(std::size_t(c.bh) * c.bw);
     const float peak = f.floating ? 1.0f : float((1 << f.bits) - 1);

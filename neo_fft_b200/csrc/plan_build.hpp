@@ -104,6 +104,10 @@ struct PlanTables {
   // FFT3D
   AxisWindow wx, wy;
   bool denoise = true, kalman = false, preview = false, sampled = false, varying = false;
+  bool needs_pattern = false;          // sampled && denoise: primary table from the pattern block
+  float pfactor = 0;
+  int px = 0, py = 0;                  // pattern block (0, 0: automatic search)
+  std::vector<float> sample_weights;   // [bh][bw/2+1] pattern scoring weights (plan.cpp:142-158)
   float sigma_eff = 0, norm = 0, beta = 1, kalman_r0 = 0, kalman_ratio2 = 0;
   Enhancement enhancement;
   // DFTTest

@@ -270,6 +270,36 @@ class Plan:
         """0: no sampled noise model; 1: waiting for one; 2: ready."""
         return int(self._lib.nf_plan_model_state(self._h))
 
+    @property
+    def needs_pattern_frame(self) -> bool:
+        """FFT3D pfactor > 0 with denoising (plan.hpp:90)."""
+        return self.model_state != 0 and isinstance(self.config, FFT3DConfig)
+
+    @property
+    def pattern_ready(self) -> bool:
+        return self.model_state == 2
+
+    def pattern_candidate(self, source, stream=None) -> np.ndarray:
+        """plan.cpp:271-277 on a device plane: the chosen block's scaled power (bins floats)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        out = np.zeros(self.bins, np.float32)
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_plan_pattern_candidate(self._h, _plane(source, True), ctypes.c_void_p(out.ctypes.data),
+                                                        out.size, ctypes.c_void_p(s), err, 512), err.value)
+        return out
+
+    def prepare_pattern(self, source, stream=None) -> None:
+        """prepare_pattern (plan.hpp:95-97): search and publish unless a model is published."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_plan_prepare_pattern(self._h, _plane(source, True), ctypes.c_void_p(s), err, 512),
+                    err.value)
+
+    def publish_pattern(self, power) -> None:
+        self.set_noise_model(power)
+
     def set_noise_model(self, power) -> None:
         p = np.ascontiguousarray(power, np.float32)
         err = ctypes.create_string_buffer(512)

@@ -72,6 +72,8 @@ def load() -> ctypes.CDLL:
             "ref_dft_profile": (ci, [ctypes.POINTER(C.NfDftConfig), ctypes.c_float, FP, cp, cs]),
             "ref_fft3d_profile": (ci, [ci, ci, FP, FP, cp, cs]),
             "ref_plan_prepare_noise": (ci, [vp, FP, ci, FP, ci, cp, cs]),
+            "ref_plan_pattern_candidate": (ci, [vp, ci, C.NfConstPlane, FP, ci, cp, cs]),
+            "ref_plan_publish_pattern": (ci, [vp, FP, ci, cp, cs]),
             "ref_dither": (ci, [FP, ci, ci, ci, ctypes.POINTER(ctypes.c_ubyte), ci, ci, ci, ci, ci, cp, cs]),
             "ref_dither_hash": (ctypes.c_uint, [ctypes.c_uint] * 5),
         }
@@ -170,6 +172,20 @@ class RefPlan:
         _raise(self.lib.ref_plan_prepare_noise(self.h, fp(slices), int(slices.shape[0]), fp(out), out.size, err, 512),
                err)
         return out
+
+    def pattern_candidate(self, src) -> np.ndarray:
+        from neo_fft_b200 import _capi as C
+        src = np.asarray(src)
+        out = np.zeros(self.bins, np.float32)
+        err = ctypes.create_string_buffer(512)
+        _raise(self.lib.ref_plan_pattern_candidate(self.h, _storage(src), C.NfConstPlane(src.ctypes.data, src.shape[1],
+               src.shape[0], src.strides[0]), fp(out), out.size, err, 512), err)
+        return out
+
+    def publish_pattern(self, power) -> None:
+        p = np.ascontiguousarray(power, np.float32)
+        err = ctypes.create_string_buffer(512)
+        _raise(self.lib.ref_plan_publish_pattern(self.h, fp(p), p.size, err, 512), err)
 
     # Kalman
     def kalman_state(self):

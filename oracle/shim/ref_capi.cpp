@@ -204,6 +204,28 @@ int ref_kalman_read(void* s, float* last, float* cov, float* proc) {
   std::memcpy(proc, st.process.data(), st.process.size() * sizeof(float));
   return 0;
 }
+// Plan::pattern_candidate<T> (plan.cpp:271-277) copied to `power`, and publish_pattern.
+int ref_plan_pattern_candidate(void* p, int storage, nf_const_plane src, float* power, int count, char* err,
+                               size_t len) {
+  const Plan& pl = *static_cast<RefPlan*>(p)->plan;
+  return guarded(err, len, [&] {
+    runtime::PublishedModel::Model m;
+    if (storage == 1)
+      m = pl.pattern_candidate<std::uint8_t>({static_cast<const std::uint8_t*>(src.data), src.width, src.height, src.stride_bytes});
+    else if (storage == 2)
+      m = pl.pattern_candidate<std::uint16_t>({static_cast<const std::uint16_t*>(src.data), src.width, src.height, src.stride_bytes});
+    else
+      m = pl.pattern_candidate<float>({static_cast<const float*>(src.data), src.width, src.height, src.stride_bytes});
+    if (!m || int(m->size()) != count) throw std::invalid_argument("pattern size mismatch");
+    std::memcpy(power, m->data(), m->size() * sizeof(float));
+  });
+}
+int ref_plan_publish_pattern(void* p, const float* power, int count, char* err, size_t len) {
+  const Plan& pl = *static_cast<RefPlan*>(p)->plan;
+  return guarded(err, len, [&] {
+    pl.publish_pattern(std::make_shared<const std::vector<float>>(power, power + count));
+  });
+}
 int ref_kalman_advance(void* p, int storage, nf_const_plane src, void* s, char* err, size_t len) {
   const Plan& pl = *static_cast<RefPlan*>(p)->plan;
   auto& st = *static_cast<KalmanState*>(s);

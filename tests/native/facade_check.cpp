@@ -56,6 +56,22 @@ int main() {
         });
     std::printf("seek%d %llu\n", n, (unsigned long long)fnv(fdst.data(), fdst.size() * 4));
   }
+  // sampled FFT3D model: prepare_pattern on a frame, then filter another
+  {
+    FFT3DConfig pc;
+    pc.bw = pc.bh = 16; pc.ow = pc.oh = 8; pc.pfactor = 1.0f;
+    std::vector<std::uint8_t> a(std::size_t(w) * h), b(a.size()), o(a.size());
+    for (std::size_t i = 0; i < a.size(); ++i) {
+      a[i] = std::uint8_t((i * 131 + (i / w) * 7) % 200 + 20);
+      b[i] = std::uint8_t((i * 97 + (i / w) * 13) % 180 + 30);
+    }
+    Plan pp(w, h, SampleFormat{8, false, false}, pc);
+    std::printf("pattern_needed %d\n", int(pp.needs_pattern_frame() && !pp.pattern_ready()));
+    pp.prepare_pattern<std::uint8_t>({a.data(), w, h, w});
+    span2d::Plane<const std::uint8_t> bs(b.data(), w, h, w);
+    pp.process_at<std::uint8_t>({&bs, 1}, span2d::Plane<std::uint8_t>(o.data(), w, h, w), 0, 0);
+    std::printf("pattern %llu\n", (unsigned long long)fnv(o.data(), o.size()));
+  }
   try {
     FFT3DConfig bad;
     bad.bt = 7;

@@ -98,6 +98,14 @@ def test_cpp_facade_matches_python_path(cuda):
     out_t = cuda.empty_like(d)
     kp.render_kalman(d, out_t, st)
     assert int(got["kalman"]) == fnv(out_t.cpu().numpy().tobytes())
+    # sampled FFT3D pattern through the facade equals the Python path
+    assert got["pattern_needed"] == "1"
+    idx = np.arange(w * h, dtype=np.int64)
+    pa = ((idx * 131 + (idx // w) * 7) % 200 + 20).astype(np.uint8).reshape(h, w)
+    pb = ((idx * 97 + (idx // w) * 13) % 180 + 30).astype(np.uint8).reshape(h, w)
+    pp = Plan(w, h, SampleFormat(8), FFT3DConfig(bw=16, bh=16, ow=8, oh=8, pfactor=1.0))
+    pp.prepare_pattern(cuda.from_numpy(pa).cuda())
+    assert int(got["pattern"]) == fnv(pp.process(pb).tobytes())
     # the C++ checkpoint/seek policy equals the Python mirror
     from neo_fft_b200.checkpoints import KalmanSeek
     frames = [cuda.from_numpy(((np.arange(w * h, dtype=np.int64) * 7919 + f * 104729) % 1000 / 1000.0)

@@ -168,6 +168,10 @@ def test_dft_plan_tables_match_reference(tb, ref, w, h, fmt, cfg):
     (DFTConfig(slocation=[0, 1, 0.5]), "DFTTest curve requires frequency/value pairs"),
     (DFTConfig(slocation=[0.1, 1, 1, 2]), "DFTTest curve requires endpoints 0 and 1"),
     (DFTConfig(pmin=5, pmax=1), "DFTTest pmin exceeds pmax"),
+    (FFT3DConfig(bw=64, bh=64, ow=16, oh=16, pfactor=1.0), "FFT3D automatic pattern search requires a 5x5 grid"),
+    (FFT3DConfig(pfactor=1.0, px=40, py=1), "FFT3D pattern coordinates outside grid"),
+    (FFT3DConfig(bw=64, bh=64, ow=16, oh=16, pshow=True, sigma2=3.0),
+     "FFT3D automatic pattern search requires a 5x5 grid"),
 ])
 def test_config_errors_match_reference(tb, ref, cfg, msg):
     algo = 0 if isinstance(cfg, FFT3DConfig) else 1

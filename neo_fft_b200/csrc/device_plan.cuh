@@ -71,6 +71,7 @@ struct DevPlan {
   float noise_uniform, noise_mult, lower;
   int kalman_fp64;
   float kalman_r0, kalman_ratio2;
+  int raw_out;  // u8 output: store the unconverted accumulator as float (input of the dither pass)
 };
 
 NF_HD bool isfin(float v) {

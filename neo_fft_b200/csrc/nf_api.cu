@@ -11,6 +11,7 @@
 #include "adjoint.cuh"
 #include "tile_temporal.cuh"
 #include "pattern.cuh"
+#include "dither.cuh"
 
 #include <cuda_runtime.h>
 
@@ -601,10 +602,55 @@ nf_status preview_pattern(const nf_plan& p, const nf_const_plane& src, const nf_
   return NF_OK;
 }
 
+// DFTTest 8-bit output with dither > 0 goes through the error-diffusion pass
+// (plan.cpp:617-623); other formats ignore dither.
+bool dithers(const nfb::PlanTables& t) {
+  return t.algo == nfb::Algo::DFTTest && t.dither > 0 && !t.format.floating && t.format.bits == 8;
+}
+
+nf_status filter_device(const nf_plan& p, const nfd::DevPlan& d, const nf_const_plane* sources, int n,
+                        const int* targets, int nt, nf_plane dst, cudaStream_t st, char* err, size_t len);
+
+// Filters into a float accumulator plane (stream-ordered scratch), then dithers it into dst.
+nf_status process_dithered(const nf_plan& p, const nf_const_plane* sources, int n, const int* targets, int nt,
+                           nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len) {
+  nfb::require(frame >= 0 && plane >= 0, "invalid dither coordinates or mode");
+  const int W = p.t.gx.length, H = p.t.gy.length;
+  const size_t pitch = ((size_t(W) * sizeof(float) + 255) / 256) * 256;
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, pitch * size_t(H) + size_t(W) * sizeof(float), st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
+  auto* acc = static_cast<float*>(scratch);
+  float* boundary = reinterpret_cast<float*>(static_cast<unsigned char*>(scratch) + pitch * size_t(H));
+  nfd::DevPlan d = p.dev;
+  d.raw_out = 1;
+  const nf_plane raw{acc, W, H, ptrdiff_t(pitch)};
+  const nf_status s = filter_device(p, d, sources, n, targets, nt, raw, st, err, len);
+  if (s == NF_OK) {
+    nfd::dither_kernel<<<1, std::min(nfd::kDitherRows, H), 0, st>>>(
+        acc, (long long)(pitch / sizeof(float)), static_cast<unsigned char*>(dst.data), (long long)dst.stride_bytes, W,
+        H, p.t.dither, unsigned(p.t.dither_seed), unsigned(frame), unsigned(plane), boundary, p.err);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(scratch, st);
+  if (s != NF_OK) return s;
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  return NF_OK;
+}
+
 nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n, const int* targets, int nt,
                           nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len) {
-  (void)frame;
-  (void)plane;
+  if (dithers(p.t)) {
+    validate_call(p, sources, n, targets, nt, dst);
+    return process_dithered(p, sources, n, targets, nt, dst, frame, plane, st, err, len);
+  }
+  return filter_device(p, p.dev, sources, n, targets, nt, dst, st, err, len);
+}
+
+// The filter proper with the device plan `d` (the plan's own, or a copy that keeps the
+// raw accumulator for the dither pass).
+nf_status filter_device(const nf_plan& p, const nfd::DevPlan& d, const nf_const_plane* sources, int n,
+                        const int* targets, int nt, nf_plane dst, cudaStream_t st, char* err, size_t len) {
   const Checked c = validate_call(p, sources, n, targets, nt, dst);
   cudaError_t e;
   if (p.t.algo == nfb::Algo::FFT3D && p.t.kalman)
@@ -615,7 +661,7 @@ nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n,
     return fail(err, len, "FFT3D sampled model not initialized", NF_INVALID_ARGUMENT);
   if (p.t.preview) return preview_pattern(p, sources[0], dst, st, err, len);
   if (c.tslots == 1 && !p.t.temporal_ola) {
-    e = run_spatial(p.dev, sources[0].data, sources[0].stride_bytes, dst.data, dst.stride_bytes, nullptr, st);
+    e = run_spatial(d, sources[0].data, sources[0].stride_bytes, dst.data, dst.stride_bytes, nullptr, st);
   } else {
     nfd::VolumeSources v{};
     for (int j = 0; j < n; ++j) {
@@ -625,7 +671,7 @@ nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n,
     v.ola = p.t.temporal_ola ? 1 : 0;
     v.nblocks = p.t.temporal_ola ? nt : 1;
     for (int i = 0; p.t.temporal_ola && i < nt; ++i) v.target[i] = targets[i];
-    e = run_volume(p.dev, v, dst.data, dst.stride_bytes, st);
+    e = run_volume(d, v, dst.data, dst.stride_bytes, st);
   }
   if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
   return NF_OK;
@@ -801,6 +847,7 @@ nf_status nf_plan_process_planes_device(const nf_plan* p, const nf_const_plane* 
     nfb::require(!(p->t.algo == nfb::Algo::FFT3D && p->t.kalman), "Kalman plans render through nf_kalman_render_device");
     nfb::require(p->t.temporal_size == 1 && !p->t.temporal_ola,
                  "multi-plane calls take single-frame plans (FFT3D bt=1, DFTTest tbsize=1)");
+    nfb::require(!dithers(p->t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
     nfd::PlaneJobs J{};
     J.n = nplanes;
     for (int i = 0; i < nplanes; ++i) {
@@ -1098,6 +1145,7 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
       const nf_plan& p = *it.plan;
       nfb::require(!p.t.kalman && (p.t.temporal_size == 1 || p.t.algo == nfb::Algo::FFT3D) && !p.t.temporal_ola,
                    "batch items must be single-frame plans");
+      nfb::require(!dithers(p.t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
       validate_call(p, &it.source, 1, nullptr, 0, it.dst);
       const int storage = storage_of(p.t.format);
       int gi = -1;
@@ -1249,6 +1297,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       nfb::require(p.t.bh == b->bh && p.t.bw == b->bw && storage == b->storage && (dft ? 1 : 0) == b->slice,
                    "clip batch items must share algorithm, block shape and sample storage");
       nfb::require(!dft || it.nframes >= p.t.temporal_size, "DFTTest clips must hold at least tbsize frames");
+      nfb::require(!dithers(p.t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
       const size_t elem = size_t(storage);
       for (int f = 0; f < it.nframes; ++f) {
         if (dft) {

@@ -46,6 +46,10 @@ __device__ __forceinline__ int floor_div_i(int v, int d) { return v >= 0 ? v / d
 // truncated; FFT3D float clipped to [0,1]; DFTTest float acc*scale unclipped.
 template <int STORAGE>
 __device__ __forceinline__ void store_sample(unsigned char* row, int x, float acc, const DevPlan& P) {
+  if (STORAGE == kStoreU8 && P.raw_out) {  // dithered u8 output: the dither pass converts
+    reinterpret_cast<float*>(row)[x] = acc;
+    return;
+  }
   if (STORAGE == kStoreF32) {
     float v;
     if (P.algo == 0) v = acc < 0.0f ? 0.0f : (1.0f < acc ? 1.0f : acc);

@@ -245,6 +245,23 @@ nf_status nf_plan_pattern_candidate_host(const nf_plan* plan, nf_const_plane sou
 nf_status nf_plan_prepare_pattern_host(nf_plan* plan, nf_const_plane source, void* stream, char* err,
                                        size_t err_len);
 
+/* Region of interest and interlaced packing (src/plugin/roi.hpp:6-40). The host layer
+ * filters the ROI of a plane as its own image; with `interlaced`, the packed image holds
+ * the top field's rows in order followed by the bottom field's rows in reverse order, so
+ * reflection at the packed image's edges stays within one field. nf_roi_make validates
+ * the margins like make_roi (chroma margins must align to the subsampling, the ROI must be
+ * nonempty, interlaced heights even); nf_roi_pack_device / nf_roi_unpack_device copy
+ * between a full device plane and its packed image (elem_bytes 1, 2 or 4). */
+typedef struct nf_roi {
+  int left, top, width, height, interlaced;
+} nf_roi;
+nf_status nf_roi_make(int width, int height, int sub_w, int sub_h, int left, int top, int right, int bottom,
+                      int interlaced, nf_roi* roi, char* err, size_t err_len);
+nf_status nf_roi_pack_device(const nf_roi* roi, nf_const_plane source, nf_plane packed, int elem_bytes, void* stream,
+                             char* err, size_t err_len);
+nf_status nf_roi_unpack_device(const nf_roi* roi, nf_const_plane packed, nf_plane dst, int elem_bytes, void* stream,
+                               char* err, size_t err_len);
+
 /* Differentiable form (no reference counterpart; the reference has no gradients).
  * DFTTest plans keep their per-bin primary table A ([tbsize][sbsize][sbsize/2+1],
  * already calibrated: the threshold the Wiener gain compares with) in device memory.

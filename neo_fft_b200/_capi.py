@@ -63,6 +63,10 @@ class NfBatchItem(ctypes.Structure):
     _fields_ = [("plan", c_void_p), ("source", NfConstPlane), ("dst", NfPlane)]
 
 
+class NfRoi(ctypes.Structure):
+    _fields_ = [("left", c_int), ("top", c_int), ("width", c_int), ("height", c_int), ("interlaced", c_int)]
+
+
 class NfClipItem(ctypes.Structure):
     _fields_ = [("plan", c_void_p), ("frames", ctypes.POINTER(NfConstPlane)), ("dsts", ctypes.POINTER(NfPlane)),
                 ("nframes", c_int)]
@@ -118,6 +122,11 @@ PROTOTYPES = {
     "nf_plan_pattern_candidate_host": (c_int, [c_void_p, NfConstPlane, c_void_p, c_int, c_void_p, ctypes.c_char_p,
                                                c_size_t]),
     "nf_plan_prepare_pattern_host": (c_int, [c_void_p, NfConstPlane, c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_roi_make": (c_int, [c_int] * 9 + [ctypes.POINTER(NfRoi), ctypes.c_char_p, c_size_t]),
+    "nf_roi_pack_device": (c_int, [ctypes.POINTER(NfRoi), NfConstPlane, NfPlane, c_int, c_void_p, ctypes.c_char_p,
+                                   c_size_t]),
+    "nf_roi_unpack_device": (c_int, [ctypes.POINTER(NfRoi), NfConstPlane, NfPlane, c_int, c_void_p, ctypes.c_char_p,
+                                     c_size_t]),
     "nf_plan_set_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_plan_get_primary": (c_int, [c_void_p, c_void_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_dft_backward_scratch_bytes": (c_int, [c_void_p, c_int, ctypes.POINTER(c_size_t)]),

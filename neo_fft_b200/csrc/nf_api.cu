@@ -1634,6 +1634,84 @@ int nf_plan_model_state(const nf_plan* p) {
   return needs ? (p->model_ready.load(std::memory_order_acquire) ? 2 : 1) : 0;
 }
 
+nf_status nf_roi_make(int width, int height, int sub_w, int sub_h, int left, int top, int right, int bottom,
+                      int interlaced, nf_roi* roi, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(roi != nullptr, "null ROI output");
+    nfb::require(sub_w >= 0 && sub_w < 8 && sub_h >= 0 && sub_h < 8 && left >= 0 && top >= 0 && right >= 0 &&
+                     bottom >= 0,
+                 "ROI margins and subsampling must be nonnegative");
+    const int ax = 1 << sub_w, ay = 1 << sub_h;
+    nfb::require(left % ax == 0 && right % ax == 0 && top % ay == 0 && bottom % ay == 0,
+                 "selected chroma ROI margins must align to subsampling");
+    const int l = left / ax, r = right / ax, t = top / ay, b = bottom / ay;
+    nfb::require(l < width && r < width - l && t < height && b < height - t, "ROI must be nonempty");
+    *roi = {l, t, width - l - r, height - t - b, interlaced ? 1 : 0};
+    nfb::require(!interlaced || roi->height % 2 == 0, "interlaced ROI height must be even");
+    return NF_OK;
+  });
+}
+
+extern "C++" {
+namespace {
+// Packed row y of the ROI <- plane row top + roi_row(y) (ROI::row, roi.hpp:8-10).
+__device__ __forceinline__ int roi_row(const nf_roi& r, int y) {
+  return r.interlaced ? (y < r.height / 2 ? 2 * y : 2 * (r.height - 1 - y) + 1) : y;
+}
+template <class T>
+__global__ void roi_copy_kernel(nf_roi r, const unsigned char* src, long long ss, unsigned char* dst, long long ds,
+                                int unpack) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= r.width) return;
+  const int py = r.top + roi_row(r, y);
+  if (!unpack) {
+    reinterpret_cast<T*>(dst + ptrdiff_t(y) * ds)[x] = reinterpret_cast<const T*>(src + ptrdiff_t(py) * ss)[r.left + x];
+  } else {
+    reinterpret_cast<T*>(dst + ptrdiff_t(py) * ds)[r.left + x] = reinterpret_cast<const T*>(src + ptrdiff_t(y) * ss)[x];
+  }
+}
+nf_status roi_copy(const nf_roi* roi, const void* src, int sw, int sh, ptrdiff_t ss, void* dst, int dw, int dh,
+                   ptrdiff_t ds, int elem, bool unpack, void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(roi && src && dst, "null ROI or plane");
+    nfb::require(elem == 1 || elem == 2 || elem == 4, "element size must be 1, 2 or 4 bytes");
+    const nf_roi& r = *roi;
+    nfb::require(r.width > 0 && r.height > 0 && r.left >= 0 && r.top >= 0 && (!r.interlaced || r.height % 2 == 0),
+                 "invalid ROI");
+    const int fw = unpack ? dw : sw, fh = unpack ? dh : sh, pw = unpack ? sw : dw, ph = unpack ? sh : dh;
+    nfb::require(r.left + r.width <= fw && r.top + r.height <= fh, "ROI outside the plane");
+    nfb::require(pw == r.width && ph == r.height, "packed plane dimensions differ from ROI");
+    plane_extent(sw, sh, ss, size_t(elem));
+    plane_extent(dw, dh, ds, size_t(elem));
+    check_pointer(src, size_t(elem));
+    check_pointer(dst, size_t(elem));
+    disjoint(src, plane_extent(sw, sh, ss, size_t(elem)), dst, plane_extent(dw, dh, ds, size_t(elem)));
+    const dim3 b(256), g((r.width + 255) / 256, r.height);
+    auto* s = static_cast<const unsigned char*>(src);
+    auto* d = static_cast<unsigned char*>(dst);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (elem == 1) roi_copy_kernel<unsigned char><<<g, b, 0, st>>>(r, s, ss, d, ds, unpack ? 1 : 0);
+    else if (elem == 2) roi_copy_kernel<unsigned short><<<g, b, 0, st>>>(r, s, ss, d, ds, unpack ? 1 : 0);
+    else roi_copy_kernel<float><<<g, b, 0, st>>>(r, s, ss, d, ds, unpack ? 1 : 0);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+    return NF_OK;
+  });
+}
+} // namespace
+} // extern "C++"
+
+nf_status nf_roi_pack_device(const nf_roi* roi, nf_const_plane source, nf_plane packed, int elem, void* stream,
+                             char* err, size_t len) {
+  return roi_copy(roi, source.data, source.width, source.height, source.stride_bytes, packed.data, packed.width,
+                  packed.height, packed.stride_bytes, elem, false, stream, err, len);
+}
+nf_status nf_roi_unpack_device(const nf_roi* roi, nf_const_plane packed, nf_plane dst, int elem, void* stream,
+                               char* err, size_t len) {
+  return roi_copy(roi, packed.data, packed.width, packed.height, packed.stride_bytes, dst.data, dst.width, dst.height,
+                  dst.stride_bytes, elem, true, stream, err, len);
+}
+
 nf_status nf_plan_set_primary(nf_plan* p, const float* table, int count, void* stream, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(p && table, "null plan or table");

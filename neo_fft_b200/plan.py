@@ -469,6 +469,54 @@ class DFTNoise:
             p.set_noise_model(self.power)
 
 
+@dataclass
+class ROI:
+    """Region of interest of a plane (src/plugin/roi.hpp:6-11); `interlaced` packs the top
+    field's rows, then the bottom field's rows in reverse order."""
+    left: int
+    top: int
+    width: int
+    height: int
+    interlaced: bool = False
+
+    @staticmethod
+    def make(width, height, sub_w, sub_h, left=0, top=0, right=0, bottom=0, interlaced=False) -> "ROI":
+        """make_roi (roi.hpp:13-23): margins in luma pixels, reduced by the subsampling."""
+        r = C.NfRoi()
+        err = ctypes.create_string_buffer(256)
+        C.raise_for(C.load().nf_roi_make(width, height, sub_w, sub_h, left, top, right, bottom, int(interlaced),
+                                         ctypes.byref(r), err, 256), err.value)
+        return ROI(r.left, r.top, r.width, r.height, bool(r.interlaced))
+
+    def row(self, y: int) -> int:
+        if not self.interlaced:
+            return y
+        return 2 * y if y < self.height // 2 else 2 * (self.height - 1 - y) + 1
+
+    def _c(self):
+        return C.NfRoi(self.left, self.top, self.width, self.height, int(self.interlaced))
+
+    def pack(self, plane, packed=None, stream=None):
+        """Copies the ROI of a device plane into its packed image (PackedROI, roi.hpp:25-35)."""
+        import torch
+        if packed is None:
+            packed = torch.empty((self.height, self.width), dtype=plane.dtype, device=plane.device)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(256)
+        C.raise_for(C.load().nf_roi_pack_device(ctypes.byref(self._c()), _plane(plane, True), _plane(packed, False),
+                                                plane.element_size(), ctypes.c_void_p(s), err, 256), err.value)
+        return packed
+
+    def unpack(self, packed, dst, stream=None):
+        """Writes a packed image back into the ROI of a device plane (PackedROI::write)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(256)
+        C.raise_for(C.load().nf_roi_unpack_device(ctypes.byref(self._c()), _plane(packed, True), _plane(dst, False),
+                                                  packed.element_size(), ctypes.c_void_p(s), err, 256), err.value)
+        return dst
+
+
 class ClipBatch:
     """Temporal clips in batched form: `clips` is a list of (plan, frames, dsts) with
     device tensors; every output frame is filtered with the host layer's frame selection

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <atomic>
 #include <cstring>
 #include <memory>
@@ -647,6 +648,117 @@ nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n,
   return filter_device(p, p.dev, sources, n, targets, nt, dst, st, err, len);
 }
 
+cudaError_t launch_temporal_shape(int bh, int bw, int storage, int slice, const nfd::BatchWork& w, int ctas,
+                                  size_t smem, cudaStream_t st);
+cudaError_t launch_volume_spectra_shape(int bh, int bw, int storage, const nfd::VolumeSpectraWork& w, int items,
+                                        size_t smem, cudaStream_t st);
+
+// Per-call temporal filtering in two passes over stream-ordered scratch (the clip form's
+// kernels for a single output): FFT3D bt 2..5 — the T slots' spatial spectra, then the
+// temporal strip; DFTTest tmode 1 with one covering block — the volume's filtered slice
+// spectra, then the slice strip of the target. The work tables travel in the same
+// allocation (uploaded from host memory, which the copy stages before returning).
+struct TwoPassHeader {
+  nfd::DevPlan plan;
+  nfd::StripShape shape;
+  nfd::PlaneJob job;
+  int base[2];
+  int tiles_x;
+  int counter;
+};
+
+nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_plane* sources, int T, int target,
+                       const nf_plane& dst, cudaStream_t st, char* err, size_t len) {
+  const auto& t = p.t;
+  const bool slice = t.algo == nfb::Algo::DFTTest;
+  const int storage = storage_of(t.format);
+  const size_t frame = size_t(t.gy.count) * t.bins * t.gx.count;  // complex per slot spectrum
+  int nbc = 1;
+  for (int n = 2; n <= std::min(slice ? 32 : 16, t.gx.count); ++n)
+    if ((slice ? nfd::volume_spectra_smem_bytes(t.bh, t.bw, T, t.gx.step, n)
+               : nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, n)) <= 100 * 1024)
+      nbc = n;
+  const size_t smem1 = slice ? nfd::volume_spectra_smem_bytes(t.bh, t.bw, T, t.gx.step, nbc)
+                             : nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, nbc);
+  const int chunks = (t.gx.count + nbc - 1) / nbc, items = chunks * t.gy.count;
+  nfd::StripShape S = pick_strip(d, plain_ctas(d));
+  const size_t smem2 = nfd::strip_smem_bytes(t.bh, t.bw, S);
+  const int tx = (t.gx.length + S.tw - 1) / S.tw, ty = (t.gy.length + S.th - 1) / S.th;
+
+  auto al = [](size_t n) { return (n + 255) & ~size_t(255); };
+  const size_t o_hdr = 0, o_slots = al(sizeof(TwoPassHeader)), o_jobs = o_slots + al(sizeof(cf*) * 16),
+               o_base = o_jobs + al(std::max(sizeof(nfd::VolumeSpectraJob), sizeof(nfd::SpectraJob) * size_t(T))),
+               o_spec = o_base + al(sizeof(int) * size_t(T + 1));
+  const size_t bytes = o_spec + size_t(T) * al(frame * sizeof(cf));
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
+  auto* b = static_cast<unsigned char*>(scratch);
+  auto spec = [&](int z) { return reinterpret_cast<cf*>(b + o_spec + size_t(z) * al(frame * sizeof(cf))); };
+
+  std::vector<unsigned char> host(o_spec, 0);
+  auto* hdr = reinterpret_cast<TwoPassHeader*>(host.data() + o_hdr);
+  hdr->plan = d;
+  hdr->shape = S;
+  const int zt = slice ? target : 0;
+  hdr->job = {nullptr, 0, static_cast<unsigned char*>(dst.data), (long long)dst.stride_bytes, nullptr, 0, zt,
+              reinterpret_cast<const cf* const*>(b + o_slots + (slice ? sizeof(cf*) * size_t(zt) : 0))};
+  hdr->base[0] = 0;
+  hdr->base[1] = tx * ty;
+  hdr->tiles_x = tx;
+  hdr->counter = 0;
+  auto* slots = reinterpret_cast<const cf**>(host.data() + o_slots);
+  for (int z = 0; z < T; ++z) slots[z] = spec(z);
+  auto* base = reinterpret_cast<int*>(host.data() + o_base);
+  if (slice) {
+    auto* vj = reinterpret_cast<nfd::VolumeSpectraJob*>(host.data() + o_jobs);
+    for (int z = 0; z < T; ++z) {
+      vj->src[z] = static_cast<const unsigned char*>(sources[z].data);
+      vj->src_stride[z] = sources[z].stride_bytes;
+      vj->out[z] = spec(z);
+    }
+    vj->plan = 0;
+    vj->chunks_x = chunks;
+    base[0] = 0;
+    base[1] = items;
+  } else {
+    auto* sj = reinterpret_cast<nfd::SpectraJob*>(host.data() + o_jobs);
+    for (int z = 0; z < T; ++z) {
+      sj[z] = {static_cast<const unsigned char*>(sources[z].data), (long long)sources[z].stride_bytes, spec(z), 0,
+               chunks};
+      base[z] = z * items;
+    }
+    base[T] = T * items;
+  }
+  e = cudaMemcpyAsync(scratch, host.data(), host.size(), cudaMemcpyHostToDevice, st);
+  const auto* dplan = reinterpret_cast<const nfd::DevPlan*>(b + o_hdr + offsetof(TwoPassHeader, plan));
+  if (e == cudaSuccess) {
+    if (slice) {
+      const nfd::VolumeSpectraWork w{dplan, reinterpret_cast<const nfd::VolumeSpectraJob*>(b + o_jobs),
+                                     reinterpret_cast<const int*>(b + o_base), 1, nbc};
+      e = launch_volume_spectra_shape(t.bh, t.bw, storage, w, items, smem1, st);
+    } else {
+      const nfd::SpectraWork w{dplan, reinterpret_cast<const nfd::SpectraJob*>(b + o_jobs),
+                               reinterpret_cast<const int*>(b + o_base), T, nbc};
+      e = launch_spectra_shape(t.bh, t.bw, storage, w, T * items, smem1, st);
+    }
+  }
+  if (e == cudaSuccess) {
+    nfd::BatchWork w{};
+    w.plans = dplan;
+    w.shapes = reinterpret_cast<const nfd::StripShape*>(b + o_hdr + offsetof(TwoPassHeader, shape));
+    w.jobs = reinterpret_cast<const nfd::PlaneJob*>(b + o_hdr + offsetof(TwoPassHeader, job));
+    w.job_tile_base = reinterpret_cast<const int*>(b + o_hdr + offsetof(TwoPassHeader, base));
+    w.job_tiles_x = reinterpret_cast<const int*>(b + o_hdr + offsetof(TwoPassHeader, tiles_x));
+    w.njobs = 1;
+    w.counter = reinterpret_cast<int*>(b + o_hdr + offsetof(TwoPassHeader, counter));
+    e = launch_temporal_shape(t.bh, t.bw, storage, slice ? 1 : 0, w, std::min(tx * ty, plain_ctas(d)), smem2, st);
+  }
+  cudaFreeAsync(scratch, st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  return NF_OK;
+}
+
 // The filter proper with the device plan `d` (the plan's own, or a copy that keeps the
 // raw accumulator for the dither pass).
 nf_status filter_device(const nf_plan& p, const nfd::DevPlan& d, const nf_const_plane* sources, int n,
@@ -662,6 +774,11 @@ nf_status filter_device(const nf_plan& p, const nfd::DevPlan& d, const nf_const_
   if (p.t.preview) return preview_pattern(p, sources[0], dst, st, err, len);
   if (c.tslots == 1 && !p.t.temporal_ola) {
     e = run_spatial(d, sources[0].data, sources[0].stride_bytes, dst.data, dst.stride_bytes, nullptr, st);
+  } else if (p.t.algo == nfb::Algo::FFT3D && c.tslots == p.t.temporal_size && !p.t.preview) {
+    return run_two_pass(p, d, sources, c.tslots, 0, dst, st, err, len);
+  } else if (p.t.algo == nfb::Algo::DFTTest && p.t.temporal_ola && nt == 1 && !p.t.center &&
+             p.t.temporal_size <= nfd::kMaxVolumeSlots) {
+    return run_two_pass(p, d, sources, p.t.temporal_size, targets[0], dst, st, err, len);
   } else {
     nfd::VolumeSources v{};
     for (int j = 0; j < n; ++j) {

@@ -113,6 +113,51 @@ __host__ __device__ inline size_t strip_smem_bytes(int bh, int bw, const StripSh
                           size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max));
 }
 
+// FFT3D bt=2..5 filter of one block row's (bin, block) elements across the T slot
+// spectra (spectral.cpp:90-160) with T = TC known at compile time; writes the recovered
+// spectrum into spec [bin][block].
+template <int TC>
+__device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const PlaneJob& J, const DevSpectral& filt,
+                                                         const cf* grid, float grid0, cf* spec, const float* dc, int NB,
+                                                         int nbx, int nel, size_t row_base, size_t cnt, int T,
+                                                         float invT, bool& bad) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+#pragma unroll 2
+  for (int e = tid; e < nel; e += nthr) {
+    const int kk = e / nbx, b = e - kk * nbx;
+    const size_t at = row_base + size_t(kk) * cnt + b;
+    cf v[TC];
+#pragma unroll
+    for (int j = 0; j < TC; ++j)
+      if (j < T) v[j] = J.tspec[j][at];
+    const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
+    if (grid && !isfin(g)) bad = true;
+    const cf M = grid ? cf{fmul(g, grid[kk].r), fmul(g, grid[kk].i)} : cf{0.0f, 0.0f};
+    const cf gT = {fmul(M.r, float(T)), fmul(M.i, float(T))};
+    const float noise = filt.primary ? fmul(filt.primary[kk], P.noise_mult) : P.noise_uniform;
+    if (!isfin(noise)) bad = true;
+    cf yv = {0.0f, 0.0f};
+#pragma unroll
+    for (int m = 0; m < TC; ++m) {
+      if (m >= T) break;
+      cf F = {0.0f, 0.0f};
+#pragma unroll
+      for (int j = 0; j < TC; ++j)
+        if (j < T) F = nf::cadd(F, nf::cmul_plain(v[j], P.tfwd[m * T + j]));
+      const cf R = m == 0 ? nf::csub(F, gT) : F;
+      const float power = fadd(fmul(R.r, R.r), fmul(R.i, R.i));
+      if (!isfin(power)) bad = true;
+      const float q = fadd(power, 1e-15f);
+      const float gr = fdiv(fsub(q, noise), q);
+      const float gain = gr < P.lower ? P.lower : gr;
+      cf Rf = {fmul(gain, R.r), fmul(gain, R.i)};
+      if (m == 0) Rf = nf::cadd(Rf, gT);
+      yv = nf::cadd(yv, nf::cmul_plain(Rf, P.tinv[m]));
+    }
+    spec[size_t(kk) * NB + b] = {fmul(yv.r, invT), fmul(yv.i, invT)};
+  }
+}
+
 template <int BHC, int BWC, int STORAGE, int SRC = kSrcPixels>
 __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, const StripShape& S, int px0, int py0,
                                            float* smem) {
@@ -275,33 +320,11 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       for (int b = tid; b < nbx; b += nthr) dc[b] = J.tspec[c][row_base + b].r;
       __syncthreads();
       const int nel = bins * nbx;
-#pragma unroll 2
-      for (int e = tid; e < nel; e += nthr) {
-        const int kk = e / nbx, b = e - kk * nbx;
-        const size_t at = row_base + size_t(kk) * cnt + b;
-        cf v[5];
-        for (int j = 0; j < T; ++j) v[j] = J.tspec[j][at];
-        const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
-        if (grid && !isfin(g)) bad = true;
-        const cf M = grid ? cf{fmul(g, grid[kk].r), fmul(g, grid[kk].i)} : cf{0.0f, 0.0f};
-        const cf gT = {fmul(M.r, float(T)), fmul(M.i, float(T))};
-        const float noise = filt.primary ? fmul(filt.primary[kk], P.noise_mult) : P.noise_uniform;
-        if (!isfin(noise)) bad = true;
-        cf yv = {0.0f, 0.0f};
-        for (int m = 0; m < T; ++m) {
-          cf F = {0.0f, 0.0f};
-          for (int j = 0; j < T; ++j) F = nf::cadd(F, nf::cmul_plain(v[j], P.tfwd[m * T + j]));
-          const cf R = m == 0 ? nf::csub(F, gT) : F;
-          const float power = fadd(fmul(R.r, R.r), fmul(R.i, R.i));
-          if (!isfin(power)) bad = true;
-          const float q = fadd(power, 1e-15f);
-          const float gr = fdiv(fsub(q, noise), q);
-          const float gain = gr < P.lower ? P.lower : gr;
-          cf Rf = {fmul(gain, R.r), fmul(gain, R.i)};
-          if (m == 0) Rf = nf::cadd(Rf, gT);
-          yv = nf::cadd(yv, nf::cmul_plain(Rf, P.tinv[m]));
-        }
-        spec[size_t(kk) * NB + b] = {fmul(yv.r, invT), fmul(yv.i, invT)};
+      switch (T) {  // compile-time slot counts keep the slot values in registers
+        case 2: temporal_filter_elements<2>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
+        case 3: temporal_filter_elements<3>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
+        case 4: temporal_filter_elements<4>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
+        default: temporal_filter_elements<5>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
       }
       __syncthreads();
       if (enh.enh) {

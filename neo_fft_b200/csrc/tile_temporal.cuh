@@ -149,6 +149,48 @@ __host__ __device__ inline size_t volume_spectra_smem_bytes(int bh, int bw, int 
   return sizeof(float) * (h + size_t(bh) * pitch + 2 * size_t(T) * bh * K * nbc + nbc);
 }
 
+// Time axis of the volume pass for T slices (TC = T at compile time, 0 = runtime): the
+// forward transform along time per bin (the volume DC is bin 0 of slice 0 afterwards),
+// then the spectral filter on all T x bins and the inverse along time, every slice
+// written out.
+template <int TC>
+__device__ __forceinline__ void volume_time(const DevPlan& P, const VolumeSpectraJob& J, cf* spec, size_t slot,
+                                            int nbc, int nb, int bins, int T_rt, size_t row_base, float* dc,
+                                            bool& bad) {
+  const int T = TC > 0 ? TC : T_rt;
+  constexpr int CAP = TC > 0 ? TC : kMaxVolumeSlots;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int task = tid; task < bins * nb; task += nthr) {
+    const int kk = task / nb, b = task - kk * nb;
+    cf* bp = spec + size_t(kk) * nbc + b;
+    cf line[CAP];
+#pragma unroll
+    for (int z = 0; z < CAP; ++z)
+      if (z < T) line[z] = bp[size_t(z) * slot];
+    nf::fft_project<true, TC, 16>(line, T, P.twt);
+#pragma unroll
+    for (int z = 0; z < CAP; ++z)
+      if (z < T) bp[size_t(z) * slot] = line[z];
+    if (kk == 0) dc[b] = line[0].r;
+  }
+  __syncthreads();
+  const size_t cnt = size_t(P.gx.count);
+  for (int task = tid; task < bins * nb; task += nthr) {
+    const int kk = task / nb, b = task - kk * nb;
+    const cf* bp = spec + size_t(kk) * nbc + b;
+    const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
+                        ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
+    cf line[CAP];
+#pragma unroll
+    for (int z = 0; z < CAP; ++z)
+      if (z < T) line[z] = spectral_bin(bp[size_t(z) * slot], P.grid, z * bins + kk, g, P.filt, bad);
+    nf::fft_project<false, TC, 16>(line, T, P.twt);
+#pragma unroll
+    for (int z = 0; z < CAP; ++z)
+      if (z < T) J.out[z][row_base + size_t(kk) * cnt + b] = line[z];
+  }
+}
+
 // Pass 1 of the DFTTest slice form: per block row chunk, the 3-D forward transform of
 // each volume (spatial per slice, then time; the volume tile's phases A, B1 and T),
 // the spectral filter and the inverse along time; all T slices written out.
@@ -235,28 +277,15 @@ __global__ void __launch_bounds__(256) volume_spectra_batch_kernel(VolumeSpectra
       if (y < BH) sp[size_t(y) * K * nbc] = col[y];
   }
   __syncthreads();
-  // forward along time; the volume DC is bin 0 of slice 0 afterwards
-  for (int task = tid; task < bins * nb; task += nthr) {
-    const int kk = task / nb, b = task - kk * nb;
-    cf* bp = spec + size_t(kk) * nbc + b;
-    cf line[kMaxVolumeSlots];
-    for (int z = 0; z < T; ++z) line[z] = bp[size_t(z) * slot];
-    nf::fft_project<true, 0, 16>(line, T, P.twt);
-    for (int z = 0; z < T; ++z) bp[size_t(z) * slot] = line[z];
-    if (kk == 0) dc[b] = line[0].r;
-  }
-  __syncthreads();
-  const size_t cnt = size_t(gx.count);
-  const size_t row_base = size_t(by) * bins * cnt + size_t(bx0);
-  for (int task = tid; task < bins * nb; task += nthr) {
-    const int kk = task / nb, b = task - kk * nb;
-    const cf* bp = spec + size_t(kk) * nbc + b;
-    const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
-                        ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
-    cf line[kMaxVolumeSlots];
-    for (int z = 0; z < T; ++z) line[z] = spectral_bin(bp[size_t(z) * slot], P.grid, z * bins + kk, g, P.filt, bad);
-    nf::fft_project<false, 0, 16>(line, T, P.twt);
-    for (int z = 0; z < T; ++z) J.out[z][row_base + size_t(kk) * cnt + b] = line[z];
+  const size_t row_base = size_t(by) * bins * size_t(gx.count) + size_t(bx0);
+  switch (T) {  // compile-time lengths keep the temporal line in registers
+    case 2: volume_time<2>(P, J, spec, slot, nbc, nb, bins, T, row_base, dc, bad); break;
+    case 3: volume_time<3>(P, J, spec, slot, nbc, nb, bins, T, row_base, dc, bad); break;
+    case 4: volume_time<4>(P, J, spec, slot, nbc, nb, bins, T, row_base, dc, bad); break;
+    case 5: volume_time<5>(P, J, spec, slot, nbc, nb, bins, T, row_base, dc, bad); break;
+    case 6: volume_time<6>(P, J, spec, slot, nbc, nb, bins, T, row_base, dc, bad); break;
+    case 7: volume_time<7>(P, J, spec, slot, nbc, nb, bins, T, row_base, dc, bad); break;
+    default: volume_time<0>(P, J, spec, slot, nbc, nb, bins, T, row_base, dc, bad); break;
   }
   if (bad) atomicOr(P.err, kErrNonFinite);
 }

@@ -11,6 +11,8 @@ Workloads (one plane per launch, seeded synthetic content):
   fft3d48  FFT3D bt=3 bw=bh=48, ow=oh=24, sigma 3, sharpen 0.3, u16 (10-bit) 3840x2160
   kalman32 FFT3D bt=0 (Kalman advance), bw=bh=32, float 1920x1080
   dft12t5  DFTTest tbsize 5 tmode 1, sbsize 12 / sosize 9, ftype 1, float 1920x1080
+  clip12t5 DFTTest tbsize 5 tmode 1 sbsize 12 / sosize 9 ftype 1, float 1920x1080 clip of 10
+           frames as one clip batch (volume spectra pass + slice strips) per launch
   clip48   FFT3D bt=3 48x48 ow=oh=24 sigma 3 sharpen 0.3, 1920x1080 YUV420P10 clip of 6
            frames as one clip batch (spectra pass + temporal strips) per launch
   adjoint16 differentiable DFTTest: 16 float 256x256 noisy patches, sbsize 16 / sosize 8,
@@ -105,6 +107,17 @@ def main():
         torch.cuda.synchronize()
         for p in pls:
             p.sync_status()
+        return
+    elif wl == "clip12t5":
+        from . import ClipBatch
+        cfg = DFTConfig(block=12, overlap=9, tbsize=5, temporal_mode=1, ftype=1, sigma=8.0)
+        p = Plan(1920, 1080, SampleFormat(32, True), cfg)
+        fr = [torch.from_numpy(_plane(1080, 1920, np.float32, 0, 1, f)).to(dev) for f in range(10)]
+        cb = ClipBatch([(p, fr, [torch.empty_like(x) for x in fr])])
+        for _ in range(a.launches):
+            cb.launch()
+        torch.cuda.synchronize()
+        p.sync_status()
         return
     elif wl == "adjoint16":
         import sys

@@ -483,7 +483,7 @@ def other_configs(args, dev):
     del cb
     out["C"] = {"workload": "FFT3D bt=3 48x48 ow=oh=24 sigma 3 sharpen 0.3, 3840x2160 YUV420P10, 10-frame clip",
                 "plain": (nf - 2) * W4 * H4 / (c_ms / 1e3) / 1e6, "plain_ms": c_ms,
-                "plain_form": "8 interior output frames, one volume launch per plane",
+                "plain_form": "8 interior output frames, one per-call two-pass filter (slot spectra, temporal strip) per plane",
                 "batched": nf * W4 * H4 / (cb_ms / 1e3) / 1e6, "batched_ms": cb_ms,
                 "batched_form": "all 10 output frames: clip batch (spectra once per frame, temporal strips), graph",
                 "unit": "Mpx/s"}
@@ -526,7 +526,7 @@ def other_configs(args, dev):
     del cb
     out["D2"] = {"workload": "DFTTest tbsize 5 tmode 1 sbsize 12 sosize 9 ftype 1 sigma 8, 1920x1080 float32, "
                              "12-frame clip", "plain": nout * w * h / (d2_ms / 1e3) / 1e6, "plain_ms": d2_ms,
-                 "plain_form": "8 output frames, one volume launch per frame",
+                 "plain_form": "8 output frames, one per-call two-pass filter (volume slices, slice strip) per frame",
                  "batched": nclip * w * h / (d2b_ms / 1e3) / 1e6, "batched_ms": d2b_ms,
                  "batched_form": "all 12 output frames: clip batch (each temporal block filtered once, slice "
                                  "strips), graph", "unit": "Mpx/s"}

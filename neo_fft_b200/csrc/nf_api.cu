@@ -1444,10 +1444,37 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
     // block-column chunk of pass 1
     std::vector<nfd::DevPlan> dplans;
     std::vector<nfd::StripShape> shapes;
+    // Segment height of the pass-2 strips: one value for the batch, chosen so that the
+    // items of one frame step (every clip's output) fill whole waves of resident CTAs;
+    // each item costs its rows plus the block-row halo above it.
+    int sms_ = 148;
+    cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, 0);
+    const long long slots = (long long)(b->bh * b->bw <= 256 ? 2 : 1) * sms_;
+    std::vector<int> strips_x(plans.size());
+    for (size_t j = 0; j < plans.size(); ++j) {
+      const nfd::StripShape S = pick_strip(plans[j]->dev, 1);
+      strips_x[j] = (plans[j]->t.gx.length + S.tw - 1) / S.tw;
+    }
+    int seg_h = 256;
+    long long best = -1;
+    for (int h : {64, 96, 128, 160, 192, 224, 256, 320, 384, 448, 512, 640, 768, 1024}) {
+      if (h < 2 * b->bh) continue;
+      long long items = 0;
+      for (int i = 0; i < count; ++i) {
+        const int j = plan_of[size_t(i)];
+        const int outputs = b->slice ? plans[size_t(j)]->t.temporal_size : 1;  // outputs per step
+        items += (long long)outputs * strips_x[size_t(j)] * ((plans[size_t(j)]->t.gy.length + h - 1) / h);
+      }
+      const long long cost = ((items + slots - 1) / slots) * (h + b->bh);
+      if (best < 0 || cost < best) {
+        best = cost;
+        seg_h = h;
+      }
+    }
     for (const nf_plan* p : plans) {
       dplans.push_back(p->dev);
       nfd::StripShape S = pick_strip(p->dev, 1);
-      const int segs = std::max(1, (p->t.gy.length + 255) / 256);
+      const int segs = std::max(1, (p->t.gy.length + seg_h - 1) / seg_h);
       S.th = (p->t.gy.length + segs - 1) / segs;
       shapes.push_back(S);
       b->smem2 = std::max(b->smem2, nfd::strip_smem_bytes(b->bh, b->bw, S));

@@ -122,37 +122,51 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
                                                          int nbx, int nel, size_t row_base, size_t cnt, int T,
                                                          float invT, bool& bad) {
   const int tid = threadIdx.x, nthr = blockDim.x;
+  // loop invariants in registers: slot pointers, temporal twiddles, scalars
+  const cf* slot[TC];
+  cf tf[TC * TC], ti[TC];
+#pragma unroll
+  for (int j = 0; j < TC; ++j) {
+    slot[j] = J.tspec[j];
+    ti[j] = P.tinv[j];
+  }
+#pragma unroll
+  for (int i = 0; i < TC * TC; ++i) tf[i] = P.tfwd[i];
+  const float mean_scale = P.mean_scale, lower = P.lower, noise_mult = P.noise_mult, noise_uniform = P.noise_uniform;
+  const float* primary = filt.primary;
+  const float fT = float(TC);
+  (void)T;
 #pragma unroll 2
   for (int e = tid; e < nel; e += nthr) {
     const int kk = e / nbx, b = e - kk * nbx;
     const size_t at = row_base + size_t(kk) * cnt + b;
     cf v[TC];
 #pragma unroll
-    for (int j = 0; j < TC; ++j)
-      if (j < T) v[j] = J.tspec[j][at];
-    const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
-    if (grid && !isfin(g)) bad = true;
-    const cf M = grid ? cf{fmul(g, grid[kk].r), fmul(g, grid[kk].i)} : cf{0.0f, 0.0f};
-    const cf gT = {fmul(M.r, float(T)), fmul(M.i, float(T))};
-    const float noise = filt.primary ? fmul(filt.primary[kk], P.noise_mult) : P.noise_uniform;
+    for (int j = 0; j < TC; ++j) v[j] = slot[j][at];
+    cf gT = {0.0f, 0.0f};
+    if (grid) {
+      const float g = fdiv(fmul(mean_scale, dc[b]), grid0);
+      if (!isfin(g)) bad = true;
+      const cf M = {fmul(g, grid[kk].r), fmul(g, grid[kk].i)};
+      gT = {fmul(M.r, fT), fmul(M.i, fT)};
+    }
+    const float noise = primary ? fmul(primary[kk], noise_mult) : noise_uniform;
     if (!isfin(noise)) bad = true;
     cf yv = {0.0f, 0.0f};
 #pragma unroll
     for (int m = 0; m < TC; ++m) {
-      if (m >= T) break;
       cf F = {0.0f, 0.0f};
 #pragma unroll
-      for (int j = 0; j < TC; ++j)
-        if (j < T) F = nf::cadd(F, nf::cmul_plain(v[j], P.tfwd[m * T + j]));
+      for (int j = 0; j < TC; ++j) F = nf::cadd(F, nf::cmul_plain(v[j], tf[m * TC + j]));
       const cf R = m == 0 ? nf::csub(F, gT) : F;
       const float power = fadd(fmul(R.r, R.r), fmul(R.i, R.i));
       if (!isfin(power)) bad = true;
       const float q = fadd(power, 1e-15f);
       const float gr = fdiv(fsub(q, noise), q);
-      const float gain = gr < P.lower ? P.lower : gr;
+      const float gain = gr < lower ? lower : gr;
       cf Rf = {fmul(gain, R.r), fmul(gain, R.i)};
       if (m == 0) Rf = nf::cadd(Rf, gT);
-      yv = nf::cadd(yv, nf::cmul_plain(Rf, P.tinv[m]));
+      yv = nf::cadd(yv, nf::cmul_plain(Rf, ti[m]));
     }
     spec[size_t(kk) * NB + b] = {fmul(yv.r, invT), fmul(yv.i, invT)};
   }

@@ -105,12 +105,13 @@ __host__ __device__ inline int strip_table_floats(const DevPlan& P) {
 
 // Shared layout (floats): tables | ring_in [bh][ring_pitch] | spec [bh][K][nbx]
 // complex (block fastest) | ob [bh][nbx][bw+4] (synthesised rows, x fastest) |
-// acc [bh][tw] | dc [2*nbx].
+// acc [bh][tw] | dc [2*nbx] | colmap [tw] (overlap-add blocks of each strip column).
 __host__ __device__ inline size_t strip_smem_bytes(int bh, int bw, const StripShape& s) {
   const size_t K = size_t(bw / 2 + 1);
   const size_t spec_cf = (size_t(s.nbx_max) * bh * K + 1) & ~size_t(1);  // keeps ob 16-byte aligned
   return sizeof(float) * (size_t(s.tab_floats) + size_t(bh) * s.ring_pitch + spec_cf * 2 +
-                          size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max));
+                          size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max) +
+                          size_t(s.tw));
 }
 
 // FFT3D bt=2..5 filter of one block row's (bin, block) elements across the T slot
@@ -206,6 +207,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   float* ob = reinterpret_cast<float*>(spec + ((size_t(BH) * K * NB + 1) & ~size_t(1)));
   float* acc = ob + size_t(BH) * NB * OBW;
   float* dc = acc + size_t(BH) * S.tw;
+  int* colmap = reinterpret_cast<int*>(dc + 2 * size_t(NB));
   const int tid = threadIdx.x, nthr = blockDim.x;
   bool bad = false;
 
@@ -248,6 +250,15 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const DevSpectral& filt = s_filt;
   const DevSpectral& enh = s_enh;
   for (int i = tid; i < BH * S.tw; i += nthr) acc[i] = 0.0f;
+  // Per strip column: the first overlapping block (relative to bx_lo), the number of
+  // overlapping blocks and the column's offset inside the first one; the same for every
+  // block row, so the overlap-add below needs no divisions.
+  for (int xx = tid; xx < tw; xx += nthr) {
+    const int X = X0 + xx;
+    const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
+    const int nblk = max(0, b1 - b0 + 1);
+    colmap[xx] = (b0 - bx_lo) | (nblk << 10) | ((nblk > 0 ? X - b0 * gx.step : 0) << 20);
+  }
   __syncthreads();
   const float grid0 = grid ? grid[0].r : 1.0f;
   const float fct = fdiv(1.0f, fmul(float(BW), float(BH)));
@@ -456,14 +467,17 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         if (ly == BH / 2 && bc >= bx_lo && bc <= bx_hi) *a = orow[size_t(bc - bx_lo) * OBW + BW / 2];
         continue;
       }
-      const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
+      // blocks b0.. in ascending order; block b0+j holds column X at offset xo - j*step
+      const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
+      const float* ov = orow + size_t(cm & 1023) * OBW + (cm >> 20);
+      const int adv = OBW - gx.step;
       if (P.algo == 0) {
         float r = 0.0f;
-        for (int bb = b0; bb <= b1; ++bb) r = fadd(r, orow[size_t(bb - bx_lo) * OBW + (X - bb * gx.step)]);
+        for (int j = 0; j < nblk; ++j, ov += adv) r = fadd(r, *ov);
         *a = fadd(*a, fmul(r, wys[ly]));
       } else {
         float sacc = *a;
-        for (int bb = b0; bb <= b1; ++bb) sacc = fadd(sacc, orow[size_t(bb - bx_lo) * OBW + (X - bb * gx.step)]);
+        for (int j = 0; j < nblk; ++j, ov += adv) sacc = fadd(sacc, *ov);
         *a = sacc;
       }
     }

@@ -212,6 +212,31 @@ nf_status nf_clip_batch_launch(nf_clip_batch* batch, void* stream, char* err, si
 nf_status nf_clip_batch_graph_launch(nf_clip_batch* batch, void* stream, char* err, size_t err_len);
 void nf_clip_batch_destroy(nf_clip_batch* batch);
 
+/* Streamed host form (the reference host layer filters frames concurrently on its
+ * frame threads, src/plugin/descriptors.hpp:58; its Plan::process call itself takes
+ * host planes, plan.hpp:58-75). Frames of single-frame planes in HOST memory pass
+ * through a ring of `depth` device slots of `frames_per_chunk` frames each: the
+ * host->device copies, the device->host copies and each slot's batched launch run on
+ * their own streams, ordered by per-slot events, so the copies hide behind the
+ * filtering and the next chunk's launch fills the SMs that the tail of the current
+ * one leaves idle. plans[p] filters plane p of every
+ * frame (the same plan may serve several planes). Overlap needs page-locked host
+ * buffers; pageable ones give the same results without it. Results equal
+ * nf_plan_process_host on every plane; non-finite values are reported through each plan's
+ * nf_plan_sync_status. One nf_host_batch serves one caller at a time. */
+typedef struct nf_host_batch nf_host_batch;
+nf_status nf_host_batch_create(const nf_plan* const* plans, int planes, int frames_per_chunk, int depth,
+                               nf_host_batch** batch, char* err, size_t err_len);
+/* sources[f * planes + p] and dsts[f * planes + p] are host planes of frame f. The
+ * copies start after the work queued on `stream` before the call, and `stream` waits
+ * for the last copy back: the outputs are complete once `stream` is synchronised. A
+ * source may be its own destination. */
+nf_status nf_host_batch_process(nf_host_batch* batch, const nf_const_plane* sources, const nf_plane* dsts,
+                                int frames, void* stream, char* err, size_t err_len);
+/* Device bytes held by the slot ring (inputs and outputs of depth x frames_per_chunk frames). */
+size_t nf_host_batch_device_bytes(const nf_host_batch* batch);
+void nf_host_batch_destroy(nf_host_batch* batch);
+
 /* Sampled noise models (the published table is the plan's per-bin primary table:
  * tbsize*bins floats for DFTTest, bins for FFT3D). DFTTest with nlocation (ftype 0/1): DFTNoise
  * (src/algorithms/dft_noise.cpp:5-41) builds the per-bin primary table from windowed

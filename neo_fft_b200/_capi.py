@@ -112,6 +112,12 @@ PROTOTYPES = {
     "nf_clip_batch_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_clip_batch_graph_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_clip_batch_destroy": (None, [c_void_p]),
+    "nf_host_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, c_int, c_int, ctypes.POINTER(c_void_p),
+                                     ctypes.c_char_p, c_size_t]),
+    "nf_host_batch_process": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfPlane), c_int,
+                                      c_void_p, ctypes.c_char_p, c_size_t]),
+    "nf_host_batch_device_bytes": (c_size_t, [c_void_p]),
+    "nf_host_batch_destroy": (None, [c_void_p]),
     "nf_dft_noise_power": (c_int, [ctypes.POINTER(NfDftConfig), c_void_p, c_int, c_void_p, c_int, ctypes.c_char_p,
                                    c_size_t]),
     "nf_plan_set_noise_model": (c_int, [c_void_p, c_void_p, c_int, ctypes.c_char_p, c_size_t]),

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -132,6 +133,49 @@ struct nf_clip_batch {
   }
 };
 
+// Streamed host form: frames in host memory through a ring of device slots; chunk c
+// uses slot c % depth. Host->device copies, device->host copies and each slot's
+// batched launch run on their own streams ordered by per-slot events (ready: inputs
+// staged; done: outputs written; free: outputs copied back), so the copies of
+// neighbouring chunks overlap the launch of this one, and the next chunk's CTAs take
+// the SMs that this launch's tail leaves idle.
+struct nf_host_batch {
+  std::vector<const nf_plan*> plans;
+  std::vector<size_t> pitch, offset;  // per plane of a frame: device row pitch, offset in the frame
+  size_t frame_bytes = 0;             // device bytes of one frame (all planes)
+  int chunk = 1, depth = 2;
+  void* dev = nullptr;                // depth slots x (chunk input frames | chunk output frames)
+  struct Slot {
+    std::vector<nf_batch*> batches;   // [n - 1]: the slot's first n frames, built on first use
+    cudaEvent_t ready = nullptr, done = nullptr, free = nullptr;
+    cudaStream_t run = nullptr;       // the slot's launches
+  };
+  std::vector<Slot> slots;
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t start = nullptr, end = nullptr;
+  unsigned char* frame_ptr(int slot, int f, bool out) const {
+    return static_cast<unsigned char*>(dev) + (size_t(slot) * 2 + (out ? 1 : 0)) * size_t(chunk) * frame_bytes +
+           size_t(f) * frame_bytes;
+  }
+  ~nf_host_batch() {
+    for (cudaStream_t s : {h2d, d2h})
+      if (s) cudaStreamSynchronize(s);
+    for (auto& s : slots)
+      if (s.run) cudaStreamSynchronize(s.run);
+    for (auto& s : slots) {
+      for (nf_batch* b : s.batches) delete b;
+      for (cudaEvent_t e : {s.ready, s.done, s.free})
+        if (e) cudaEventDestroy(e);
+      if (s.run) cudaStreamDestroy(s.run);
+    }
+    for (cudaEvent_t e : {start, end})
+      if (e) cudaEventDestroy(e);
+    for (cudaStream_t s : {h2d, d2h})
+      if (s) cudaStreamDestroy(s);
+    if (dev) cudaFree(dev);
+  }
+};
+
 namespace {
 
 nf_status fail(char* err, size_t len, const std::string& msg, nf_status code) {
@@ -144,10 +188,20 @@ nf_status fail(char* err, size_t len, const std::string& msg, nf_status code) {
 nf_status cuda_fail(char* err, size_t len, cudaError_t e, const char* what) {
   return fail(err, len, std::string(what) + ": " + cudaGetErrorString(e), NF_DEVICE_ERROR);
 }
+// A failed CUDA call inside a guarded body (reported as NF_DEVICE_ERROR).
+struct CudaFailure {
+  cudaError_t e;
+  const char* what;
+};
+inline void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaFailure{e, what};
+}
 template <class F>
 nf_status guarded(char* err, size_t len, F&& f) {
   try {
     return f();
+  } catch (const CudaFailure& c) {
+    return cuda_fail(err, len, c.e, c.what);
   } catch (const std::invalid_argument& e) {
     return fail(err, len, e.what(), NF_INVALID_ARGUMENT);
   } catch (const std::runtime_error& e) {
@@ -373,6 +427,50 @@ nfd::StripShape pick_strip(const nfd::DevPlan& d, int target_ctas) {
   const int segs = std::max(1, std::min(target_ctas / strips, d.gy.length / std::max(1, 3 * d.bh)));
   S.th = std::max(1, (d.gy.length + segs - 1) / segs);
   return S;
+}
+
+// Segment height of the strips of a batch group. The device queue hands tiles to the
+// resident CTAs in list order, so a launch lasts about as long as the greedy list
+// schedule of its tiles over those CTAs. A tile costs its block rows (segment plus the
+// vertical overlap) times its block columns, plus a setup of two block rows; the
+// candidate height with the shortest schedule wins. `queue` lists each job's plan and
+// strip width in queue order.
+int batch_segment_height(const std::vector<std::pair<const nfd::DevPlan*, int>>& queue, int bh, long long slots) {
+  int seg_h = 256;
+  long long best = -1;
+  std::vector<long long> costs;
+  for (int h : {64, 96, 128, 160, 192, 224, 256, 320, 384, 448, 512, 640, 768, 1024}) {
+    if (h < 2 * bh) continue;
+    costs.clear();
+    for (const auto& q : queue) {
+      const nfd::DevPlan& d = *q.first;
+      const int len = d.gy.length, segs = std::max(1, (len + h - 1) / h), th = (len + segs - 1) / segs;
+      for (int y0 = 0; y0 < len; y0 += th) {
+        const int rows = std::min(th, len - y0);
+        const long long brows = (rows + d.bh - d.gy.step + d.gy.step - 1) / d.gy.step + 2;
+        for (int x0 = 0; x0 < d.gx.length; x0 += q.second) {
+          const int cols = std::min(q.second, d.gx.length - x0);
+          costs.push_back(brows * ((cols + d.bw - d.gx.step + d.gx.step - 1) / d.gx.step));
+        }
+      }
+    }
+    std::priority_queue<long long, std::vector<long long>, std::greater<long long>> free_at;
+    long long span = 0;
+    for (long long c : costs) {
+      long long t0 = 0;
+      if ((long long)free_at.size() >= slots) {
+        t0 = free_at.top();
+        free_at.pop();
+      }
+      free_at.push(t0 + c);
+      span = std::max(span, t0 + c);
+    }
+    if (best < 0 || span < best) {
+      best = span;
+      seg_h = h;
+    }
+  }
+  return seg_h;
 }
 
 // Resident CTAs of the plain launch: two per SM for blocks up to 16x16, else one.
@@ -1304,19 +1402,23 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
       std::vector<nfd::StripShape> shapes;
       for (const nf_plan* p : plans) {
         dplans.push_back(p->dev);
-        // Tall strips: the batch already supplies parallelism; segments of about
-        // 256 rows keep the dynamic queue balanced.
-        nfd::StripShape S = pick_strip(p->dev, 1);
-        const int segs = std::max(1, (p->t.gy.length + 255) / 256);
-        S.th = (p->t.gy.length + segs - 1) / segs;
-        shapes.push_back(S);
-        g.smem = std::max(g.smem, nfd::strip_smem_bytes(g.bh, g.bw, S));
+        shapes.push_back(pick_strip(p->dev, 1));
       }
       std::vector<Entry> mine;
       for (auto& e : entries)
         if (e.group == int(gi)) mine.push_back(e);
       // Largest planes first: shortens the tail of the dynamic queue.
       std::stable_sort(mine.begin(), mine.end(), [](const Entry& a, const Entry& c) { return a.cost > c.cost; });
+      // Tall strips (the batch already supplies parallelism), one segment height for
+      // the group, chosen by the queue's schedule over the resident CTAs.
+      std::vector<std::pair<const nfd::DevPlan*, int>> queue;
+      for (auto& e : mine) queue.emplace_back(&plans[size_t(e.plan)]->dev, shapes[size_t(e.plan)].tw);
+      const int seg_h = batch_segment_height(queue, g.bh, (long long)(g.bh * g.bw <= 256 ? 2 : 1) * sms);
+      for (size_t j = 0; j < plans.size(); ++j) {
+        const int segs = std::max(1, (plans[j]->t.gy.length + seg_h - 1) / seg_h);
+        shapes[j].th = (plans[j]->t.gy.length + segs - 1) / segs;
+        g.smem = std::max(g.smem, nfd::strip_smem_bytes(g.bh, g.bw, shapes[j]));
+      }
       std::vector<nfd::PlaneJob> jobs;
       std::vector<int> base(1, 0), tiles_x;
       for (auto& e : mine) {
@@ -1719,6 +1821,147 @@ nf_status nf_clip_batch_graph_launch(nf_clip_batch* b, void* stream, char* err, 
 }
 
 void nf_clip_batch_destroy(nf_clip_batch* b) { delete b; }
+
+nf_status nf_host_batch_create(const nf_plan* const* plans, int planes, int frames_per_chunk, int depth,
+                               nf_host_batch** out, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(out && plans, "null host batch output or plans");
+    nfb::require(planes > 0 && planes <= 16, "host batches take 1..16 planes per frame");
+    nfb::require(frames_per_chunk > 0 && frames_per_chunk <= 256, "frames_per_chunk must be 1..256");
+    nfb::require(depth >= 2 && depth <= 8, "depth must be 2..8 slots");
+    auto h = std::make_unique<nf_host_batch>();
+    h->chunk = frames_per_chunk;
+    h->depth = depth;
+    for (int p = 0; p < planes; ++p) {
+      nfb::require(plans[p] != nullptr, "null plan in host batch");
+      const auto& t = plans[p]->t;
+      nfb::require(!t.kalman && (t.temporal_size == 1 || t.algo == nfb::Algo::FFT3D) && !t.temporal_ola,
+                   "host batch planes must use single-frame plans");
+      nfb::require(!dithers(t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
+      const size_t elem = size_t(storage_of(t.format));
+      const size_t pitch = ((size_t(t.gx.length) * elem + 255) / 256) * 256;
+      h->plans.push_back(plans[p]);
+      h->pitch.push_back(pitch);
+      h->offset.push_back(h->frame_bytes);
+      h->frame_bytes += pitch * size_t(t.gy.length);
+    }
+    cudaError_t e;
+    const size_t total = size_t(depth) * 2 * size_t(frames_per_chunk) * h->frame_bytes;
+    if ((e = cudaMalloc(&h->dev, total)) != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
+    for (cudaStream_t* s : {&h->h2d, &h->d2h})
+      if ((e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_fail(err, len, e, "stream creation failed");
+    for (cudaEvent_t* ev : {&h->start, &h->end})
+      if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess)
+        return cuda_fail(err, len, e, "event creation failed");
+    h->slots.resize(size_t(depth));
+    for (auto& s : h->slots) {
+      s.batches.assign(size_t(frames_per_chunk), nullptr);
+      for (cudaEvent_t* ev : {&s.ready, &s.done, &s.free})
+        if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess)
+          return cuda_fail(err, len, e, "event creation failed");
+      if ((e = cudaStreamCreateWithFlags(&s.run, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_fail(err, len, e, "stream creation failed");
+    }
+    *out = h.release();
+    return NF_OK;
+  });
+}
+
+namespace {
+// The batch over the first n frames of a slot, built on first use.
+nf_status host_slot_batch(nf_host_batch& h, int slot, int n, nf_batch** b, char* err, size_t len) {
+  nf_batch*& cached = h.slots[size_t(slot)].batches[size_t(n - 1)];
+  if (!cached) {
+    const int planes = int(h.plans.size());
+    std::vector<nf_batch_item> items;
+    for (int f = 0; f < n; ++f)
+      for (int p = 0; p < planes; ++p) {
+        const auto& t = h.plans[size_t(p)]->t;
+        const long long stride = (long long)h.pitch[size_t(p)];
+        items.push_back({h.plans[size_t(p)],
+                         {h.frame_ptr(slot, f, false) + h.offset[size_t(p)], t.gx.length, t.gy.length, stride},
+                         {h.frame_ptr(slot, f, true) + h.offset[size_t(p)], t.gx.length, t.gy.length, stride}});
+      }
+    const nf_status s = nf_batch_create(items.data(), int(items.size()), &cached, err, len);
+    if (s != NF_OK) return s;
+  }
+  *b = cached;
+  return NF_OK;
+}
+}  // namespace
+
+nf_status nf_host_batch_process(nf_host_batch* h, const nf_const_plane* sources, const nf_plane* dsts, int frames,
+                                void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(h != nullptr, "null host batch");
+    nfb::require(frames >= 0, "negative frame count");
+    if (frames == 0) return NF_OK;
+    nfb::require(sources && dsts, "null sources or destinations");
+    const int planes = int(h->plans.size());
+    for (int f = 0; f < frames; ++f)
+      for (int p = 0; p < planes; ++p) {
+        const auto& t = h->plans[size_t(p)]->t;
+        const nf_const_plane& s = sources[size_t(f) * planes + p];
+        const nf_plane& d = dsts[size_t(f) * planes + p];
+        const size_t elem = size_t(storage_of(t.format));
+        nfb::require(s.width == t.gx.length && s.height == t.gy.length && d.width == t.gx.length &&
+                         d.height == t.gy.length,
+                     "frame dimensions differ from plan");
+        plane_extent(s.width, s.height, s.stride_bytes, elem);
+        plane_extent(d.width, d.height, d.stride_bytes, elem);
+        check_pointer(s.data, elem);
+        check_pointer(d.data, elem);
+      }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    auto ck = cuda_check;
+    ck(cudaEventRecord(h->start, st), "event record failed");
+    ck(cudaStreamWaitEvent(h->h2d, h->start, 0), "stream wait failed");
+    const int nchunks = (frames + h->chunk - 1) / h->chunk;
+    for (int c = 0; c < nchunks; ++c) {
+      const int slot = c % h->depth, f0 = c * h->chunk, n = std::min(h->chunk, frames - f0);
+      auto& S = h->slots[size_t(slot)];
+      nf_batch* b = nullptr;
+      const nf_status bs = host_slot_batch(*h, slot, n, &b, err, len);
+      if (bs != NF_OK) return bs;
+      ck(cudaStreamWaitEvent(h->h2d, S.free, 0), "stream wait failed");
+      for (int f = 0; f < n; ++f)
+        for (int p = 0; p < planes; ++p) {
+          const auto& t = h->plans[size_t(p)]->t;
+          const nf_const_plane& s = sources[size_t(f0 + f) * planes + p];
+          ck(cudaMemcpy2DAsync(h->frame_ptr(slot, f, false) + h->offset[size_t(p)], h->pitch[size_t(p)], s.data,
+                               size_t(s.stride_bytes), size_t(t.gx.length) * size_t(storage_of(t.format)),
+                               size_t(t.gy.length), cudaMemcpyHostToDevice, h->h2d),
+             "host to device copy failed");
+        }
+      ck(cudaEventRecord(S.ready, h->h2d), "event record failed");
+      ck(cudaStreamWaitEvent(S.run, S.ready, 0), "stream wait failed");
+      const nf_status ls = nf_batch_graph_launch(b, S.run, err, len);
+      if (ls != NF_OK) return ls;
+      ck(cudaEventRecord(S.done, S.run), "event record failed");
+      ck(cudaStreamWaitEvent(h->d2h, S.done, 0), "stream wait failed");
+      for (int f = 0; f < n; ++f)
+        for (int p = 0; p < planes; ++p) {
+          const auto& t = h->plans[size_t(p)]->t;
+          const nf_plane& d = dsts[size_t(f0 + f) * planes + p];
+          ck(cudaMemcpy2DAsync(d.data, size_t(d.stride_bytes), h->frame_ptr(slot, f, true) + h->offset[size_t(p)],
+                               h->pitch[size_t(p)], size_t(t.gx.length) * size_t(storage_of(t.format)),
+                               size_t(t.gy.length), cudaMemcpyDeviceToHost, h->d2h),
+             "device to host copy failed");
+        }
+      ck(cudaEventRecord(S.free, h->d2h), "event record failed");
+    }
+    ck(cudaEventRecord(h->end, h->d2h), "event record failed");
+    ck(cudaStreamWaitEvent(st, h->end, 0), "stream wait failed");
+    return NF_OK;
+  });
+}
+
+size_t nf_host_batch_device_bytes(const nf_host_batch* h) {
+  return h ? size_t(h->depth) * 2 * size_t(h->chunk) * h->frame_bytes : 0;
+}
+
+void nf_host_batch_destroy(nf_host_batch* h) { delete h; }
 
 nf_status nf_dft_noise_power(const nf_dft_config* c, const float* slices, int nlocations, float* power, int count,
                              char* err, size_t len) {

@@ -416,6 +416,59 @@ class Batch:
             self._h = None
 
 
+class HostBatch:
+    """Streamed host form: frames of single-frame planes in host memory (numpy arrays
+    or CPU torch tensors; page-locked ones let the copies overlap the filtering)
+    pass through a ring of `depth` device slots of `frames_per_chunk` frames.
+    `plans[p]` filters plane p of every frame. Outputs equal `Plan.process` per plane."""
+
+    def __init__(self, plans, frames_per_chunk: int = 2, depth: int = 3):
+        self._lib = C.load()
+        self._plans = list(plans)
+        arr = (ctypes.c_void_p * len(self._plans))(*[p._h.value for p in self._plans])
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_host_batch_create(arr, len(self._plans), int(frames_per_chunk), int(depth),
+                                                   ctypes.byref(self._h), err, 512), err.value)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._lib.nf_host_batch_device_bytes(self._h))
+
+    def process(self, frames, outputs=None, stream=None, wait: bool = True):
+        """frames[f][p] -> outputs[f][p] (allocated like the sources when omitted).
+        Enqueued after the work on `stream` (torch's current stream by default); with
+        wait=False the outputs are complete once that stream is synchronised."""
+        import torch
+        planes = len(self._plans)
+        frames = [list(f) for f in frames]
+        if any(len(f) != planes for f in frames):
+            raise ValueError(f"every frame must hold {planes} planes")
+        if outputs is None:
+            outputs = [[torch.empty_like(x) if _is_torch(x) else np.empty_like(np.asarray(x)) for x in f]
+                       for f in frames]
+        n = len(frames)
+        srcs = (C.NfConstPlane * max(1, n * planes))(*[_plane(x, True) for f in frames for x in f])
+        dsts = (C.NfPlane * max(1, n * planes))(*[_plane(x, False) for f in outputs for x in f])
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_host_batch_process(self._h, srcs, dsts, n, ctypes.c_void_p(s), err, 512),
+                    err.value)
+        if wait:
+            torch.cuda.synchronize()
+        return outputs
+
+    def sync_status(self) -> None:
+        for p in {id(p): p for p in self._plans}.values():
+            p.sync_status()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.nf_host_batch_destroy(h)
+            self._h = None
+
+
 def gather_noise(frames, location, z, block: int, fmt: SampleFormat) -> np.ndarray:
     """The host layer's sample gather (src/plugin/filter.hpp:381-389): rows
     y..y+block, columns x..x+block of plane `location[1]` of frame location[0] + z,

@@ -237,6 +237,40 @@ nf_status nf_host_batch_process(nf_host_batch* batch, const nf_const_plane* sour
 size_t nf_host_batch_device_bytes(const nf_host_batch* batch);
 void nf_host_batch_destroy(nf_host_batch* batch);
 
+/* Host request layer (the reference host layer's request/process pair over its frame
+ * server, src/plugin/filter.hpp:253-528): output frames of a clip of `num_frames`
+ * frames with `planes` planes each, filtered in ranges of about `range_frames`
+ * consecutive output frames per batched launch, with the host layer's frame selection.
+ * FFT3D bt 2..5 and DFTTest tmode 1 with tosize 0 run the clip form (each source
+ * frame's spectra computed once per range: the device ring in place of SpectraCache);
+ * single-frame plans run the batched form; other DFTTest temporal modes and pshow
+ * previews run one nf_plan_process_device call per frame over device-resident
+ * sources. Two banks of device buffers hold consecutive ranges: the next range is
+ * computed while the current one is read out. plans[p] NULL copies plane p from the
+ * source frame (a plane that is not processed). Kalman plans are served through
+ * neo_fft::KalmanSeek instead. FFT3D sampled noise models (pfactor) are prepared from
+ * the pattern frame on first use; DFTTest sampled models (nlocation) must be
+ * published before the first request. Calls are serialised internally. */
+typedef struct nf_frame_server nf_frame_server;
+/* Returns the view of plane `plane` of source frame `frame` (host or device memory)
+ * in *view; 0 on success. The view must stay valid until the call that asked for it
+ * returns. */
+typedef int (*nf_frame_source)(void* user, int frame, int plane, nf_const_plane* view);
+nf_status nf_frame_server_create(const nf_plan* const* plans, int planes, int num_frames, int range_frames,
+                                 nf_frame_source source, void* user, nf_frame_server** server, char* err,
+                                 size_t err_len);
+/* Filter::request: the source frames output frame n reads, ascending and unique
+ * (*count of them; at most `capacity` written). */
+nf_status nf_frame_server_request(const nf_frame_server* server, int n, int* frames, int capacity, int* count,
+                                  char* err, size_t err_len);
+/* Filter::process: output frame n into dsts[planes] (host or device memory); returns
+ * once the planes are written. */
+nf_status nf_frame_server_get(nf_frame_server* server, int n, const nf_plane* dsts, char* err, size_t err_len);
+/* Output frames computed so far and source frames fetched so far (for hosts that
+ * size their caches). */
+void nf_frame_server_counters(const nf_frame_server* server, long long* computed, long long* fetched);
+void nf_frame_server_destroy(nf_frame_server* server);
+
 /* Sampled noise models (the published table is the plan's per-bin primary table:
  * tbsize*bins floats for DFTTest, bins for FFT3D). DFTTest with nlocation (ftype 0/1): DFTNoise
  * (src/algorithms/dft_noise.cpp:5-41) builds the per-bin primary table from windowed

@@ -2,6 +2,6 @@
 
 The public surface mirrors the reference core's `Plan` API; see `plan.py`.
 """
-from .plan import (ROI, Axis, Batch, ClipBatch, DFTConfig, DFTNoise, FFT3DConfig, Geometry, HostBatch, KalmanState, Plan, SampleFormat,  # noqa: F401
+from .plan import (ROI, Axis, Batch, ClipBatch, DFTConfig, DFTNoise, FFT3DConfig, FrameServer, Geometry, HostBatch, KalmanState, Plan, SampleFormat,  # noqa: F401
                    kernel_info)
 from ._capi import DeviceError, NonFiniteError  # noqa: F401

@@ -118,6 +118,14 @@ PROTOTYPES = {
                                       c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_host_batch_device_bytes": (c_size_t, [c_void_p]),
     "nf_host_batch_destroy": (None, [c_void_p]),
+    "nf_frame_server_create": (c_int, [ctypes.POINTER(c_void_p), c_int, c_int, c_int, c_void_p, c_void_p,
+                                       ctypes.POINTER(c_void_p), ctypes.c_char_p, c_size_t]),
+    "nf_frame_server_request": (c_int, [c_void_p, c_int, ctypes.POINTER(c_int), c_int, ctypes.POINTER(c_int),
+                                        ctypes.c_char_p, c_size_t]),
+    "nf_frame_server_get": (c_int, [c_void_p, c_int, ctypes.POINTER(NfPlane), ctypes.c_char_p, c_size_t]),
+    "nf_frame_server_counters": (None, [c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_longlong)]),
+    "nf_frame_server_destroy": (None, [c_void_p]),
     "nf_dft_noise_power": (c_int, [ctypes.POINTER(NfDftConfig), c_void_p, c_int, c_void_p, c_int, ctypes.c_char_p,
                                    c_size_t]),
     "nf_plan_set_noise_model": (c_int, [c_void_p, c_void_p, c_int, ctypes.c_char_p, c_size_t]),

@@ -30,7 +30,7 @@ NVCCFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-f
 HOST_SOURCES = ["plan_build.cpp"]
 # (source, object stem, extra defines): the tile kernel is compiled once per block shape.
 SPATIAL_SHAPES = [(8, 8), (16, 16), (32, 32), (12, 12), (48, 48), (0, 0)]
-CUDA_UNITS = [("nf_api.cu", "nf_api", []), ("nf_noalloc.cu", "nf_noalloc", [])] + \
+CUDA_UNITS = [("nf_api.cu", "nf_api", []), ("nf_noalloc.cu", "nf_noalloc", []), ("nf_server.cu", "nf_server", [])] + \
     [("spatial_inst.cu", f"spatial_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \
     [("volume_inst.cu", f"volume_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \
     [("temporal_inst.cu", f"temporal_{h}x{w}", [f"-DNF_BH={h}", f"-DNF_BW={w}"]) for h, w in SPATIAL_SHAPES] + \

@@ -12,6 +12,7 @@
 #include "tile_temporal.cuh"
 #include "pattern.cuh"
 #include "dither.cuh"
+#include "plan_info.hpp"
 
 #include <cuda_runtime.h>
 
@@ -87,6 +88,7 @@ struct BatchGroup {
 
 struct nf_batch {
   std::vector<BatchGroup> groups;
+  std::vector<const nf_plan*> plans;  // distinct plans (sampled noise models are checked per launch)
   int* counters = nullptr;  // one queue head per group
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -105,6 +107,7 @@ struct nf_batch {
 // clip into its ring of T frame spectra) then pass 2 (the outputs whose windows are
 // complete). Work lists of every step are built and uploaded once at creation.
 struct nf_clip_batch {
+  std::vector<const nf_plan*> plans;  // distinct plans (sampled noise models are checked per launch)
   int bh = 0, bw = 0, storage = 0;
   int slice = 0;  // 0: FFT3D temporal clips; 1: DFTTest tmode 1 slice form
   size_t smem1 = 0, smem2 = 0;
@@ -212,6 +215,11 @@ nf_status guarded(char* err, size_t len, F&& f) {
 }
 
 int storage_of(nf_format f) { return f.floating ? nfd::kStoreF32 : (f.bits == 8 ? nfd::kStoreU8 : nfd::kStoreU16); }
+
+// Batched forms read each plan's primary table when they run, so a sampled noise model
+// (DFTTest nlocation, FFT3D pfactor) must be published before every launch, as for
+// nf_plan_process_device.
+nf_status check_models(const std::vector<const nf_plan*>& plans, char* err, size_t len);
 
 // Packs host tables into one aligned blob and records each table's offset.
 struct Blob {
@@ -857,6 +865,16 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
   return NF_OK;
 }
 
+nf_status check_models(const std::vector<const nf_plan*>& plans, char* err, size_t len) {
+  for (const nf_plan* p : plans) {
+    if (p->t.noise_model && !p->model_ready.load(std::memory_order_acquire))
+      return fail(err, len, "DFTTest sample model not initialized", NF_INVALID_ARGUMENT);
+    if (p->t.needs_pattern && !p->model_ready.load(std::memory_order_acquire))
+      return fail(err, len, "FFT3D sampled model not initialized", NF_INVALID_ARGUMENT);
+  }
+  return NF_OK;
+}
+
 // The filter proper with the device plan `d` (the plan's own, or a copy that keeps the
 // raw accumulator for the dither pass).
 nf_status filter_device(const nf_plan& p, const nfd::DevPlan& d, const nf_const_plane* sources, int n,
@@ -1361,7 +1379,9 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
       nfb::require(!p.t.kalman && (p.t.temporal_size == 1 || p.t.algo == nfb::Algo::FFT3D) && !p.t.temporal_ola,
                    "batch items must be single-frame plans");
       nfb::require(!dithers(p.t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
+      nfb::require(!p.t.preview, "pshow previews run through nf_plan_process_device");
       validate_call(p, &it.source, 1, nullptr, 0, it.dst);
+      if (std::find(b->plans.begin(), b->plans.end(), &p) == b->plans.end()) b->plans.push_back(&p);
       const int storage = storage_of(p.t.format);
       int gi = -1;
       for (size_t g = 0; g < b->groups.size(); ++g)
@@ -1455,6 +1475,7 @@ nf_status nf_batch_launch(nf_batch* b, void* stream, char* err, size_t len) {
   if (!b) return fail(err, len, "null batch", NF_INVALID_ARGUMENT);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (b->groups.empty()) return NF_OK;
+  if (const nf_status ms = check_models(b->plans, err, len)) return ms;
   cudaError_t e = cudaMemsetAsync(b->counters, 0, sizeof(int) * b->groups.size(), st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
   for (const auto& g : b->groups)
@@ -1465,6 +1486,7 @@ nf_status nf_batch_launch(nf_batch* b, void* stream, char* err, size_t len) {
 nf_status nf_batch_graph_launch(nf_batch* b, void* stream, char* err, size_t len) {
   if (!b) return fail(err, len, "null batch", NF_INVALID_ARGUMENT);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (const nf_status ms = check_models(b->plans, err, len)) return ms;
   cudaError_t e;
   if (!b->exec) {
     // Capture needs a non-legacy stream; capture on a private one and replay on `st`.
@@ -1517,6 +1539,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
                    "clip batch items must share algorithm, block shape and sample storage");
       nfb::require(!dft || it.nframes >= p.t.temporal_size, "DFTTest clips must hold at least tbsize frames");
       nfb::require(!dithers(p.t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
+      nfb::require(!p.t.preview, "pshow previews run through nf_plan_process_device");
       const size_t elem = size_t(storage);
       for (int f = 0; f < it.nframes; ++f) {
         if (dft) {
@@ -1542,6 +1565,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       }
       plan_of[size_t(i)] = pi;
     }
+    b->plans = plans;
     // strips of pass 2 (tall segments: the batch supplies the parallelism) and the
     // block-column chunk of pass 1
     std::vector<nfd::DevPlan> dplans;
@@ -1778,6 +1802,7 @@ nf_status nf_clip_batch_launch(nf_clip_batch* b, void* stream, char* err, size_t
   if (!b) return fail(err, len, "null clip batch", NF_INVALID_ARGUMENT);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (b->steps.empty()) return NF_OK;
+  if (const nf_status ms = check_models(b->plans, err, len)) return ms;
   cudaError_t e = cudaMemsetAsync(b->counters, 0, sizeof(int) * b->steps.size(), st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
   for (const auto& s : b->steps) {
@@ -1798,6 +1823,7 @@ nf_status nf_clip_batch_launch(nf_clip_batch* b, void* stream, char* err, size_t
 nf_status nf_clip_batch_graph_launch(nf_clip_batch* b, void* stream, char* err, size_t len) {
   if (!b) return fail(err, len, "null clip batch", NF_INVALID_ARGUMENT);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (const nf_status ms = check_models(b->plans, err, len)) return ms;
   cudaError_t e;
   if (!b->exec) {
     if (!b->capture_stream && (e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -2238,3 +2264,26 @@ nf_status nf_kernel_info(char* fft_backend, size_t fb_len, char* target, size_t 
 }
 
 } // extern "C"
+
+namespace nfi {
+PlanInfo plan_info(const nf_plan* p) {
+  const auto& t = p->t;
+  PlanInfo i;
+  i.fft3d = t.algo == nfb::Algo::FFT3D;
+  i.width = t.gx.length;
+  i.height = t.gy.length;
+  i.elem = storage_of(t.format);
+  i.temporal_size = t.temporal_size;
+  i.tmode1 = t.temporal_ola;
+  i.temporal_overlap = t.temporal_overlap;
+  i.kalman = t.kalman;
+  i.preview = t.preview;
+  i.single = !t.kalman && !t.preview && !dithers(t) && (t.temporal_size == 1 || i.fft3d) && !t.temporal_ola;
+  i.clip = !t.preview && !dithers(t) &&
+           ((i.fft3d && !t.kalman && t.temporal_size >= 2 && t.temporal_size <= 5) ||
+            (!i.fft3d && t.temporal_ola && t.temporal_overlap == 0 && !t.center && t.temporal_size >= 2 &&
+             t.temporal_size <= nfd::kMaxVolumeSlots));
+  i.pframe = t.pframe;
+  return i;
+}
+}  // namespace nfi

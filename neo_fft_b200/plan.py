@@ -469,6 +469,88 @@ class HostBatch:
             self._h = None
 
 
+_FRAME_SOURCE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(C.NfConstPlane))
+
+
+class FrameServer:
+    """Host request layer (src/plugin/filter.hpp:253-528): output frames of a clip of
+    `num_frames` frames, filtered in ranges of about `range_frames` frames per batched
+    launch with the host layer's frame selection. `source(frame, plane)` returns a 2-D
+    plane (numpy array or torch tensor, host or CUDA); `plans[p]` None passes plane p
+    through. `get(n)` returns frame n's planes; `request(n)` the source frames it reads."""
+
+    def __init__(self, plans, num_frames: int, source, range_frames: int = 16):
+        self._lib = C.load()
+        self._plans = list(plans)
+        self._source = source
+        self._held = []
+        self._error = None
+
+        def fetch(_user, frame, plane, view):
+            try:
+                a = source(frame, plane)
+                self._held.append(a)
+                view[0] = _plane(a, True)
+                return 0
+            except Exception as e:  # reported through the status of the calling entry point
+                self._error = e
+                return 1
+
+        self._fetch = _FRAME_SOURCE(fetch)
+        arr = (ctypes.c_void_p * len(self._plans))(*[p._h.value if p is not None else None for p in self._plans])
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_frame_server_create(arr, len(self._plans), int(num_frames), int(range_frames),
+                                                     ctypes.cast(self._fetch, ctypes.c_void_p), None,
+                                                     ctypes.byref(self._h), err, 512), err.value)
+
+    def request(self, n: int) -> list[int]:
+        frames = (ctypes.c_int * 512)()
+        count = ctypes.c_int()
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_frame_server_request(self._h, int(n), frames, 512, ctypes.byref(count), err, 512),
+                    err.value)
+        return list(frames[:count.value])
+
+    def get(self, n: int, outputs=None):
+        """Output frame n: outputs[p] (allocated as numpy arrays when omitted)."""
+        if outputs is None:
+            outputs = []
+            for p, plan in enumerate(self._plans):
+                if plan is None:
+                    a = np.asarray(self._source(n, p))
+                    outputs.append(np.empty_like(a))
+                else:
+                    g = plan.geometry
+                    outputs.append(np.empty((g.y.length, g.x.length), dtype=plan.dtype))
+        dsts = (C.NfPlane * len(outputs))(*[_plane(o, False) for o in outputs])
+        err = ctypes.create_string_buffer(512)
+        self._held, self._error = [], None
+        try:
+            st = self._lib.nf_frame_server_get(self._h, int(n), dsts, err, 512)
+        finally:
+            self._held = []
+        e, self._error = self._error, None
+        if st != C.NF_OK and e is not None:
+            raise e  # the frame source's own exception
+        C.raise_for(st, err.value)
+        return outputs
+
+    @property
+    def counters(self) -> tuple[int, int]:
+        """(output frames computed, source frames fetched) so far."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._lib.nf_frame_server_counters(self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.nf_frame_server_destroy(h)
+            self._h = None
+
+
 def gather_noise(frames, location, z, block: int, fmt: SampleFormat) -> np.ndarray:
     """The host layer's sample gather (src/plugin/filter.hpp:381-389): rows
     y..y+block, columns x..x+block of plane `location[1]` of frame location[0] + z,

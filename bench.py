@@ -171,7 +171,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    from neo_fft_b200 import Batch, HostBatch, Plan, SampleFormat
+    from neo_fft_b200 import Batch, FrameServer, HostBatch, Plan, SampleFormat
     from neo_fft_b200 import _capi as C
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -291,6 +291,17 @@ def run_ours(args):
     plane_bytes = FRAMES * plane_px * 2
     e2e_value = world * FRAMES * W * H / (e2e_ms / 1e3) / 1e6
     serial_value = world * FRAMES * W * H / (serial_ms / 1e3) / 1e6
+    # The host request layer: every output frame requested in order from a frame server
+    # over the same pinned host frames (ranges of 4 frames, two ranges prefetched).
+    server = FrameServer(plans, FRAMES, lambda f, p: pin_in[f][p].numpy(), range_frames=4)
+    server_out = [[o.numpy() for o in f] for f in pin_out]
+    for n in range(FRAMES):
+        server.get(n, server_out[n])
+    t0 = time.perf_counter()
+    for n in range(FRAMES):
+        server.get(n, server_out[n])
+    server_value = FRAMES * W * H / (time.perf_counter() - t0) / 1e6
+    del server
     # Same through the per-plane host-memory entry point (copies + launch + sync per plane).
     t0 = time.perf_counter()
     for f in range(FRAMES):
@@ -321,6 +332,7 @@ def run_ours(args):
                 "path": f"HostBatch.process (nf_host_batch_process): pinned host frames through {HOST_CHUNK}-frame "
                         "device slots, copies overlapped with the batched launch on separate streams",
                 "serial_copies_value": serial_value,
+                "frame_server_value": server_value,
                 "per_plane_host_api_value": host_plane_value},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",

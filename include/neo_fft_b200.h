@@ -245,8 +245,8 @@ void nf_host_batch_destroy(nf_host_batch* batch);
  * frame's spectra computed once per range: the device ring in place of SpectraCache);
  * single-frame plans run the batched form; other DFTTest temporal modes and pshow
  * previews run one nf_plan_process_device call per frame over device-resident
- * sources. Two banks of device buffers hold consecutive ranges: the next range is
- * computed while the current one is read out. plans[p] NULL copies plane p from the
+ * sources. Three banks of device buffers hold consecutive ranges: the next two
+ * ranges are fetched and computed while the current one is read out. plans[p] NULL copies plane p from the
  * source frame (a plane that is not processed). Kalman plans are served through
  * neo_fft::KalmanSeek instead. FFT3D sampled noise models (pfactor) are prepared from
  * the pattern frame on first use; DFTTest sampled models (nlocation) must be

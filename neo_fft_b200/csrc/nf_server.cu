@@ -1,8 +1,8 @@
 // Host request layer: the reference host layer's request/process pair
 // (src/plugin/filter.hpp:253-528) over the batched forms of this library. Output frames
 // are produced in ranges of consecutive frames; each range is one batched launch over
-// device-resident source frames, and the next range is computed in a second bank of
-// device buffers while the current one is read out.
+// device-resident source frames, and the next two ranges are fetched and computed in
+// further banks of device buffers while the current one is read out.
 //
 // Frame selection per output frame n (clip of N frames) follows filter.hpp:
 //   FFT3D bt 2..5       frames n - bt/2 .. n + (bt-1)/2, or n alone where that window
@@ -78,7 +78,8 @@ struct nf_frame_server {
   bool preview = false;
   nf_frame_source source = nullptr;
   void* user = nullptr;
-  Bank banks[2];
+  static constexpr int kBanks = 3;  // the range being read out and two ranges ahead
+  Bank banks[kBanks];
   unsigned long long tick = 0;
   long long computed = 0, fetched = 0;
   bool patterns_done = false;
@@ -319,7 +320,9 @@ struct nf_frame_server {
       prepare_patterns(banks[0].stream);
       b = holding(n);
       if (!b) {
-        b = banks[0].used <= banks[1].used ? &banks[0] : &banks[1];
+        b = &banks[0];
+        for (auto& c : banks)
+          if (c.used < b->used) b = &c;
         compute(*b, range_of(n));
       }
       b->used = ++tick;
@@ -358,18 +361,27 @@ struct nf_frame_server {
         }
       b->checked = true;
     }
-    // Sequential readers: start the next range in the other bank.
+    // Sequential readers: the ranges after this one go into the other banks, so the
+    // next range's source copies overlap the filtering of the one before it.
     if (b) {
-      const int next = b->r.n1;
-      if (next < N && !holding(next)) {
-        Bank& other = (b == &banks[0]) ? banks[1] : banks[0];
-        try {
-          compute(other, range_of(next));
-        } catch (const Failure&) {
-          other.valid = false;  // reported when one of its frames is requested
-        } catch (const std::exception&) {
-          other.valid = false;
+      std::vector<const Bank*> keep{b};
+      int next = b->r.n1;
+      while (next < N && int(keep.size()) < kBanks) {
+        Bank* h = holding(next);
+        if (!h) {
+          for (auto& c : banks)
+            if (std::find(keep.begin(), keep.end(), &c) == keep.end() && (!h || c.used < h->used)) h = &c;
+          try {
+            compute(*h, range_of(next));
+            h->used = ++tick;
+          } catch (const std::exception&) {
+            break;  // reported when one of its frames is requested
+          } catch (const Failure&) {
+            break;
+          }
         }
+        keep.push_back(h);
+        next = h->r.n1;
       }
     }
   }

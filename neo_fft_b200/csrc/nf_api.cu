@@ -20,9 +20,11 @@
 #include <cstddef>
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <queue>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -406,66 +408,137 @@ Checked validate_call(const nf_plan& p, const nf_const_plane* sources, int n, co
   return c;
 }
 
-// Strip geometry: width by block size (the horizontal halo costs (bw-step)/tw of
-// recomputed blocks), height chosen so one plane yields about `target_ctas` CTAs
-// (two resident CTAs per SM on 148 SMs) in the plain launch; batches use tall
-// strips because many planes already fill the GPU.
-nfd::StripShape pick_strip(const nfd::DevPlan& d, int target_ctas) {
-  nfd::StripShape S;
-  S.tab_floats = nfd::strip_table_floats(d);
-  // Block columns per strip: the row phases run nbx*bh tasks on 256 threads, so
-  // aim for a multiple of 256 (two rounds for blocks up to 16x16, one above).
-  const int rounds = d.bh * d.bw <= 256 ? 2 : 1;
-  int nbx = std::max(2, (256 * rounds) / std::max(1, d.bh));
-  const int edge = (d.bw + d.gx.step - 1) / d.gx.step - 1;  // blocks beyond the owned columns
-  for (;;) {
-    S.tw = std::min(std::max(d.gx.step, (nbx - edge) * d.gx.step), d.gx.length);
-    S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
-    S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
-    int q = (S.win_max + 3) / 4;
-    if (q % 2 == 0) ++q;  // odd float4 count: consecutive staged rows start in different banks
-    S.ring_pitch = 4 * q;
-    S.th = d.gy.length;
-    if (nfd::strip_smem_bytes(d.bh, d.bw, S) <= (rounds == 2 ? 110 : 200) * 1024 || nbx <= edge + 2) break;
-    nbx = std::max(edge + 2, nbx * 3 / 4);
+// Resident CTAs of the plain launch: two per SM for blocks up to 16x16, else one.
+int plain_ctas(const nfd::DevPlan& d) { return (d.bh * d.bw <= 256 ? 2 : 1) * 148; }
+
+// What the tiles of a strip launch compute: pixels staged and transformed forward and
+// back (all phases), or spectra that are already in memory (FFT3D temporal pass 2,
+// DFTTest slices, Kalman render), whose tiles skip the staging ring and the forward rows.
+enum class StripWork { Pixels, Temporal, Slice, Kalman };
+
+// Modelled duration of one strip tile of `cols` x `rows` output samples: per block row,
+// rounds of 256 threads over the row phases (nb*bh real rows forward and inverse, weight
+// 1 each) and the column phase (nb*(bw/2+1) complex columns: forward, filter and
+// inverse, weight 3; temporal filter or Kalman gain and inverse, 2; inverse only, 1),
+// times the block rows plus a setup of two.
+double tile_cost(const nfd::DevPlan& d, int cols, int rows, StripWork w) {
+  const int K = d.bw / 2 + 1;
+  const int nb = (cols + d.bw - d.gx.step + d.gx.step - 1) / d.gx.step;
+  const int br = (rows + d.bh - d.gy.step + d.gy.step - 1) / d.gy.step + 2;
+  const double wrows = w == StripWork::Pixels ? 2.0 : 1.0;
+  const double wcols = w == StripWork::Pixels ? 3.0 : w == StripWork::Slice ? 1.0 : 2.0;
+  return (wrows * ((nb * d.bh + 255) / 256) + wcols * ((nb * K + 255) / 256)) * br;
+}
+
+// Strip geometry. plain_planes > 0: one plain launch over that many planes (grid of
+// strips x segments x planes); the segment height aims the grid at one wave of resident
+// CTAs and the strip width minimises the modelled launch time (the tiles' greedy
+// schedule over the resident CTAs). plain_planes == 0: batched forms, whose callers set
+// the segment height; the width minimises the modelled work per owned column. Both keep
+// the shared-memory budget of the occupancy target (two CTAs per SM up to 16x16 blocks,
+// one above). Results are cached per geometry: plain launches ask on every call.
+nfd::StripShape pick_strip(const nfd::DevPlan& d, int plain_planes, StripWork work) {
+  struct Key {
+    int len_x, len_y, bh, bw, sx, sy, tab, planes, work;
+    bool operator<(const Key& o) const {
+      return std::tie(len_x, len_y, bh, bw, sx, sy, tab, planes, work) <
+             std::tie(o.len_x, o.len_y, o.bh, o.bw, o.sx, o.sy, o.tab, o.planes, o.work);
+    }
+  };
+  static std::mutex memo_mu;
+  static std::map<Key, nfd::StripShape> memo;
+  const Key key{d.gx.length, d.gy.length, d.bh, d.bw, d.gx.step, d.gy.step, nfd::strip_table_floats(d), plain_planes,
+                int(work)};
+  {
+    std::lock_guard<std::mutex> lock(memo_mu);
+    const auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
   }
-  const int strips = (d.gx.length + S.tw - 1) / S.tw;
-  // At most one wave in the plain launch (a partial second wave doubles the time).
-  // Segments shorter than 3 block heights recompute too many vertical neighbours.
-  const int segs = std::max(1, std::min(target_ctas / strips, d.gy.length / std::max(1, 3 * d.bh)));
-  S.th = std::max(1, (d.gy.length + segs - 1) / segs);
+  const int edge = (d.bw + d.gx.step - 1) / d.gx.step - 1;  // blocks beyond the owned columns
+  auto shape = [&](int nbx) {
+    nfd::StripShape c;
+    c.tab_floats = nfd::strip_table_floats(d);
+    c.tw = std::min(std::max(d.gx.step, (nbx - edge) * d.gx.step), d.gx.length);
+    c.nbx_max = (c.tw + d.bw - 1) / d.gx.step + 2;
+    c.win_max = (c.nbx_max - 1) * d.gx.step + d.bw;
+    int q = (c.win_max + 3) / 4;
+    if (q % 2 == 0) ++q;  // odd float4 count: consecutive staged rows start in different banks
+    // Staging ring: pixel tiles only. FFT3D clip launches keep it for their single-frame
+    // fallback tiles at the clip edges; DFTTest slices and Kalman renders have no pixel tiles.
+    c.ring_pitch = work == StripWork::Slice || work == StripWork::Kalman ? 0 : 4 * q;
+    c.th = d.gy.length;
+    return c;
+  };
+  const size_t budget = size_t(d.bh * d.bw <= 256 ? 110 : 200) * 1024;
+  const int slots = plain_ctas(d);
+  nfd::StripShape S = shape(edge + 2);
+  double best = -1.0;
+  std::vector<double> costs;
+  for (int nbx = edge + 2; nbx <= 128; ++nbx) {
+    nfd::StripShape c = shape(nbx);
+    if (nfd::strip_smem_bytes(d.bh, d.bw, c) > budget) continue;
+    double cost;
+    if (plain_planes > 0) {
+      const int strips = (d.gx.length + c.tw - 1) / c.tw;
+      // At most one wave (a partial second wave doubles the time); segments shorter
+      // than 3 block heights recompute too many vertical neighbours.
+      const int target = std::max(1, slots / plain_planes);
+      const int segs = std::max(1, std::min(target / strips, d.gy.length / std::max(1, 3 * d.bh)));
+      c.th = std::max(1, (d.gy.length + segs - 1) / segs);
+      costs.clear();
+      for (int z = 0; z < plain_planes; ++z)
+        for (int y0 = 0; y0 < d.gy.length; y0 += c.th)
+          for (int x0 = 0; x0 < d.gx.length; x0 += c.tw)
+            costs.push_back(tile_cost(d, std::min(c.tw, d.gx.length - x0), std::min(c.th, d.gy.length - y0), work));
+      std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+      double span = 0;
+      for (double t : costs) {
+        double t0 = 0;
+        if (int(free_at.size()) >= slots) {
+          t0 = free_at.top();
+          free_at.pop();
+        }
+        free_at.push(t0 + t);
+        span = std::max(span, t0 + t);
+      }
+      cost = span;
+    } else {
+      cost = tile_cost(d, c.tw, 0, work) / double(c.tw);
+    }
+    if (best < 0 || cost < best) {
+      best = cost;
+      S = c;
+    }
+    if (c.tw >= d.gx.length) break;  // wider strips own no more columns
+  }
+  std::lock_guard<std::mutex> lock(memo_mu);
+  memo.emplace(key, S);
   return S;
 }
 
 // Segment height of the strips of a batch group. The device queue hands tiles to the
 // resident CTAs in list order, so a launch lasts about as long as the greedy list
-// schedule of its tiles over those CTAs. A tile costs its block rows (segment plus the
-// vertical overlap) times its block columns, plus a setup of two block rows; the
-// candidate height with the shortest schedule wins. `queue` lists each job's plan and
-// strip width in queue order.
-int batch_segment_height(const std::vector<std::pair<const nfd::DevPlan*, int>>& queue, int bh, long long slots) {
+// schedule of its tiles (tile_cost) over those CTAs; the candidate height with the
+// shortest schedule wins. `queue` lists each job's plan and strip width in queue order.
+int batch_segment_height(const std::vector<std::pair<const nfd::DevPlan*, int>>& queue, int bh, long long slots,
+                         StripWork work) {
   int seg_h = 256;
-  long long best = -1;
-  std::vector<long long> costs;
+  double best = -1;
+  std::vector<double> costs;
   for (int h : {64, 96, 128, 160, 192, 224, 256, 320, 384, 448, 512, 640, 768, 1024}) {
     if (h < 2 * bh) continue;
     costs.clear();
     for (const auto& q : queue) {
       const nfd::DevPlan& d = *q.first;
       const int len = d.gy.length, segs = std::max(1, (len + h - 1) / h), th = (len + segs - 1) / segs;
-      for (int y0 = 0; y0 < len; y0 += th) {
-        const int rows = std::min(th, len - y0);
-        const long long brows = (rows + d.bh - d.gy.step + d.gy.step - 1) / d.gy.step + 2;
-        for (int x0 = 0; x0 < d.gx.length; x0 += q.second) {
-          const int cols = std::min(q.second, d.gx.length - x0);
-          costs.push_back(brows * ((cols + d.bw - d.gx.step + d.gx.step - 1) / d.gx.step));
-        }
-      }
+      for (int y0 = 0; y0 < len; y0 += th)
+        for (int x0 = 0; x0 < d.gx.length; x0 += q.second)
+          costs.push_back(tile_cost(d, std::min(q.second, d.gx.length - x0), std::min(th, len - y0), work));
     }
-    std::priority_queue<long long, std::vector<long long>, std::greater<long long>> free_at;
-    long long span = 0;
-    for (long long c : costs) {
-      long long t0 = 0;
+    std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+    double span = 0;
+    for (double c : costs) {
+      double t0 = 0;
       if ((long long)free_at.size() >= slots) {
         t0 = free_at.top();
         free_at.pop();
@@ -481,8 +554,6 @@ int batch_segment_height(const std::vector<std::pair<const nfd::DevPlan*, int>>&
   return seg_h;
 }
 
-// Resident CTAs of the plain launch: two per SM for blocks up to 16x16, else one.
-int plain_ctas(const nfd::DevPlan& d) { return (d.bh * d.bw <= 256 ? 2 : 1) * 148; }
 
 cudaError_t launch_spatial_shape(const nfd::DevPlan& d, const nfd::StripShape& S, dim3 grid, size_t smem,
                                  const nfd::PlaneJobs& job, cudaStream_t st) {
@@ -502,7 +573,9 @@ cudaError_t launch_spatial_shape(const nfd::DevPlan& d, const nfd::StripShape& S
 // One launch over J.n planes of one plan; the strip shape aims the whole grid at one
 // wave of resident CTAs.
 cudaError_t run_spatial_planes(const nfd::DevPlan& d, const nfd::PlaneJobs& J, cudaStream_t st) {
-  const nfd::StripShape S = pick_strip(d, std::max(1, plain_ctas(d) / J.n));
+  bool render = true;  // every plane renders a Kalman state: no pixel tiles
+  for (int i = 0; i < J.n; ++i) render = render && J.job[i].kalman_L != nullptr;
+  const nfd::StripShape S = pick_strip(d, J.n, render ? StripWork::Kalman : StripWork::Pixels);
   const size_t smem = nfd::strip_smem_bytes(d.bh, d.bw, S);
   const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th, J.n);
   return launch_spatial_shape(d, S, grid, smem, J, st);
@@ -787,7 +860,7 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
   const size_t smem1 = slice ? nfd::volume_spectra_smem_bytes(t.bh, t.bw, T, t.gx.step, nbc)
                              : nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, nbc);
   const int chunks = (t.gx.count + nbc - 1) / nbc, items = chunks * t.gy.count;
-  nfd::StripShape S = pick_strip(d, plain_ctas(d));
+  nfd::StripShape S = pick_strip(d, 1, slice ? StripWork::Slice : StripWork::Temporal);
   const size_t smem2 = nfd::strip_smem_bytes(t.bh, t.bw, S);
   const int tx = (t.gx.length + S.tw - 1) / S.tw, ty = (t.gy.length + S.th - 1) / S.th;
 
@@ -1422,7 +1495,7 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
       std::vector<nfd::StripShape> shapes;
       for (const nf_plan* p : plans) {
         dplans.push_back(p->dev);
-        shapes.push_back(pick_strip(p->dev, 1));
+        shapes.push_back(pick_strip(p->dev, 0, StripWork::Pixels));
       }
       std::vector<Entry> mine;
       for (auto& e : entries)
@@ -1433,7 +1506,8 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
       // the group, chosen by the queue's schedule over the resident CTAs.
       std::vector<std::pair<const nfd::DevPlan*, int>> queue;
       for (auto& e : mine) queue.emplace_back(&plans[size_t(e.plan)]->dev, shapes[size_t(e.plan)].tw);
-      const int seg_h = batch_segment_height(queue, g.bh, (long long)(g.bh * g.bw <= 256 ? 2 : 1) * sms);
+      const int seg_h =
+          batch_segment_height(queue, g.bh, (long long)(g.bh * g.bw <= 256 ? 2 : 1) * sms, StripWork::Pixels);
       for (size_t j = 0; j < plans.size(); ++j) {
         const int segs = std::max(1, (plans[j]->t.gy.length + seg_h - 1) / seg_h);
         shapes[j].th = (plans[j]->t.gy.length + segs - 1) / segs;
@@ -1578,7 +1652,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
     const long long slots = (long long)(b->bh * b->bw <= 256 ? 2 : 1) * sms_;
     std::vector<int> strips_x(plans.size());
     for (size_t j = 0; j < plans.size(); ++j) {
-      const nfd::StripShape S = pick_strip(plans[j]->dev, 1);
+      const nfd::StripShape S = pick_strip(plans[j]->dev, 0, b->slice ? StripWork::Slice : StripWork::Temporal);
       strips_x[j] = (plans[j]->t.gx.length + S.tw - 1) / S.tw;
     }
     int seg_h = 256;
@@ -1599,7 +1673,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
     }
     for (const nf_plan* p : plans) {
       dplans.push_back(p->dev);
-      nfd::StripShape S = pick_strip(p->dev, 1);
+      nfd::StripShape S = pick_strip(p->dev, 0, b->slice ? StripWork::Slice : StripWork::Temporal);
       const int segs = std::max(1, (p->t.gy.length + seg_h - 1) / seg_h);
       S.th = (p->t.gy.length + segs - 1) / segs;
       shapes.push_back(S);

@@ -38,7 +38,9 @@
 
 namespace nf {
 
-struct cf {
+// 8-byte aligned, so a complex value moves with one 64-bit access: consecutive
+// threads touching consecutive values hit distinct shared-memory banks.
+struct alignas(8) cf {
   float r, i;
 };
 

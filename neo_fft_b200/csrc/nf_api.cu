@@ -58,7 +58,21 @@ struct nf_plan {
   };
   mutable Pattern pattern;
   mutable std::mutex pattern_mu;
+  // Page-locked host slots for the per-call work tables of the two-pass temporal path:
+  // a copy from pageable memory would first wait for all earlier work on the stream.
+  static constexpr int kUploadSlots = 8;
+  mutable std::mutex upload_mu;
+  mutable unsigned char* upload = nullptr;  // kUploadSlots x upload_slot bytes
+  mutable size_t upload_slot = 0;
+  mutable cudaEvent_t upload_done[kUploadSlots] = {};
+  mutable int upload_next = 0;
   ~nf_plan() {
+    for (cudaEvent_t& e : upload_done)
+      if (e) {
+        cudaEventSynchronize(e);
+        cudaEventDestroy(e);
+      }
+    if (upload) cudaFreeHost(upload);
     if (pattern.dev) cudaFree(pattern.dev);
     if (tables) cudaFree(tables);
     if (err) cudaFree(err);
@@ -217,6 +231,37 @@ nf_status guarded(char* err, size_t len, F&& f) {
 }
 
 int storage_of(nf_format f) { return f.floating ? nfd::kStoreF32 : (f.bits == 8 ? nfd::kStoreU8 : nfd::kStoreU16); }
+
+// Stream-ordered scratch of the per-call paths comes from a pool per device that this
+// library owns and that keeps freed memory for reuse. The device's default pool hands
+// memory back to the system at every synchronisation, so the next call would map its
+// scratch (hundreds of MB for the temporal paths at 1080p) afresh, and the mapping
+// stalls the stream. The pools live until the process exits and hold their high-water
+// mark of scratch.
+cudaError_t scratch_alloc(void** ptr, size_t bytes, cudaStream_t st) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(dev);
+    if (it == pools.end()) {
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+      unsigned long long keep = ~0ull;
+      if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+      it = pools.emplace(dev, pool).first;
+    }
+    pool = it->second;
+  }
+  return cudaMallocFromPoolAsync(ptr, bytes, pool, st);
+}
 
 // Batched forms read each plan's primary table when they run, so a sampled noise model
 // (DFTTest nlocation, FFT3D pfactor) must be published before every launch, as for
@@ -798,7 +843,7 @@ nf_status process_dithered(const nf_plan& p, const nf_const_plane* sources, int 
   const int W = p.t.gx.length, H = p.t.gy.length;
   const size_t pitch = ((size_t(W) * sizeof(float) + 255) / 256) * 256;
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, pitch * size_t(H) + size_t(W) * sizeof(float), st);
+  cudaError_t e = scratch_alloc(&scratch, pitch * size_t(H) + size_t(W) * sizeof(float), st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
   auto* acc = static_cast<float*>(scratch);
   float* boundary = reinterpret_cast<float*>(static_cast<unsigned char*>(scratch) + pitch * size_t(H));
@@ -870,13 +915,34 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
                o_spec = o_base + al(sizeof(int) * size_t(T + 1));
   const size_t bytes = o_spec + size_t(T) * al(frame * sizeof(cf));
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, bytes, st);
+  cudaError_t e = scratch_alloc(&scratch, bytes, st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
   auto* b = static_cast<unsigned char*>(scratch);
   auto spec = [&](int z) { return reinterpret_cast<cf*>(b + o_spec + size_t(z) * al(frame * sizeof(cf))); };
 
-  std::vector<unsigned char> host(o_spec, 0);
-  auto* hdr = reinterpret_cast<TwoPassHeader*>(host.data() + o_hdr);
+  std::lock_guard<std::mutex> upload_lock(p.upload_mu);
+  if (!p.upload || p.upload_slot < o_spec) {
+    for (cudaEvent_t& ev : p.upload_done) {
+      if (ev) cudaEventSynchronize(ev);
+      else if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) break;
+    }
+    if (p.upload) cudaFreeHost(p.upload);
+    p.upload = nullptr;
+    p.upload_slot = 0;
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&p.upload), nf_plan::kUploadSlots * al(o_spec));
+    if (e != cudaSuccess) {
+      p.upload = nullptr;
+      cudaFreeAsync(scratch, st);
+      return cuda_fail(err, len, e, "host allocation failed");
+    }
+    p.upload_slot = al(o_spec);
+  }
+  const int us = p.upload_next;
+  p.upload_next = (us + 1) % nf_plan::kUploadSlots;
+  cudaEventSynchronize(p.upload_done[us]);  // the slot's previous copy has been read
+  unsigned char* host = p.upload + size_t(us) * p.upload_slot;
+  std::memset(host, 0, o_spec);
+  auto* hdr = reinterpret_cast<TwoPassHeader*>(host + o_hdr);
   hdr->plan = d;
   hdr->shape = S;
   const int zt = slice ? target : 0;
@@ -886,11 +952,11 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
   hdr->base[1] = tx * ty;
   hdr->tiles_x = tx;
   hdr->counter = 0;
-  auto* slots = reinterpret_cast<const cf**>(host.data() + o_slots);
+  auto* slots = reinterpret_cast<const cf**>(host + o_slots);
   for (int z = 0; z < T; ++z) slots[z] = spec(z);
-  auto* base = reinterpret_cast<int*>(host.data() + o_base);
+  auto* base = reinterpret_cast<int*>(host + o_base);
   if (slice) {
-    auto* vj = reinterpret_cast<nfd::VolumeSpectraJob*>(host.data() + o_jobs);
+    auto* vj = reinterpret_cast<nfd::VolumeSpectraJob*>(host + o_jobs);
     for (int z = 0; z < T; ++z) {
       vj->src[z] = static_cast<const unsigned char*>(sources[z].data);
       vj->src_stride[z] = sources[z].stride_bytes;
@@ -901,7 +967,7 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
     base[0] = 0;
     base[1] = items;
   } else {
-    auto* sj = reinterpret_cast<nfd::SpectraJob*>(host.data() + o_jobs);
+    auto* sj = reinterpret_cast<nfd::SpectraJob*>(host + o_jobs);
     for (int z = 0; z < T; ++z) {
       sj[z] = {static_cast<const unsigned char*>(sources[z].data), (long long)sources[z].stride_bytes, spec(z), 0,
                chunks};
@@ -909,7 +975,8 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
     }
     base[T] = T * items;
   }
-  e = cudaMemcpyAsync(scratch, host.data(), host.size(), cudaMemcpyHostToDevice, st);
+  e = cudaMemcpyAsync(scratch, host, o_spec, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaEventRecord(p.upload_done[us], st);
   const auto* dplan = reinterpret_cast<const nfd::DevPlan*>(b + o_hdr + offsetof(TwoPassHeader, plan));
   if (e == cudaSuccess) {
     if (slice) {

@@ -96,7 +96,7 @@ struct nf_kalman_state {
 
 // One persistent launch group: planes of one block shape and storage.
 struct BatchGroup {
-  int bh = 0, bw = 0, storage = 0, ctas = 0;
+  int bh = 0, bw = 0, storage = 0, algo = 0, ctas = 0;
   size_t smem = 0;
   void* dev = nullptr;  // plans | shapes | jobs | tile_base | tiles_x
   nfd::BatchWork work{};
@@ -1086,15 +1086,15 @@ void check_kalman_source(const nf_plan& p, const nf_const_plane& s) {
 cudaError_t launch_batch_group(const BatchGroup& g, cudaStream_t st) {
   if (g.bh == g.bw) {
     switch (g.bw) {
-      case 8: return nfd::launch_spatial_batch_8x8(g.storage, g.work, g.ctas, g.smem, st);
-      case 16: return nfd::launch_spatial_batch_16x16(g.storage, g.work, g.ctas, g.smem, st);
-      case 32: return nfd::launch_spatial_batch_32x32(g.storage, g.work, g.ctas, g.smem, st);
-      case 12: return nfd::launch_spatial_batch_12x12(g.storage, g.work, g.ctas, g.smem, st);
-      case 48: return nfd::launch_spatial_batch_48x48(g.storage, g.work, g.ctas, g.smem, st);
+      case 8: return nfd::launch_spatial_batch_8x8(g.storage, g.algo, g.work, g.ctas, g.smem, st);
+      case 16: return nfd::launch_spatial_batch_16x16(g.storage, g.algo, g.work, g.ctas, g.smem, st);
+      case 32: return nfd::launch_spatial_batch_32x32(g.storage, g.algo, g.work, g.ctas, g.smem, st);
+      case 12: return nfd::launch_spatial_batch_12x12(g.storage, g.algo, g.work, g.ctas, g.smem, st);
+      case 48: return nfd::launch_spatial_batch_48x48(g.storage, g.algo, g.work, g.ctas, g.smem, st);
       default: break;
     }
   }
-  return nfd::launch_spatial_batch_0x0(g.storage, g.work, g.ctas, g.smem, st);
+  return nfd::launch_spatial_batch_0x0(g.storage, g.algo, g.work, g.ctas, g.smem, st);
 }
 
 cudaError_t launch_spectra_shape(int bh, int bw, int storage, const nfd::SpectraWork& w, int items, size_t smem,
@@ -1522,16 +1522,19 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
       nfb::require(!p.t.preview, "pshow previews run through nf_plan_process_device");
       validate_call(p, &it.source, 1, nullptr, 0, it.dst);
       if (std::find(b->plans.begin(), b->plans.end(), &p) == b->plans.end()) b->plans.push_back(&p);
-      const int storage = storage_of(p.t.format);
+      const int storage = storage_of(p.t.format), algo = p.t.algo == nfb::Algo::FFT3D ? 0 : 1;
       int gi = -1;
       for (size_t g = 0; g < b->groups.size(); ++g)
-        if (b->groups[g].bh == p.t.bh && b->groups[g].bw == p.t.bw && b->groups[g].storage == storage) gi = int(g);
+        if (b->groups[g].bh == p.t.bh && b->groups[g].bw == p.t.bw && b->groups[g].storage == storage &&
+            b->groups[g].algo == algo)
+          gi = int(g);
       if (gi < 0) {
         gi = int(b->groups.size());
         BatchGroup g;
         g.bh = p.t.bh;
         g.bw = p.t.bw;
         g.storage = storage;
+        g.algo = algo;
         b->groups.push_back(g);
         group_plans.emplace_back();
       }

@@ -44,20 +44,22 @@ __device__ __forceinline__ int floor_div_i(int v, int d) { return v >= 0 ? v / d
 // Output conversion (kernels/scalar/spatial.cpp:89-129): FFT3D integer
 // (acc+0.5)+base, DFTTest integer acc*scale+0.5, clipped to [0, peak] and
 // truncated; FFT3D float clipped to [0,1]; DFTTest float acc*scale unclipped.
-template <int STORAGE>
+// ALGO: 0 FFT3D, 1 DFTTest known at compile time, -1 read from the plan.
+template <int STORAGE, int ALGO = -1>
 __device__ __forceinline__ void store_sample(unsigned char* row, int x, float acc, const DevPlan& P) {
+  const bool fft3d = ALGO >= 0 ? ALGO == 0 : P.algo == 0;
   if (STORAGE == kStoreU8 && P.raw_out) {  // dithered u8 output: the dither pass converts
     reinterpret_cast<float*>(row)[x] = acc;
     return;
   }
   if (STORAGE == kStoreF32) {
     float v;
-    if (P.algo == 0) v = acc < 0.0f ? 0.0f : (1.0f < acc ? 1.0f : acc);
+    if (fft3d) v = acc < 0.0f ? 0.0f : (1.0f < acc ? 1.0f : acc);
     else v = fmul(acc, P.out_scale);
     reinterpret_cast<float*>(row)[x] = v;
     return;
   }
-  const float v = P.algo == 0 ? fadd(fadd(acc, 0.5f), P.out_base) : fadd(fmul(acc, P.out_scale), 0.5f);
+  const float v = fft3d ? fadd(fadd(acc, 0.5f), P.out_base) : fadd(fmul(acc, P.out_scale), 0.5f);
   const float c = v < 0.0f ? 0.0f : (P.out_peak < v ? P.out_peak : v);
   if (STORAGE == kStoreU8) row[x] = (unsigned char)(c);
   else reinterpret_cast<unsigned short*>(row)[x] = (unsigned short)(c);
@@ -173,9 +175,12 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
   }
 }
 
-template <int BHC, int BWC, int STORAGE, int SRC = kSrcPixels>
+// ALGO: 0 FFT3D, 1 DFTTest (the launch knows the plan's algorithm, so the other
+// algorithm's branches are compiled out), -1 read from the plan.
+template <int BHC, int BWC, int STORAGE, int SRC = kSrcPixels, int ALGO = -1>
 __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, const StripShape& S, int px0, int py0,
                                            float* smem) {
+  const bool fft3d = ALGO >= 0 ? ALGO == 0 : P.algo == 0;
   const int BH = BHC > 0 ? BHC : P.bh;
   const int BW = BWC > 0 ? BWC : P.bw;
   const int K = BW / 2 + 1;
@@ -223,7 +228,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     return d;
   };
   const float *wxa = nullptr, *wya = nullptr, *wxs = nullptr, *wys = nullptr, *h = nullptr, *hsyn = nullptr;
-  if (P.algo == 0) {
+  if (fft3d) {
     wxa = stage(P.wxa, BW);
     wya = stage(P.wya, BH);
     wxs = stage(P.wxs, BW);
@@ -308,7 +313,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         }
 #pragma unroll UW
         for (int x = 0; x < CAPW; ++x)
-          if (x < BW) row[x] = P.algo == 0 ? fmul(fmul(row[x], wya[y]), wxa[x]) : fmul(row[x], h[y * BW + x]);
+          if (x < BW) row[x] = fft3d ? fmul(fmul(row[x], wya[y]), wxa[x]) : fmul(row[x], h[y * BW + x]);
         nf::row_forward<BWC>(row, BW, spec + size_t(y) * K * NB + b, P.tww, codelet, NB);
       }
       __syncthreads();
@@ -400,14 +405,14 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       __syncthreads();
       if (active) {
         const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
-        if (P.algo == 1 || P.fft3d_mode != kEnhanceOnly) {
+        if (!fft3d || P.fft3d_mode != kEnhanceOnly) {
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
             if (y < BH) col[y] = spectral_bin(col[y], grid, y * K + k, g, filt, bad);
         }
-        if (P.algo == 0 && P.fft3d_mode == kWienerThenEnh && k == 0) dc[NB + b] = col[0].r;
+        if (fft3d && P.fft3d_mode == kWienerThenEnh && k == 0) dc[NB + b] = col[0].r;
       }
-      if (P.algo == 0 && P.fft3d_mode != kWienerFused && enh.enh) {
+      if (fft3d && P.fft3d_mode != kWienerFused && enh.enh) {
         // enhance(): template ratio recomputed from the spectrum being enhanced
         // (plan.cpp:325-329).
         if (P.fft3d_mode == kWienerThenEnh) __syncthreads();
@@ -441,7 +446,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         if (x < BW) {
           if (!isfin(row[x])) bad = true;
           if constexpr (SRC == kSrcSlice) row[x] = fmul(fmul(volume, row[x]), h[y * BW + x]);
-          else row[x] = P.algo == 0 ? fmul(row[x], wxs[x]) : fmul(row[x], hsyn[y * BW + x]);
+          else row[x] = fft3d ? fmul(row[x], wxs[x]) : fmul(row[x], hsyn[y * BW + x]);
         }
       }
       if ((BW & 3) == 0) {
@@ -471,7 +476,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
       const float* ov = orow + size_t(cm & 1023) * OBW + (cm >> 20);
       const int adv = OBW - gx.step;
-      if (P.algo == 0) {
+      if (fft3d) {
         float r = 0.0f;
         for (int j = 0; j < nblk; ++j, ov += adv) r = fadd(r, *ov);
         *a = fadd(*a, fmul(r, wys[ly]));
@@ -490,7 +495,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       float* a = acc + size_t(Y % BH) * S.tw + xx;
       const float v = *a;
       if (!isfin(v)) bad = true;
-      store_sample<STORAGE>(J.dst + ptrdiff_t(Y - gy.offset) * J.dst_stride, px0 + xx, v, P);
+      store_sample<STORAGE, ALGO>(J.dst + ptrdiff_t(Y - gy.offset) * J.dst_stride, px0 + xx, v, P);
       *a = 0.0f;
     }
   }
@@ -513,11 +518,12 @@ struct PlaneJobs {
   int n;
 };
 
-template <int BHC, int BWC, int STORAGE>
+template <int BHC, int BWC, int STORAGE, int ALGO>
 __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value)
     spatial_strip_kernel(DevPlan P, StripShape S, const __grid_constant__ PlaneJobs J) {
   extern __shared__ float smem[];
-  strip_tile<BHC, BWC, STORAGE>(P, J.job[blockIdx.z], S, blockIdx.x * S.tw, blockIdx.y * S.th, smem);
+  strip_tile<BHC, BWC, STORAGE, kSrcPixels, ALGO>(P, J.job[blockIdx.z], S, blockIdx.x * S.tw, blockIdx.y * S.th,
+                                                  smem);
 }
 
 // Batched launch: a persistent grid pulls (plane, strip, segment) work items from
@@ -533,7 +539,8 @@ struct BatchWork {
   int* counter;              // work-queue head, reset by the host before launch
 };
 
-template <int BHC, int BWC, int STORAGE>
+// Batched launch over planes of one algorithm (ALGO 0 FFT3D, 1 DFTTest).
+template <int BHC, int BWC, int STORAGE, int ALGO>
 __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_batch_kernel(BatchWork W) {
   extern __shared__ float smem[];
   __shared__ int item;
@@ -563,7 +570,7 @@ __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_
     __syncthreads();
     const int local = t - W.job_tile_base[lo];
     const int sx = local % W.job_tiles_x[lo], sy = local / W.job_tiles_x[lo];
-    strip_tile<BHC, BWC, STORAGE>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+    strip_tile<BHC, BWC, STORAGE, kSrcPixels, ALGO>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
   }
 }
 

@@ -322,10 +322,10 @@ __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) temporal
     const int local = t - W.job_tile_base[lo];
     const int sx = local % W.job_tiles_x[lo], sy = local / W.job_tiles_x[lo];
     if constexpr (SRC == kSrcSlice) {
-      strip_tile<BHC, BWC, STORAGE, kSrcSlice>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+      strip_tile<BHC, BWC, STORAGE, kSrcSlice, 1>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
     } else {
-      if (sJ.tspec) strip_tile<BHC, BWC, STORAGE, kSrcTemporal>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
-      else strip_tile<BHC, BWC, STORAGE, kSrcPixels>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+      if (sJ.tspec) strip_tile<BHC, BWC, STORAGE, kSrcTemporal, 0>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+      else strip_tile<BHC, BWC, STORAGE, kSrcPixels, 0>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
     }
   }
 }

@@ -116,6 +116,27 @@ __host__ __device__ inline size_t strip_smem_bytes(int bh, int bw, const StripSh
                           size_t(s.tw));
 }
 
+// Walks the linear indices start, start + step, ... of a rows x width range as (y, x)
+// pairs with one division at the start: each step adds the step's quotient and
+// remainder and carries once. `i < rows * width` is `y < rows`; width must be positive.
+struct Cursor2 {
+  int y, x, dq, dr, w;
+  __device__ __forceinline__ Cursor2(int start, int step, int width) : w(width) {
+    y = start / width;
+    x = start - y * width;
+    dq = step / width;
+    dr = step - dq * width;
+  }
+  __device__ __forceinline__ void next() {
+    y += dq;
+    x += dr;
+    if (x >= w) {
+      x -= w;
+      ++y;
+    }
+  }
+};
+
 // FFT3D bt=2..5 filter of one block row's (bin, block) elements across the T slot
 // spectra (spectral.cpp:90-160) with T = TC known at compile time; writes the recovered
 // spectrum into spec [bin][block].
@@ -139,9 +160,10 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
   const float* primary = filt.primary;
   const float fT = float(TC);
   (void)T;
+  const int nrow_e = nel / nbx;  // bins
 #pragma unroll 2
-  for (int e = tid; e < nel; e += nthr) {
-    const int kk = e / nbx, b = e - kk * nbx;
+  for (Cursor2 c(tid, nthr, nbx); c.y < nrow_e; c.next()) {
+    const int kk = c.y, b = c.x;
     const size_t at = row_base + size_t(kk) * cnt + b;
     cf v[TC];
 #pragma unroll
@@ -280,8 +302,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       // ---- 0: stage the rows this block row adds ----------------------------
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
       const int nrows = oy + BH - r0;
-      for (int i = tid; i < nrows * win; i += nthr) {
-        const int rr = i / win, xx = i - rr * win;
+      for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
+        const int rr = c.y, xx = c.x;
         const int cy = r0 + rr;
         const unsigned char* srow = J.src + ptrdiff_t(reflect_axis(cy, gy)) * J.src_stride;
         const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
@@ -291,8 +313,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       }
       __syncthreads();
       // ---- A: row transforms (block index fastest) --------------------------
-      for (int task = tid; task < nbx * BH; task += nthr) {
-        const int y = task / nbx, b = task - y * nbx;
+      for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
+        const int y = c.y, b = c.x;
         const float* in = ring_in + size_t((oy + y) % BH) * S.ring_pitch + b * gx.step;
         float row[CAPW];
         if (vec4) {
@@ -324,8 +346,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       // DFTTest tmode 1 (plan.cpp:544-601): the slice's spectrum was filtered in 3-D by
       // the volume pass; only the column inverses remain.
       const cf* S = J.tspec[0] + size_t(by) * bins * size_t(gx.count) + size_t(bx_lo);
-      for (int task = tid; task < ncol; task += nthr) {
-        const int k = task / nbx, b = task - k * nbx;
+      for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
+        const int k = c.y, b = c.x;
         cf col[CAPH];
 #pragma unroll UH
         for (int y = 0; y < CAPH; ++y)
@@ -360,16 +382,16 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       if (enh.enh) {
         for (int b = tid; b < nbx; b += nthr) dc[NB + b] = spec[b].r;  // recovered DC
         __syncthreads();
-        for (int e = tid; e < nel; e += nthr) {
-          const int kk = e / nbx, b = e - kk * nbx;
+        for (Cursor2 c(tid, nthr, nbx); c.y < bins; c.next()) {
+          const int kk = c.y, b = c.x;
           const float g2 = grid ? fdiv(fmul(P.mean_scale, dc[NB + b]), grid0) : 0.0f;
           cf* sp = spec + size_t(kk) * NB + b;
           *sp = spectral_bin(*sp, grid, kk, g2, enh, bad);
         }
         __syncthreads();
       }
-      for (int task = tid; task < ncol; task += nthr) {
-        const int k = task / nbx, b = task - k * nbx;
+      for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
+        const int k = c.y, b = c.x;
         cf col[CAPH];
         cf* sp = spec + size_t(k) * NB + b;
 #pragma unroll UH
@@ -382,10 +404,10 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       }
       __syncthreads();
     } else {
-    for (int base = 0; base < ncol; base += nthr) {
-      const int task = base + tid;
-      const bool active = task < ncol;
-      const int k = active ? task / nbx : 0, b = active ? task - k * nbx : 0;
+    Cursor2 cb(tid, nthr, nbx);
+    for (int base = 0; base < ncol; base += nthr, cb.next()) {
+      const bool active = cb.y < K;  // task < ncol
+      const int k = active ? cb.y : 0, b = active ? cb.x : 0;
       cf col[CAPH];
       cf* sp = spec + size_t(k) * NB + b;  // + y*K*NB
       if (active) {
@@ -434,8 +456,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     }
     }
     // ---- C: row inverses and synthesis weighting -----------------------------
-    for (int task = tid; task < nbx * BH; task += nthr) {
-      const int y = task / nbx, b = task - y * nbx;
+    for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
+      const int y = c.y, b = c.x;
       if (P.center && y != BH / 2) continue;
       float row[CAPW];
       nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, SRC == kSrcSlice ? fct3 : fct, row, P.tww, codelet,
@@ -462,8 +484,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     __syncthreads();
     // ---- D: ordered overlap-add into the ring accumulator --------------------
     const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
-    for (int i = tid; yhi > ylo && i < (yhi - ylo) * tw; i += nthr) {
-      const int yy = i / tw, xx = i - yy * tw;
+    for (Cursor2 c(tid, nthr, tw); c.y < yhi - ylo; c.next()) {
+      const int yy = c.y, xx = c.x;
       const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;
       const float* orow = ob + size_t(ly) * NB * OBW;
@@ -489,8 +511,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     __syncthreads();
     // ---- E: retire rows that no later block row touches ---------------------
     const int rlo = max(oy, Y0), rhi = min(by == by_hi ? Y0 + th : oy + gy.step, Y0 + th);
-    for (int i = tid; rhi > rlo && i < (rhi - rlo) * tw; i += nthr) {
-      const int yy = i / tw, xx = i - yy * tw;
+    for (Cursor2 c(tid, nthr, tw); c.y < rhi - rlo; c.next()) {
+      const int yy = c.y, xx = c.x;
       const int Y = rlo + yy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;
       const float v = *a;

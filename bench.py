@@ -70,13 +70,46 @@ def make_clip(rank: int, frames: int):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled every 10 ms during the timed
+    region through NVML (read-only queries), or through nvidia-smi where NVML cannot be
+    loaded. The GPU is found by its PCI address, so CUDA_VISIBLE_DEVICES renumbering
+    does not matter."""
 
     def __init__(self, index: int):
         self.index, self.samples, self._stop = index, [], threading.Event()
+        try:  # NVML is opened before the timed region starts
+            self._nv = self._nvml_handle()
+        except Exception:
+            self._nv = None
         self._t = threading.Thread(target=self._run, daemon=True)
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.index)
+        try:
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
     def _run(self):
+        try:
+            nv, h = self._nv
+            bits = [getattr(nv, "nvmlClocksEventReason" + n, None) or getattr(nv, "nvmlClocksThrottleReason" + n)
+                    for n in ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                r = reasons(h)
+                self.samples.append([str(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), str(mx), "",
+                                     *["Active" if r & b else "Not Active" for b in bits]])
+                self._stop.wait(0.01)
+            return
+        except Exception:
+            pass
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")

@@ -447,7 +447,7 @@ def differentiable_pass(args, dev, world=1):
     m.table.grad = None
     static_x.grad = None
     graph = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(graph):
+    with torch.cuda.graph(graph, capture_error_mode="thread_local"):
         ((m(static_x) - cl) ** 2).mean().backward()
     g_ms = measure(graph.replay, steps)
     del graph

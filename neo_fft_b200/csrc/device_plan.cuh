@@ -36,6 +36,7 @@ struct DevSpectral {
   float sharpen, dehalo, ea, eb, ec;
   const float* sharpen_w;
   const float* halo_w;
+  int emode;  // ftype 0 gain from the exponent: 0 the Wiener ratio, 1 its square root, 2 its power
 };
 
 enum StoreKind : int { kStoreU8 = 1, kStoreU16 = 2, kStoreF32 = 4 };
@@ -121,9 +122,8 @@ NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectra
     case 0: {
       const float r = fdiv(fsub(power, a), fadd(power, 1e-15f));
       const float wiener = r < 0.0f ? 0.0f : r;
-      const float e1 = fsub(p.exponent, 1.0f), e5 = fsub(p.exponent, 0.5f);
-      if ((e1 < 0 ? -e1 : e1) < 0.00005f) gain = wiener;
-      else if ((e5 < 0 ? -e5 : e5) < 0.00005f) gain = fsqrt(wiener);
+      if (p.emode == 0) gain = wiener;
+      else if (p.emode == 1) gain = fsqrt(wiener);
       else gain = powf(wiener, p.exponent);
       break;
     }
@@ -145,9 +145,11 @@ NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectra
   }
   if (p.enh) gain = fmul(gain, enhancement_gain(fadd(power, 1e-15f), k, p));
   const cf out = {fadd(fmul(gain, re), mr), fadd(fmul(gain, im), mi)};
-  if (!isfin(mr) || !isfin(mi) || !isfin(re) || !isfin(im) || !isfin(power) || !isfin(gain) || !isfin(out.r) ||
-      !isfin(out.i))
-    bad = true;
+  // The reference checks mr, mi, re, im, power, gain and both outputs. A non-finite mr,
+  // re or gain always makes out.r non-finite (inf or NaN propagate through the product
+  // and the sum; inf * 0 is NaN), and mi, im or gain out.i, so power and the two
+  // outputs decide the same error.
+  if (!isfin(power) || !isfin(out.r) || !isfin(out.i)) bad = true;
   return out;
 }
 

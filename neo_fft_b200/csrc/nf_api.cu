@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <atomic>
 #include <cstring>
@@ -376,6 +377,10 @@ nf_status finalize_plan(std::unique_ptr<nf_plan>& p, char* err, size_t len) {
             static_cast<const float*>(ptr(o_sw)), static_cast<const float*>(ptr(o_hw))};
   d.enh = {-2, 0, 0, 0, 0, 1, 0, nullptr, en.active() ? 1 : 0, en.sharpen, en.dehalo, en.a, en.b, en.c,
            static_cast<const float*>(ptr(o_sw)), static_cast<const float*>(ptr(o_hw))};
+  {  // ftype 0 exponent tests of spectral.cpp:25-27, once per plan instead of per bin
+    const float e1 = s.exponent - 1.0f, e5 = s.exponent - 0.5f;
+    d.filt.emode = std::fabs(e1) < 0.00005f ? 0 : std::fabs(e5) < 0.00005f ? 1 : 2;
+  }
   if (d.algo == 0)
     d.fft3d_mode = !t.denoise ? nfd::kEnhanceOnly
                               : (!s.primary.empty() || t.needs_pattern ? nfd::kWienerThenEnh : nfd::kWienerFused);

@@ -308,7 +308,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         const unsigned char* srow = J.src + ptrdiff_t(reflect_axis(cy, gy)) * J.src_stride;
         const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
         const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
-        if (!isfin(v)) bad = true;
+        if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
         ring_in[size_t(cy % BH) * S.ring_pitch + xx] = v;
       }
       __syncthreads();
@@ -463,14 +463,18 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, SRC == kSrcSlice ? fct3 : fct, row, P.tww, codelet,
                            NB);
       float* o = ob + (size_t(y) * NB + b) * OBW;
+      // NaN once any inverse sample is non-finite (x * 0 is NaN for inf and NaN, and a
+      // signed zero otherwise): one multiply-add per sample instead of a compare.
+      float guard = 0.0f;
 #pragma unroll UW
       for (int x = 0; x < CAPW; ++x) {
         if (x < BW) {
-          if (!isfin(row[x])) bad = true;
+          guard = __fmaf_rn(row[x], 0.0f, guard);
           if constexpr (SRC == kSrcSlice) row[x] = fmul(fmul(volume, row[x]), h[y * BW + x]);
           else row[x] = fft3d ? fmul(row[x], wxs[x]) : fmul(row[x], hsyn[y * BW + x]);
         }
       }
+      if (guard != guard) bad = true;
       if ((BW & 3) == 0) {
 #pragma unroll UW
         for (int x = 0; x < CAPW; x += 4)

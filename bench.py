@@ -39,8 +39,8 @@ sys.path.insert(0, str(ROOT))
 W, H, CW, CH, FRAMES = 1920, 1080, 960, 540, 60
 HOST_CHUNK = 2  # frames per device slot of the streamed host form
 # DRAM bytes of one batch launch over the 60-frame clip: ncu capture of a 16-frame launch of
-# the same kernel (100.18 MB read + 75.36 MB written), scaled by the frames processed.
-TRAFFIC_PER_LAUNCH = (100.18e6 + 75.36e6) * FRAMES / 16
+# the same kernel (100.73 MB read + 60.34 MB written), scaled by the frames processed.
+TRAFFIC_PER_LAUNCH = (100.73e6 + 60.34e6) * FRAMES / 16
 METRIC = "Mpx/s per config on 1 B200 (plain vs batched/graph), fwd+bwd Mpx/s, vs host CPU"
 WORKLOAD = "DFTTest tbsize=1 sbsize=16 sosize=12 ftype=0 sigma=8 flat curve, 1920x1080 YUV420P16, 60 frames"
 
@@ -371,8 +371,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved_gbs / hbm_peak, "traffic": TRAFFIC_PER_LAUNCH,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 16-frame launch "
-                                       "of the same kernel (175.5 MB), scaled by 60/16",
-                     "kernel": "spatial_batch_kernel<16,16,u16> (whole clip per launch)", "launch_ms": ms_step,
+                                       "of the same kernel (161.1 MB), scaled by 60/16",
+                     "kernel": "spatial_batch_kernel<16,16,u16,DFTTest> (whole clip per launch)", "launch_ms": ms_step,
                      "alg_bytes_per_launch": alg_bytes,
                      "fp32": {"achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
                               "frac": achieved_tf / fp32_peak, "alg_flops_per_launch": alg_flops,

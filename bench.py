@@ -376,7 +376,10 @@ def run_ours(args):
                      "alg_bytes_per_launch": alg_bytes,
                      "fp32": {"achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
                               "frac": achieved_tf / fp32_peak, "alg_flops_per_launch": alg_flops,
-                              "peak_source": "148 SMs x 128 FP32 lanes x 2 x max SM clock (nominal)"}},
+                              "peak_source": "148 SMs x 128 FP32 lanes x 2 x max SM clock (nominal)",
+                              # the reference's binary32 rounding of every add and multiply rules out
+                              # fused multiply-adds, so one flop per lane per clock is the ceiling
+                              "peak_unfused": fp32_peak / 2, "frac_unfused": 2 * achieved_tf / fp32_peak}},
         "clocks": clocks.summary() if clocks else None,
         "cpu_baseline": cpu,
         "fwd_bwd": train,

@@ -154,8 +154,8 @@ def cpu_baseline(frames_sample: int = 2):
     fmt = SampleFormat(16)
     luma = R.RefPlan(W, H, fmt, dft_config())
     chroma = R.RefPlan(CW, CH, fmt, dft_config())
-    clip = make_clip(0, max(frames_sample, threads))
-    n = max(frames_sample, threads)
+    n = max(frames_sample, 2 * threads)  # about 15-20 s of CPU work over all threads
+    clip = make_clip(0, n)
     t0 = time.perf_counter()
     luma.process_many([[c[0]] for c in clip[:n]], threads)
     chroma.process_many([[c[p]] for c in clip[:n] for p in (1, 2)], threads)

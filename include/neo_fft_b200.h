@@ -178,8 +178,11 @@ typedef struct nf_batch_item {
   nf_plane dst;
 } nf_batch_item;
 nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** batch, char* err, size_t err_len);
-/* Enqueues the batch on `stream`: no allocation or synchronisation, so the call
- * may be captured in a CUDA graph. */
+/* Enqueues the batch on `stream`: no allocation. The first call outside a stream
+ * capture also tunes the strip geometry: it launches each of up to three candidate
+ * geometries once (after a warm-up launch; all write the same outputs) and waits for
+ * them, keeping the fastest. Later calls do not synchronise and may be captured in a
+ * CUDA graph; a first call inside a capture keeps the modelled geometry. */
 nf_status nf_batch_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
 /* Captures nf_batch_launch into a CUDA graph on first use, then replays the graph. */
 nf_status nf_batch_graph_launch(nf_batch* batch, void* stream, char* err, size_t err_len);

@@ -104,7 +104,9 @@ struct BatchGroup {
 };
 
 struct nf_batch {
-  std::vector<BatchGroup> groups;
+  std::vector<BatchGroup> groups;                 // the strip geometry in use (one of `variants`)
+  std::vector<std::vector<BatchGroup>> variants;  // candidate geometries, timed on the first launch
+  bool tuned = false;
   std::vector<const nf_plan*> plans;  // distinct plans (sampled noise models are checked per launch)
   int* counters = nullptr;  // one queue head per group
   cudaGraph_t graph = nullptr;
@@ -114,8 +116,9 @@ struct nf_batch {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (capture_stream) cudaStreamDestroy(capture_stream);
-    for (auto& g : groups)
-      if (g.dev) cudaFree(g.dev);
+    for (auto& v : variants)
+      for (auto& g : v)
+        if (g.dev) cudaFree(g.dev);
     if (counters) cudaFree(counters);
   }
 };
@@ -486,8 +489,10 @@ double tile_cost(const nfd::DevPlan& d, int cols, int rows, StripWork w) {
 // schedule over the resident CTAs). plain_planes == 0: batched forms, whose callers set
 // the segment height; the width minimises the modelled work per owned column. Both keep
 // the shared-memory budget of the occupancy target (two CTAs per SM up to 16x16 blocks,
-// one above). Results are cached per geometry: plain launches ask on every call.
-nfd::StripShape pick_strip(const nfd::DevPlan& d, int plain_planes, StripWork work) {
+// one above). Returns every feasible width, best modelled first (batched forms time the
+// first few on their first launch). Results are cached per geometry: plain launches ask on
+// every call.
+std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_planes, StripWork work) {
   struct Key {
     int len_x, len_y, bh, bw, sx, sy, tab, planes, work;
     bool operator<(const Key& o) const {
@@ -496,7 +501,7 @@ nfd::StripShape pick_strip(const nfd::DevPlan& d, int plain_planes, StripWork wo
     }
   };
   static std::mutex memo_mu;
-  static std::map<Key, nfd::StripShape> memo;
+  static std::map<Key, std::vector<nfd::StripShape>> memo;
   const Key key{d.gx.length, d.gy.length, d.bh, d.bw, d.gx.step, d.gy.step, nfd::strip_table_floats(d), plain_planes,
                 int(work)};
   {
@@ -521,8 +526,7 @@ nfd::StripShape pick_strip(const nfd::DevPlan& d, int plain_planes, StripWork wo
   };
   const size_t budget = size_t(d.bh * d.bw <= 256 ? 110 : 200) * 1024;
   const int slots = plain_ctas(d);
-  nfd::StripShape S = shape(edge + 2);
-  double best = -1.0;
+  std::vector<std::pair<double, nfd::StripShape>> ranked;
   std::vector<double> costs;
   for (int nbx = edge + 2; nbx <= 128; ++nbx) {
     nfd::StripShape c = shape(nbx);
@@ -555,15 +559,20 @@ nfd::StripShape pick_strip(const nfd::DevPlan& d, int plain_planes, StripWork wo
     } else {
       cost = tile_cost(d, c.tw, 0, work) / double(c.tw);
     }
-    if (best < 0 || cost < best) {
-      best = cost;
-      S = c;
-    }
+    ranked.emplace_back(cost, c);
     if (c.tw >= d.gx.length) break;  // wider strips own no more columns
   }
+  std::stable_sort(ranked.begin(), ranked.end(),
+                   [](const auto& a, const auto& b) { return a.first < b.first; });
+  std::vector<nfd::StripShape> out;
+  for (const auto& r : ranked) out.push_back(r.second);
+  if (out.empty()) out.push_back(shape(edge + 2));  // over the budget even at its narrowest
   std::lock_guard<std::mutex> lock(memo_mu);
-  memo.emplace(key, S);
-  return S;
+  return memo.emplace(key, out).first->second;
+}
+
+nfd::StripShape pick_strip(const nfd::DevPlan& d, int plain_planes, StripWork work) {
+  return strip_candidates(d, plain_planes, work).front();
 }
 
 // Segment height of the strips of a batch group. The device queue hands tiles to the
@@ -1563,72 +1572,136 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
       return cuda_fail(err, len, ce, "device allocation failed");
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
-      BatchGroup& g = b->groups[gi];
-      const auto& plans = group_plans[gi];
-      std::vector<nfd::DevPlan> dplans;
-      std::vector<nfd::StripShape> shapes;
-      for (const nf_plan* p : plans) {
-        dplans.push_back(p->dev);
-        shapes.push_back(pick_strip(p->dev, 0, StripWork::Pixels));
+    // Candidate geometries: variant v gives every plan its v-th best strip width by the
+    // tile-cost model (or its last one); the first launch times them (nf_batch_launch).
+    constexpr int kVariants = 3;
+    int nvar = 1;
+    for (const auto& plans : group_plans)
+      for (const nf_plan* p : plans)
+        nvar = std::max(nvar, std::min(kVariants, int(strip_candidates(p->dev, 0, StripWork::Pixels).size())));
+    const std::vector<BatchGroup> proto = b->groups;
+    for (int v = 0; v < nvar; ++v) {
+      std::vector<BatchGroup> groups = proto;
+      for (size_t gi = 0; gi < groups.size(); ++gi) {
+        BatchGroup& g = groups[gi];
+        const auto& plans = group_plans[gi];
+        std::vector<nfd::DevPlan> dplans;
+        std::vector<nfd::StripShape> shapes;
+        for (const nf_plan* p : plans) {
+          dplans.push_back(p->dev);
+          const auto& cand = strip_candidates(p->dev, 0, StripWork::Pixels);
+          shapes.push_back(cand[std::min(size_t(v), cand.size() - 1)]);
+        }
+        std::vector<Entry> mine;
+        for (auto& e : entries)
+          if (e.group == int(gi)) mine.push_back(e);
+        // Largest planes first: shortens the tail of the dynamic queue.
+        std::stable_sort(mine.begin(), mine.end(), [](const Entry& a, const Entry& c) { return a.cost > c.cost; });
+        // Tall strips (the batch already supplies parallelism), one segment height for
+        // the group, chosen by the queue's schedule over the resident CTAs.
+        std::vector<std::pair<const nfd::DevPlan*, int>> queue;
+        for (auto& e : mine) queue.emplace_back(&plans[size_t(e.plan)]->dev, shapes[size_t(e.plan)].tw);
+        const int seg_h =
+            batch_segment_height(queue, g.bh, (long long)(g.bh * g.bw <= 256 ? 2 : 1) * sms, StripWork::Pixels);
+        for (size_t j = 0; j < plans.size(); ++j) {
+          const int segs = std::max(1, (plans[j]->t.gy.length + seg_h - 1) / seg_h);
+          shapes[j].th = (plans[j]->t.gy.length + segs - 1) / segs;
+          g.smem = std::max(g.smem, nfd::strip_smem_bytes(g.bh, g.bw, shapes[j]));
+        }
+        std::vector<nfd::PlaneJob> jobs;
+        std::vector<int> base(1, 0), tiles_x;
+        for (auto& e : mine) {
+          const nfd::StripShape& S = shapes[size_t(e.plan)];
+          const nf_plan* p = plans[size_t(e.plan)];
+          const int tx = (p->t.gx.length + S.tw - 1) / S.tw, ty = (p->t.gy.length + S.th - 1) / S.th;
+          jobs.push_back(e.job);
+          tiles_x.push_back(tx);
+          base.push_back(base.back() + tx * ty);
+        }
+        Blob blob;
+        const size_t o_p = blob.add(dplans), o_s = blob.add(shapes), o_j = blob.add(jobs), o_b = blob.add(base),
+                     o_t = blob.add(tiles_x);
+        if ((ce = cudaMalloc(&g.dev, blob.bytes.size())) != cudaSuccess) {
+          b->variants.push_back(groups);  // freed with the batch
+          return cuda_fail(err, len, ce, "device allocation failed");
+        }
+        if ((ce = cudaMemcpy(g.dev, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+          b->variants.push_back(groups);
+          return cuda_fail(err, len, ce, "batch upload failed");
+        }
+        auto* base_ptr = static_cast<unsigned char*>(g.dev);
+        g.work.plans = reinterpret_cast<const nfd::DevPlan*>(base_ptr + o_p);
+        g.work.shapes = reinterpret_cast<const nfd::StripShape*>(base_ptr + o_s);
+        g.work.jobs = reinterpret_cast<const nfd::PlaneJob*>(base_ptr + o_j);
+        g.work.job_tile_base = reinterpret_cast<const int*>(base_ptr + o_b);
+        g.work.job_tiles_x = reinterpret_cast<const int*>(base_ptr + o_t);
+        g.work.njobs = int(jobs.size());
+        g.work.counter = b->counters + gi;
+        g.ctas = std::max(1, std::min(base.back(), 2 * sms));
       }
-      std::vector<Entry> mine;
-      for (auto& e : entries)
-        if (e.group == int(gi)) mine.push_back(e);
-      // Largest planes first: shortens the tail of the dynamic queue.
-      std::stable_sort(mine.begin(), mine.end(), [](const Entry& a, const Entry& c) { return a.cost > c.cost; });
-      // Tall strips (the batch already supplies parallelism), one segment height for
-      // the group, chosen by the queue's schedule over the resident CTAs.
-      std::vector<std::pair<const nfd::DevPlan*, int>> queue;
-      for (auto& e : mine) queue.emplace_back(&plans[size_t(e.plan)]->dev, shapes[size_t(e.plan)].tw);
-      const int seg_h =
-          batch_segment_height(queue, g.bh, (long long)(g.bh * g.bw <= 256 ? 2 : 1) * sms, StripWork::Pixels);
-      for (size_t j = 0; j < plans.size(); ++j) {
-        const int segs = std::max(1, (plans[j]->t.gy.length + seg_h - 1) / seg_h);
-        shapes[j].th = (plans[j]->t.gy.length + segs - 1) / segs;
-        g.smem = std::max(g.smem, nfd::strip_smem_bytes(g.bh, g.bw, shapes[j]));
-      }
-      std::vector<nfd::PlaneJob> jobs;
-      std::vector<int> base(1, 0), tiles_x;
-      for (auto& e : mine) {
-        const nfd::StripShape& S = shapes[size_t(e.plan)];
-        const nf_plan* p = plans[size_t(e.plan)];
-        const int tx = (p->t.gx.length + S.tw - 1) / S.tw, ty = (p->t.gy.length + S.th - 1) / S.th;
-        jobs.push_back(e.job);
-        tiles_x.push_back(tx);
-        base.push_back(base.back() + tx * ty);
-      }
-      Blob blob;
-      const size_t o_p = blob.add(dplans), o_s = blob.add(shapes), o_j = blob.add(jobs), o_b = blob.add(base),
-                   o_t = blob.add(tiles_x);
-      if ((ce = cudaMalloc(&g.dev, blob.bytes.size())) != cudaSuccess)
-        return cuda_fail(err, len, ce, "device allocation failed");
-      if ((ce = cudaMemcpy(g.dev, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
-        return cuda_fail(err, len, ce, "batch upload failed");
-      auto* base_ptr = static_cast<unsigned char*>(g.dev);
-      g.work.plans = reinterpret_cast<const nfd::DevPlan*>(base_ptr + o_p);
-      g.work.shapes = reinterpret_cast<const nfd::StripShape*>(base_ptr + o_s);
-      g.work.jobs = reinterpret_cast<const nfd::PlaneJob*>(base_ptr + o_j);
-      g.work.job_tile_base = reinterpret_cast<const int*>(base_ptr + o_b);
-      g.work.job_tiles_x = reinterpret_cast<const int*>(base_ptr + o_t);
-      g.work.njobs = int(jobs.size());
-      g.work.counter = b->counters + gi;
-      g.ctas = std::max(1, std::min(base.back(), 2 * sms));
+      b->variants.push_back(groups);
     }
+    b->groups = b->variants.empty() ? std::vector<BatchGroup>{} : b->variants.front();
+    b->tuned = b->variants.size() <= 1;
     *out = b.release();
     return NF_OK;
   });
 }
+
+namespace {
+cudaError_t launch_groups(nf_batch& b, const std::vector<BatchGroup>& groups, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(b.counters, 0, sizeof(int) * groups.size(), st);
+  for (const auto& g : groups)
+    if (e == cudaSuccess) e = launch_batch_group(g, st);
+  return e;
+}
+
+// Autotuning on the first launch outside a stream capture: every candidate geometry
+// writes the same outputs bit for bit, so each is launched and timed once on `st` (after
+// one warm-up launch) and the fastest is kept. The host waits for these launches once.
+cudaError_t tune_batch(nf_batch& b, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(st, &cs);
+  if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone) return e;  // keep the modelled choice
+  const size_t n = b.variants.size();
+  std::vector<cudaEvent_t> ev(n + 1, nullptr);
+  for (auto& x : ev)
+    if (e == cudaSuccess) e = cudaEventCreate(&x);
+  if (e == cudaSuccess) e = launch_groups(b, b.variants[0], st);  // warm-up
+  for (size_t v = 0; v < n && e == cudaSuccess; ++v) {
+    e = cudaEventRecord(ev[v], st);
+    if (e == cudaSuccess) e = launch_groups(b, b.variants[v], st);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ev[n], st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev[n]);
+  size_t best = 0;
+  float best_ms = -1.0f;
+  for (size_t v = 0; v < n && e == cudaSuccess; ++v) {
+    float ms = 0.0f;
+    e = cudaEventElapsedTime(&ms, ev[v], ev[v + 1]);
+    if (e == cudaSuccess && (best_ms < 0 || ms < best_ms)) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  for (auto& x : ev)
+    if (x) cudaEventDestroy(x);
+  if (e == cudaSuccess) {
+    b.groups = b.variants[best];
+    b.tuned = true;
+  }
+  return e;
+}
+}  // namespace
 
 nf_status nf_batch_launch(nf_batch* b, void* stream, char* err, size_t len) {
   if (!b) return fail(err, len, "null batch", NF_INVALID_ARGUMENT);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (b->groups.empty()) return NF_OK;
   if (const nf_status ms = check_models(b->plans, err, len)) return ms;
-  cudaError_t e = cudaMemsetAsync(b->counters, 0, sizeof(int) * b->groups.size(), st);
-  if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
-  for (const auto& g : b->groups)
-    if ((e = launch_batch_group(g, st)) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  cudaError_t e = cudaSuccess;
+  if (!b->tuned && (e = tune_batch(*b, st)) != cudaSuccess) return cuda_fail(err, len, e, "batch tuning failed");
+  if ((e = launch_groups(*b, b->groups, st)) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
   return NF_OK;
 }
 
@@ -1637,6 +1710,8 @@ nf_status nf_batch_graph_launch(nf_batch* b, void* stream, char* err, size_t len
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (const nf_status ms = check_models(b->plans, err, len)) return ms;
   cudaError_t e;
+  if (!b->tuned && !b->groups.empty() && (e = tune_batch(*b, st)) != cudaSuccess)
+    return cuda_fail(err, len, e, "batch tuning failed");
   if (!b->exec) {
     // Capture needs a non-legacy stream; capture on a private one and replay on `st`.
     if (!b->capture_stream && (e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)

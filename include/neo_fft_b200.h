@@ -249,9 +249,13 @@ void nf_host_batch_destroy(nf_host_batch* batch);
  * single-frame plans run the batched form; other DFTTest temporal modes and pshow
  * previews run one nf_plan_process_device call per frame over device-resident
  * sources. Three banks of device buffers hold consecutive ranges: the next two
- * ranges are fetched and computed while the current one is read out. plans[p] NULL copies plane p from the
- * source frame (a plane that is not processed). Kalman plans are served through
- * neo_fft::KalmanSeek instead. FFT3D sampled noise models (pfactor) are prepared from
+ * ranges are fetched and computed while the current one is read out. plans[p] NULL
+ * copies plane p from the source frame (a plane that is not processed). FFT3D bt=0
+ * (Kalman) plans follow the host layer's random-access rule (filter.hpp:152-250): frame
+ * 0 passes through, frame n continues the latest of up to four device-resident state
+ * snapshots not older than n - kalman_warmup - 1 (or the initial state), renders n and
+ * publishes its state (64 MiB budget, one snapshot always kept); request(n) then lists
+ * the frames a cold request reads. FFT3D sampled noise models (pfactor) are prepared from
  * the pattern frame on first use; DFTTest sampled models (nlocation) must be
  * published before the first request. Calls are serialised internally. */
 typedef struct nf_frame_server nf_frame_server;

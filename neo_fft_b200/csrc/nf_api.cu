@@ -2508,6 +2508,7 @@ PlanInfo plan_info(const nf_plan* p) {
             (!i.fft3d && t.temporal_ola && t.temporal_overlap == 0 && !t.center && t.temporal_size >= 2 &&
              t.temporal_size <= nfd::kMaxVolumeSlots));
   i.pframe = t.pframe;
+  i.kalman_warmup = t.kalman_warmup;
   return i;
 }
 }  // namespace nfi

@@ -27,7 +27,7 @@
 
 namespace {
 
-enum class Kind { Copy, Single, ClipFFT3D, ClipDFT, PerFrame };
+enum class Kind { Copy, Single, ClipFFT3D, ClipDFT, PerFrame, Kalman };
 
 struct Range {
   int n0 = 0, n1 = 0;  // outputs delivered: [n0, n1)
@@ -69,6 +69,28 @@ struct nf_frame_server {
     }
   };
 
+  // FFT3D bt=0: snapshots of the per-plane Kalman states with the host layer's policy
+  // (runtime/checkpoints.hpp:32-79): up to four, least recently used evicted first, a
+  // 64 MiB budget that always keeps one; the first snapshot of a frame wins.
+  struct Snapshot {
+    int frame = -1;
+    std::vector<nf_kalman_state*> planes;
+    size_t bytes = 0;
+    unsigned age = 0;
+    void release() {
+      for (nf_kalman_state*& k : planes)
+        if (k) {
+          nf_kalman_state_destroy(k);
+          k = nullptr;
+        }
+      frame = -1;
+      bytes = 0;
+    }
+  };
+  static constexpr size_t kSnapshotBudget = size_t(64) << 20;
+  Snapshot snaps[4];
+  int warmup = 8;
+
   std::vector<const nf_plan*> plans;  // per plane; nullptr: copied
   std::vector<nfi::PlanInfo> info;
   std::vector<size_t> pitch, offset;  // processed planes in a device frame slot
@@ -86,6 +108,9 @@ struct nf_frame_server {
   mutable std::mutex mu;
 
   ~nf_frame_server() {
+    for (auto& b : banks)
+      if (b.stream) cudaStreamSynchronize(b.stream);
+    for (auto& sn : snaps) sn.release();
     for (auto& b : banks) {
       if (b.stream) cudaStreamSynchronize(b.stream);
       b.drop_forms();
@@ -98,6 +123,10 @@ struct nf_frame_server {
   // Source frames of output n, in slot order, with the temporal targets of DFTTest tmode 1.
   std::vector<int> slots(int n, std::vector<int>* targets = nullptr) const {
     std::vector<int> s;
+    if (kind == Kind::Kalman) {  // at most the warm-up window before n (none at frame 0)
+      for (int f = n > warmup ? n - warmup : std::min(n, 1); f <= n; ++f) s.push_back(f);
+      return s;
+    }
     if (kind == Kind::Copy || kind == Kind::Single || preview) return {n};
     if (info_of_processed().fft3d) {
       if (n < left || N - 1 - n < right) return {n};
@@ -313,8 +342,156 @@ struct nf_frame_server {
     return nullptr;
   }
 
+  // ---- FFT3D bt=0 (Kalman) ------------------------------------------------------
+  void touch(Snapshot& sel) {
+    for (auto& sn : snaps)
+      if (sn.frame >= 0 && &sn != &sel && sn.age < sel.age) ++sn.age;
+    sel.age = 0;
+  }
+  // The latest snapshot of a frame in [earliest, frame] (Checkpoints::acquire).
+  Snapshot* acquire(int frame, int earliest) {
+    Snapshot* best = nullptr;
+    for (auto& sn : snaps)
+      if (sn.frame >= 0 && sn.frame >= earliest && sn.frame <= frame && (!best || sn.frame > best->frame)) best = &sn;
+    if (best) touch(*best);
+    return best;
+  }
+  // Checkpoints::publish: takes ownership of s's states.
+  void publish(Snapshot& s) {
+    if (s.frame < 1) {
+      s.release();
+      return;
+    }
+    const size_t need = s.bytes, limit = need > kSnapshotBudget ? need : kSnapshotBudget;
+    for (auto& sn : snaps)
+      if (sn.frame == s.frame) {  // the first snapshot of a frame wins
+        touch(sn);
+        s.release();
+        return;
+      }
+    auto used = [&] {
+      size_t u = 0;
+      for (auto& sn : snaps) u += sn.frame >= 0 ? sn.bytes : 0;
+      return u;
+    };
+    auto held = [&] {
+      int h = 0;
+      for (auto& sn : snaps) h += sn.frame >= 0 ? 1 : 0;
+      return h;
+    };
+    while (used() > limit - need || held() == 4) {
+      Snapshot* oldest = nullptr;
+      for (auto& sn : snaps)
+        if (sn.frame >= 0 && (!oldest || sn.age > oldest->age)) oldest = &sn;
+      oldest->release();
+    }
+    for (auto& sn : snaps)
+      if (sn.frame < 0) {
+        sn.frame = s.frame;
+        sn.planes = s.planes;
+        sn.bytes = s.bytes;
+        s.planes.assign(s.planes.size(), nullptr);
+        s.frame = -1;
+        sn.age = 4;
+        touch(sn);
+        return;
+      }
+  }
+
+  void upload(Bank& b, int frame) {
+    for (int p = 0; p < planes; ++p) {
+      if (!plans[size_t(p)]) continue;
+      const nf_const_plane v = fetch(frame, p);
+      const auto& in = info[size_t(p)];
+      check(cudaMemcpy2DAsync(slot(b.src, 0, p), pitch[size_t(p)], v.data, size_t(v.stride_bytes),
+                              size_t(in.width) * size_t(in.elem), size_t(in.height), cudaMemcpyDefault, b.stream),
+            "source copy failed");
+    }
+    ++fetched;
+  }
+
+  // The host layer's random-access rule for Kalman plans (filter.hpp:152-250): frame 0
+  // passes through; frame n continues the latest snapshot not older than n - warmup - 1
+  // (or the initial state from there) over the frames up to n, renders n from that state
+  // and publishes it.
+  void get_kalman(int n, const nf_plane* dsts) {
+    Bank& b = banks[0];
+    cudaStream_t st = b.stream;
+    prepare_patterns(st);
+    ensure(b, 1, 1);
+    b.valid = false;  // slot 0 holds Kalman sources, not a range
+    char err[512] = {0};
+    Snapshot cur;
+    const Snapshot* state = nullptr;
+    bool have_n = false;
+    try {
+      if (n > 0) {
+        const int earliest = n > warmup ? n - warmup - 1 : 0;
+        Snapshot* start = acquire(n, earliest);
+        const int replay_start = start ? start->frame : earliest;
+        if (replay_start < n) {
+          cur.planes.assign(size_t(planes), nullptr);
+          for (int p = 0; p < planes; ++p) {
+            if (!plans[size_t(p)]) continue;
+            if (start) check(nf_kalman_state_clone(start->planes[size_t(p)], &cur.planes[size_t(p)], st, err, sizeof err), err);
+            else check(nf_kalman_state_create(plans[size_t(p)], 0, &cur.planes[size_t(p)], err, sizeof err), err);
+            cur.bytes += nf_kalman_state_bytes(cur.planes[size_t(p)]);
+          }
+          for (int f = replay_start + 1; f <= n; ++f) {
+            upload(b, f);
+            for (int p = 0; p < planes; ++p)
+              if (plans[size_t(p)])
+                check(nf_kalman_advance_device(plans[size_t(p)], device_plane(b.src, 0, p), cur.planes[size_t(p)], st,
+                                               err, sizeof err),
+                      err);
+          }
+          cur.frame = n;
+          have_n = true;
+          state = &cur;
+        } else {
+          state = start;
+        }
+      }
+      if (state && !have_n) upload(b, n);
+      for (int p = 0; p < planes; ++p) {
+        const nf_plane& d = dsts[p];
+        if (!d.data) raise(NF_INVALID_ARGUMENT, "null destination plane");
+        if (plans[size_t(p)] && state) {
+          const auto& in = info[size_t(p)];
+          if (d.width != in.width || d.height != in.height) raise(NF_INVALID_ARGUMENT, "frame dimensions differ from plan");
+          check(nf_kalman_render_device(plans[size_t(p)], device_plane(b.src, 0, p), out_plane(b.out, 0, p),
+                                        state->planes[size_t(p)], st, err, sizeof err),
+                err);
+          check(cudaMemcpy2DAsync(d.data, size_t(d.stride_bytes), slot(b.out, 0, p), pitch[size_t(p)],
+                                  size_t(in.width) * size_t(in.elem), size_t(in.height), cudaMemcpyDefault, st),
+                "output copy failed");
+        } else {
+          // Frame 0 and planes that are not processed: the source plane (filter.hpp:216-218).
+          const nf_const_plane v = fetch(n, p);
+          if (d.width != v.width || d.height != v.height) raise(NF_INVALID_ARGUMENT, "frame dimensions differ from source");
+          check(cudaMemcpy2DAsync(d.data, size_t(d.stride_bytes), v.data, size_t(v.stride_bytes),
+                                  size_t(v.width) * size_t(elem_of(p)), size_t(v.height), cudaMemcpyDefault, st),
+                "plane copy failed");
+        }
+      }
+      check(cudaStreamSynchronize(st), "Kalman filtering failed");
+      for (const nf_plan* plan : plans)
+        if (plan) check(nf_plan_sync_status(plan, st, err, sizeof err), err);
+    } catch (...) {
+      cudaStreamSynchronize(st);
+      cur.release();
+      throw;
+    }
+    ++computed;
+    if (have_n) publish(cur);
+  }
+
   void get(int n, const nf_plane* dsts) {
     if (n < 0 || n >= N) raise(NF_INVALID_ARGUMENT, "frame outside clip");
+    if (kind == Kind::Kalman) {
+      get_kalman(n, dsts);
+      return;
+    }
     Bank* b = nullptr;
     if (kind != Kind::Copy) {
       prepare_patterns(banks[0].stream);
@@ -424,13 +601,12 @@ nf_status nf_frame_server_create(const nf_plan* const* plans, int planes, int nu
         continue;
       }
       const nfi::PlanInfo& i = s->info.back();
-      if (i.kalman) return fail(NF_INVALID_ARGUMENT, "Kalman plans are served through neo_fft::KalmanSeek");
       if (first) {
         ref = i;
         first = false;
       } else if (i.fft3d != ref.fft3d || i.temporal_size != ref.temporal_size || i.tmode1 != ref.tmode1 ||
                  i.temporal_overlap != ref.temporal_overlap || i.preview != ref.preview || i.single != ref.single ||
-                 i.clip != ref.clip) {
+                 i.clip != ref.clip || i.kalman != ref.kalman) {
         return fail(NF_INVALID_ARGUMENT, "planes of a frame server must share the temporal configuration");
       }
       const size_t pitch = ((size_t(i.width) * size_t(i.elem) + 255) / 256) * 256;
@@ -450,7 +626,11 @@ nf_status nf_frame_server_create(const nf_plan* const* plans, int planes, int nu
         s->left = s->T / 2;
         s->right = (s->T - 1) / 2;
       }
-      if (ref.preview) s->kind = Kind::PerFrame;
+      if (ref.kalman) {
+        s->kind = Kind::Kalman;
+        s->warmup = ref.kalman_warmup;
+        s->left = s->right = 0;
+      } else if (ref.preview) s->kind = Kind::PerFrame;
       else if (ref.clip) s->kind = ref.fft3d ? Kind::ClipFFT3D : Kind::ClipDFT;
       else if (ref.single && s->T == 1) s->kind = Kind::Single;
       else s->kind = Kind::PerFrame;

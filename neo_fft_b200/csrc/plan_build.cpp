@@ -577,6 +577,7 @@ PlanTables build_fft3d(int w, int h, nf_format f, const nf_fft3d_config& c) {
   p.px = c.px;
   p.py = c.py;
   p.pframe = c.pframe;
+  p.kalman_warmup = c.kalman_warmup;
   p.needs_pattern = p.sampled && p.denoise;
   if (p.preview || p.needs_pattern) {
     // plan.cpp:142-158: candidate grid and the scoring weights q/(q+cutoff^2) with

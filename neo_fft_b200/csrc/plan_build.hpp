@@ -108,6 +108,7 @@ struct PlanTables {
   float pfactor = 0;
   int px = 0, py = 0;                  // pattern block (0, 0: automatic search)
   int pframe = 0;                      // frame the pattern is sampled from (before clamping)
+  int kalman_warmup = 8;               // host layer's bounded Kalman warm-up on random access
   std::vector<float> sample_weights;   // [bh][bw/2+1] pattern scoring weights (plan.cpp:142-158)
   float sigma_eff = 0, norm = 0, beta = 1, kalman_r0 = 0, kalman_ratio2 = 0;
   Enhancement enhancement;

@@ -15,6 +15,7 @@ struct PlanInfo {
   bool single = false;  // accepted by nf_batch (single-frame filter)
   bool clip = false;    // accepted by nf_clip_batch
   int pframe = 0;       // FFT3D pattern frame (pfactor)
+  int kalman_warmup = 8;  // FFT3D bt=0: frames replayed at most before a random-access request
 };
 
 PlanInfo plan_info(const nf_plan* p);

@@ -119,8 +119,9 @@ def test_server_prepares_fft3d_pattern(cuda):
 def test_server_errors(cuda):
     fmt = SampleFormat(8)
     clip = [[plane(48, 64, 8, False, seed=(330, f, 0))] for f in range(4)]
-    with pytest.raises(ValueError, match="KalmanSeek"):
-        FrameServer([Plan(64, 48, fmt, FFT3DConfig(bw=16, bh=16, bt=0))], 4, lambda f, p: clip[f][p])
+    with pytest.raises(ValueError, match="temporal configuration"):
+        FrameServer([Plan(64, 48, fmt, FFT3DConfig(bw=16, bh=16, bt=0)),
+                     Plan(64, 48, fmt, FFT3DConfig(bw=16, bh=16, bt=1))], 4, lambda f, p: clip[f][p])
     with pytest.raises(ValueError, match="at least one processed plane"):
         FrameServer([None], 4, lambda f, p: clip[f][p])
     with pytest.raises(ValueError, match="tbsize"):
@@ -141,3 +142,29 @@ def test_server_errors(cuda):
     wrong = FrameServer([good], 4, lambda f, p: np.zeros((40, 64), np.uint8))
     with pytest.raises(ValueError, match="dimensions"):
         wrong.get(0)
+
+
+def test_server_kalman_random_access_matches_reference(ref, cuda):
+    """FFT3D bt=0 through the frame server: frame 0 passes through, other frames follow
+    the host layer's bounded warm-up with four checkpoints, so each output equals the
+    reference advanced from the frame its replay starts at (as in the KalmanSeek test)."""
+    w, h, warmup = 96, 64, 4
+    fmt = SampleFormat(32, True)
+    cfg = FFT3DConfig(bw=16, bh=16, bt=0, sigma=2.5, kratio=2.0, kalman_warmup=warmup)
+    host = [plane(h, w, 32, True, seed=(97, 0, f)) for f in range(24)]
+    chroma = [plane(h // 2, w // 2, 32, True, seed=(97, 1, f)) for f in range(24)]
+    server = FrameServer([Plan(w, h, fmt, cfg), None], 24,
+                         lambda f, p: host[f] if p == 0 else chroma[f], range_frames=4)
+    assert server.request(20) == [16, 17, 18, 19, 20] and server.request(0) == [0]
+    rp = ref.RefPlan(w, h, fmt, cfg)
+    first = {5: 1, 6: 1, 7: 1, 20: 16, 3: 1, 21: 16}
+    for n in (5, 6, 7, 20, 3, 21, 0):
+        got, passed = server.get(n)
+        assert np.array_equal(passed, chroma[n])
+        if n == 0:
+            assert np.array_equal(got, host[0])
+            continue
+        st = rp.kalman_state()
+        for f in range(first[n], n + 1):
+            rp.advance_kalman(host[f], st)
+        assert np.array_equal(got, rp.render_kalman(host[n], st)), n

@@ -186,6 +186,12 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** batc
 nf_status nf_batch_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
 /* Captures nf_batch_launch into a CUDA graph on first use, then replays the graph. */
 nf_status nf_batch_graph_launch(nf_batch* batch, void* stream, char* err, size_t err_len);
+/* Candidate strip geometries the batch holds (1..3; 0 = the tile-cost model's choice), the
+ * one in use (-1 until the first launch has tuned), and a fixed choice: selecting one skips
+ * the tuning and drops a captured graph. Every candidate writes the same outputs. */
+int nf_batch_geometry_count(const nf_batch* batch);
+int nf_batch_geometry(const nf_batch* batch);
+nf_status nf_batch_select_geometry(nf_batch* batch, int index, char* err, size_t err_len);
 void nf_batch_destroy(nf_batch* batch);
 
 /* Temporal clips in batched form: every output frame of every clip, with the host

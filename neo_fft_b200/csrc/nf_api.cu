@@ -107,6 +107,7 @@ struct nf_batch {
   std::vector<BatchGroup> groups;                 // the strip geometry in use (one of `variants`)
   std::vector<std::vector<BatchGroup>> variants;  // candidate geometries, timed on the first launch
   bool tuned = false;
+  int chosen = -1;  // index into `variants` once tuned or selected
   std::vector<const nf_plan*> plans;  // distinct plans (sampled noise models are checked per launch)
   int* counters = nullptr;  // one queue head per group
   cudaGraph_t graph = nullptr;
@@ -1643,6 +1644,7 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
     }
     b->groups = b->variants.empty() ? std::vector<BatchGroup>{} : b->variants.front();
     b->tuned = b->variants.size() <= 1;
+    if (b->tuned) b->chosen = 0;
     *out = b.release();
     return NF_OK;
   });
@@ -1689,6 +1691,7 @@ cudaError_t tune_batch(nf_batch& b, cudaStream_t st) {
   if (e == cudaSuccess) {
     b.groups = b.variants[best];
     b.tuned = true;
+    b.chosen = int(best);
   }
   return e;
 }
@@ -1731,6 +1734,23 @@ nf_status nf_batch_graph_launch(nf_batch* b, void* stream, char* err, size_t len
       return cuda_fail(err, len, e, "graph instantiation failed");
   }
   if ((e = cudaGraphLaunch(b->exec, st)) != cudaSuccess) return cuda_fail(err, len, e, "graph launch failed");
+  return NF_OK;
+}
+
+int nf_batch_geometry_count(const nf_batch* b) { return b ? int(b->variants.size()) : 0; }
+int nf_batch_geometry(const nf_batch* b) { return b ? b->chosen : -1; }
+
+nf_status nf_batch_select_geometry(nf_batch* b, int index, char* err, size_t len) {
+  if (!b) return fail(err, len, "null batch", NF_INVALID_ARGUMENT);
+  if (index < 0 || index >= int(b->variants.size()))
+    return fail(err, len, "geometry index outside the batch's candidates", NF_INVALID_ARGUMENT);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->groups = b->variants[size_t(index)];
+  b->chosen = index;
+  b->tuned = true;
   return NF_OK;
 }
 

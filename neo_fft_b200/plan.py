@@ -405,6 +405,21 @@ class Batch:
         fn = self._lib.nf_batch_graph_launch if graph else self._lib.nf_batch_launch
         C.raise_for(fn(self._h, ctypes.c_void_p(s), err, 512), err.value)
 
+    @property
+    def geometry_count(self) -> int:
+        """Candidate strip geometries (the first launch times them and keeps the fastest)."""
+        return int(self._lib.nf_batch_geometry_count(self._h))
+
+    @property
+    def geometry(self) -> int:
+        """Index of the geometry in use; -1 before the first launch has tuned."""
+        return int(self._lib.nf_batch_geometry(self._h))
+
+    def select_geometry(self, index: int) -> None:
+        """Fix the geometry (skips tuning; a captured graph is dropped)."""
+        err = ctypes.create_string_buffer(512)
+        C.raise_for(self._lib.nf_batch_select_geometry(self._h, int(index), err, 512), err.value)
+
     def sync_status(self) -> None:
         for p in {id(p): p for p in self._plans}.values():
             p.sync_status()

@@ -82,3 +82,37 @@ def test_multi_plane_launch_rejects_temporal_plans(cuda):
     a = cuda.zeros((48, 64), dtype=cuda.uint8, device="cuda")
     with pytest.raises(ValueError, match="single-frame plans"):
         p.process_planes([a], [cuda.empty_like(a)])
+
+
+def test_batch_every_geometry_equals_per_plane(cuda):
+    """Each candidate strip geometry of a batch (the first launch times them all) writes
+    the per-plane outputs bit for bit; the tuned choice is one of them."""
+    dft = DFTConfig(block=16, overlap=12, ftype=0, sigma=8.0)
+    f16 = SampleFormat(16)
+    sizes = [(640, 360), (320, 180), (320, 180)]
+    plans = {s: Plan(s[0], s[1], f16, dft) for s in set(sizes)}
+    items, refs = [], []
+    for i, (w, h) in enumerate(sizes * 2):
+        src = cuda.from_numpy(plane(h, w, 16, False, seed=(8, 0, i))).cuda()
+        items.append((plans[(w, h)], src, cuda.empty_like(src)))
+        r = cuda.empty_like(src)
+        plans[(w, h)].process_at([src], r)
+        refs.append(r)
+    b = Batch(items)
+    assert b.geometry == -1 and 1 <= b.geometry_count <= 3
+    b.launch()
+    cuda.cuda.synchronize()
+    assert 0 <= b.geometry < b.geometry_count
+    for (p, s, d), r in zip(items, refs):
+        assert cuda.equal(d, r)
+    for g in range(b.geometry_count):
+        b.select_geometry(g)
+        for graph in (False, True):
+            for (_, _, d) in items:
+                d.zero_()
+            b.launch(graph=graph)
+            cuda.cuda.synchronize()
+            for (p, s, d), r in zip(items, refs):
+                assert cuda.equal(d, r), (g, graph)
+    with pytest.raises(ValueError, match="geometry index"):
+        b.select_geometry(b.geometry_count)

@@ -119,7 +119,10 @@ nf_status nf_plan_process_device(const nf_plan* plan, const nf_const_plane* sour
                                  const int* targets, int ntargets, nf_plane dst, int frame, int plane,
                                  void* stream, char* err, size_t err_len);
 /* Same as above with host planes: copies in, launches, copies out and synchronises;
- * returns NF_NON_FINITE like the reference's frame evaluation. */
+ * returns NF_NON_FINITE like the reference's frame evaluation, for this call's planes
+ * only. A null stream means the calling thread's default stream, so host threads that
+ * each filter their own frames (the host layer's frame threads) overlap on the GPU.
+ * Page-locked host planes let the copies run asynchronously. */
 nf_status nf_plan_process_host(const nf_plan* plan, const nf_const_plane* sources, int nsources,
                                const int* targets, int ntargets, nf_plane dst, int frame, int plane,
                                void* stream, char* err, size_t err_len);

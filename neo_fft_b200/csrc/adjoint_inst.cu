@@ -12,7 +12,7 @@ namespace nfd {
   cudaError_t launch_adjoint_##BH##x##BW(const DevPlan& d, const AdjointShape& S, const AdjointBatch& b,          \
                                          size_t smem, cudaStream_t st) {                                         \
     auto k = dft_adjoint_kernel<BH, BW>;                                                                         \
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));             \
+    const cudaError_t e = set_smem_limit(k, smem);                                                              \
     if (e != cudaSuccess) return e;                                                                              \
     k<<<b.n * S.tiles_x * S.tiles_y, 256, smem, st>>>(d, S, b);                                                  \
     return cudaGetLastError();                                                                                   \

@@ -5,7 +5,37 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+
 namespace nfd {
+// Every kernel's dynamic shared-memory limit is set to the most it can take (the device's
+// opt-in maximum less the kernel's static shared memory), so any launch size up to it is
+// valid and host threads launching the same kernel with different sizes set the same
+// value (a per-launch value would race with another thread's launch).
+inline int dynamic_smem_max(const void* kernel) {
+  static std::mutex mu;
+  static std::map<const void*, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return 0;
+  const int m = optin - int(fa.sharedSizeBytes);
+  cache.emplace(kernel, m);
+  return m;
+}
+template <class K>
+cudaError_t set_smem_limit(K k, size_t smem) {
+  const int m = dynamic_smem_max(reinterpret_cast<const void*>(k));
+  if (m <= 0 || smem > size_t(m)) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  return e;
+}
 struct StripShape;
 struct PlaneJobs;
 struct BatchWork;

@@ -853,7 +853,8 @@ nf_status filter_device(const nf_plan& p, const nfd::DevPlan& d, const nf_const_
 
 // Filters into a float accumulator plane (stream-ordered scratch), then dithers it into dst.
 nf_status process_dithered(const nf_plan& p, const nf_const_plane* sources, int n, const int* targets, int nt,
-                           nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len) {
+                           nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len,
+                           int* err_word = nullptr) {
   nfb::require(frame >= 0 && plane >= 0, "invalid dither coordinates or mode");
   const int W = p.t.gx.length, H = p.t.gy.length;
   const size_t pitch = ((size_t(W) * sizeof(float) + 255) / 256) * 256;
@@ -864,12 +865,13 @@ nf_status process_dithered(const nf_plan& p, const nf_const_plane* sources, int 
   float* boundary = reinterpret_cast<float*>(static_cast<unsigned char*>(scratch) + pitch * size_t(H));
   nfd::DevPlan d = p.dev;
   d.raw_out = 1;
+  if (err_word) d.err = err_word;
   const nf_plane raw{acc, W, H, ptrdiff_t(pitch)};
   const nf_status s = filter_device(p, d, sources, n, targets, nt, raw, st, err, len);
   if (s == NF_OK) {
     nfd::dither_kernel<<<1, std::min(nfd::kDitherRows, H), 0, st>>>(
         acc, (long long)(pitch / sizeof(float)), static_cast<unsigned char*>(dst.data), (long long)dst.stride_bytes, W,
-        H, p.t.dither, unsigned(p.t.dither_seed), unsigned(frame), unsigned(plane), boundary, p.err);
+        H, p.t.dither, unsigned(p.t.dither_seed), unsigned(frame), unsigned(plane), boundary, d.err);
     e = cudaGetLastError();
   }
   cudaFreeAsync(scratch, st);
@@ -878,13 +880,19 @@ nf_status process_dithered(const nf_plan& p, const nf_const_plane* sources, int 
   return NF_OK;
 }
 
+// err_word: a per-call error flag in place of the plan's (host-memory calls from several
+// threads then report their own non-finite data).
 nf_status process_device(const nf_plan& p, const nf_const_plane* sources, int n, const int* targets, int nt,
-                          nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len) {
+                          nf_plane dst, int frame, int plane, cudaStream_t st, char* err, size_t len,
+                          int* err_word = nullptr) {
   if (dithers(p.t)) {
     validate_call(p, sources, n, targets, nt, dst);
-    return process_dithered(p, sources, n, targets, nt, dst, frame, plane, st, err, len);
+    return process_dithered(p, sources, n, targets, nt, dst, frame, plane, st, err, len, err_word);
   }
-  return filter_device(p, p.dev, sources, n, targets, nt, dst, st, err, len);
+  if (!err_word) return filter_device(p, p.dev, sources, n, targets, nt, dst, st, err, len);
+  nfd::DevPlan d = p.dev;
+  d.err = err_word;
+  return filter_device(p, d, sources, n, targets, nt, dst, st, err, len);
 }
 
 cudaError_t launch_temporal_shape(int bh, int bw, int storage, int slice, const nfd::BatchWork& w, int ctas,
@@ -1261,7 +1269,7 @@ nf_status nf_plan_process_host(const nf_plan* p, const nf_const_plane* sources, 
     nfb::require(p != nullptr, "null plan");
     const Checked c = validate_call(*p, sources, nsources, targets, ntargets, dst);
     (void)c;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamPerThread;
     const size_t elem = size_t(storage_of(p->t.format));
     const size_t pitch = ((size_t(p->t.gx.length) * elem + 255) / 256) * 256;
     const size_t plane_bytes = pitch * size_t(p->t.gy.length);
@@ -1279,34 +1287,48 @@ nf_status nf_plan_process_host(const nf_plan* p, const nf_const_plane* sources, 
         uniq.push_back(j);
       }
     }
-    const size_t need = plane_bytes * (uniq.size() + 1);
-    std::lock_guard<std::mutex> lock(p->staging_mu);
-    cudaError_t e;
-    if (p->staging_bytes < need) {
-      if (p->staging) cudaFree(p->staging);
-      p->staging = nullptr;
-      p->staging_bytes = 0;
-      if ((e = cudaMalloc(&p->staging, need)) != cudaSuccess) return cuda_fail(err, err_len, e, "device allocation failed");
-      p->staging_bytes = need;
-    }
-    auto* base = static_cast<unsigned char*>(p->staging);
+    // Per-call device staging from the library's pool on the caller's stream (the
+    // calling thread's default stream when none is given), so calls from several host
+    // threads overlap their copies and kernels; a per-call error flag keeps each call's
+    // non-finite report its own.
+    const size_t need = plane_bytes * (uniq.size() + 1) + 256;
+    void* scratch = nullptr;
+    cudaError_t e = scratch_alloc(&scratch, need, st);
+    if (e != cudaSuccess) return cuda_fail(err, err_len, e, "device allocation failed");
+    auto* base = static_cast<unsigned char*>(scratch);
+    int* err_word = reinterpret_cast<int*>(base + plane_bytes * (uniq.size() + 1));
+    auto finish = [&](nf_status s) {
+      cudaFreeAsync(scratch, st);
+      return s;
+    };
+    if ((e = cudaMemsetAsync(err_word, 0, sizeof(int), st)) != cudaSuccess)
+      return finish(cuda_fail(err, err_len, e, "device memset failed"));
     std::vector<nf_const_plane> dsrc(static_cast<size_t>(nsources));
     for (size_t u = 0; u < uniq.size(); ++u) {
       const auto& s = sources[uniq[u]];
       e = cudaMemcpy2DAsync(base + u * plane_bytes, pitch, s.data, size_t(s.stride_bytes), size_t(s.width) * elem,
                             size_t(s.height), cudaMemcpyHostToDevice, st);
-      if (e != cudaSuccess) return cuda_fail(err, err_len, e, "host to device copy failed");
+      if (e != cudaSuccess) return finish(cuda_fail(err, err_len, e, "host to device copy failed"));
     }
     for (int j = 0; j < nsources; ++j)
       dsrc[size_t(j)] = {base + size_t(slot_of[size_t(j)]) * plane_bytes, sources[j].width, sources[j].height,
                          ptrdiff_t(pitch)};
     nf_plane ddst{base + uniq.size() * plane_bytes, dst.width, dst.height, ptrdiff_t(pitch)};
-    nf_status s = process_device(*p, dsrc.data(), nsources, targets, ntargets, ddst, frame, plane, st, err, err_len);
-    if (s != NF_OK) return s;
+    nf_status s = process_device(*p, dsrc.data(), nsources, targets, ntargets, ddst, frame, plane, st, err, err_len,
+                                 err_word);
+    if (s != NF_OK) {
+      cudaStreamSynchronize(st);  // no copy from the caller's host memory stays in flight
+      return finish(s);
+    }
     e = cudaMemcpy2DAsync(dst.data, size_t(dst.stride_bytes), ddst.data, pitch, size_t(dst.width) * elem,
                           size_t(dst.height), cudaMemcpyDeviceToHost, st);
+    int flag = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, err_word, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(scratch, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(err, err_len, e, "device to host copy failed");
-    return read_error_word(*p, st, err, err_len);
+    if (flag) return fail(err, err_len, "non-finite sample or intermediate", NF_NON_FINITE);
+    return NF_OK;
   });
 }
 

@@ -12,9 +12,7 @@ namespace nfd {
 namespace {
 template <class K>
 cudaError_t prepare(K k, size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  return e;
+  return set_smem_limit(k, smem);
 }
 template <int ST, int ALGO>
 cudaError_t launch_one(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem, const PlaneJobs& job,

@@ -11,9 +11,7 @@ namespace nfd {
 namespace {
 template <class K>
 cudaError_t prepare(K k, size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  return e;
+  return set_smem_limit(k, smem);
 }
 template <int ST>
 cudaError_t spectra(const SpectraWork& w, int items, size_t smem, cudaStream_t st) {

@@ -13,8 +13,7 @@ template <int ST>
 cudaError_t launch_one(const DevPlan& d, const VolumeShape& S, dim3 grid, size_t smem, const VolumeSources& v,
                        void* dst, ptrdiff_t ds, cudaStream_t st) {
   auto k = volume_tile_kernel<NF_BH, NF_BW, ST>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  const cudaError_t e = set_smem_limit(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, S.threads, smem, st>>>(d, S, v, static_cast<unsigned char*>(dst), ds);
   return cudaGetLastError();

@@ -534,29 +534,40 @@ std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_p
     if (nfd::strip_smem_bytes(d.bh, d.bw, c) > budget) continue;
     double cost;
     if (plain_planes > 0) {
+      // Segment count: the shortest simulated schedule of the grid over the resident
+      // CTAs (taller segments recompute fewer overlapping block rows; more segments fill
+      // more SMs on small planes).
       const int strips = (d.gx.length + c.tw - 1) / c.tw;
-      // At most one wave (a partial second wave doubles the time); segments shorter
-      // than 3 block heights recompute too many vertical neighbours.
-      const int target = std::max(1, slots / plain_planes);
-      const int segs = std::max(1, std::min(target / strips, d.gy.length / std::max(1, 3 * d.bh)));
-      c.th = std::max(1, (d.gy.length + segs - 1) / segs);
-      costs.clear();
-      for (int z = 0; z < plain_planes; ++z)
-        for (int y0 = 0; y0 < d.gy.length; y0 += c.th)
-          for (int x0 = 0; x0 < d.gx.length; x0 += c.tw)
-            costs.push_back(tile_cost(d, std::min(c.tw, d.gx.length - x0), std::min(c.th, d.gy.length - y0), work));
-      std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
-      double span = 0;
-      for (double t : costs) {
-        double t0 = 0;
-        if (int(free_at.size()) >= slots) {
-          t0 = free_at.top();
-          free_at.pop();
+      const int max_segs = std::max(1, std::min(d.gy.length / std::max(8, d.gy.step),
+                                                (4 * slots + strips * plain_planes - 1) / (strips * plain_planes)));
+      double best_span = -1.0;
+      int best_th = d.gy.length;
+      for (int segs = 1; segs <= max_segs; ++segs) {
+        const int th = std::max(1, (d.gy.length + segs - 1) / segs);
+        if (segs > 1 && th == (d.gy.length + segs - 2) / (segs - 1)) continue;  // same height as segs - 1
+        costs.clear();
+        for (int z = 0; z < plain_planes; ++z)
+          for (int y0 = 0; y0 < d.gy.length; y0 += th)
+            for (int x0 = 0; x0 < d.gx.length; x0 += c.tw)
+              costs.push_back(tile_cost(d, std::min(c.tw, d.gx.length - x0), std::min(th, d.gy.length - y0), work));
+        std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+        double span = 0;
+        for (double t : costs) {
+          double t0 = 0;
+          if (int(free_at.size()) >= slots) {
+            t0 = free_at.top();
+            free_at.pop();
+          }
+          free_at.push(t0 + t);
+          span = std::max(span, t0 + t);
         }
-        free_at.push(t0 + t);
-        span = std::max(span, t0 + t);
+        if (best_span < 0 || span < best_span) {
+          best_span = span;
+          best_th = th;
+        }
       }
-      cost = span;
+      c.th = best_th;
+      cost = best_span;
     } else {
       cost = tile_cost(d, c.tw, 0, work) / double(c.tw);
     }

@@ -42,7 +42,7 @@ __host__ __device__ inline size_t adjoint_smem_bytes(int bh, int bw, const Adjoi
   const size_t spec_cf = (size_t(s.nbx_max) * bh * K + 1) & ~size_t(1);
   return sizeof(float) * (size_t(s.tab_floats) + 2 * size_t(bh) * s.ring_pitch + 2 * spec_cf * 2 +
                           size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max) +
-                          size_t(s.nbx_max) * bins + bins + 2 * size_t(s.nbx_max) * K);
+                          size_t(s.nbx_max) * bins + bins + 2 * size_t(s.nbx_max) * K + size_t(s.tw));
 }
 
 // Per-bin backward of spectral_bin for ftype 0 (Wiener, any exponent), 1 (hard
@@ -127,6 +127,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
   float* da_blk = dc + 2 * size_t(NB);
   float* da_tile = da_blk + size_t(NB) * bins;
   float* dg_part = da_tile + bins;  // [NB][K]
+  int* colmap = reinterpret_cast<int*>(dg_part + 2 * size_t(NB) * K);  // [tw], as in strip_tile
 
   // tables
   int off = 0;
@@ -147,6 +148,12 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
   }
   for (int i = tid; i < BH * S.tw; i += nthr) acc[i] = 0.0f;
   for (int i = tid; i < bins; i += nthr) da_tile[i] = 0.0f;
+  for (int xx = tid; xx < tw; xx += nthr) {  // first overlapping block, count, offset in it
+    const int X = X0 + xx;
+    const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
+    const int nblk = max(0, b1 - b0 + 1);
+    colmap[xx] = (b0 - bx_lo) | (nblk << 10) | ((nblk > 0 ? X - b0 * gx.step : 0) << 20);
+  }
   __syncthreads();
   const DevSpectral& filt = s_filt;
   const float grid0 = grid ? grid[0].r : 1.0f;
@@ -159,8 +166,8 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     // ---- stage source rows (decoded) and upstream-gradient rows -------------
     const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
     const int nrows = oy + BH - r0;
-    for (int i = tid; i < nrows * win; i += nthr) {
-      const int rr = i / win, xx = i - rr * win;
+    for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
+      const int rr = c.y, xx = c.x;
       const int cy = r0 + rr, cx = cx0 + xx;
       const float* srow = reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(J.src) +
                                                          ptrdiff_t(reflect_axis(cy, gy)) * J.src_stride);
@@ -174,9 +181,8 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     }
     __syncthreads();
     // ---- rows: forward spectrum rows and gradient rows ----------------------
-    for (int task = tid; task < 2 * nbx * BH; task += nthr) {
-      const int which = task / (nbx * BH), t2 = task - which * nbx * BH;
-      const int y = t2 / nbx, b = t2 - y * nbx;
+    for (Cursor2 c(tid, nthr, nbx); c.y < 2 * BH; c.next()) {
+      const int which = c.y >= BH ? 1 : 0, y = c.y - which * BH, b = c.x;
       const float* in = (which ? gring : ring) + size_t((oy + y) % BH) * S.ring_pitch + b * gx.step;
       float row[CAPW];
 #pragma unroll UW
@@ -188,10 +194,10 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     // ---- columns: forward transforms, DC exchange, per-bin adjoint -----------
     // (k = 0 tasks come first, so every block's DC is exchanged in the first pass)
     const int ncol = nbx * K;
-    for (int base = 0; base < ncol; base += nthr) {
-      const int task = base + tid;
-      const bool active = task < ncol;
-      const int k = active ? task / nbx : 0, b = active ? task - k * nbx : 0;
+    Cursor2 cb(tid, nthr, nbx);
+    for (int base = 0; base < ncol; base += nthr, cb.next()) {
+      const bool active = cb.y < K;  // task < ncol
+      const int k = active ? cb.y : 0, b = active ? cb.x : 0;
       cf x[CAPH], gcol[CAPH];
       cf* sp = spec + size_t(k) * NB + b;
       cf* gp = gspec + size_t(k) * NB + b;
@@ -225,8 +231,8 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     }
     __syncthreads();
     // ---- columns: template-ratio gradient, adjoint of r2c, inverse -----------
-    for (int task = tid; task < ncol; task += nthr) {
-      const int k = task / nbx, b = task - k * nbx;
+    for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
+      const int k = c.y, b = c.x;
       cf x[CAPH];
       cf* sp = spec + size_t(k) * NB + b;
 #pragma unroll UH
@@ -255,8 +261,8 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
       da_tile[i] = s;
     }
     // ---- rows: unnormalised inverse, analysis-window weighting ---------------
-    for (int task = tid; task < nbx * BH; task += nthr) {
-      const int y = task / nbx, b = task - y * nbx;
+    for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
+      const int y = c.y, b = c.x;
       float row[CAPW];
       nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, 1.0f, row, P.tww, codelet, NB);
       float* o = ob + (size_t(y) * NB + b) * OBW;
@@ -267,20 +273,21 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     __syncthreads();
     // ---- ordered gather into the cover-gradient ring; retire rows -------------
     const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
-    for (int i = tid; yhi > ylo && i < (yhi - ylo) * tw; i += nthr) {
-      const int yy = i / tw, xx = i - yy * tw;
-      const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
+    for (Cursor2 c(tid, nthr, tw); c.y < yhi - ylo; c.next()) {
+      const int yy = c.y, xx = c.x;
+      const int Y = ylo + yy, ly = Y - oy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;
-      const float* orow = ob + size_t(ly) * NB * OBW;
-      const int b0 = max(bx_lo, floor_div_i(X - BW, gx.step) + 1), b1 = min(bx_hi, floor_div_i(X, gx.step));
+      // blocks b0.. in ascending order; block b0+j holds column X at offset xo - j*step
+      const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
+      const float* ov = ob + size_t(ly) * NB * OBW + size_t(cm & 1023) * OBW + (cm >> 20);
       float sacc = *a;
-      for (int bb = b0; bb <= b1; ++bb) sacc += orow[size_t(bb - bx_lo) * OBW + (X - bb * gx.step)];
+      for (int j = 0; j < nblk; ++j, ov += OBW - gx.step) sacc += *ov;
       *a = sacc;
     }
     __syncthreads();
     const int rlo = max(oy, Y0), rhi = min(by == by_hi ? Y0 + th : oy + gy.step, Y0 + th);
-    for (int i = tid; rhi > rlo && i < (rhi - rlo) * tw; i += nthr) {
-      const int yy = i / tw, xx = i - yy * tw;
+    for (Cursor2 c(tid, nthr, tw); c.y < rhi - rlo; c.next()) {
+      const int yy = c.y, xx = c.x;
       const int Y = rlo + yy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;
       J.dcov[size_t(Y) * gx.cover + X0 + xx] = *a;

@@ -83,17 +83,17 @@ __global__ void __launch_bounds__(256) spectra_batch_kernel(SpectraWork W) {
   for (int i = tid; i < BH; i += nthr) wya[i] = P.wya[i];
   bool bad = false;
   // stage the block row's samples (decoded, reflected) with coalesced loads
-  for (int i = tid; i < BH * win; i += nthr) {
-    const int y = i / win, xx = i - y * win;
+  for (Cursor2 c(tid, nthr, win); c.y < BH; c.next()) {
+    const int y = c.y, xx = c.x;
     const unsigned char* srow = sJ.src + ptrdiff_t(reflect_axis(oy + y, gy)) * sJ.src_stride;
     const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
     const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
-    if (!isfin(v)) bad = true;
+    if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
     ring[size_t(y) * pitch + xx] = v;
   }
   __syncthreads();
-  for (int task = tid; task < nb * BH; task += nthr) {
-    const int y = task / nb, b = task - y * nb;
+  for (Cursor2 c(tid, nthr, nb); c.y < BH; c.next()) {
+    const int y = c.y, b = c.x;
     const float* in = ring + size_t(y) * pitch + b * gx.step;
     float row[CAPW];
 #pragma unroll UW
@@ -104,8 +104,8 @@ __global__ void __launch_bounds__(256) spectra_batch_kernel(SpectraWork W) {
   __syncthreads();
   const size_t cnt = size_t(gx.count);
   cf* out = sJ.out + size_t(by) * P.bins * cnt + bx0;
-  for (int task = tid; task < nb * K; task += nthr) {
-    const int k = task / nb, b = task - k * nb;
+  for (Cursor2 c(tid, nthr, nb); c.y < K; c.next()) {
+    const int k = c.y, b = c.x;
     cf col[CAPH];
     const cf* sp = spec + size_t(k) * nbc + b;
 #pragma unroll UH
@@ -160,8 +160,8 @@ __device__ __forceinline__ void volume_time(const DevPlan& P, const VolumeSpectr
   const int T = TC > 0 ? TC : T_rt;
   constexpr int CAP = TC > 0 ? TC : kMaxVolumeSlots;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  for (int task = tid; task < bins * nb; task += nthr) {
-    const int kk = task / nb, b = task - kk * nb;
+  for (Cursor2 c(tid, nthr, nb); c.y < bins; c.next()) {
+    const int kk = c.y, b = c.x;
     cf* bp = spec + size_t(kk) * nbc + b;
     cf line[CAP];
 #pragma unroll
@@ -175,8 +175,8 @@ __device__ __forceinline__ void volume_time(const DevPlan& P, const VolumeSpectr
   }
   __syncthreads();
   const size_t cnt = size_t(P.gx.count);
-  for (int task = tid; task < bins * nb; task += nthr) {
-    const int kk = task / nb, b = task - kk * nb;
+  for (Cursor2 c(tid, nthr, nb); c.y < bins; c.next()) {
+    const int kk = c.y, b = c.x;
     const cf* bp = spec + size_t(kk) * nbc + b;
     const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
                         ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
@@ -244,17 +244,17 @@ __global__ void __launch_bounds__(256) volume_spectra_batch_kernel(VolumeSpectra
   bool bad = false;
   for (int z = 0; z < T; ++z) {
     __syncthreads();
-    for (int i = tid; i < BH * win; i += nthr) {
-      const int y = i / win, xx = i - y * win;
+    for (Cursor2 c(tid, nthr, win); c.y < BH; c.next()) {
+      const int y = c.y, xx = c.x;
       const unsigned char* srow = J.src[z] + ptrdiff_t(reflect_axis(oy + y, gy)) * J.src_stride[z];
       const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
       const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
-      if (!isfin(v)) bad = true;
+      if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
       ring[size_t(y) * pitch + xx] = v;
     }
     __syncthreads();
-    for (int task = tid; task < nb * BH; task += nthr) {
-      const int y = task / nb, b = task - y * nb;
+    for (Cursor2 c(tid, nthr, nb); c.y < BH; c.next()) {
+      const int y = c.y, b = c.x;
       const float* in = ring + size_t(y) * pitch + b * gx.step;
       float row[CAPW];
 #pragma unroll UW
@@ -264,8 +264,8 @@ __global__ void __launch_bounds__(256) volume_spectra_batch_kernel(VolumeSpectra
     }
   }
   __syncthreads();
-  for (int task = tid; task < T * nb * K; task += nthr) {
-    const int z = task / (nb * K), r = task - z * nb * K, k = r / nb, b = r - k * nb;
+  for (Cursor2 c(tid, nthr, nb); c.y < T * K; c.next()) {
+    const int z = c.y / K, k = c.y - z * K, b = c.x;  // rows of (slot, bin); K is small
     cf col[CAPH];
     cf* sp = spec + size_t(z) * slot + size_t(k) * nbc + b;
 #pragma unroll UH

@@ -168,3 +168,20 @@ def test_server_kalman_random_access_matches_reference(ref, cuda):
         for f in range(first[n], n + 1):
             rp.advance_kalman(host[f], st)
         assert np.array_equal(got, rp.render_kalman(host[n], st)), n
+
+
+def test_server_dithered_output_uses_frame_and_plane(cuda):
+    """8-bit DFTTest with dither: the server's per-frame path passes each output's frame
+    and plane number, so the dither hash matches a direct call with the same coordinates."""
+    fmt = SampleFormat(8)
+    cfg = DFTConfig(block=16, overlap=8, sigma=4.0, dither=2, dither_seed=7)
+    w, h, N = 96, 64, 5
+    clip = [[plane(h, w, 8, False, seed=(340, f, p)) for p in range(2)] for f in range(N)]
+    plans = [Plan(w, h, fmt, cfg), Plan(w, h, fmt, cfg)]
+    server = FrameServer(plans, N, lambda f, p: clip[f][p], range_frames=2)
+    for n in (3, 0, 4, 1):
+        got = server.get(n)
+        for p in range(2):
+            exp = np.empty_like(clip[n][p])
+            plans[p].process_at([clip[n][p]], exp, frame=n, plane=p)
+            assert np.array_equal(got[p], exp), (n, p)

@@ -85,3 +85,45 @@ def test_random_configuration_matches_reference(ref, cuda, seed):
     assert exp_err == got_err, (cfg, exp_err, got_err)
     if exp is not None:
         assert np.array_equal(got, exp), (cfg, fmt, w, h)
+
+
+def _per_frame(plan, cfg, clip, n):
+    """One per-frame call with the host layer's frame selection."""
+    from neo_fft_b200.temporal import centred_slots, fft3d_slots
+    N = len(clip)
+    if isinstance(cfg, FFT3DConfig):
+        return plan.process([clip[f] for f in fft3d_slots(n, N, plan.temporal_size)])
+    T = plan.temporal_size
+    if T == 1:
+        return plan.process([clip[n]])
+    if cfg.temporal_mode == 1:
+        blocks = temporal_blocks(n, N, T, cfg.temporal_overlap)
+        return plan.process_at([clip[f] for b in blocks for f in b["slots"]], np.empty_like(clip[n]),
+                               targets=[b["target"] for b in blocks])
+    return plan.process([clip[f] for f in centred_slots(n, N, T)])
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_configuration_through_frame_server(cuda, seed):
+    """The frame server picks the batched, clip or per-frame form from the plan; every
+    output frame of a random valid configuration equals the per-frame call."""
+    from neo_fft_b200.plan import FrameServer
+    rng = np.random.default_rng([502, seed])
+    fmt = FORMATS[int(rng.integers(0, len(FORMATS)))]
+    for _ in range(20):  # draw until the configuration is valid
+        cfg = _dft(rng) if rng.random() < 0.6 else _fft3d(rng)
+        w, h = int(rng.integers(40, 160)), int(rng.integers(40, 120))
+        try:
+            p = Plan(w, h, fmt, cfg)
+            break
+        except ValueError:
+            continue
+    else:
+        pytest.skip("no valid draw")
+    N = 7
+    if p.temporal_size > N:
+        pytest.skip("temporal size above the clip")
+    clip = [plane(h, w, fmt.bits, fmt.floating, seed=(503, seed, f)) for f in range(N)]
+    server = FrameServer([p], N, lambda f, _p: clip[f], range_frames=int(rng.integers(1, 5)))
+    for n in rng.permutation(N):
+        assert np.array_equal(server.get(int(n))[0], _per_frame(p, cfg, clip, int(n))), (cfg, fmt, w, h, n)

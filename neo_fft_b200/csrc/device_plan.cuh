@@ -102,6 +102,8 @@ NF_HD float enhancement_gain(float q, int k, const DevSpectral& e) {
 // One bin of spectral_prevalidated: residual against the scaled template, gain
 // by type, optional enhancement, restore the template. Returns the new bin and
 // flags non-finite intermediates through `bad`.
+// FT >= 0 fixes the filter type at compile time (a DFTTest ftype: no enhancement).
+template <int FT = -3>
 NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectral& p, bool& bad) {
   const float a = p.primary ? p.primary[k] : p.a;
   const float mr = grid ? fmul(scale, grid[k].r) : 0.0f;
@@ -109,7 +111,7 @@ NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectra
   const float re = fsub(x.r, mr), im = fsub(x.i, mi);
   const float power = fadd(fmul(re, re), fmul(im, im));
   float gain = 0.0f;
-  switch (p.type) {
+  switch (FT >= -2 ? FT : p.type) {
     case -2:
       gain = 1.0f;
       break;
@@ -143,7 +145,7 @@ NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectra
       break;
     }
   }
-  if (p.enh) gain = fmul(gain, enhancement_gain(fadd(power, 1e-15f), k, p));
+  if (FT < 0 && p.enh) gain = fmul(gain, enhancement_gain(fadd(power, 1e-15f), k, p));
   const cf out = {fadd(fmul(gain, re), mr), fadd(fmul(gain, im), mi)};
   // The reference checks mr, mi, re, im, power, gain and both outputs. A non-finite mr,
   // re or gain always makes out.r non-finite (inf or NaN propagate through the product

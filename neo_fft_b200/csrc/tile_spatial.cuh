@@ -427,7 +427,11 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       __syncthreads();
       if (active) {
         const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
-        if (!fft3d || P.fft3d_mode != kEnhanceOnly) {
+        if (ALGO == 1 && filt.type == 0) {  // DFTTest ftype 0: the filter type fixed at compile time
+#pragma unroll UH
+          for (int y = 0; y < CAPH; ++y)
+            if (y < BH) col[y] = spectral_bin<0>(col[y], grid, y * K + k, g, filt, bad);
+        } else if (!fft3d || P.fft3d_mode != kEnhanceOnly) {
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
             if (y < BH) col[y] = spectral_bin(col[y], grid, y * K + k, g, filt, bad);

@@ -23,6 +23,7 @@
 // two strips are computed by both (the horizontal halo); vertically the strip is
 // tall, so little work is repeated.
 #pragma once
+#include <type_traits>
 #include "device_plan.cuh"
 
 namespace nfd {
@@ -427,14 +428,25 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       __syncthreads();
       if (active) {
         const float g = grid ? fdiv(fmul(P.mean_scale, dc[b]), grid0) : 0.0f;
-        if (ALGO == 1 && filt.type == 0) {  // DFTTest ftype 0: the filter type fixed at compile time
+        // The filter type is fixed at compile time per branch: one uniform branch per
+        // column instead of a switch per bin.
+        auto filter_column = [&](auto ft) {
+          constexpr int FT = decltype(ft)::value;
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = spectral_bin<0>(col[y], grid, y * K + k, g, filt, bad);
+            if (y < BH) col[y] = spectral_bin<FT>(col[y], grid, y * K + k, g, filt, bad);
+        };
+        if (ALGO == 1) {
+          switch (filt.type) {
+            case 0: filter_column(std::integral_constant<int, 0>{}); break;
+            case 1: filter_column(std::integral_constant<int, 1>{}); break;
+            case 2: filter_column(std::integral_constant<int, 2>{}); break;
+            case 3: filter_column(std::integral_constant<int, 3>{}); break;
+            default: filter_column(std::integral_constant<int, 4>{}); break;
+          }
         } else if (!fft3d || P.fft3d_mode != kEnhanceOnly) {
-#pragma unroll UH
-          for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = spectral_bin(col[y], grid, y * K + k, g, filt, bad);
+          if (filt.type == -1) filter_column(std::integral_constant<int, -1>{});
+          else filter_column(std::integral_constant<int, -3>{});
         }
         if (fft3d && P.fft3d_mode == kWienerThenEnh && k == 0) dc[NB + b] = col[0].r;
       }

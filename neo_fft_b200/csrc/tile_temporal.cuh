@@ -175,19 +175,31 @@ __device__ __forceinline__ void volume_time(const DevPlan& P, const VolumeSpectr
   }
   __syncthreads();
   const size_t cnt = size_t(P.gx.count);
-  for (Cursor2 c(tid, nthr, nb); c.y < bins; c.next()) {
-    const int kk = c.y, b = c.x;
-    const cf* bp = spec + size_t(kk) * nbc + b;
-    const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
-                        ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
-    cf line[CAP];
+  // The ftype is fixed at compile time per branch (one uniform branch per launch item
+  // instead of a switch per element).
+  auto filter_lines = [&](auto ft) {
+    constexpr int FT = decltype(ft)::value;
+    for (Cursor2 c(tid, nthr, nb); c.y < bins; c.next()) {
+      const int kk = c.y, b = c.x;
+      const cf* bp = spec + size_t(kk) * nbc + b;
+      const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
+                          ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
+      cf line[CAP];
 #pragma unroll
-    for (int z = 0; z < CAP; ++z)
-      if (z < T) line[z] = spectral_bin(bp[size_t(z) * slot], P.grid, z * bins + kk, g, P.filt, bad);
-    nf::fft_project<false, TC, 16>(line, T, P.twt);
+      for (int z = 0; z < CAP; ++z)
+        if (z < T) line[z] = spectral_bin<FT>(bp[size_t(z) * slot], P.grid, z * bins + kk, g, P.filt, bad);
+      nf::fft_project<false, TC, 16>(line, T, P.twt);
 #pragma unroll
-    for (int z = 0; z < CAP; ++z)
-      if (z < T) J.out[z][row_base + size_t(kk) * cnt + b] = line[z];
+      for (int z = 0; z < CAP; ++z)
+        if (z < T) J.out[z][row_base + size_t(kk) * cnt + b] = line[z];
+    }
+  };
+  switch (P.filt.type) {
+    case 0: filter_lines(std::integral_constant<int, 0>{}); break;
+    case 1: filter_lines(std::integral_constant<int, 1>{}); break;
+    case 2: filter_lines(std::integral_constant<int, 2>{}); break;
+    case 3: filter_lines(std::integral_constant<int, 3>{}); break;
+    default: filter_lines(std::integral_constant<int, 4>{}); break;
   }
 }
 

@@ -387,7 +387,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
           const int kk = c.y, b = c.x;
           const float g2 = grid ? fdiv(fmul(P.mean_scale, dc[NB + b]), grid0) : 0.0f;
           cf* sp = spec + size_t(kk) * NB + b;
-          *sp = spectral_bin(*sp, grid, kk, g2, enh, bad);
+          *sp = spectral_bin<-2>(*sp, grid, kk, g2, enh, bad);  // enh is always type -2
         }
         __syncthreads();
       }
@@ -459,7 +459,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
           const float g2 = grid ? fdiv(fmul(P.mean_scale, dcv), grid0) : 0.0f;
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = spectral_bin(col[y], grid, y * K + k, g2, enh, bad);
+            if (y < BH) col[y] = spectral_bin<-2>(col[y], grid, y * K + k, g2, enh, bad);
         }
       }
       if (active) {

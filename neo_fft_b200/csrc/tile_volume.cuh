@@ -179,16 +179,29 @@ __global__ void __launch_bounds__(256) volume_tile_kernel(DevPlan P, VolumeShape
             if (kk == 0) dc[b] = line[0].r;
           }
           __syncthreads();
-          for (int task = tid; task < nbin; task += nthr) {
-            const int b = task / int(slot_bins), kk = task - b * int(slot_bins);
-            cf* bp = spec + b * blk_bins + kk;
-            const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
-                                ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
-            cf line[15];
-            for (int z = 0; z < T; ++z)
-              line[z] = spectral_bin(bp[size_t(z) * slot_bins], P.grid, z * int(slot_bins) + kk, g, P.filt, bad);
-            nf::fft_project<false, 0, 16>(line, T, P.twt);
-            bp[0] = line[zt];  // target slice in slot 0
+          // The filter type fixed at compile time per branch (no switch per element).
+          auto filter_lines = [&](auto ft) {
+            constexpr int FT = decltype(ft)::value;
+            for (int task = tid; task < nbin; task += nthr) {
+              const int b = task / int(slot_bins), kk = task - b * int(slot_bins);
+              cf* bp = spec + b * blk_bins + kk;
+              const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
+                                  ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
+              cf line[15];
+              for (int z = 0; z < T; ++z)
+                line[z] = spectral_bin<FT>(bp[size_t(z) * slot_bins], P.grid, z * int(slot_bins) + kk, g, P.filt, bad);
+              nf::fft_project<false, 0, 16>(line, T, P.twt);
+              bp[0] = line[zt];  // target slice in slot 0
+            }
+          };
+          switch (P.filt.type) {
+            case -1: filter_lines(std::integral_constant<int, -1>{}); break;
+            case 0: filter_lines(std::integral_constant<int, 0>{}); break;
+            case 1: filter_lines(std::integral_constant<int, 1>{}); break;
+            case 2: filter_lines(std::integral_constant<int, 2>{}); break;
+            case 3: filter_lines(std::integral_constant<int, 3>{}); break;
+            case 4: filter_lines(std::integral_constant<int, 4>{}); break;
+            default: filter_lines(std::integral_constant<int, -3>{}); break;
           }
           __syncthreads();
         }
@@ -204,7 +217,7 @@ __global__ void __launch_bounds__(256) volume_tile_kernel(DevPlan P, VolumeShape
             const float g2 = P.grid ? fdiv(fmul(P.mean_scale, spec[b * blk_bins].r), P.grid[0].r) : 0.0f;
 #pragma unroll UH
             for (int y = 0; y < CAPH; ++y)
-              if (y < BH) col[y] = spectral_bin(col[y], P.grid, y * K + k, g2, P.enh, bad);
+              if (y < BH) col[y] = spectral_bin<-2>(col[y], P.grid, y * K + k, g2, P.enh, bad);
           }
           nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
           // Slot 0 keeps the recovered spectrum whose DC other threads still read

@@ -37,7 +37,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 W, H, CW, CH, FRAMES = 1920, 1080, 960, 540, 60
-HOST_CHUNK = 2  # frames per device slot of the streamed host form
+HOST_CHUNK = 1  # frames per device slot of the streamed host form (4 slots)
 # DRAM bytes of one batch launch over the 60-frame clip: ncu capture of a 16-frame launch of
 # the same kernel (100.73 MB read + 60.34 MB written), scaled by the frames processed.
 TRAFFIC_PER_LAUNCH = (100.73e6 + 60.34e6) * FRAMES / 16
@@ -305,7 +305,7 @@ def run_ours(args):
     pin_in = [[torch.from_numpy(p).pin_memory() for p in f] for f in clip]
     pin_out = [[torch.empty(p.shape, dtype=torch.uint16).pin_memory() for p in f] for f in clip]
 
-    host_batch = HostBatch(plans, frames_per_chunk=HOST_CHUNK, depth=3)
+    host_batch = HostBatch(plans, frames_per_chunk=HOST_CHUNK, depth=4)
 
     def e2e_step():
         host_batch.process(pin_in, pin_out, wait=False)

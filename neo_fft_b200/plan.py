@@ -437,7 +437,7 @@ class HostBatch:
     pass through a ring of `depth` device slots of `frames_per_chunk` frames.
     `plans[p]` filters plane p of every frame. Outputs equal `Plan.process` per plane."""
 
-    def __init__(self, plans, frames_per_chunk: int = 2, depth: int = 3):
+    def __init__(self, plans, frames_per_chunk: int = 1, depth: int = 4):
         self._lib = C.load()
         self._plans = list(plans)
         arr = (ctypes.c_void_p * len(self._plans))(*[p._h.value for p in self._plans])

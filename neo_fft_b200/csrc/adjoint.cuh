@@ -48,24 +48,26 @@ __host__ __device__ inline size_t adjoint_smem_bytes(int bh, int bw, const Adjoi
 // Per-bin backward of spectral_bin for ftype 0 (Wiener, any exponent), 1 (hard
 // threshold) and 2 (constant gain). x: forward spectrum bin; dy: incoming complex
 // gradient. Returns dX; adds the template gradient to dg and the table gradient to da.
+// FT >= 0 fixes the ftype at compile time.
+template <int FT = -1>
 __device__ __forceinline__ cf spectral_bin_adjoint(cf x, cf dy, const cf* grid, int k, float g, const DevSpectral& p,
                                                    float& dg, float& da) {
+  const int type = FT >= 0 ? FT : p.type;
   const float a = p.primary ? p.primary[k] : p.a;
   const float mr = grid ? g * grid[k].r : 0.0f;
   const float mi = grid ? g * grid[k].i : 0.0f;
   const float re = x.r - mr, im = x.i - mi;
   const float power = re * re + im * im;
   float gain = 0.0f, dgain_dp = 0.0f, dgain_da = 0.0f;
-  if (p.type == 0) {
+  if (type == 0) {
     const float q = power + 1e-15f;
     const float r = (power - a) / q;
     if (r > 0.0f) {
       float dw;  // d gain / d r
-      const float e1 = p.exponent - 1.0f, e5 = p.exponent - 0.5f;
-      if (fabsf(e1) < 0.00005f) {
+      if (p.emode == 0) {  // the forward's exponent test (spectral.cpp:25-27), made once per plan
         gain = r;
         dw = 1.0f;
-      } else if (fabsf(e5) < 0.00005f) {
+      } else if (p.emode == 1) {
         gain = sqrtf(r);
         dw = 0.5f / gain;
       } else {
@@ -75,7 +77,7 @@ __device__ __forceinline__ cf spectral_bin_adjoint(cf x, cf dy, const cf* grid, 
       dgain_dp = dw * (a + 1e-15f) / (q * q);
       dgain_da = -dw / q;
     }
-  } else if (p.type == 1) {
+  } else if (type == 1) {
     gain = power < a ? 0.0f : 1.0f;
   } else {
     gain = a;
@@ -218,14 +220,21 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
         const float g = grid ? fmul(P.mean_scale, dc[b]) / grid0 : 0.0f;
         const float mk = (k == 0 || (BW % 2 == 0 && k == BW / 2)) ? invN : 2.0f * invN;
         const bool own = (bx_lo + b) * gx.step >= X0 && (bx_lo + b) * gx.step < X0 + tw && oy >= Y0 && oy < Y0 + th;
+        // The ftype fixed at compile time per branch (no switch per bin).
+        auto adjoint_column = [&](auto ft) {
+          constexpr int FT = decltype(ft)::value;
 #pragma unroll UH
-        for (int y = 0; y < CAPH; ++y)
-          if (y < BH) {
-            float da = 0.0f;
-            const cf dY = {gcol[y].r * mk, gcol[y].i * mk};
-            sp[size_t(y) * K * NB] = spectral_bin_adjoint(x[y], dY, grid, y * K + k, g, filt, dg, da);
-            da_blk[size_t(b) * bins + y * K + k] = own ? da : 0.0f;
-          }
+          for (int y = 0; y < CAPH; ++y)
+            if (y < BH) {
+              float da = 0.0f;
+              const cf dY = {gcol[y].r * mk, gcol[y].i * mk};
+              sp[size_t(y) * K * NB] = spectral_bin_adjoint<FT>(x[y], dY, grid, y * K + k, g, filt, dg, da);
+              da_blk[size_t(b) * bins + y * K + k] = own ? da : 0.0f;
+            }
+        };
+        if (filt.type == 0) adjoint_column(std::integral_constant<int, 0>{});
+        else if (filt.type == 1) adjoint_column(std::integral_constant<int, 1>{});
+        else adjoint_column(std::integral_constant<int, 2>{});
         dg_part[size_t(b) * K + k] = dg;
       }
     }

@@ -295,6 +295,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const float fct3 = fdiv(1.0f, fmul(fmul(float(P.T), float(BH)), float(BW)));
   const float volume = fmul(fmul(float(P.T), float(BW)), float(BH));
   const bool vec4 = (gx.step & 3) == 0 && (BW & 3) == 0;
+  const bool ola4 = !P.center && vec4 && (S.tw & 3) == 0 && (tw & 3) == 0 && (X0 & 3) == 0;
 
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
@@ -504,7 +505,38 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     __syncthreads();
     // ---- D: ordered overlap-add into the ring accumulator --------------------
     const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
-    for (Cursor2 c(tid, nthr, tw); c.y < yhi - ylo; c.next()) {
+    if (ola4) {
+      // Four consecutive columns per thread (X0, tw and the step multiples of 4): they
+      // share their first block and block count, so one 16-byte load per block serves
+      // all four, each component summed in the same block order as the scalar path.
+      const int adv4 = (OBW - gx.step) >> 2;
+      for (Cursor2 c(tid, nthr, tw >> 2); c.y < yhi - ylo; c.next()) {
+        const int Y = ylo + c.y, xx = c.x << 2, ly = Y - oy;
+        float4* a = reinterpret_cast<float4*>(acc + size_t(Y % BH) * S.tw + xx);
+        const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
+        const float4* ov =
+            reinterpret_cast<const float4*>(ob + size_t(ly) * NB * OBW + size_t(cm & 1023) * OBW + (cm >> 20));
+        if (fft3d) {
+          float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          for (int j = 0; j < nblk; ++j, ov += adv4) {
+            const float4 o = *ov;
+            r = make_float4(fadd(r.x, o.x), fadd(r.y, o.y), fadd(r.z, o.z), fadd(r.w, o.w));
+          }
+          const float w = wys[ly];
+          const float4 v = *a;
+          *a = make_float4(fadd(v.x, fmul(r.x, w)), fadd(v.y, fmul(r.y, w)), fadd(v.z, fmul(r.z, w)),
+                           fadd(v.w, fmul(r.w, w)));
+        } else {
+          float4 sacc = *a;
+          for (int j = 0; j < nblk; ++j, ov += adv4) {
+            const float4 o = *ov;
+            sacc = make_float4(fadd(sacc.x, o.x), fadd(sacc.y, o.y), fadd(sacc.z, o.z), fadd(sacc.w, o.w));
+          }
+          *a = sacc;
+        }
+      }
+    }
+    for (Cursor2 c(tid, nthr, tw); !ola4 && c.y < yhi - ylo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;

@@ -130,6 +130,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
   float* da_tile = da_blk + size_t(NB) * bins;
   float* dg_part = da_tile + bins;  // [NB][K]
   int* colmap = reinterpret_cast<int*>(dg_part + 2 * size_t(NB) * K);  // [tw], as in strip_tile
+  const bool ola4 = (gx.step & 3) == 0 && (BW & 3) == 0 && (S.tw & 3) == 0 && (tw & 3) == 0 && (X0 & 3) == 0;
 
   // tables
   int off = 0;
@@ -282,7 +283,23 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     __syncthreads();
     // ---- ordered gather into the cover-gradient ring; retire rows -------------
     const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
-    for (Cursor2 c(tid, nthr, tw); c.y < yhi - ylo; c.next()) {
+    if (ola4) {  // four columns per thread, one 16-byte load per block (as in strip_tile)
+      const int adv4 = (OBW - gx.step) >> 2;
+      for (Cursor2 c(tid, nthr, tw >> 2); c.y < yhi - ylo; c.next()) {
+        const int Y = ylo + c.y, xx = c.x << 2, ly = Y - oy;
+        float4* a = reinterpret_cast<float4*>(acc + size_t(Y % BH) * S.tw + xx);
+        const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
+        const float4* ov =
+            reinterpret_cast<const float4*>(ob + size_t(ly) * NB * OBW + size_t(cm & 1023) * OBW + (cm >> 20));
+        float4 sacc = *a;
+        for (int j = 0; j < nblk; ++j, ov += adv4) {
+          const float4 o = *ov;
+          sacc = make_float4(sacc.x + o.x, sacc.y + o.y, sacc.z + o.z, sacc.w + o.w);
+        }
+        *a = sacc;
+      }
+    }
+    for (Cursor2 c(tid, nthr, tw); !ola4 && c.y < yhi - ylo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = ylo + yy, ly = Y - oy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;

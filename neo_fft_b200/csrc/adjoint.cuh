@@ -42,7 +42,7 @@ __host__ __device__ inline size_t adjoint_smem_bytes(int bh, int bw, const Adjoi
   const size_t spec_cf = (size_t(s.nbx_max) * bh * K + 1) & ~size_t(1);
   return sizeof(float) * (size_t(s.tab_floats) + 2 * size_t(bh) * s.ring_pitch + 2 * spec_cf * 2 +
                           size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max) +
-                          size_t(s.nbx_max) * bins + bins + 2 * size_t(s.nbx_max) * K + size_t(s.tw));
+                          size_t(s.nbx_max | 1) * bins + bins + 2 * size_t(s.nbx_max) * K + size_t(s.tw));
 }
 
 // Per-bin backward of spectral_bin for ftype 0 (Wiener, any exponent), 1 (hard
@@ -126,8 +126,12 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
   float* ob = reinterpret_cast<float*>(gspec + spec_cf);
   float* acc = ob + size_t(BH) * NB * OBW;
   float* dc = acc + size_t(BH) * S.tw;
+  // Per-block table gradients [bin][block] with an odd block stride: the column threads
+  // (consecutive blocks) write consecutive words and the per-bin sums read rows whose
+  // starts fall in distinct banks.
+  const int NBp = NB | 1;
   float* da_blk = dc + 2 * size_t(NB);
-  float* da_tile = da_blk + size_t(NB) * bins;
+  float* da_tile = da_blk + size_t(NBp) * bins;
   float* dg_part = da_tile + bins;  // [NB][K]
   int* colmap = reinterpret_cast<int*>(dg_part + 2 * size_t(NB) * K);  // [tw], as in strip_tile
   const bool ola4 = (gx.step & 3) == 0 && (BW & 3) == 0 && (S.tw & 3) == 0 && (tw & 3) == 0 && (X0 & 3) == 0;
@@ -230,7 +234,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
               float da = 0.0f;
               const cf dY = {gcol[y].r * mk, gcol[y].i * mk};
               sp[size_t(y) * K * NB] = spectral_bin_adjoint<FT>(x[y], dY, grid, y * K + k, g, filt, dg, da);
-              da_blk[size_t(b) * bins + y * K + k] = own ? da : 0.0f;
+              da_blk[size_t(y * K + k) * NBp + b] = own ? da : 0.0f;
             }
         };
         if (filt.type == 0) adjoint_column(std::integral_constant<int, 0>{});
@@ -267,7 +271,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     // ---- table gradient of owned blocks, in block order ----------------------
     for (int i = tid; i < bins; i += nthr) {
       float s = da_tile[i];
-      for (int b = 0; b < nbx; ++b) s += da_blk[size_t(b) * bins + i];
+      for (int b = 0; b < nbx; ++b) s += da_blk[size_t(i) * NBp + b];
       da_tile[i] = s;
     }
     // ---- rows: unnormalised inverse, analysis-window weighting ---------------

@@ -2438,31 +2438,48 @@ void check_adjoint_plan(const nf_plan& p) {
 // whole waves of resident CTAs (two per SM), weighing each CTA by the rows it
 // transforms (tile height plus the block-height halo).
 nfd::AdjointShape adjoint_shape(const nfd::DevPlan& d, int nplanes) {
-  nfd::AdjointShape S{};
-  S.tab_floats = 2 * d.bh * d.bw + (d.grid ? 2 * d.bins : 0) + d.bins;
-  S.tab_floats = (S.tab_floats + 3) & ~3;
-  S.tw = std::min(d.gx.cover, std::max(d.gx.step, 64 / d.gx.step * d.gx.step));
-  S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
-  S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
-  int q = (S.win_max + 3) / 4;
-  if (q % 2 == 0) ++q;
-  S.ring_pitch = 4 * q;
-  S.tiles_x = (d.gx.cover + S.tw - 1) / S.tw;
+  // Cover tiles: width and height by a modelled schedule. Per block row a tile runs the
+  // two forward row passes (pixels and upstream gradient, 2·nb·bh rows), the column pass
+  // (two forward columns and the per-bin adjoint, nb·(bw/2+1) columns, weight 3), the
+  // inverse columns (weight 1.5) and the inverse rows, each in rounds of 256 threads; the
+  // launch lasts about ceil(tiles / resident CTAs) tiles. Two CTAs per SM must fit.
+  const int K = d.bw / 2 + 1;
   const long long slots = 2LL * 148;
-  const int lo = std::min(d.gy.cover, std::max(2 * d.bh, 32));
-  long long best = -1;
-  for (int th = lo; th <= d.gy.cover; th += std::max(1, d.gy.step)) {
-    const long long tiles_y = (d.gy.cover + th - 1) / th;
-    const long long ctas = (long long)std::max(1, nplanes) * S.tiles_x * tiles_y;
-    const long long cost = ((ctas + slots - 1) / slots) * (th + d.bh);
-    if (best < 0 || cost < best) {
-      best = cost;
-      S.th = th;
+  const int edge = (d.bw + d.gx.step - 1) / d.gx.step - 1;
+  nfd::AdjointShape best_s{};
+  double best = -1.0;
+  for (int nbx = edge + 2; nbx <= 64; ++nbx) {
+    nfd::AdjointShape S{};
+    S.tab_floats = 2 * d.bh * d.bw + (d.grid ? 2 * d.bins : 0) + d.bins;
+    S.tab_floats = (S.tab_floats + 3) & ~3;
+    S.tw = std::min(d.gx.cover, std::max(d.gx.step, (nbx - edge) * d.gx.step));
+    S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
+    S.win_max = (S.nbx_max - 1) * d.gx.step + d.bw;
+    int q = (S.win_max + 3) / 4;
+    if (q % 2 == 0) ++q;
+    S.ring_pitch = 4 * q;
+    S.tiles_x = (d.gx.cover + S.tw - 1) / S.tw;
+    if (nbx > edge + 2 && nfd::adjoint_smem_bytes(d.bh, d.bw, S) > size_t(110) * 1024) break;
+    const int nb = (S.tw + d.bw - d.gx.step + d.gx.step - 1) / d.gx.step;
+    const double per_row = double((2 * nb * d.bh + 255) / 256) + 4.5 * double((nb * K + 255) / 256) +
+                           double((nb * d.bh + 255) / 256);
+    const int lo = std::min(d.gy.cover, std::max(2 * d.bh, 32));
+    for (int th = lo; th <= d.gy.cover; th += std::max(1, d.gy.step)) {
+      const long long tiles_y = (d.gy.cover + th - 1) / th;
+      const long long ctas = (long long)std::max(1, nplanes) * S.tiles_x * tiles_y;
+      const double rows = double(th + d.bh) / d.gy.step + 2.0;
+      const double cost = double((ctas + slots - 1) / slots) * rows * per_row;
+      if (best < 0 || cost < best) {
+        best = cost;
+        best_s = S;
+        best_s.th = th;
+      }
+      if (tiles_y == 1) break;
     }
-    if (tiles_y == 1) break;
+    if (S.tw >= d.gx.cover) break;
   }
-  S.tiles_y = (d.gy.cover + S.th - 1) / S.th;
-  return S;
+  best_s.tiles_y = (d.gy.cover + best_s.th - 1) / best_s.th;
+  return best_s;
 }
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 } // namespace

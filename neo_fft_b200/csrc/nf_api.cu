@@ -911,6 +911,34 @@ cudaError_t launch_temporal_shape(int bh, int bw, int storage, int slice, const 
 cudaError_t launch_volume_spectra_shape(int bh, int bw, int storage, const nfd::VolumeSpectraWork& w, int items,
                                         size_t smem, cudaStream_t st);
 
+// Block columns per chunk of the spectra passes. FFT3D frames: the least modelled work per
+// block column (rounds of 256 threads over the n·bh rows and n·(bw/2+1) columns of the
+// chunk) within the shared-memory budget of the occupancy the kernel's registers allow (two
+// CTAs per SM up to 16x16 blocks, one above); ties go to the wider chunk. DFTTest volumes:
+// the widest chunk within 100 KB. smem(n) is the pass's shared memory for n columns.
+template <class SmemFn>
+int pass1_chunk(int bh, int bw, int T, bool slice, int max_count, SmemFn smem) {
+  const int K = bw / 2 + 1, tt = slice ? T : 1;
+  const size_t budget = size_t(bh * bw <= 256 ? 100 : 200) * 1024;
+  int best_n = 1;
+  double best = -1.0;
+  if (slice) {  // DFTTest volumes: the widest chunk within 100 KB measured fastest
+    for (int n = 2; n <= std::min(32, max_count); ++n)
+      if (smem(n) <= size_t(100) * 1024) best_n = n;
+    return best_n;
+  }
+  for (int n = 1; n <= std::min(16, max_count); ++n) {
+    if (n > 1 && smem(n) > budget) break;  // shared memory grows with n
+    const double c = (double((tt * n * bh + 255) / 256) + double((tt * n * K + 255) / 256) +
+                      (slice ? double((bh * K * n + 255) / 256) : 0.0)) / double(n);
+    if (best < 0 || c <= best) {
+      best = c;
+      best_n = n;
+    }
+  }
+  return best_n;
+}
+
 // Per-call temporal filtering in two passes over stream-ordered scratch (the clip form's
 // kernels for a single output): FFT3D bt 2..5 — the T slots' spatial spectra, then the
 // temporal strip; DFTTest tmode 1 with one covering block — the volume's filtered slice
@@ -931,11 +959,10 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
   const bool slice = t.algo == nfb::Algo::DFTTest;
   const int storage = storage_of(t.format);
   const size_t frame = size_t(t.gy.count) * t.bins * t.gx.count;  // complex per slot spectrum
-  int nbc = 1;
-  for (int n = 2; n <= std::min(slice ? 32 : 16, t.gx.count); ++n)
-    if ((slice ? nfd::volume_spectra_smem_bytes(t.bh, t.bw, T, t.gx.step, n)
-               : nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, n)) <= 100 * 1024)
-      nbc = n;
+  const int nbc = pass1_chunk(t.bh, t.bw, T, slice, t.gx.count, [&](int n) {
+    return slice ? nfd::volume_spectra_smem_bytes(t.bh, t.bw, T, t.gx.step, n)
+                 : nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, n);
+  });
   const size_t smem1 = slice ? nfd::volume_spectra_smem_bytes(t.bh, t.bw, T, t.gx.step, nbc)
                              : nfd::spectra_smem_bytes(t.bh, t.bw, t.gx.step, nbc);
   const int chunks = (t.gx.count + nbc - 1) / nbc, items = chunks * t.gy.count;
@@ -1891,9 +1918,11 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       return b->slice ? nfd::volume_spectra_smem_bytes(b->bh, b->bw, tmax, st, n)
                       : nfd::spectra_smem_bytes(b->bh, b->bw, st, n);
     };
-    b->nbc = 1;
-    for (int n = 2; n <= std::min(b->slice ? 32 : 16, max_count); ++n)
-      if (pass1_smem(step, n) <= 100 * 1024) b->nbc = n;
+    b->nbc = pass1_chunk(b->bh, b->bw, tmax, b->slice != 0, max_count, [&](int n) {
+      size_t m = 0;  // the largest over the plans' steps (wider windows need more)
+      for (const nf_plan* p : plans) m = std::max(m, pass1_smem(p->t.gx.step, n));
+      return m;
+    });
     b->smem1 = 0;
     for (const nf_plan* p : plans) b->smem1 = std::max(b->smem1, pass1_smem(p->t.gx.step, b->nbc));
     nfb::require(b->smem1 <= 200 * 1024, "block size too large for the spectra pass");

@@ -297,9 +297,11 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const bool vec4 = (gx.step & 3) == 0 && (BW & 3) == 0;
   const bool ola4 = !P.center && vec4 && (S.tw & 3) == 0 && (tw & 3) == 0 && (X0 & 3) == 0;
 
+  // No barrier between a block row's retire phase (accumulator ring and the output) and the
+  // next block row's first phase (staging ring, or the column phase's spectrum and DC
+  // buffers): they touch disjoint shared memory, and every later phase is behind a barrier.
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
-    __syncthreads();
     if (SRC == kSrcPixels && !kalman_L) {
       // ---- 0: stage the rows this block row adds ----------------------------
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);

@@ -167,9 +167,11 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
   const float invN = 1.0f / (float(BW) * float(BH));
   const float out_scale = P.out_scale;
 
+  // No barrier between a block row's retire phase (accumulator ring and the cover gradient) and
+  // the next block row's staging (source and gradient rings): they touch disjoint shared memory,
+  // and every later phase is behind a barrier.
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
-    __syncthreads();
     // ---- stage source rows (decoded) and upstream-gradient rows -------------
     const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
     const int nrows = oy + BH - r0;

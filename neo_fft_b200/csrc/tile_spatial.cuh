@@ -138,6 +138,21 @@ struct Cursor2 {
   }
 };
 
+// Warm L2 with one block row of slot spectra (nslots x bins runs of nbx values at
+// `at` + bin * cnt in each slot) while the current row is filtered and reconstructed:
+// one prefetch per 128-byte line, each at an element address inside its run.
+__device__ __forceinline__ void prefetch_row_l2(const cf* const* slots, int nslots, size_t at, int bins, size_t cnt,
+                                                int nbx) {
+  const int lines = (nbx * int(sizeof(cf)) + 127) / 128 + 1;
+  for (Cursor2 q(threadIdx.x, blockDim.x, lines); q.y < nslots * bins; q.next()) {
+    const int z = q.y / bins, kk = q.y - z * bins;
+    const uintptr_t lo = reinterpret_cast<uintptr_t>(slots[z] + at + size_t(kk) * cnt);
+    const uintptr_t hi = lo + size_t(nbx) * sizeof(cf);
+    const uintptr_t a = max(lo, (lo & ~uintptr_t(127)) + uintptr_t(q.x) * 128);
+    if (a < hi) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  }
+}
+
 // FFT3D bt=2..5 filter of one block row's (bin, block) elements across the T slot
 // spectra (spectral.cpp:90-160) with T = TC known at compile time; writes the recovered
 // spectrum into spec [bin][block].
@@ -350,6 +365,9 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       // DFTTest tmode 1 (plan.cpp:544-601): the slice's spectrum was filtered in 3-D by
       // the volume pass; only the column inverses remain.
       const cf* S = J.tspec[0] + size_t(by) * bins * size_t(gx.count) + size_t(bx_lo);
+      if (by < by_hi)
+        prefetch_row_l2(J.tspec, 1, size_t(by + 1) * bins * size_t(gx.count) + size_t(bx_lo), bins,
+                        size_t(gx.count), nbx);
       for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
         const int k = c.y, b = c.x;
         cf col[CAPH];
@@ -373,6 +391,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const size_t cnt = size_t(gx.count);
       const size_t row_base = size_t(by) * bins * cnt + size_t(bx_lo);
       const float invT = fdiv(1.0f, float(T));
+      if (by < by_hi) prefetch_row_l2(J.tspec, T, row_base + size_t(bins) * cnt, bins, cnt, nbx);
       for (int b = tid; b < nbx; b += nthr) dc[b] = J.tspec[c][row_base + b].r;
       __syncthreads();
       const int nel = bins * nbx;

@@ -319,22 +319,6 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     const int oy = by * gy.step;
     if (SRC == kSrcPixels && !kalman_L) {
       // ---- 0: stage the rows this block row adds ----------------------------
-      if (by < by_hi) {
-        // Warm L2 with the source rows the next block row adds (their in-plane column
-        // span), one prefetch per 128-byte line at an address inside the row.
-        const int nr0 = oy + BH, nrows_next = gy.step < BH ? gy.step : BH;
-        const int c_lo = max(0, cx0 - gx.offset), c_hi = min(gx.length, cx0 + win - gx.offset);
-        if (c_lo < c_hi) {
-          const uintptr_t bytes = uintptr_t(c_hi - c_lo) * STORAGE;
-          const int lines = int((bytes + 127) / 128) + 1;
-          for (Cursor2 q(tid, nthr, lines); q.y < nrows_next; q.next()) {
-            const unsigned char* srow = J.src + ptrdiff_t(reflect_axis(nr0 + q.y, gy)) * J.src_stride;
-            const uintptr_t lo = reinterpret_cast<uintptr_t>(srow) + uintptr_t(c_lo) * STORAGE, hi = lo + bytes;
-            const uintptr_t a = max(lo, (lo & ~uintptr_t(127)) + uintptr_t(q.x) * 128);
-            if (a < hi) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
-          }
-        }
-      }
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
       const int nrows = oy + BH - r0;
       for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {

@@ -366,7 +366,8 @@ nf_status nf_dft_backward_device(const nf_plan* plan, const nf_const_plane* sour
  * allocator to borrow from, and cudaMalloc/cudaFree synchronise the device, which
  * stalls every other stream such a host keeps busy. Calls whose scratch need
  * (nf_dft_backward_scratch_bytes) exceeds nf_dft_backward_static_capacity() fail
- * with NF_INVALID_ARGUMENT. The first call on each device looks the buffer's
+ * with NF_INVALID_ARGUMENT, and so do calls made while a device other than the
+ * plan's is current (the buffer is per device). The first call on each device looks the buffer's
  * address up (cudaGetSymbolAddress) and should come before any stream capture;
  * later calls only launch kernels. The buffer is shared: calls that overlap in
  * time (other threads or unordered streams) race on it and must be serialised. */

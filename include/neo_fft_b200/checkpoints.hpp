@@ -1,12 +1,13 @@
 // Kalman checkpoints and bounded-warmup seeks over device-resident states.
 //
 // neo_fft::KalmanCheckpoints keeps up to four snapshots of the per-plane Kalman states
-// (each a device allocation, copied device to device) with the reference's policy
-// (src/runtime/checkpoints.hpp:32-79): acquire(frame, earliest) leases the latest
-// snapshot in [earliest, frame]; publish() ignores frame < 1 and frames already held,
-// then evicts least-recently used snapshots until the new one fits the budget. The
-// default budget is 64 MiB and always retains one snapshot even when a single one is
-// larger (large geometries keep continuing sequentially); an explicit budget is hard.
+// (each a device allocation, copied device to device) with the observable policy of the
+// reference's runtime::Checkpoints (src/runtime/checkpoints.hpp:32-79), implemented by
+// SnapshotShelf: acquire(frame, earliest) leases the latest snapshot in [earliest, frame];
+// publish() ignores frame < 1 and frames already held, then evicts least-recently used
+// snapshots until the new one fits the budget. The default budget is 64 MiB and always
+// retains one snapshot even when a single one is larger (large geometries keep
+// continuing sequentially); an explicit budget is hard.
 //
 // neo_fft::KalmanSeek reproduces the host layer's random-access rule
 // (src/plugin/filter.hpp:152-250): frame 0 is passed through; for frame n > 0 the
@@ -15,6 +16,7 @@
 // the frame is rendered from that state and the new state is published.
 #pragma once
 #include "neo_fft_b200/plan.hpp"
+#include "neo_fft_b200/snapshot_shelf.hpp"
 
 #include <array>
 #include <cstddef>
@@ -34,76 +36,37 @@ struct KalmanCheckpoint {
   }
 };
 
+// The snapshots of one plane set, held on a SnapshotShelf (snapshot_shelf.hpp): leases
+// are shared, so a snapshot evicted while a request still continues from it stays alive
+// until that request drops it.
 class KalmanCheckpoints {
  public:
   using Lease = std::shared_ptr<const KalmanCheckpoint>;
-  KalmanCheckpoints() : budget_(64u << 20), retain_one_(true) {}
-  explicit KalmanCheckpoints(std::size_t budget) : budget_(budget), retain_one_(false) {}
+  KalmanCheckpoints() : shelf_(std::size_t(64) << 20, true) {}
+  explicit KalmanCheckpoints(std::size_t budget) : shelf_(budget, false) {}
 
   Lease acquire(int frame, int earliest = 0) {
     std::lock_guard<std::mutex> lock(mutex_);
-    Slot* best = nullptr;
-    for (auto& s : slots_)
-      if (s.value && s.value->frame >= earliest && s.value->frame <= frame && (!best || s.value->frame > best->value->frame))
-        best = &s;
-    if (!best) return {};
-    touch(*best);
-    return best->value;
+    Lease* hit = shelf_.latest(frame, earliest);
+    return hit ? *hit : Lease{};
   }
 
   void publish(std::unique_ptr<KalmanCheckpoint> owned) {
-    if (!owned || owned->frame < 1) return;
-    Lease value(owned.release());
-    const std::size_t need = sizeof(*this) + value->bytes();
-    const std::size_t limit = retain_one_ && need > budget_ ? need : budget_;
-    if (need > limit) return;
+    if (!owned) return;
+    const int frame = owned->frame;
+    const std::size_t size = owned->bytes();
+    Lease lease(owned.release());
     std::lock_guard<std::mutex> lock(mutex_);
-    for (auto& s : slots_)
-      if (s.value && s.value->frame == value->frame) {  // first snapshot of a frame wins
-        touch(s);
-        return;
-      }
-    while (used_ > limit - need || held() == slots_.size()) {
-      Slot* oldest = nullptr;
-      for (auto& s : slots_)
-        if (s.value && (!oldest || s.age > oldest->age)) oldest = &s;
-      used_ -= oldest->value->bytes();
-      oldest->value.reset();
-    }
-    for (auto& s : slots_)
-      if (!s.value) {
-        used_ += value->bytes();
-        s.value = std::move(value);
-        s.age = 4;
-        touch(s);
-        break;
-      }
+    shelf_.offer(frame, std::move(lease), size, [](Lease&) {});
   }
 
   std::size_t bytes() const {
     std::lock_guard<std::mutex> lock(mutex_);
-    return used_ + sizeof(*this);
+    return shelf_.used_bytes() + sizeof(*this);
   }
 
  private:
-  struct Slot {
-    Lease value;
-    unsigned age = 0;
-  };
-  void touch(Slot& selected) {
-    for (auto& s : slots_)
-      if (s.value && &s != &selected && s.age < selected.age) ++s.age;
-    selected.age = 0;
-  }
-  std::size_t held() const {
-    std::size_t n = 0;
-    for (const auto& s : slots_) n += s.value ? 1 : 0;
-    return n;
-  }
-  std::array<Slot, 4> slots_{};
-  const std::size_t budget_;
-  const bool retain_one_;
-  std::size_t used_ = 0;
+  SnapshotShelf<Lease> shelf_;
   mutable std::mutex mutex_;
 };
 

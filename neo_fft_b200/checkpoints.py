@@ -2,12 +2,12 @@
 include/neo_fft_b200/checkpoints.hpp).
 
 KalmanCheckpoints keeps up to four snapshots of per-plane device states with the
-reference's policy (src/runtime/checkpoints.hpp:32-79); KalmanSeek applies the host
-layer's random-access rule (src/plugin/filter.hpp:152-250) on top of Plan's Kalman calls.
+observable policy of the reference's runtime::Checkpoints (src/runtime/checkpoints.hpp:32-79);
+KalmanSeek applies the host layer's random-access rule (src/plugin/filter.hpp:152-250) on
+top of Plan's Kalman calls.
 """
 from __future__ import annotations
 
-import sys
 import threading
 from dataclasses import dataclass, field
 
@@ -18,7 +18,7 @@ class KalmanCheckpoint:
     planes: list = field(default_factory=lambda: [None] * 4)
 
     def nbytes(self) -> int:
-        return sys.getsizeof(self) + sum(p.nbytes for p in self.planes if p is not None)
+        return 64 + sum(p.nbytes for p in self.planes if p is not None)
 
     def clone(self) -> "KalmanCheckpoint":
         return KalmanCheckpoint(self.frame, [p.clone() if p is not None else None for p in self.planes])
@@ -28,65 +28,57 @@ class KalmanCheckpoints:
     """At most four snapshots; acquire(frame, earliest) leases the latest snapshot in
     [earliest, frame]; publish() ignores frame < 1 and frames already held, then evicts
     least-recently used snapshots until the new one fits. Default budget 64 MiB that
-    always retains one snapshot; an explicit budget is hard."""
+    always retains one snapshot; an explicit budget is hard.
+
+    Mirror of SnapshotShelf (include/neo_fft_b200/snapshot_shelf.hpp): a dict of frame ->
+    (checkpoint, bytes, stamp), where every hit and every store takes the next value of a
+    use counter and the smallest stamp is the least recently used."""
 
     SLOTS = 4
 
     def __init__(self, budget: int | None = None):
         self._budget = 64 << 20 if budget is None else int(budget)
-        self._retain_one = budget is None
-        self._slots = [[None, 0] for _ in range(self.SLOTS)]  # [checkpoint, age]
-        self._used = 0
+        self._keep_oversized = budget is None
+        self._held: dict[int, list] = {}  # frame -> [checkpoint, bytes, stamp]
+        self._clock = 0
         self._lock = threading.Lock()
 
-    def _touch(self, sel):
-        for s in self._slots:
-            if s[0] is not None and s is not sel and s[1] < sel[1]:
-                s[1] += 1
-        sel[1] = 0
+    def _stamp(self) -> int:
+        self._clock += 1
+        return self._clock
 
     def acquire(self, frame: int, earliest: int = 0):
         with self._lock:
-            best = None
-            for s in self._slots:
-                c = s[0]
-                if c is not None and earliest <= c.frame <= frame and (best is None or c.frame > best[0].frame):
-                    best = s
-            if best is None:
+            inside = [f for f in self._held if earliest <= f <= frame]
+            if not inside:
                 return None
-            self._touch(best)
-            return best[0]
+            entry = self._held[max(inside)]
+            entry[2] = self._stamp()
+            return entry[0]
 
     def publish(self, cp: KalmanCheckpoint | None) -> None:
         if cp is None or cp.frame < 1:
             return
-        need = sys.getsizeof(self) + cp.nbytes()
-        limit = need if self._retain_one and need > self._budget else self._budget
-        if need > limit:
+        size = cp.nbytes()
+        cap = size if self._keep_oversized and size > self._budget else self._budget
+        if size > cap:
             return
         with self._lock:
-            for s in self._slots:
-                if s[0] is not None and s[0].frame == cp.frame:
-                    self._touch(s)
-                    return
-            while self._used > limit - need or sum(s[0] is not None for s in self._slots) == self.SLOTS:
-                oldest = max((s for s in self._slots if s[0] is not None), key=lambda s: s[1])
-                self._used -= oldest[0].nbytes()
-                oldest[0] = None
-            for s in self._slots:
-                if s[0] is None:
-                    self._used += cp.nbytes()
-                    s[0], s[1] = cp, 4
-                    self._touch(s)
-                    break
+            if cp.frame in self._held:  # the snapshot already held for this frame stays
+                self._held[cp.frame][2] = self._stamp()
+                return
+            while len(self._held) >= self.SLOTS or sum(e[1] for e in self._held.values()) + size > cap:
+                lru = min(self._held, key=lambda f: self._held[f][2])
+                del self._held[lru]
+            self._held[cp.frame] = [cp, size, self._stamp()]
 
     def frames(self) -> list[int]:
         with self._lock:
-            return sorted(s[0].frame for s in self._slots if s[0] is not None)
+            return sorted(self._held)
 
     def nbytes(self) -> int:
         with self._lock:
-            return self._used + sys.getsizeof(self)
+            return sum(e[1] for e in self._held.values())
 
 
 class KalmanSeek:

@@ -2608,6 +2608,15 @@ PlanInfo plan_info(const nf_plan* p) {
              t.temporal_size <= nfd::kMaxVolumeSlots));
   i.pframe = t.pframe;
   i.kalman_warmup = t.kalman_warmup;
+  i.device = p->device;
   return i;
+}
+nf_status check_backward_call(const nf_plan* p, int nplanes, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p, "null plan");
+    check_adjoint_plan(*p);
+    nfb::require(nplanes > 0 && nplanes <= nfd::kAdjointMaxPlanes, "backward takes 1..32 planes per call");
+    return NF_OK;
+  });
 }
 }  // namespace nfi

@@ -13,6 +13,7 @@
 #include "neo_fft_b200.h"
 #include "plan_build.hpp"
 #include "plan_info.hpp"
+#include "neo_fft_b200/snapshot_shelf.hpp"
 
 #include <cuda_runtime.h>
 
@@ -69,26 +70,25 @@ struct nf_frame_server {
     }
   };
 
-  // FFT3D bt=0: snapshots of the per-plane Kalman states with the host layer's policy
-  // (runtime/checkpoints.hpp:32-79): up to four, least recently used evicted first, a
-  // 64 MiB budget that always keeps one; the first snapshot of a frame wins.
-  struct Snapshot {
+  // FFT3D bt=0: snapshots of the per-plane Kalman states (device states, one per plane)
+  // on a SnapshotShelf with the host layer's policy (runtime/checkpoints.hpp:32-79): up to
+  // four, least recently used evicted first, a 64 MiB budget that always keeps one; the
+  // first snapshot of a frame wins.
+  using PlaneStates = std::vector<nf_kalman_state*>;
+  static void release_states(PlaneStates& v) {
+    for (nf_kalman_state*& k : v)
+      if (k) {
+        nf_kalman_state_destroy(k);
+        k = nullptr;
+      }
+  }
+  struct Snapshot {  // a state being advanced by a request, not yet on the shelf
     int frame = -1;
-    std::vector<nf_kalman_state*> planes;
+    PlaneStates planes;
     size_t bytes = 0;
-    unsigned age = 0;
-    void release() {
-      for (nf_kalman_state*& k : planes)
-        if (k) {
-          nf_kalman_state_destroy(k);
-          k = nullptr;
-        }
-      frame = -1;
-      bytes = 0;
-    }
   };
   static constexpr size_t kSnapshotBudget = size_t(64) << 20;
-  Snapshot snaps[4];
+  neo_fft::SnapshotShelf<PlaneStates> snaps{kSnapshotBudget, true};
   int warmup = 8;
 
   std::vector<const nf_plan*> plans;  // per plane; nullptr: copied
@@ -110,7 +110,7 @@ struct nf_frame_server {
   ~nf_frame_server() {
     for (auto& b : banks)
       if (b.stream) cudaStreamSynchronize(b.stream);
-    for (auto& sn : snaps) sn.release();
+    snaps.clear(release_states);
     for (auto& b : banks) {
       if (b.stream) cudaStreamSynchronize(b.stream);
       b.drop_forms();
@@ -343,59 +343,13 @@ struct nf_frame_server {
   }
 
   // ---- FFT3D bt=0 (Kalman) ------------------------------------------------------
-  void touch(Snapshot& sel) {
-    for (auto& sn : snaps)
-      if (sn.frame >= 0 && &sn != &sel && sn.age < sel.age) ++sn.age;
-    sel.age = 0;
-  }
-  // The latest snapshot of a frame in [earliest, frame] (Checkpoints::acquire).
-  Snapshot* acquire(int frame, int earliest) {
-    Snapshot* best = nullptr;
-    for (auto& sn : snaps)
-      if (sn.frame >= 0 && sn.frame >= earliest && sn.frame <= frame && (!best || sn.frame > best->frame)) best = &sn;
-    if (best) touch(*best);
-    return best;
-  }
-  // Checkpoints::publish: takes ownership of s's states.
+  // The snapshot's states go onto the shelf, or are destroyed when the shelf declines
+  // them (frame already held, or over the budget).
   void publish(Snapshot& s) {
-    if (s.frame < 1) {
-      s.release();
-      return;
-    }
-    const size_t need = s.bytes, limit = need > kSnapshotBudget ? need : kSnapshotBudget;
-    for (auto& sn : snaps)
-      if (sn.frame == s.frame) {  // the first snapshot of a frame wins
-        touch(sn);
-        s.release();
-        return;
-      }
-    auto used = [&] {
-      size_t u = 0;
-      for (auto& sn : snaps) u += sn.frame >= 0 ? sn.bytes : 0;
-      return u;
-    };
-    auto held = [&] {
-      int h = 0;
-      for (auto& sn : snaps) h += sn.frame >= 0 ? 1 : 0;
-      return h;
-    };
-    while (used() > limit - need || held() == 4) {
-      Snapshot* oldest = nullptr;
-      for (auto& sn : snaps)
-        if (sn.frame >= 0 && (!oldest || sn.age > oldest->age)) oldest = &sn;
-      oldest->release();
-    }
-    for (auto& sn : snaps)
-      if (sn.frame < 0) {
-        sn.frame = s.frame;
-        sn.planes = s.planes;
-        sn.bytes = s.bytes;
-        s.planes.assign(s.planes.size(), nullptr);
-        s.frame = -1;
-        sn.age = 4;
-        touch(sn);
-        return;
-      }
+    if (!snaps.offer(s.frame, std::move(s.planes), s.bytes, release_states)) release_states(s.planes);
+    s.planes.clear();
+    s.frame = -1;
+    s.bytes = 0;
   }
 
   void upload(Bank& b, int frame) {
@@ -422,18 +376,19 @@ struct nf_frame_server {
     b.valid = false;  // slot 0 holds Kalman sources, not a range
     char err[512] = {0};
     Snapshot cur;
-    const Snapshot* state = nullptr;
+    const PlaneStates* state = nullptr;
     bool have_n = false;
     try {
       if (n > 0) {
         const int earliest = n > warmup ? n - warmup - 1 : 0;
-        Snapshot* start = acquire(n, earliest);
-        const int replay_start = start ? start->frame : earliest;
+        int start_frame = 0;
+        PlaneStates* start = snaps.latest(n, earliest, &start_frame);
+        const int replay_start = start ? start_frame : earliest;
         if (replay_start < n) {
           cur.planes.assign(size_t(planes), nullptr);
           for (int p = 0; p < planes; ++p) {
             if (!plans[size_t(p)]) continue;
-            if (start) check(nf_kalman_state_clone(start->planes[size_t(p)], &cur.planes[size_t(p)], st, err, sizeof err), err);
+            if (start) check(nf_kalman_state_clone((*start)[size_t(p)], &cur.planes[size_t(p)], st, err, sizeof err), err);
             else check(nf_kalman_state_create(plans[size_t(p)], 0, &cur.planes[size_t(p)], err, sizeof err), err);
             cur.bytes += nf_kalman_state_bytes(cur.planes[size_t(p)]);
           }
@@ -447,7 +402,7 @@ struct nf_frame_server {
           }
           cur.frame = n;
           have_n = true;
-          state = &cur;
+          state = &cur.planes;
         } else {
           state = start;
         }
@@ -460,7 +415,7 @@ struct nf_frame_server {
           const auto& in = info[size_t(p)];
           if (d.width != in.width || d.height != in.height) raise(NF_INVALID_ARGUMENT, "frame dimensions differ from plan");
           check(nf_kalman_render_device(plans[size_t(p)], device_plane(b.src, 0, p), out_plane(b.out, 0, p),
-                                        state->planes[size_t(p)], st, err, sizeof err),
+                                        (*state)[size_t(p)], st, err, sizeof err),
                 err);
           check(cudaMemcpy2DAsync(d.data, size_t(d.stride_bytes), slot(b.out, 0, p), pitch[size_t(p)],
                                   size_t(in.width) * size_t(in.elem), size_t(in.height), cudaMemcpyDefault, st),
@@ -479,7 +434,7 @@ struct nf_frame_server {
         if (plan) check(nf_plan_sync_status(plan, st, err, sizeof err), err);
     } catch (...) {
       cudaStreamSynchronize(st);
-      cur.release();
+      release_states(cur.planes);
       throw;
     }
     ++computed;

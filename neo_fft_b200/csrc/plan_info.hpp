@@ -16,8 +16,13 @@ struct PlanInfo {
   bool clip = false;    // accepted by nf_clip_batch
   int pframe = 0;       // FFT3D pattern frame (pfactor)
   int kalman_warmup = 8;  // FFT3D bt=0: frames replayed at most before a random-access request
+  int device = 0;         // CUDA device the plan's tables live on
 };
 
 PlanInfo plan_info(const nf_plan* p);
+
+// The checks nf_dft_backward_device applies to its plan and plane count (a float DFTTest
+// plan with tbsize 1, smode 1 and ftype 0..2; 1..32 planes), as a status and message.
+nf_status check_backward_call(const nf_plan* p, int nplanes, char* err, size_t len);
 
 }  // namespace nfi

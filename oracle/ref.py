@@ -16,7 +16,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_ref" / "libneofft_ref.so"
-REFERENCE = Path(os.environ.get("NEO_FFT_REFERENCE", "/root/reference"))
+# The neo-fft sources: $NEO_FFT_REFERENCE, else a checkout named `reference` beside this repository.
+REFERENCE = Path(os.environ.get("NEO_FFT_REFERENCE", HERE.parent.parent / "reference"))
 
 _lib = None
 

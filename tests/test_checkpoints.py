@@ -94,3 +94,18 @@ def test_seek_replays_bounded_warmup(warmup):
     assert out[20] == (20, list(range(20 - warmup, 21)))  # no snapshot in reach: warmup frames
     assert out[3] == (3, [1, 2, 3])
     assert out[21] == (21, list(range(20 - warmup, 22)))
+
+
+def test_cpp_snapshot_shelf_policy():
+    """The C++ shelf behind KalmanCheckpoints and the frame server's Kalman snapshots
+    (include/neo_fft_b200/snapshot_shelf.hpp) passes the same cases on the CPU."""
+    import subprocess
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    exe = root / "tests" / "_build" / "shelf_check"
+    exe.parent.mkdir(exist_ok=True)
+    subprocess.run(["g++", "-std=c++17", "-O1", f"-I{root / 'include'}", str(root / "tests" / "native" / "shelf_check.cpp"),
+                    "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout
+    assert out.stdout.count("ok ") == 10

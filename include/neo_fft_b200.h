@@ -384,6 +384,18 @@ nf_status nf_kernel_info(char* fft_backend, size_t fft_backend_len, char* target
 /* Library/ABI version for loaders. */
 int nf_abi_version(void);
 
+/* Row copy of the host layer's ROI packing (Plan::copy_row, src/algorithms/plan.hpp:82;
+ * CopyRow and copy_row_scalar, src/kernels/rows.hpp:4-7): `bytes` bytes from source to
+ * dst, each in host or device memory (device rows are copied with cudaMemcpy, host rows
+ * with memcpy). Signature-compatible with neo_fft::CopyRow. */
+void nf_copy_row(const void* source, void* dst, size_t bytes);
+
+/* A non-blocking CUDA stream for one request's workspace (the facade's
+ * runtime::Workspace, in place of the reference's per-request host workspace,
+ * src/runtime/workspace_pool.hpp:12-75). Destroying waits for the stream's work. */
+nf_status nf_stream_create(void** stream, char* err, size_t err_len);
+void nf_stream_destroy(void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,7 @@
 #include <array>
 #include <complex>
 #include <cstdint>
+#include <cstring>
 #include <functional>
 #include <memory>
 #include <mutex>
@@ -31,9 +32,135 @@
 
 namespace neo_fft {
 
+// Row copy used by the host layer's ROI packing (kernels/rows.hpp:4-7). Plan::copy_row()
+// returns nf_copy_row, which also copies rows that live in device memory.
+using CopyRow = void (*)(const void*, void*, std::size_t);
+inline void copy_row_scalar(const void* source, void* dst, std::size_t bytes) {
+  if (bytes) std::memcpy(dst, source, bytes);
+}
+
 namespace runtime {
 class SpectraCache;     // host-side raw-spectrum cache: not used by the B200 path
 class Retention;
+
+// Per-request working state (src/runtime/workspace.hpp, workspace_pool.hpp:12-75). On the
+// B200 path a request's working set is device staging taken from the library's memory pool
+// per call; the workspace carries the CUDA stream the request's calls are ordered on, so
+// requests served by different host threads overlap on the GPU.
+struct WorkspaceBudget {
+  std::size_t total_bytes = 0;  // device staging of one request (its source slots and output)
+  int temporal_slots = 1;
+};
+
+class Workspace {
+ public:
+  explicit Workspace(const WorkspaceBudget& budget) : budget_(budget) {
+    char err[256] = {0};
+    if (nf_stream_create(&stream_, err, sizeof(err)) != NF_OK) throw std::runtime_error(err);
+  }
+  Workspace(const Workspace&) = delete;
+  Workspace& operator=(const Workspace&) = delete;
+  ~Workspace() { nf_stream_destroy(stream_); }
+  const WorkspaceBudget& budget() const noexcept { return budget_; }
+  void* stream() const noexcept { return stream_; }
+
+ private:
+  WorkspaceBudget budget_;
+  void* stream_ = nullptr;
+};
+
+class WorkspacePool;
+
+// A leased workspace; returned to its pool when the lease ends.
+class WorkspaceLease {
+ public:
+  WorkspaceLease() noexcept = default;
+  WorkspaceLease(WorkspacePool* pool, std::unique_ptr<Workspace> ws) noexcept : pool_(pool), ws_(std::move(ws)) {}
+  WorkspaceLease(WorkspaceLease&& o) noexcept : pool_(o.pool_), ws_(std::move(o.ws_)) { o.pool_ = nullptr; }
+  WorkspaceLease& operator=(WorkspaceLease&& o) noexcept {
+    if (this != &o) {
+      reset();
+      pool_ = o.pool_;
+      ws_ = std::move(o.ws_);
+      o.pool_ = nullptr;
+    }
+    return *this;
+  }
+  WorkspaceLease(const WorkspaceLease&) = delete;
+  WorkspaceLease& operator=(const WorkspaceLease&) = delete;
+  ~WorkspaceLease() { reset(); }
+  Workspace* get() const noexcept { return ws_.get(); }
+  Workspace* operator->() const noexcept { return ws_.get(); }
+  Workspace& operator*() const noexcept { return *ws_; }
+  explicit operator bool() const noexcept { return ws_ != nullptr; }
+  inline void reset() noexcept;
+
+ private:
+  WorkspacePool* pool_ = nullptr;
+  std::unique_ptr<Workspace> ws_;
+};
+
+// Any number of workspaces may be leased at once; at most max_capacity idle ones are kept
+// for reuse, the rest are released when their lease ends.
+class WorkspacePool {
+ public:
+  explicit WorkspacePool(WorkspaceBudget budget, std::size_t max_capacity = 1)
+      : budget_(budget), max_capacity_(max_capacity) {}
+  WorkspacePool(const WorkspacePool&) = delete;
+  WorkspacePool& operator=(const WorkspacePool&) = delete;
+  WorkspaceLease acquire() {
+    std::unique_ptr<Workspace> ws;
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      ++active_;
+      if (!idle_.empty()) {
+        ws = std::move(idle_.back());
+        idle_.pop_back();
+      }
+    }
+    if (!ws) {
+      try {
+        ws = std::make_unique<Workspace>(budget_);
+      } catch (...) {
+        std::lock_guard<std::mutex> lock(mu_);
+        --active_;
+        throw;
+      }
+    }
+    return WorkspaceLease(this, std::move(ws));
+  }
+  const WorkspaceBudget& budget() const noexcept { return budget_; }
+  std::size_t max_capacity() const noexcept { return max_capacity_; }
+  std::size_t active_count() const {
+    std::lock_guard<std::mutex> lock(mu_);
+    return active_;
+  }
+  std::size_t idle_count() const {
+    std::lock_guard<std::mutex> lock(mu_);
+    return idle_.size();
+  }
+
+ private:
+  friend class WorkspaceLease;
+  void give_back(std::unique_ptr<Workspace> ws) noexcept {
+    std::unique_ptr<Workspace> drop;
+    std::lock_guard<std::mutex> lock(mu_);
+    --active_;
+    if (idle_.size() < max_capacity_) idle_.push_back(std::move(ws));
+    else drop = std::move(ws);
+  }
+  WorkspaceBudget budget_;
+  std::size_t max_capacity_;
+  std::size_t active_ = 0;
+  std::vector<std::unique_ptr<Workspace>> idle_;
+  mutable std::mutex mu_;
+};
+
+inline void WorkspaceLease::reset() noexcept {
+  if (pool_ && ws_) pool_->give_back(std::move(ws_));
+  pool_ = nullptr;
+  ws_.reset();
+}
 }  // namespace runtime
 
 enum class Algorithm { FFT3D, DFTTest };
@@ -248,27 +375,35 @@ class Plan {
     std::size_t bins() const { return bins_; }
   } fft;
 
+  // process (plan.hpp:58-75): one plane or temporal slots, with the plan's pooled
+  // workspace or the caller's.
   template <class T>
   void process(span2d::Plane<const T> src, span2d::Plane<T> dst) const {
     process_at<T>({&src, 1}, dst, 0, 0);
   }
   template <class T>
+  void process(span2d::Plane<const T> src, span2d::Plane<T> dst, runtime::Workspace& ws) const {
+    run<T>({&src, 1}, dst, 0, 0, {}, ws.stream());
+  }
+  template <class T>
   void process(span2d::Span<const span2d::Plane<const T>> sources, span2d::Plane<T> dst) const {
     process_at<T>(sources, dst, 0, 0);
   }
-  // process_at (plan.hpp:77-80); the SpectraCache arguments are accepted and ignored.
+  template <class T>
+  void process(span2d::Span<const span2d::Plane<const T>> sources, span2d::Plane<T> dst,
+               runtime::Workspace& ws) const {
+    run<T>(sources, dst, 0, 0, {}, ws.stream());
+  }
+  // process_at (plan.hpp:77-80): a workspace leased from the plan's pool for the call; the
+  // SpectraCache arguments are accepted and ignored.
   template <class T, class Cache = runtime::SpectraCache, class Request = void>
   void process_at(span2d::Span<const span2d::Plane<const T>> sources, span2d::Plane<T> dst, int frame, int plane,
                   span2d::Span<const int> targets = {}, Cache* = nullptr, Request* = nullptr) const {
-    if (noise_) upload_noise();
-    std::vector<nf_const_plane> s;
-    s.reserve(sources.size());
-    for (const auto& p : sources) s.push_back(detail::cplane(p));
-    char err[512] = {0};
-    detail::check(nf_plan_process_host(plan_, s.data(), int(s.size()), targets.data(), int(targets.size()),
-                                       detail::mplane(dst), frame, plane, nullptr, err, sizeof(err)),
-                  err);
+    auto lease = pool_->acquire();
+    run<T>(sources, dst, frame, plane, targets, lease->stream());
   }
+  CopyRow copy_row() const { return &nf_copy_row; }
+  runtime::WorkspacePool& workspace_pool() const noexcept { return *pool_; }
 
   bool kalman() const { return kalman_; }
   bool preview() const { return preview_; }
@@ -317,6 +452,18 @@ class Plan {
   const nf_plan* handle() const { return plan_; }
 
  private:
+  template <class T>
+  void run(span2d::Span<const span2d::Plane<const T>> sources, span2d::Plane<T> dst, int frame, int plane,
+           span2d::Span<const int> targets, void* stream) const {
+    if (noise_) upload_noise();
+    std::vector<nf_const_plane> s;
+    s.reserve(sources.size());
+    for (const auto& p : sources) s.push_back(detail::cplane(p));
+    char err[512] = {0};
+    detail::check(nf_plan_process_host(plan_, s.data(), int(s.size()), targets.data(), int(targets.size()),
+                                       detail::mplane(dst), frame, plane, stream, err, sizeof(err)),
+                  err);
+  }
   // Publishes the shared noise model's table to this plan once it exists.
   void upload_noise() const {
     auto power = noise_->power();
@@ -338,8 +485,13 @@ class Plan {
     geometry.y = {y.length, y.block, y.overlap, y.step, y.count, y.cover, y.offset};
     temporal_size = t;
     fft.bins_ = std::size_t(b);
+    const std::size_t sample = format.floating ? 4 : (format.bits > 8 ? 2 : 1);
+    const std::size_t plane_bytes = std::size_t(x.length) * std::size_t(y.length) * sample;
+    pool_ = std::make_unique<runtime::WorkspacePool>(
+        runtime::WorkspaceBudget{plane_bytes * std::size_t(t + 1), t});
   }
   nf_plan* plan_ = nullptr;
+  std::unique_ptr<runtime::WorkspacePool> pool_;
   bool kalman_ = false;
   bool preview_ = false;
 };

@@ -156,6 +156,9 @@ PROTOTYPES = {
                                               c_size_t]),
     "nf_kernel_info": (c_int, [ctypes.c_char_p, c_size_t, ctypes.c_char_p, c_size_t, ctypes.c_char_p,
                                c_size_t, _IP]),
+    "nf_copy_row": (None, [c_void_p, c_void_p, c_size_t]),
+    "nf_stream_create": (c_int, [ctypes.POINTER(c_void_p), ctypes.c_char_p, c_size_t]),
+    "nf_stream_destroy": (None, [c_void_p]),
 }
 
 _lib = None

@@ -1209,6 +1209,32 @@ extern "C" {
 
 int nf_abi_version(void) { return NF_ABI_VERSION; }
 
+void nf_copy_row(const void* source, void* dst, size_t bytes) {
+  if (!bytes) return;
+  // Pageable host memory the runtime has never seen reports cudaMemoryTypeUnregistered.
+  cudaPointerAttributes a{}, b{};
+  const bool src_host = cudaPointerGetAttributes(&a, source) == cudaSuccess && a.type == cudaMemoryTypeUnregistered;
+  const bool dst_host = cudaPointerGetAttributes(&b, dst) == cudaSuccess && b.type == cudaMemoryTypeUnregistered;
+  if (src_host && dst_host) std::memcpy(dst, source, bytes);
+  else cudaMemcpy(dst, source, bytes, cudaMemcpyDefault);
+}
+
+nf_status nf_stream_create(void** stream, char* err, size_t len) {
+  if (!stream) return NF_INVALID_ARGUMENT;
+  cudaStream_t s = nullptr;
+  const cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "stream creation failed");
+  *stream = s;
+  return NF_OK;
+}
+
+void nf_stream_destroy(void* stream) {
+  if (stream) {
+    cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    cudaStreamDestroy(static_cast<cudaStream_t>(stream));
+  }
+}
+
 void nf_fft3d_config_default(nf_fft3d_config* c) {
   *c = nf_fft3d_config{};
   c->bw = 32; c->bh = 32; c->ow = -1; c->oh = -1; c->wintype = 0; c->opt = 0; c->bt = 1;

@@ -431,6 +431,7 @@ class FP64Kalman:
         n = plan.ay.count * plan.ax.count * plan.sbins
         r0 = plan.sigma_eff * plan.sigma_eff / plan.norm
         self.r0 = r0
+        self.ambiguous = 0  # motion-test decisions within binary32 rounding of the threshold
         self.last = np.zeros(n, np.complex128)
         self.cov = np.full(n, r0)
         self.proc = np.full(n, r0)
@@ -447,6 +448,10 @@ class FP64Kalman:
         thr = r * p.kratio2
         d = X - self.last
         reset = (d.real ** 2 > thr) | (d.imag ** 2 > thr)
+        # decisions a binary32 evaluation can take the other way: a squared difference
+        # within 1e-5 (relative) of the threshold
+        near = (np.abs(d.real ** 2 - thr) <= 1e-5 * thr) | (np.abs(d.imag ** 2 - thr) <= 1e-5 * thr)
+        self.ambiguous += int(near.sum())
         if p.table is None and self.r0 == 0:
             reset[:] = True
         s = self.cov + self.proc

@@ -5,6 +5,7 @@
 #include "neo_fft_b200/checkpoints.hpp"
 #include "neo_fft_b200/plan.hpp"
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <vector>
@@ -29,6 +30,27 @@ int main() {
   span2d::Plane<std::uint16_t> d(dst.data(), w, h, w * 2);
   plan.process_at<std::uint16_t>({&s, 1}, d, 0, 0, {}, static_cast<runtime::SpectraCache*>(nullptr));
   std::printf("dft %llu\n", (unsigned long long)fnv(dst.data(), dst.size() * 2));
+  // the Workspace& overloads and the plan's pool (plan.hpp:62-75, 98): two leases at once,
+  // one idle workspace kept afterwards (tests/unit/execution.cpp:15-18 checks the same)
+  {
+    auto& pool = plan.workspace_pool();
+    std::printf("pool_capacity %zu\n", pool.max_capacity());
+    {
+      auto one = pool.acquire(), two = pool.acquire();
+      std::printf("pool_active %zu\n", pool.active_count());
+      std::fill(dst.begin(), dst.end(), std::uint16_t(0));
+      plan.process<std::uint16_t>(s, d, *one);
+      std::printf("dft_ws %llu\n", (unsigned long long)fnv(dst.data(), dst.size() * 2));
+      std::fill(dst.begin(), dst.end(), std::uint16_t(0));
+      plan.process<std::uint16_t>({&s, 1}, d, *two);
+      std::printf("dft_ws_span %llu\n", (unsigned long long)fnv(dst.data(), dst.size() * 2));
+    }
+    std::printf("pool_idle %zu pool_budget %zu\n", pool.idle_count(), pool.budget().total_bytes);
+    // copy_row() copies a host row (filter.hpp passes it to PackedROI)
+    std::vector<std::uint16_t> row(static_cast<std::size_t>(w));
+    plan.copy_row()(src.data() + std::size_t(w) * 5, row.data(), std::size_t(w) * 2);
+    std::printf("copy_row %d\n", int(std::equal(row.begin(), row.end(), src.begin() + std::size_t(w) * 5)));
+  }
 
   FFT3DConfig k;
   k.bt = 0; k.sigma = 2.5f; k.kratio = 2.0f; k.bw = k.bh = 16;

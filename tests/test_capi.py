@@ -64,6 +64,28 @@ def _build_facade_check():
     return exe
 
 
+def build_roi_facade_check(reference):
+    """The reference host layer's src/plugin/roi.hpp, unchanged, compiled against the facade
+    (tests/native/roi_facade_check.cpp); the binary is kept in tests/_build for the GPU test."""
+    import subprocess
+    exe = ROOT / "tests" / "_build" / "roi_facade_check"
+    exe.parent.mkdir(exist_ok=True)
+    subprocess.run(["g++", "-std=c++17", "-O1", f"-I{ROOT / 'tests' / 'native' / 'shim'}", f"-I{reference / 'src'}",
+                    f"-I{ROOT / 'include'}", f"-I{ROOT / 'oracle' / 'shim'}",
+                    str(ROOT / "tests" / "native" / "roi_facade_check.cpp"), "-o", str(exe),
+                    f"-L{ROOT / 'neo_fft_b200'}", "-lneofft_b200", f"-Wl,-rpath,{ROOT / 'neo_fft_b200'}"], check=True)
+    return exe
+
+
+def test_reference_roi_code_compiles_against_facade():
+    """filter.hpp's ROI calls (PackedROI with plan->copy_row(), process_at over packed views,
+    render_kalman and prepare_pattern through PackedROI) compile unchanged against the facade."""
+    from oracle import ref as R
+    if not (R.REFERENCE / "src" / "plugin" / "roi.hpp").exists():
+        pytest.skip("reference sources absent")
+    assert build_roi_facade_check(R.REFERENCE).exists()
+
+
 def test_cpp_facade_compiles_and_links():
     """include/neo_fft_b200/plan.hpp (the reference Plan's class signature over the
     C ABI) compiles against a span2d provider and links to the library."""
@@ -88,6 +110,10 @@ def test_cpp_facade_matches_python_path(cuda):
             v = ((v ^ c) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
         return v
     assert int(got["dft"]) == fnv(dst.tobytes())
+    assert int(got["dft_ws"]) == int(got["dft_ws_span"]) == int(got["dft"])
+    assert got["pool_capacity"] == "1" and got["pool_active"] == "2"
+    assert got["pool_idle"].split()[0] == "1" and int(got["pool_idle"].split()[2]) == 2 * w * h * 2
+    assert got["copy_row"] == "1"
     assert got["error"] == "FFT3D bt outside -1..5"
     fsrc = ((np.arange(w * h) * 7919) % 1000 / 1000.0).astype(np.float32).reshape(h, w)
     kp = Plan(w, h, SampleFormat(32, True), FFT3DConfig(bw=16, bh=16, bt=0, sigma=2.5, kratio=2.0))

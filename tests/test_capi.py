@@ -68,12 +68,15 @@ def build_roi_facade_check(reference):
     """The reference host layer's src/plugin/roi.hpp, unchanged, compiled against the facade
     (tests/native/roi_facade_check.cpp); the binary is kept in tests/_build for the GPU test."""
     import subprocess
-    exe = ROOT / "tests" / "_build" / "roi_facade_check"
+    # kept beside its source (git-ignored, but shipped with the tree to GPU hosts, which
+    # have no reference sources to build it from)
+    exe = ROOT / "tests" / "native" / "_bin" / "roi_facade_check"
     exe.parent.mkdir(exist_ok=True)
     subprocess.run(["g++", "-std=c++17", "-O1", f"-I{ROOT / 'tests' / 'native' / 'shim'}", f"-I{reference / 'src'}",
                     f"-I{ROOT / 'include'}", f"-I{ROOT / 'oracle' / 'shim'}",
                     str(ROOT / "tests" / "native" / "roi_facade_check.cpp"), "-o", str(exe),
-                    f"-L{ROOT / 'neo_fft_b200'}", "-lneofft_b200", f"-Wl,-rpath,{ROOT / 'neo_fft_b200'}"], check=True)
+                    f"-L{ROOT / 'neo_fft_b200'}", "-lneofft_b200", "-Wl,-rpath,$ORIGIN/../../../neo_fft_b200"],
+                   check=True)
     return exe
 
 

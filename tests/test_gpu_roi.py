@@ -51,12 +51,12 @@ def test_interlaced_roi_filtering_matches_reference(cuda, ref, fmt, cfg):
 
 def test_reference_roi_code_through_facade(cuda, ref, tmp_path):
     """The reference host layer's ROI code (src/plugin/roi.hpp, compiled unchanged against the
-    facade by tests/test_capi.py into tests/_build/roi_facade_check) on an interlaced ROI:
+    facade by tests/test_capi.py into tests/native/_bin/roi_facade_check) on an interlaced ROI:
     FFT3D bt=3, Kalman render and the sampled-pattern filter each equal the reference core
     on the host-packed image, written back in the ROI's row order."""
     import subprocess
     from pathlib import Path
-    exe = Path(__file__).resolve().parent / "_build" / "roi_facade_check"
+    exe = Path(__file__).resolve().parent / "native" / "_bin" / "roi_facade_check"
     if not exe.exists():
         pytest.skip("roi_facade_check not built (needs the reference sources at build time)")
     W, H = 160, 120

@@ -342,8 +342,12 @@ nf_status nf_roi_unpack_device(const nf_roi* roi, nf_const_plane packed, nf_plan
  * already calibrated: the threshold the Wiener gain compares with) in device memory.
  * nf_plan_set_primary replaces it from device memory on `stream`, so a training loop
  * can learn it; a plan without sigma curves starts from its uniform value, which
- * nf_plan_get_primary copies out. Replacing the table changes the plan: calls on
- * other streams that use the plan must be ordered with the replacement. */
+ * nf_plan_get_primary copies out. FFT3D plans with bt=1 (no Kalman, no sampled pattern,
+ * no preview) keep a per-bin noise table a ([bh][bw/2+1]: sigma^2/norm when sigma is
+ * uniform, else the sigma profile) the same way; once replaced, per-call launches
+ * filter with it (batches built earlier keep the previous filter). Replacing the table
+ * changes the plan: calls on other streams that use the plan must be ordered with the
+ * replacement. */
 nf_status nf_plan_set_primary(nf_plan* plan, const float* table_device, int count, void* stream, char* err,
                               size_t err_len);
 nf_status nf_plan_get_primary(const nf_plan* plan, float* table_device, int count, void* stream, char* err,
@@ -358,6 +362,21 @@ nf_status nf_dft_backward_scratch_bytes(const nf_plan* plan, int nplanes, size_t
 nf_status nf_dft_backward_device(const nf_plan* plan, const nf_const_plane* sources, const nf_const_plane* grad_out,
                                  const nf_plane* grad_sources, int nplanes, float* grad_primary, void* scratch,
                                  size_t scratch_bytes, void* stream, char* err, size_t err_len);
+
+/* Backward of nf_plan_process_device for float FFT3D plans with bt=1 (no Kalman, no
+ * sampled pattern, no preview) whose sharpen/dehalo factors are fused into the Wiener
+ * gain (uniform sigma, or no enhancement): gradients of sum(grad_out * output) for the
+ * source pixels and the per-bin noise table a of the gain max((q - a)/q, floor)
+ * (kernels/scalar/spectral.cpp:18-22; enhancement fft3d_profile.cpp:69-81). The noise
+ * table is read and replaced with nf_plan_get_primary/nf_plan_set_primary (bins values).
+ * `outputs` are the forward outputs (the float output is clamped to [0, 1], and the
+ * gradient passes only where it lies strictly inside). Scratch as nf_dft_backward_device
+ * (nf_dft_backward_scratch_bytes bytes); at most 32 planes per call. No counterpart in
+ * the reference (it has no gradients). */
+nf_status nf_fft3d_backward_device(const nf_plan* plan, const nf_const_plane* sources, const nf_const_plane* outputs,
+                                   const nf_const_plane* grad_out, const nf_plane* grad_sources, int nplanes,
+                                   float* grad_primary, void* scratch, size_t scratch_bytes, void* stream, char* err,
+                                   size_t err_len);
 
 /* Allocation-free backward: nf_dft_backward_device with its scratch in a fixed
  * 16 MiB device buffer inside the library (one per device) instead of a caller

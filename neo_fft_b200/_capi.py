@@ -150,6 +150,9 @@ PROTOTYPES = {
     "nf_dft_backward_device": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfConstPlane),
                                        ctypes.POINTER(NfPlane), c_int, c_void_p, c_void_p, c_size_t, c_void_p,
                                        ctypes.c_char_p, c_size_t]),
+    "nf_fft3d_backward_device": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfConstPlane),
+                                         ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfPlane), c_int, c_void_p,
+                                         c_void_p, c_size_t, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_dft_backward_static_capacity": (c_size_t, []),
     "nf_dft_backward_device_static": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfConstPlane),
                                               ctypes.POINTER(NfPlane), c_int, c_void_p, c_void_p, ctypes.c_char_p,

@@ -1,4 +1,5 @@
-"""Differentiable DFTTest (tbsize=1, smode=1, float planes, ftype 0/1/2) for PyTorch.
+"""Differentiable DFTTest (tbsize=1, smode=1, float planes, ftype 0/1/2) and FFT3D (bt=1,
+float planes, sharpen/dehalo fused into the gain) for PyTorch.
 
 `DFTTestFunction.apply(x, table, plan)` filters a batch of float32 CUDA planes
 x[B, H, W] with the primary table `table` (the per-bin threshold the Wiener gain
@@ -7,7 +8,12 @@ respect to both. Forward runs the sm_100a strip kernel over up to 32 planes per 
 identical to `Plan.process`); backward runs the hand-written adjoint kernels through the C ABI
 (nf_dft_backward_device), recomputing block spectra instead of storing them.
 
-`SigmaTableDenoiser` wraps it as a module with a learnable table; in data-parallel
+`FFT3DFunction.apply(x, table, plan)` does the same for an FFT3D plan, whose table is the
+per-bin noise power a of the Wiener gain max((q - a)/q, floor) (a uniform-sigma plan starts
+from sigma^2/norm in every bin); its backward (nf_fft3d_backward_device) also takes the
+forward output, because the float output is clamped to [0, 1].
+
+`SigmaTableDenoiser` wraps either as a module with a learnable table; in data-parallel
 training its table gradient is all-reduced once per step (`allreduce_table_grad`).
 """
 from __future__ import annotations
@@ -17,7 +23,7 @@ import ctypes
 import torch
 
 from . import _capi as C
-from .plan import DFTConfig, Plan, SampleFormat
+from .plan import DFTConfig, FFT3DConfig, Plan, SampleFormat
 
 
 def _set_primary(plan: Plan, table: torch.Tensor, stream) -> torch.Tensor:
@@ -85,15 +91,67 @@ class DFTTestFunction(torch.autograd.Function):
         return gx, gtab.to(table.dtype).view_as(table), None
 
 
-class SigmaTableDenoiser(torch.nn.Module):
-    """DFTTest with a learnable per-frequency table (sbsize x (sbsize//2+1))."""
+class FFT3DFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x: torch.Tensor, table: torch.Tensor, plan: Plan):
+        if x.dim() != 3 or x.dtype != torch.float32 or not x.is_cuda:
+            raise ValueError("x must be a float32 CUDA tensor [batch, height, width]")
+        x = x.contiguous()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        keep = _set_primary(plan, table, stream)
+        out = torch.empty_like(x)
+        err = ctypes.create_string_buffer(256)
+        for start in range(0, x.shape[0], 32):
+            n = min(32, x.shape[0] - start)
+            C.raise_for(plan._lib.nf_plan_process_planes_device(plan._h, _plane_array(x, start, n, True),
+                                                                _plane_array(out, start, n, False), n, stream,
+                                                                err, 256), err.value)
+        ctx.save_for_backward(x, keep, out)
+        ctx.plan = plan
+        return out
 
-    def __init__(self, width: int, height: int, config: DFTConfig, initial: torch.Tensor | None = None):
+    @staticmethod
+    def backward(ctx, gout: torch.Tensor):
+        x, table, out = ctx.saved_tensors
+        plan: Plan = ctx.plan
+        gout = gout.contiguous()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        keep = _set_primary(plan, table, stream)  # noqa: F841 (kept alive until the launch is enqueued)
+        gx = torch.empty_like(x)
+        lib = plan._lib
+        err = ctypes.create_string_buffer(256)
+        nb = x.shape[0]
+        chunks = [(s0, min(32, nb - s0)) for s0 in range(0, nb, 32)]
+        parts = torch.empty((len(chunks), table.numel()), dtype=torch.float32, device=x.device)
+        need = ctypes.c_size_t()
+        lib.nf_dft_backward_scratch_bytes(plan._h, chunks[0][1], ctypes.byref(need))
+        scratch = torch.empty(max(1, need.value), dtype=torch.uint8, device=x.device)
+        for c, (start, n) in enumerate(chunks):
+            st = lib.nf_fft3d_backward_device(plan._h, _plane_array(x, start, n, True), _plane_array(out, start, n, True),
+                                              _plane_array(gout, start, n, True), _plane_array(gx, start, n, False), n,
+                                              ctypes.c_void_p(parts[c].data_ptr()),
+                                              ctypes.c_void_p(scratch.data_ptr()), need.value, stream, err, 256)
+            C.raise_for(st, err.value)
+        gtab = parts[0] if len(chunks) == 1 else parts.sum(0)
+        return gx, gtab.to(table.dtype).view_as(table), None
+
+
+class SigmaTableDenoiser(torch.nn.Module):
+    """DFTTest or FFT3D with a learnable per-frequency table: DFTTest's threshold table
+    (sbsize x (sbsize//2+1)) or FFT3D's noise power table (bh x (bw//2+1))."""
+
+    def __init__(self, width: int, height: int, config, initial: torch.Tensor | None = None):
         super().__init__()
-        if config.tbsize != 1 or config.mode != 1 or config.ftype not in (0, 1, 2):
-            raise ValueError("differentiable DFTTest needs tbsize=1, smode=1 and ftype 0, 1 or 2")
+        self.fft3d = isinstance(config, FFT3DConfig)
+        if self.fft3d:
+            if config.bt != 1 or config.pfactor > 0 or config.pshow:
+                raise ValueError("differentiable FFT3D needs bt=1 without pattern sampling or preview")
+            k = config.bh * (config.bw // 2 + 1)
+        else:
+            if config.tbsize != 1 or config.mode != 1 or config.ftype not in (0, 1, 2):
+                raise ValueError("differentiable DFTTest needs tbsize=1, smode=1 and ftype 0, 1 or 2")
+            k = config.block * (config.block // 2 + 1)
         self.plan = Plan(width, height, SampleFormat(32, True), config)
-        k = config.block * (config.block // 2 + 1)
         if initial is None:
             initial = torch.empty(k, dtype=torch.float32, device="cuda")
             err = ctypes.create_string_buffer(256)
@@ -103,7 +161,7 @@ class SigmaTableDenoiser(torch.nn.Module):
         self.table = torch.nn.Parameter(initial.clone().float().cuda())
 
     def forward(self, x: torch.Tensor) -> torch.Tensor:
-        return DFTTestFunction.apply(x, self.table, self.plan)
+        return (FFT3DFunction if self.fft3d else DFTTestFunction).apply(x, self.table, self.plan)
 
 
 def shard(n: int, rank: int, world: int) -> range:

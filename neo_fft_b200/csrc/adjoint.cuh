@@ -1,6 +1,8 @@
-// Adjoint (backward) of the single-frame DFTTest pipeline for float planes
-// (tbsize=1, smode=1, ftype 0/1/2, zmean on or off), with respect to the source
-// pixels and to the per-bin primary table A (the learnable sigma table).
+// Adjoint (backward) of the single-frame pipelines for float planes, with respect to
+// the source pixels and to the per-bin primary table A (the learnable sigma table):
+// DFTTest (tbsize=1, smode=1, ftype 0/1/2, zmean on or off) and FFT3D (bt=1: Wiener
+// gain with the beta floor, degrid template, sharpen/dehalo fused into the gain, output
+// clamped to [0, 1]).
 //
 // Forward per block (src/algorithms/plan.cpp:538-607, kernels/scalar/spectral.cpp):
 //   v = 255*s (decode), b = v*h, X = r2c(b), g = mean*Re X0 / Re G0, M = g*G,
@@ -14,9 +16,14 @@
 //            dA += <dY,R>*dgain/dA; dg = sum_k <dM_k, G_k>; dX0.re += dg*mean/Re G0
 //   db = c2r_unnormalised(dX')        adjoint of r2c (dX' halves interior columns)
 //   dv = db*h -> d_cover (ordered gather, like the forward overlap-add)
+// FFT3D differs only in the windows and the gain (src/algorithms/plan.cpp:432-537,
+// kernels/scalar/spectral.cpp:18-22, algorithms/fft3d_profile.cpp:69-81):
+//   b = (v*wy)*wx, gain = max((q - A)/q, floor) * S(q) * D(q) with q = p + 1e-15,
+//   acc += (y*wxs)*wys, out = clamp(acc, 0, 1): the upstream gradient passes only where
+//   the forward output lies strictly inside (0, 1).
 // A second kernel folds the cover gradient onto the source through the single
-// reflection and multiplies by 255; a third reduces the per-tile table gradients
-// in a fixed order. Every sum has a fixed order, so gradients are deterministic.
+// reflection and multiplies by the decode scale; a third reduces the per-tile table
+// gradients in a fixed order. Every sum has a fixed order, so gradients are deterministic.
 #pragma once
 #include "tile_spatial.cuh"
 
@@ -35,6 +42,8 @@ struct AdjointJob {
   long long gout_stride;
   float* dcov;          // scratch: cover-plane gradient [cover_h][cover_w]
   float* partial;       // scratch: per-tile table gradients [tiles][bins]
+  const float* fwd;     // FFT3D: the forward output plane (clamp mask); nullptr for DFTTest
+  long long fwd_stride;
 };
 
 __host__ __device__ inline size_t adjoint_smem_bytes(int bh, int bw, const AdjointShape& s) {
@@ -46,13 +55,13 @@ __host__ __device__ inline size_t adjoint_smem_bytes(int bh, int bw, const Adjoi
 }
 
 // Per-bin backward of spectral_bin for ftype 0 (Wiener, any exponent), 1 (hard
-// threshold) and 2 (constant gain). x: forward spectrum bin; dy: incoming complex
-// gradient. Returns dX; adds the template gradient to dg and the table gradient to da.
-// FT >= 0 fixes the ftype at compile time.
-template <int FT = -1>
+// threshold), 2 (constant gain) and -1 (FFT3D Wiener with floor, enhancement fused).
+// x: forward spectrum bin; dy: incoming complex gradient. Returns dX; adds the template
+// gradient to dg and the table gradient to da. FT fixes the type at compile time.
+template <int FT>
 __device__ __forceinline__ cf spectral_bin_adjoint(cf x, cf dy, const cf* grid, int k, float g, const DevSpectral& p,
                                                    float& dg, float& da) {
-  const int type = FT >= 0 ? FT : p.type;
+  const int type = FT;
   const float a = p.primary ? p.primary[k] : p.a;
   const float mr = grid ? g * grid[k].r : 0.0f;
   const float mi = grid ? g * grid[k].i : 0.0f;
@@ -77,6 +86,41 @@ __device__ __forceinline__ cf spectral_bin_adjoint(cf x, cf dy, const cf* grid, 
       dgain_dp = dw * (a + 1e-15f) / (q * q);
       dgain_da = -dw / q;
     }
+  } else if (type == -1) {
+    // wiener = max((q - a)/q, floor); the ratio wins ties, as in the forward
+    const float q = power + 1e-15f;
+    const float r = (q - a) / q;
+    float w = p.floor, dw_dq = 0.0f, dw_da = 0.0f;
+    if (!(r < p.floor)) {
+      w = r;
+      dw_dq = a / (q * q);
+      dw_da = -1.0f / q;
+    }
+    float e = 1.0f, de_dq = 0.0f;
+    if (p.enh) {  // S(q) * D(q) and its derivative (fft3d_profile.cpp:69-81)
+      float sv = 1.0f, ds = 0.0f, dv = 1.0f, dd = 0.0f;
+      if (p.sharpen != 0.0f && p.eb != 0.0f) {
+        const float qa = q + p.ea, qb = q + p.eb;
+        const float u = q * p.eb / (qa * qb);
+        const float str = p.sharpen * p.sharpen_w[k];
+        const float su = sqrtf(u);
+        sv = 1.0f + str * su;
+        // du/dq = eb (ea eb - q^2) / ((q+ea)(q+eb))^2
+        const float du = p.eb * (p.ea * p.eb - q * q) / ((qa * qb) * (qa * qb));
+        ds = su > 0.0f ? str * du / (2.0f * su) : 0.0f;
+      }
+      if (p.dehalo != 0.0f) {
+        const float hd = p.dehalo * p.halo_w[k];
+        const float qc = q + p.ec, den = qc + hd * q;
+        dv = qc / den;
+        dd = -hd * p.ec / (den * den);
+      }
+      e = sv * dv;
+      de_dq = ds * dv + sv * dd;
+    }
+    gain = w * e;
+    dgain_dp = dw_dq * e + w * de_dq;
+    dgain_da = dw_da * e;
   } else if (type == 1) {
     gain = power < a ? 0.0f : 1.0f;
   } else {
@@ -91,9 +135,11 @@ __device__ __forceinline__ cf spectral_bin_adjoint(cf x, cf dy, const cf* grid, 
   return dr;
 }
 
-template <int BHC, int BWC>
+// ALGO: 0 FFT3D, 1 DFTTest.
+template <int BHC, int BWC, int ALGO>
 __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob& J, const AdjointShape& S, int tile,
                                              float* smem) {
+  constexpr bool kFft3d = ALGO == 0;
   const int BH = BHC > 0 ? BHC : P.bh;
   const int BW = BWC > 0 ? BWC : P.bw;
   const int K = BW / 2 + 1;
@@ -144,14 +190,26 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     off += n;
     return d;
   };
-  const float* h = stage(P.h, BH * BW);
-  const float* hsyn = stage(P.hsyn, BH * BW);
+  const float *h = nullptr, *hsyn = nullptr, *wxa = nullptr, *wya = nullptr, *wxs = nullptr, *wys = nullptr;
+  if constexpr (kFft3d) {
+    wxa = stage(P.wxa, BW);
+    wya = stage(P.wya, BH);
+    wxs = stage(P.wxs, BW);
+    wys = stage(P.wys, BH);
+  } else {
+    h = stage(P.h, BH * BW);
+    hsyn = stage(P.hsyn, BH * BW);
+  }
   const cf* grid = P.grid ? reinterpret_cast<const cf*>(stage(reinterpret_cast<const float*>(P.grid), 2 * bins)) : nullptr;
   __shared__ DevSpectral s_filt;
   const float* prim = P.filt.primary ? stage(P.filt.primary, bins) : nullptr;
+  const float* shw = kFft3d && P.filt.enh && P.filt.sharpen_w ? stage(P.filt.sharpen_w, bins) : nullptr;
+  const float* hlw = kFft3d && P.filt.enh && P.filt.halo_w ? stage(P.filt.halo_w, bins) : nullptr;
   if (tid == 0) {
     s_filt = P.filt;
     if (prim) s_filt.primary = prim;
+    if (shw) s_filt.sharpen_w = shw;
+    if (hlw) s_filt.halo_w = hlw;
   }
   for (int i = tid; i < BH * S.tw; i += nthr) acc[i] = 0.0f;
   for (int i = tid; i < bins; i += nthr) da_tile[i] = 0.0f;
@@ -183,9 +241,15 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
       ring[size_t(cy % BH) * S.ring_pitch + xx] = srow[reflect_axis(cx, gx)] * P.dec_scale;
       const int py = cy - gy.offset, px = cx - gx.offset;
       float gv = 0.0f;
-      if (py >= 0 && py < gy.length && px >= 0 && px < gx.length)
+      if (py >= 0 && py < gy.length && px >= 0 && px < gx.length) {
         gv = reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(J.gout) +
                                             ptrdiff_t(py) * J.gout_stride)[px] * out_scale;
+        if constexpr (kFft3d) {  // out = clamp(acc, 0, 1)
+          const float y = reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(J.fwd) +
+                                                         ptrdiff_t(py) * J.fwd_stride)[px];
+          if (!(y > 0.0f && y < 1.0f)) gv = 0.0f;
+        }
+      }
       gring[size_t(cy % BH) * S.ring_pitch + xx] = gv;
     }
     __syncthreads();
@@ -196,7 +260,12 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
       float row[CAPW];
 #pragma unroll UW
       for (int x = 0; x < CAPW; ++x)
-        if (x < BW) row[x] = which ? in[x] * hsyn[y * BW + x] : fmul(in[x], h[y * BW + x]);
+        if (x < BW) {
+          if constexpr (kFft3d)  // the forward's (v*wy)*wx; the synthesis weight wxs*wys
+            row[x] = which ? in[x] * (wxs[x] * wys[y]) : fmul(fmul(in[x], wya[y]), wxa[x]);
+          else
+            row[x] = which ? in[x] * hsyn[y * BW + x] : fmul(in[x], h[y * BW + x]);
+        }
       nf::row_forward<BWC>(row, BW, (which ? gspec : spec) + size_t(y) * K * NB + b, P.tww, codelet, NB);
     }
     __syncthreads();
@@ -239,7 +308,8 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
               da_blk[size_t(y * K + k) * NBp + b] = own ? da : 0.0f;
             }
         };
-        if (filt.type == 0) adjoint_column(std::integral_constant<int, 0>{});
+        if constexpr (kFft3d) adjoint_column(std::integral_constant<int, -1>{});
+        else if (filt.type == 0) adjoint_column(std::integral_constant<int, 0>{});
         else if (filt.type == 1) adjoint_column(std::integral_constant<int, 1>{});
         else adjoint_column(std::integral_constant<int, 2>{});
         dg_part[size_t(b) * K + k] = dg;
@@ -284,7 +354,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
       float* o = ob + (size_t(y) * NB + b) * OBW;
 #pragma unroll UW
       for (int x = 0; x < CAPW; ++x)
-        if (x < BW) o[x] = row[x] * h[y * BW + x];
+        if (x < BW) o[x] = kFft3d ? row[x] * (wya[y] * wxa[x]) : row[x] * h[y * BW + x];
     }
     __syncthreads();
     // ---- ordered gather into the cover-gradient ring; retire rows -------------
@@ -342,12 +412,20 @@ template <int BHC, int BWC>
 __global__ void __launch_bounds__(256, 2) dft_adjoint_kernel(DevPlan P, AdjointShape S, AdjointBatch B) {
   extern __shared__ float smem[];
   const int tiles = S.tiles_x * S.tiles_y;
-  adjoint_tile<BHC, BWC>(P, B.job[blockIdx.x / tiles], S, blockIdx.x % tiles, smem);
+  adjoint_tile<BHC, BWC, 1>(P, B.job[blockIdx.x / tiles], S, blockIdx.x % tiles, smem);
+}
+
+template <int BHC, int BWC>
+__global__ void __launch_bounds__(256, 2) fft3d_adjoint_kernel(DevPlan P, AdjointShape S, AdjointBatch B) {
+  extern __shared__ float smem[];
+  const int tiles = S.tiles_x * S.tiles_y;
+  adjoint_tile<BHC, BWC, 0>(P, B.job[blockIdx.x / tiles], S, blockIdx.x % tiles, smem);
 }
 
 #ifdef NF_ADJOINT_AUX_KERNELS  // defined by the one unit that launches them (nf_api.cu)
 // Source gradient: each source pixel gathers the cover positions that reflect onto
-// it (single reflection per axis, ascending cover row then column) times 255.
+// it (single reflection per axis, ascending cover row then column) times the decode
+// scale (255 for DFTTest, 1 for FFT3D).
 __global__ void dft_adjoint_fold_kernel(DevPlan P, AdjointBatch B) {
   const AdjointJob& J = B.job[blockIdx.z];
   const DevAxis gx = P.gx, gy = P.gy;

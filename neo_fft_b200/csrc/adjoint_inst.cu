@@ -1,4 +1,5 @@
-// Instantiates the DFTTest adjoint for one block shape (NF_BH x NF_BW, 0 = runtime).
+// Instantiates the DFTTest and FFT3D adjoints for one block shape (NF_BH x NF_BW,
+// 0 = runtime).
 #include "adjoint.cuh"
 #include "launch.hpp"
 
@@ -11,7 +12,7 @@ namespace nfd {
 #define NF_DEFINE_(BH, BW)                                                                                        \
   cudaError_t launch_adjoint_##BH##x##BW(const DevPlan& d, const AdjointShape& S, const AdjointBatch& b,          \
                                          size_t smem, cudaStream_t st) {                                         \
-    auto k = dft_adjoint_kernel<BH, BW>;                                                                         \
+    auto k = d.algo == 0 ? fft3d_adjoint_kernel<BH, BW> : dft_adjoint_kernel<BH, BW>;                         \
     const cudaError_t e = set_smem_limit(k, smem);                                                              \
     if (e != cudaSuccess) return e;                                                                              \
     k<<<b.n * S.tiles_x * S.tiles_y, 256, smem, st>>>(d, S, b);                                                  \

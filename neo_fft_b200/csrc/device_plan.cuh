@@ -99,19 +99,26 @@ NF_HD float enhancement_gain(float q, int k, const DevSpectral& e) {
   return fmul(s, d);
 }
 
+// Compile-time filter codes beyond the types: DFTTest ftype 0 with its exponent mode
+// fixed as well (the Wiener ratio, its square root, its power), so the common ratio
+// path carries no square-root or power code.
+constexpr int kFt0Ratio = 10, kFt0Sqrt = 11, kFt0Pow = 12;
+
 // One bin of spectral_prevalidated: residual against the scaled template, gain
 // by type, optional enhancement, restore the template. Returns the new bin and
 // flags non-finite intermediates through `bad`.
-// FT >= 0 fixes the filter type at compile time (a DFTTest ftype: no enhancement).
+// FT >= 0 fixes the filter type at compile time (a DFTTest ftype: no enhancement;
+// kFt0Ratio..kFt0Pow fix ftype 0's exponent mode too).
 template <int FT = -3>
 NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectral& p, bool& bad) {
+  constexpr int kType = FT >= kFt0Ratio ? 0 : FT;
   const float a = p.primary ? p.primary[k] : p.a;
   const float mr = grid ? fmul(scale, grid[k].r) : 0.0f;
   const float mi = grid ? fmul(scale, grid[k].i) : 0.0f;
   const float re = fsub(x.r, mr), im = fsub(x.i, mi);
   const float power = fadd(fmul(re, re), fmul(im, im));
   float gain = 0.0f;
-  switch (FT >= -2 ? FT : p.type) {
+  switch (kType >= -2 ? kType : p.type) {
     case -2:
       gain = 1.0f;
       break;
@@ -124,8 +131,9 @@ NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectra
     case 0: {
       const float r = fdiv(fsub(power, a), fadd(power, 1e-15f));
       const float wiener = r < 0.0f ? 0.0f : r;
-      if (p.emode == 0) gain = wiener;
-      else if (p.emode == 1) gain = fsqrt(wiener);
+      const int em = FT >= kFt0Ratio ? FT - kFt0Ratio : p.emode;
+      if (em == 0) gain = wiener;
+      else if (em == 1) gain = fsqrt(wiener);
       else gain = powf(wiener, p.exponent);
       break;
     }

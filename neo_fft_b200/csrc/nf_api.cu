@@ -37,6 +37,7 @@ struct nf_plan {
   void* tables = nullptr;  // one device allocation holding every table
   int* err = nullptr;      // device error word
   int device = 0;
+  float* learn = nullptr;  // FFT3D bt=1: replaceable per-bin noise table (inside `tables`)
   mutable std::mutex staging_mu;
   mutable void* staging = nullptr;  // device staging for the host-memory path
   mutable size_t staging_bytes = 0;
@@ -313,6 +314,20 @@ void temporal_twiddles(int T, int c, std::vector<cf>& fwd, std::vector<cf>& inv)
 // DFTTest plans always carry a device primary table so it can be replaced
 // (nf_plan_set_primary); without sigma curves it holds the uniform value a, which
 // gives the same per-bin arithmetic as the uniform path.
+// FFT3D bt=1 denoising plans (no Kalman, no sampled pattern, no preview) keep a per-bin
+// noise table that nf_plan_set_primary can replace (the learnable table of the
+// differentiable FFT3D): the profile table of varying sigmas, or the uniform value a.
+// Until it is replaced the plan filters with its own table or uniform value.
+bool fft3d_learnable(const nfb::PlanTables& t) {
+  return t.algo == nfb::Algo::FFT3D && t.temporal_size == 1 && t.denoise && !t.kalman && !t.needs_pattern &&
+         !t.preview;
+}
+std::vector<float> learn_table(const nfb::PlanTables& t) {
+  if (!fft3d_learnable(t)) return {};
+  if (!t.spectral.primary.empty()) return t.spectral.primary;
+  return std::vector<float>(size_t(t.bins), t.spectral.a);
+}
+
 std::vector<float> primary_table(const nfb::PlanTables& t) {
   if (t.algo == nfb::Algo::FFT3D && t.needs_pattern) return std::vector<float>(size_t(t.bins), 0.0f);
   if (t.algo != nfb::Algo::DFTTest || !t.spectral.primary.empty()) return t.spectral.primary;
@@ -329,7 +344,7 @@ nf_status finalize_plan(std::unique_ptr<nf_plan>& p, char* err, size_t len) {
   temporal_twiddles(std::max(1, t.temporal_size), t.temporal_size / 2, tfwd, tinv);
   const size_t o_wxa = blob.add(t.wx.analysis), o_wya = blob.add(t.wy.analysis), o_wxs = blob.add(t.wx.synthesis),
                o_wys = blob.add(t.wy.synthesis), o_h = blob.add(t.h), o_hs = blob.add(t.h_synthesis),
-               o_grid = blob.add(t.grid), o_prim = blob.add(primary_table(t)),
+               o_grid = blob.add(t.grid), o_prim = blob.add(primary_table(t)), o_learn = blob.add(learn_table(t)),
                o_sw = blob.add(t.enhancement.sharpen_window), o_hw = blob.add(t.enhancement.halo_window),
                o_twh = blob.add(twh), o_tww = blob.add(tww), o_twt = blob.add(twt), o_tf = blob.add(tfwd),
                o_ti = blob.add(tinv);
@@ -402,6 +417,7 @@ nf_status finalize_plan(std::unique_ptr<nf_plan>& p, char* err, size_t len) {
   d.noise_mult = float(t.temporal_size);
   d.kalman_r0 = t.kalman_r0;
   d.kalman_ratio2 = t.kalman_ratio2;
+  p->learn = static_cast<float*>(const_cast<void*>(ptr(o_learn)));
   return NF_OK;
 }
 
@@ -2460,11 +2476,17 @@ nf_status nf_roi_unpack_device(const nf_roi* roi, nf_const_plane packed, nf_plan
 nf_status nf_plan_set_primary(nf_plan* p, const float* table, int count, void* stream, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(p && table, "null plan or table");
-    nfb::require(p->t.algo == nfb::Algo::DFTTest, "primary tables are replaceable on DFTTest plans only");
-    nfb::require(count == p->t.temporal_size * p->t.bins, "primary table shape mismatch");
-    const cudaError_t e = cudaMemcpyAsync(const_cast<float*>(p->dev.filt.primary), table, size_t(count) * sizeof(float),
-                                          cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
+    const bool fft3d = p->t.algo == nfb::Algo::FFT3D;
+    nfb::require(!fft3d || p->learn,
+                 "primary tables are replaceable on DFTTest plans and FFT3D bt=1 plans without Kalman or pattern");
+    nfb::require(count == (fft3d ? p->t.bins : p->t.temporal_size * p->t.bins), "primary table shape mismatch");
+    float* dst = fft3d ? p->learn : const_cast<float*>(p->dev.filt.primary);
+    const cudaError_t e = cudaMemcpyAsync(dst, table, size_t(count) * sizeof(float), cudaMemcpyDeviceToDevice,
+                                          static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(err, len, e, "table copy failed");
+    // FFT3D: calls launched from now on read the per-bin table (batches built earlier
+    // keep the plan's previous filter).
+    if (fft3d) p->dev.filt.primary = p->learn;
     return NF_OK;
   });
 }
@@ -2472,10 +2494,13 @@ nf_status nf_plan_set_primary(nf_plan* p, const float* table, int count, void* s
 nf_status nf_plan_get_primary(const nf_plan* p, float* table, int count, void* stream, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(p && table, "null plan or table");
-    nfb::require(p->t.algo == nfb::Algo::DFTTest, "primary tables are replaceable on DFTTest plans only");
-    nfb::require(count == p->t.temporal_size * p->t.bins, "primary table shape mismatch");
-    const cudaError_t e = cudaMemcpyAsync(table, p->dev.filt.primary, size_t(count) * sizeof(float),
-                                          cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
+    const bool fft3d = p->t.algo == nfb::Algo::FFT3D;
+    nfb::require(!fft3d || p->learn,
+                 "primary tables are replaceable on DFTTest plans and FFT3D bt=1 plans without Kalman or pattern");
+    nfb::require(count == (fft3d ? p->t.bins : p->t.temporal_size * p->t.bins), "primary table shape mismatch");
+    const float* src = fft3d ? p->learn : p->dev.filt.primary;
+    const cudaError_t e = cudaMemcpyAsync(table, src, size_t(count) * sizeof(float), cudaMemcpyDeviceToDevice,
+                                          static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(err, len, e, "table copy failed");
     return NF_OK;
   });
@@ -2487,6 +2512,13 @@ void check_adjoint_plan(const nf_plan& p) {
   nfb::require(t.algo == nfb::Algo::DFTTest && t.temporal_size == 1 && !t.center && t.format.floating &&
                    (t.spectral.type >= 0 && t.spectral.type <= 2),
                "backward requires a float DFTTest plan with tbsize=1, smode=1 and ftype 0, 1 or 2");
+}
+void check_fft3d_adjoint_plan(const nf_plan& p) {
+  const auto& t = p.t;
+  nfb::require(fft3d_learnable(t) && t.format.floating &&
+                   (p.dev.fft3d_mode == nfd::kWienerFused || !t.enhancement.active()),
+               "FFT3D backward requires a float plan with bt=1, no Kalman or pattern, and sharpen/dehalo fused "
+               "into the Wiener gain (uniform sigma)");
 }
 // Cover tiles of the backward: 64-pixel-wide strips (a whole number of block steps);
 // the tile height is chosen for the whole call so that the CTAs of all planes fill
@@ -2505,7 +2537,10 @@ nfd::AdjointShape adjoint_shape(const nfd::DevPlan& d, int nplanes) {
   double best = -1.0;
   for (int nbx = edge + 2; nbx <= 64; ++nbx) {
     nfd::AdjointShape S{};
-    S.tab_floats = 2 * d.bh * d.bw + (d.grid ? 2 * d.bins : 0) + d.bins;
+    // tables staged per tile: DFTTest h and h*V; FFT3D its four windows and the fused
+    // enhancement windows; both the template and the primary table
+    S.tab_floats = (d.algo == 0 ? 2 * (d.bh + d.bw) + (d.filt.enh ? 2 * d.bins : 0) : 2 * d.bh * d.bw) +
+                   (d.grid ? 2 * d.bins : 0) + d.bins;
     S.tab_floats = (S.tab_floats + 3) & ~3;
     S.tw = std::min(d.gx.cover, std::max(d.gx.step, (nbx - edge) * d.gx.step));
     S.nbx_max = (S.tw + d.bw - 1) / d.gx.step + 2;
@@ -2548,52 +2583,80 @@ nf_status nf_dft_backward_scratch_bytes(const nf_plan* p, int nplanes, size_t* b
   return NF_OK;
 }
 
+namespace {
+// The backward launch shared by both algorithms (checked by the caller): the adjoint
+// tiles, the fold onto the source and the ordered table-gradient reduction.
+nf_status run_backward(const nf_plan* p, const nf_const_plane* sources, const nf_const_plane* outputs,
+                       const nf_const_plane* grad_out, const nf_plane* grad_src, int nplanes, float* grad_primary,
+                       void* scratch, size_t scratch_bytes, void* stream, char* err, size_t len) {
+  nfb::require(nplanes > 0 && nplanes <= nfd::kAdjointMaxPlanes, "backward takes 1..32 planes per call");
+  size_t need = 0;
+  nf_dft_backward_scratch_bytes(p, nplanes, &need);
+  nfb::require(scratch && scratch_bytes >= need, "backward scratch too small");
+  auto check_plane = [&](const nf_const_plane& v) {
+    nfb::require(v.width == p->t.gx.length && v.height == p->t.gy.length, "frame dimensions differ from plan");
+    plane_extent(v.width, v.height, v.stride_bytes, 4);
+    check_pointer(v.data, 4);
+  };
+  for (int i = 0; i < nplanes; ++i) {
+    nf_plane gs = grad_src[i];
+    validate_call(*p, &sources[i], 1, nullptr, 0, gs);
+    check_plane(grad_out[i]);
+    if (outputs) check_plane(outputs[i]);
+  }
+  const nfd::DevPlan& d = p->dev;
+  const nfd::AdjointShape S = adjoint_shape(d, nplanes);
+  const size_t tiles = size_t(S.tiles_x) * S.tiles_y;
+  const size_t cov = align256(size_t(p->t.gx.cover) * p->t.gy.cover * 4), part = tiles * p->t.bins * 4;
+  auto* base = static_cast<unsigned char*>(scratch);
+  nfd::AdjointBatch B{};
+  B.n = nplanes;
+  for (int i = 0; i < nplanes; ++i) {
+    B.job[i] = {static_cast<const float*>(sources[i].data), (long long)sources[i].stride_bytes,
+                static_cast<const float*>(grad_out[i].data), (long long)grad_out[i].stride_bytes,
+                reinterpret_cast<float*>(base + size_t(i) * cov),
+                reinterpret_cast<float*>(base + size_t(nplanes) * cov + size_t(i) * part),
+                outputs ? static_cast<const float*>(outputs[i].data) : nullptr,
+                outputs ? (long long)outputs[i].stride_bytes : 0};
+    B.gsrc[i] = static_cast<float*>(grad_src[i].data);
+    B.gsrc_stride[i] = grad_src[i].stride_bytes;
+  }
+  const size_t smem = nfd::adjoint_smem_bytes(d.bh, d.bw, S);
+  nfb::require(smem <= 227 * 1024, "block size too large for the backward tile");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = (d.bh == 16 && d.bw == 16) ? nfd::launch_adjoint_16x16(d, S, B, smem, st)
+                                              : nfd::launch_adjoint_0x0(d, S, B, smem, st);
+  if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  const dim3 fb(32, 8), fg((p->t.gx.length + 31) / 32, (p->t.gy.length + 7) / 8, nplanes);
+  nfd::dft_adjoint_fold_kernel<<<fg, fb, 0, st>>>(d, B);
+  // partials of all planes are contiguous: tiles*nplanes rows of `bins`
+  nfd::dft_adjoint_reduce_kernel<<<(p->t.bins + 31) / 32, dim3(32, 32), 0, st>>>(
+      reinterpret_cast<const float*>(base + size_t(nplanes) * cov), int(tiles) * nplanes, p->t.bins, grad_primary);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  return NF_OK;
+}
+}  // namespace
+
 nf_status nf_dft_backward_device(const nf_plan* p, const nf_const_plane* sources, const nf_const_plane* grad_out,
                                  const nf_plane* grad_src, int nplanes, float* grad_primary, void* scratch,
                                  size_t scratch_bytes, void* stream, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(p && sources && grad_out && grad_src && grad_primary, "null argument");
     check_adjoint_plan(*p);
-    nfb::require(nplanes > 0 && nplanes <= nfd::kAdjointMaxPlanes, "backward takes 1..32 planes per call");
-    size_t need = 0;
-    nf_dft_backward_scratch_bytes(p, nplanes, &need);
-    nfb::require(scratch && scratch_bytes >= need, "backward scratch too small");
-    for (int i = 0; i < nplanes; ++i) {
-      nf_plane gs = grad_src[i];
-      validate_call(*p, &sources[i], 1, nullptr, 0, gs);
-      nfb::require(grad_out[i].width == p->t.gx.length && grad_out[i].height == p->t.gy.length,
-                   "frame dimensions differ from plan");
-      plane_extent(grad_out[i].width, grad_out[i].height, grad_out[i].stride_bytes, 4);
-      check_pointer(grad_out[i].data, 4);
-    }
-    const nfd::DevPlan& d = p->dev;
-    const nfd::AdjointShape S = adjoint_shape(d, nplanes);
-    const size_t tiles = size_t(S.tiles_x) * S.tiles_y;
-    const size_t cov = align256(size_t(p->t.gx.cover) * p->t.gy.cover * 4), part = tiles * p->t.bins * 4;
-    auto* base = static_cast<unsigned char*>(scratch);
-    nfd::AdjointBatch B{};
-    B.n = nplanes;
-    for (int i = 0; i < nplanes; ++i) {
-      B.job[i] = {static_cast<const float*>(sources[i].data), (long long)sources[i].stride_bytes,
-                  static_cast<const float*>(grad_out[i].data), (long long)grad_out[i].stride_bytes,
-                  reinterpret_cast<float*>(base + size_t(i) * cov),
-                  reinterpret_cast<float*>(base + size_t(nplanes) * cov + size_t(i) * part)};
-      B.gsrc[i] = static_cast<float*>(grad_src[i].data);
-      B.gsrc_stride[i] = grad_src[i].stride_bytes;
-    }
-    const size_t smem = nfd::adjoint_smem_bytes(d.bh, d.bw, S);
-    nfb::require(smem <= 227 * 1024, "block size too large for the backward tile");
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = (d.bh == 16 && d.bw == 16) ? nfd::launch_adjoint_16x16(d, S, B, smem, st)
-                                                : nfd::launch_adjoint_0x0(d, S, B, smem, st);
-    if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
-    const dim3 fb(32, 8), fg((p->t.gx.length + 31) / 32, (p->t.gy.length + 7) / 8, nplanes);
-    nfd::dft_adjoint_fold_kernel<<<fg, fb, 0, st>>>(d, B);
-    // partials of all planes are contiguous: tiles*nplanes rows of `bins`
-    nfd::dft_adjoint_reduce_kernel<<<(p->t.bins + 31) / 32, dim3(32, 32), 0, st>>>(
-        reinterpret_cast<const float*>(base + size_t(nplanes) * cov), int(tiles) * nplanes, p->t.bins, grad_primary);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
-    return NF_OK;
+    return run_backward(p, sources, nullptr, grad_out, grad_src, nplanes, grad_primary, scratch, scratch_bytes,
+                        stream, err, len);
+  });
+}
+
+nf_status nf_fft3d_backward_device(const nf_plan* p, const nf_const_plane* sources, const nf_const_plane* outputs,
+                                   const nf_const_plane* grad_out, const nf_plane* grad_src, int nplanes,
+                                   float* grad_primary, void* scratch, size_t scratch_bytes, void* stream, char* err,
+                                   size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && sources && outputs && grad_out && grad_src && grad_primary, "null argument");
+    check_fft3d_adjoint_plan(*p);
+    return run_backward(p, sources, outputs, grad_out, grad_src, nplanes, grad_primary, scratch, scratch_bytes,
+                        stream, err, len);
   });
 }
 

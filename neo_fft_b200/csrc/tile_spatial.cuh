@@ -209,9 +209,13 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
       if (m == 0) Rf = nf::cadd(Rf, gT);
       yv = nf::cadd(yv, nf::cmul_plain(Rf, ti[m]));
     }
-    spec[size_t(kk) * NB + b] = {fmul(yv.r, invT), fmul(yv.i, invT)};
+    spec[kk * NB + b] = {fmul(yv.r, invT), fmul(yv.i, invT)};
   }
 }
+
+// Source samples per thread of the next block row loaded ahead, during the current
+// block row's column phase (software pipelining of the staging).
+constexpr int kStagePf = 4;
 
 // ALGO: 0 FFT3D, 1 DFTTest (the launch knows the plan's algorithm, so the other
 // algorithm's branches are compiled out), -1 read from the plan.
@@ -246,11 +250,13 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
 
   float* tab = smem;
   float* ring_in = tab + S.tab_floats;
-  cf* spec = reinterpret_cast<cf*>(ring_in + size_t(BH) * S.ring_pitch);
-  float* ob = reinterpret_cast<float*>(spec + ((size_t(BH) * K * NB + 1) & ~size_t(1)));
-  float* acc = ob + size_t(BH) * NB * OBW;
-  float* dc = acc + size_t(BH) * S.tw;
-  int* colmap = reinterpret_cast<int*>(dc + 2 * size_t(NB));
+  // Shared-memory offsets are 32-bit: the whole layout is below 227 KB.
+  const int KNB = K * NB;  // complex stride between spectrum rows
+  cf* spec = reinterpret_cast<cf*>(ring_in + BH * S.ring_pitch);
+  float* ob = reinterpret_cast<float*>(spec + ((BH * KNB + 1) & ~1));
+  float* acc = ob + BH * NB * OBW;
+  float* dc = acc + BH * S.tw;
+  int* colmap = reinterpret_cast<int*>(dc + 2 * NB);
   const int tid = threadIdx.x, nthr = blockDim.x;
   bool bad = false;
 
@@ -312,6 +318,17 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const bool vec4 = (gx.step & 3) == 0 && (BW & 3) == 0;
   const bool ola4 = !P.center && vec4 && (S.tw & 3) == 0 && (tw & 3) == 0 && (X0 & 3) == 0;
 
+  // One source sample in cover coordinates (cy, cx): rows and columns inside the visible
+  // plane are read directly, the margins through the single reflection.
+  auto source_sample = [&](int cy, int cx) -> float {
+    const int sy = cy - gy.offset, sx = cx - gx.offset;
+    const bool in = unsigned(sy) < unsigned(gy.length) && unsigned(sx) < unsigned(gx.length);
+    const int ry = in ? sy : reflect_axis(cy, gy), rx = in ? sx : reflect_axis(cx, gx);
+    return load_sample<STORAGE>(J.src + ptrdiff_t(ry) * J.src_stride, rx);
+  };
+  float pf[kStagePf];
+#pragma unroll
+  for (int j = 0; j < kStagePf; ++j) pf[j] = 0.0f;
   // No barrier between a block row's retire phase (accumulator ring and the output) and the
   // next block row's first phase (staging ring, or the column phase's spectrum and DC
   // buffers): they touch disjoint shared memory, and every later phase is behind a barrier.
@@ -319,22 +336,30 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     const int oy = by * gy.step;
     if (SRC == kSrcPixels && !kalman_L) {
       // ---- 0: stage the rows this block row adds ----------------------------
+      // The first kStagePf samples of each thread were loaded during the previous block
+      // row's column phase (registers `pf`); the rest, and the first block row, load here.
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
       const int nrows = oy + BH - r0;
-      for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
-        const int rr = c.y, xx = c.x;
-        const int cy = r0 + rr;
-        const unsigned char* srow = J.src + ptrdiff_t(reflect_axis(cy, gy)) * J.src_stride;
-        const float sv = load_sample<STORAGE>(srow, reflect_axis(cx0 + xx, gx));
+      int i = 0;
+      for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next(), ++i) {
+        const int cy = r0 + c.y;
+        float sv;
+        if (by > by_lo && i < kStagePf) {
+#pragma unroll
+          for (int j = 0; j < kStagePf; ++j)
+            if (j == i) sv = pf[j];
+        } else {
+          sv = source_sample(cy, cx0 + c.x);
+        }
         const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
         if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
-        ring_in[size_t(cy % BH) * S.ring_pitch + xx] = v;
+        ring_in[int(unsigned(cy) % unsigned(BH)) * S.ring_pitch + c.x] = v;
       }
       __syncthreads();
       // ---- A: row transforms (block index fastest) --------------------------
       for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
         const int y = c.y, b = c.x;
-        const float* in = ring_in + size_t((oy + y) % BH) * S.ring_pitch + b * gx.step;
+        const float* in = ring_in + int(unsigned(oy + y) % unsigned(BH)) * S.ring_pitch + b * gx.step;
         float row[CAPW];
         if (vec4) {
 #pragma unroll UW
@@ -355,9 +380,16 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
 #pragma unroll UW
         for (int x = 0; x < CAPW; ++x)
           if (x < BW) row[x] = fft3d ? fmul(fmul(row[x], wya[y]), wxa[x]) : fmul(row[x], h[y * BW + x]);
-        nf::row_forward<BWC>(row, BW, spec + size_t(y) * K * NB + b, P.tww, codelet, NB);
+        nf::row_forward<BWC>(row, BW, spec + y * KNB + b, P.tww, codelet, NB);
       }
       __syncthreads();
+      if (by < by_hi) {  // next block row's first samples: loads in flight during phases B-E
+        const int noy = oy + gy.step, nr0 = max(noy, noy + BH - gy.step), nn = noy + BH - nr0;
+        Cursor2 c(tid, nthr, win);
+#pragma unroll
+        for (int j = 0; j < kStagePf; ++j, c.next())
+          if (c.y < nn) pf[j] = source_sample(nr0 + c.y, cx0 + c.x);
+      }
     }
     // ---- B: column forward, filter, column inverse --------------------------
     const int ncol = nbx * K;
@@ -375,10 +407,10 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         for (int y = 0; y < CAPH; ++y)
           if (y < BH) col[y] = S[size_t(y * K + k) * gx.count + b];
         nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
-        cf* sp = spec + size_t(k) * NB + b;
+        cf* sp = spec + k * NB + b;
 #pragma unroll UH
         for (int y = 0; y < CAPH; ++y)
-          if (y < BH) sp[size_t(y) * K * NB] = col[y];
+          if (y < BH) sp[y * KNB] = col[y];
       }
       __syncthreads();
     } else if constexpr (SRC == kSrcTemporal) {
@@ -408,7 +440,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         for (Cursor2 c(tid, nthr, nbx); c.y < bins; c.next()) {
           const int kk = c.y, b = c.x;
           const float g2 = grid ? fdiv(fmul(P.mean_scale, dc[NB + b]), grid0) : 0.0f;
-          cf* sp = spec + size_t(kk) * NB + b;
+          cf* sp = spec + kk * NB + b;
           *sp = spectral_bin<-2>(*sp, grid, kk, g2, enh, bad);  // enh is always type -2
         }
         __syncthreads();
@@ -416,14 +448,14 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
         const int k = c.y, b = c.x;
         cf col[CAPH];
-        cf* sp = spec + size_t(k) * NB + b;
+        cf* sp = spec + k * NB + b;
 #pragma unroll UH
         for (int y = 0; y < CAPH; ++y)
-          if (y < BH) col[y] = sp[size_t(y) * K * NB];
+          if (y < BH) col[y] = sp[y * KNB];
         nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
 #pragma unroll UH
         for (int y = 0; y < CAPH; ++y)
-          if (y < BH) sp[size_t(y) * K * NB] = col[y];
+          if (y < BH) sp[y * KNB] = col[y];
       }
       __syncthreads();
     } else {
@@ -432,7 +464,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const bool active = cb.y < K;  // task < ncol
       const int k = active ? cb.y : 0, b = active ? cb.x : 0;
       cf col[CAPH];
-      cf* sp = spec + size_t(k) * NB + b;  // + y*K*NB
+      cf* sp = spec + k * NB + b;  // + y*KNB
       if (active) {
         if (kalman_L) {
           const cf* L = kalman_L + (size_t(by) * gx.count + (bx_lo + b)) * P.bins + k;
@@ -442,7 +474,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         } else {
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = sp[size_t(y) * K * NB];
+            if (y < BH) col[y] = sp[y * KNB];
           nf::fft_1d<true, BHC>(col, BH, P.twh, codelet);
         }
         if (k == 0) dc[b] = col[0].r;
@@ -460,7 +492,11 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         };
         if (ALGO == 1) {
           switch (filt.type) {
-            case 0: filter_column(std::integral_constant<int, 0>{}); break;
+            case 0:  // the exponent mode fixed too
+              if (filt.emode == 0) filter_column(std::integral_constant<int, kFt0Ratio>{});
+              else if (filt.emode == 1) filter_column(std::integral_constant<int, kFt0Sqrt>{});
+              else filter_column(std::integral_constant<int, kFt0Pow>{});
+              break;
             case 1: filter_column(std::integral_constant<int, 1>{}); break;
             case 2: filter_column(std::integral_constant<int, 2>{}); break;
             case 3: filter_column(std::integral_constant<int, 3>{}); break;
@@ -488,7 +524,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
 #pragma unroll UH
         for (int y = 0; y < CAPH; ++y)
-          if (y < BH) sp[size_t(y) * K * NB] = col[y];
+          if (y < BH) sp[y * KNB] = col[y];
       }
       __syncthreads();
     }
@@ -498,9 +534,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const int y = c.y, b = c.x;
       if (P.center && y != BH / 2) continue;
       float row[CAPW];
-      nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, SRC == kSrcSlice ? fct3 : fct, row, P.tww, codelet,
-                           NB);
-      float* o = ob + (size_t(y) * NB + b) * OBW;
+      nf::row_inverse<BWC>(spec + y * KNB + b, BW, SRC == kSrcSlice ? fct3 : fct, row, P.tww, codelet, NB);
+      float* o = ob + (y * NB + b) * OBW;
       // NaN once any inverse sample is non-finite (x * 0 is NaN for inf and NaN, and a
       // signed zero otherwise): one multiply-add per sample instead of a compare.
       float guard = 0.0f;
@@ -533,10 +568,9 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const int adv4 = (OBW - gx.step) >> 2;
       for (Cursor2 c(tid, nthr, tw >> 2); c.y < yhi - ylo; c.next()) {
         const int Y = ylo + c.y, xx = c.x << 2, ly = Y - oy;
-        float4* a = reinterpret_cast<float4*>(acc + size_t(Y % BH) * S.tw + xx);
+        float4* a = reinterpret_cast<float4*>(acc + int(unsigned(Y) % unsigned(BH)) * S.tw + xx);
         const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
-        const float4* ov =
-            reinterpret_cast<const float4*>(ob + size_t(ly) * NB * OBW + size_t(cm & 1023) * OBW + (cm >> 20));
+        const float4* ov = reinterpret_cast<const float4*>(ob + (ly * NB + (cm & 1023)) * OBW + (cm >> 20));
         if (fft3d) {
           float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           for (int j = 0; j < nblk; ++j, ov += adv4) {
@@ -549,7 +583,15 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
                            fadd(v.w, fmul(r.w, w)));
         } else {
           float4 sacc = *a;
-          for (int j = 0; j < nblk; ++j, ov += adv4) {
+          int j = 0;
+          for (; j + 4 <= nblk; j += 4, ov += 4 * adv4) {  // four blocks per step, added in block order
+            const float4 o0 = ov[0], o1 = ov[adv4], o2 = ov[2 * adv4], o3 = ov[3 * adv4];
+            sacc = make_float4(fadd(fadd(fadd(fadd(sacc.x, o0.x), o1.x), o2.x), o3.x),
+                               fadd(fadd(fadd(fadd(sacc.y, o0.y), o1.y), o2.y), o3.y),
+                               fadd(fadd(fadd(fadd(sacc.z, o0.z), o1.z), o2.z), o3.z),
+                               fadd(fadd(fadd(fadd(sacc.w, o0.w), o1.w), o2.w), o3.w));
+          }
+          for (; j < nblk; ++j, ov += adv4) {
             const float4 o = *ov;
             sacc = make_float4(fadd(sacc.x, o.x), fadd(sacc.y, o.y), fadd(sacc.z, o.z), fadd(sacc.w, o.w));
           }
@@ -560,16 +602,16 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     for (Cursor2 c(tid, nthr, tw); !ola4 && c.y < yhi - ylo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
-      float* a = acc + size_t(Y % BH) * S.tw + xx;
-      const float* orow = ob + size_t(ly) * NB * OBW;
+      float* a = acc + int(unsigned(Y) % unsigned(BH)) * S.tw + xx;
+      const float* orow = ob + ly * NB * OBW;
       if (P.center) {
         const int bc = X - BW / 2;  // block whose centre is X (step 1)
-        if (ly == BH / 2 && bc >= bx_lo && bc <= bx_hi) *a = orow[size_t(bc - bx_lo) * OBW + BW / 2];
+        if (ly == BH / 2 && bc >= bx_lo && bc <= bx_hi) *a = orow[(bc - bx_lo) * OBW + BW / 2];
         continue;
       }
       // blocks b0.. in ascending order; block b0+j holds column X at offset xo - j*step
       const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
-      const float* ov = orow + size_t(cm & 1023) * OBW + (cm >> 20);
+      const float* ov = orow + (cm & 1023) * OBW + (cm >> 20);
       const int adv = OBW - gx.step;
       if (fft3d) {
         float r = 0.0f;
@@ -587,7 +629,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     for (Cursor2 c(tid, nthr, tw); c.y < rhi - rlo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = rlo + yy;
-      float* a = acc + size_t(Y % BH) * S.tw + xx;
+      float* a = acc + int(unsigned(Y) % unsigned(BH)) * S.tw + xx;
       const float v = *a;
       if (!isfin(v)) bad = true;
       store_sample<STORAGE, ALGO>(J.dst + ptrdiff_t(Y - gy.offset) * J.dst_stride, px0 + xx, v, P);

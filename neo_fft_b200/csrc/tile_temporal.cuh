@@ -195,7 +195,11 @@ __device__ __forceinline__ void volume_time(const DevPlan& P, const VolumeSpectr
     }
   };
   switch (P.filt.type) {
-    case 0: filter_lines(std::integral_constant<int, 0>{}); break;
+    case 0:  // the exponent mode fixed too
+      if (P.filt.emode == 0) filter_lines(std::integral_constant<int, kFt0Ratio>{});
+      else if (P.filt.emode == 1) filter_lines(std::integral_constant<int, kFt0Sqrt>{});
+      else filter_lines(std::integral_constant<int, kFt0Pow>{});
+      break;
     case 1: filter_lines(std::integral_constant<int, 1>{}); break;
     case 2: filter_lines(std::integral_constant<int, 2>{}); break;
     case 3: filter_lines(std::integral_constant<int, 3>{}); break;

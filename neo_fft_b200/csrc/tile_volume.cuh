@@ -196,7 +196,11 @@ __global__ void __launch_bounds__(256) volume_tile_kernel(DevPlan P, VolumeShape
           };
           switch (P.filt.type) {
             case -1: filter_lines(std::integral_constant<int, -1>{}); break;
-            case 0: filter_lines(std::integral_constant<int, 0>{}); break;
+            case 0:  // the exponent mode fixed too
+              if (P.filt.emode == 0) filter_lines(std::integral_constant<int, kFt0Ratio>{});
+              else if (P.filt.emode == 1) filter_lines(std::integral_constant<int, kFt0Sqrt>{});
+              else filter_lines(std::integral_constant<int, kFt0Pow>{});
+              break;
             case 1: filter_lines(std::integral_constant<int, 1>{}); break;
             case 2: filter_lines(std::integral_constant<int, 2>{}); break;
             case 3: filter_lines(std::integral_constant<int, 3>{}); break;

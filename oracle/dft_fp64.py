@@ -98,9 +98,108 @@ class DFTTestFP64:
         oy, ox = self.gy["offset"], self.gx["offset"]
         return acc[:, oy:oy + self.height, ox:ox + self.width] / 255.0
 
+    def kink_distance(self, x, table):
+        """Per block [B, ny, nx]: the smallest relative distance |p - a| / a of any bin's power
+        from the threshold where the ftype 0 gain has its kink (binary64)."""
+        import torch
+        with torch.no_grad():
+            b = self.config.block
+            step = b - self.config.overlap
+            h = torch.from_numpy(self.h.astype(np.float64))
+            padded = 255.0 * x[:, torch.from_numpy(self.iy)][:, :, torch.from_numpy(self.ix)]
+            ny, nx = self.gy["count"], self.gx["count"]
+            spec = torch.fft.rfft2(padded.unfold(1, b, step).unfold(2, b, step)[:, :ny, :nx] * h)
+            a = table.reshape(b, b // 2 + 1)
+            if self.config.zmean:
+                grid = torch.fft.rfft2(255.0 * h)
+                spec = spec - (spec[..., 0, 0].real / grid[0, 0].real)[..., None, None] * grid
+            p = spec.real ** 2 + spec.imag ** 2
+            return (torch.abs(p - a) / a).amin(dim=(-2, -1))
+
     def uniform_table(self):
         """The table a DFTTest plan without curves uses: sigma / wscale for ftype 0/1, sigma for 2."""
         c = self.config
         b = c.block
         v = np.float32(c.sigma) / np.float32(self.wscale) if c.ftype < 2 else np.float32(c.sigma)
         return np.full(b * (b // 2 + 1), v, np.float32)
+
+
+class FFT3DFP64:
+    """Binary64, differentiable restatement of the reference FFT3D bt=1 path for float planes
+    (src/algorithms/plan.cpp:432-537): decode (no scale), single reflection into the cover,
+    blocks (v*wy)*wx, r2c, degrid template M = degrid * X0/G0 * G with G = r2c(wy*wx),
+    gain max((q - a)/q, floor) with q = |X - M|^2 + 1e-15 (kernels/scalar/spectral.cpp:18-22)
+    times the sharpen/dehalo factor S(q)D(q) (algorithms/fft3d_profile.cpp:69-81; windows in
+    binary64 as in oracle/fp64_pipeline.py), Y = gain*R + M, c2r / (bw*bh), synthesis wxs*wys,
+    overlap-add, output clamp(z, 0, 1) whose gradient passes where 0 < z < 1.
+
+    forward(x [B, H, W] float64 tensor, table [bh*(bw/2+1)] float64 tensor) -> [B, H, W]; the
+    table is the per-bin noise power a (uniform sigma: sigma^2/norm in every bin)."""
+
+    def __init__(self, width: int, height: int, config):
+        from . import ref
+        from .fp64_pipeline import FP64Plan
+        from neo_fft_b200.plan import SampleFormat
+        if config.bt != 1 or config.pfactor > 0 or config.pshow:
+            raise ValueError("restatement covers FFT3D bt=1 without pattern sampling")
+        self.fp = FP64Plan(width, height, SampleFormat(32, True), config)
+        rp = self.fp.ref
+        self.gx, self.gy = rp.x, rp.y
+        self.width, self.height, self.config = width, height, config
+        self.iy = _reflect_index(height, self.gy["offset"], self.gy["cover"])
+        self.ix = _reflect_index(width, self.gx["offset"], self.gx["cover"])
+
+    def forward(self, x, table):
+        import torch
+        import torch.nn.functional as F
+        fp, c = self.fp, self.config
+        bh, bw = c.bh, c.bw
+        dev = x.device
+        t = lambda a: torch.from_numpy(np.asarray(a, np.float64)).to(dev)  # noqa: E731
+        wa = t(np.outer(fp.wya, fp.wxa))
+        ws = t(np.outer(fp.wys, fp.wxs))
+        padded = x[:, torch.from_numpy(self.iy).to(dev)][:, :, torch.from_numpy(self.ix).to(dev)]
+        B, ch, cw = padded.shape
+        sy, sx = self.gy["step"], self.gx["step"]
+        ny, nx = self.gy["count"], self.gx["count"]
+        blocks = padded.unfold(1, bh, sy).unfold(2, bw, sx)[:, :ny, :nx] * wa
+        spec = torch.fft.rfft2(blocks)
+        K = bw // 2 + 1
+        if fp.grid is not None:
+            grid = t(fp.grid.real).reshape(bh, K) + 1j * t(fp.grid.imag).reshape(bh, K)
+            mean = (fp.mean_scale * spec[..., 0, 0].real / grid[0, 0].real)[..., None, None] * grid
+        else:
+            mean = torch.zeros_like(spec)
+        R = spec - mean
+        q = R.real ** 2 + R.imag ** 2 + 1e-15
+        a = table.reshape(bh, K)
+        r = (q - a) / q
+        gain = torch.where(r >= fp.floor, r, torch.full_like(r, fp.floor))
+        e = fp.enh
+        if e.active:
+            s = torch.ones_like(q)
+            d = torch.ones_like(q)
+            if e.sharpen and e.b != 0:
+                s = 1.0 + e.sharpen * t(e.sw).reshape(bh, K) * torch.sqrt(q * e.b / ((q + e.a) * (q + e.b)))
+            if e.dehalo:
+                qc = q + e.c
+                d = qc / (qc + e.dehalo * t(e.hw).reshape(bh, K) * q)
+            gain = gain * s * d
+        out_blocks = torch.fft.irfft2(gain * R + mean, s=(bh, bw)) * ws
+        cols = out_blocks.permute(0, 3, 4, 1, 2).reshape(B, bh * bw, ny * nx)
+        acc = F.fold(cols, output_size=(ch, cw), kernel_size=(bh, bw), stride=(sy, sx))[:, 0]
+        oy, ox = self.gy["offset"], self.gx["offset"]
+        z = acc[:, oy:oy + self.height, ox:ox + self.width]
+        self.last_z, self.last_kink = z.detach(), None
+        # per block: smallest relative distance of q from the kink of max((q - a)/q, floor),
+        # q = a / (1 - floor)
+        qk = a / (1.0 - fp.floor)
+        self.last_kink = (torch.abs(q.detach() - qk) / qk).amin(dim=(-2, -1))
+        return torch.where((z > 0) & (z < 1), z, z.detach().clamp(0.0, 1.0))
+
+    def uniform_table(self):
+        """The table of a uniform-sigma plan: a = sigma_eff^2 / norm in every bin (binary32)."""
+        c = self.config
+        sig = np.float32(np.float32(c.sigma) * np.float32(1.0 / 255.0))
+        a = np.float32(np.float32(sig * sig) / np.float32(1.0 / (np.float32(c.bw) * np.float32(c.bh))))
+        return np.full(c.bh * (c.bw // 2 + 1), a, np.float32)

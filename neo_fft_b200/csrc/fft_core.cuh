@@ -476,6 +476,91 @@ NF_HD void fft_ct(cf* a, const cf* table) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Team form of fft_ct<N>: the transform shared by T = F.r[0] lanes (the outermost
+// radix), each holding M = N / T elements in registers instead of N.
+//
+// After the digit-reversed load, every level but the outermost combines elements inside
+// one run of M consecutive positions (its groups have LEN <= M elements and start at
+// multiples of LEN), so lane t runs those levels on positions [t*M, t*M + M) with the
+// same butterflies, twiddles and operation order as fft_ct. The digit-reversed input of
+// position t*M + i is element t + off(i) (the outermost digit is the lowest one of the
+// input index), so each lane gathers its run directly. The outermost level's butterfly
+// k1 takes run position k1 of every lane and writes positions k1 + M*q; lane t computes
+// the butterflies k1 = t, t + T, ... after the runs have been exchanged through memory
+// the caller provides. Results are bit-identical to fft_ct<N>.
+// ---------------------------------------------------------------------------
+template <bool FORWARD, int N, int LEV, int INNER, int EXTENT>
+NF_HD void ct_level_run(cf* a, const cf* table) {
+  constexpr Factors F = factorize(N);
+  constexpr int R = F.r[LEV];
+  constexpr int LEN = R * INNER;
+  constexpr int STEP = N / LEN;
+  static_assert(EXTENT % LEN == 0, "inner levels must stay inside a run");
+#pragma unroll
+  for (int base = 0; base < EXTENT; base += LEN) {
+#pragma unroll
+    for (int k1 = 0; k1 < INNER; ++k1) {
+      cf t[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        cf v = a[base + j * INNER + k1];
+        if (j * k1 != 0) {
+          cf w = table[j * k1 * STEP];
+          if (!FORWARD) w.i = -w.i;
+          v = cmul_plain(v, w);
+        }
+        t[j] = v;
+      }
+      butterfly_ct<FORWARD, R>(t, table, N);
+#pragma unroll
+      for (int q = 0; q < R; ++q) a[base + k1 + INNER * q] = t[q];
+    }
+  }
+  if constexpr (LEV > 1) ct_level_run<FORWARD, N, LEV - 1, LEN, EXTENT>(a, table);
+}
+
+template <bool FORWARD, int N>
+struct TeamFFT {
+  static constexpr Factors F = factorize(N);
+  static constexpr int T = F.r[0];  // lanes of a team
+  static constexpr int M = N / T;   // elements per lane
+  static_assert(F.count >= 2 && M % T == 0, "team transforms need M = N/T divisible by T");
+  static constexpr DigitReversal<N> perm{};
+
+  // Input element of run position i of lane t.
+  NF_HD static constexpr int source(int t, int i) { return t + perm.v[i]; }
+  // The lane's run after every level but the outermost: local[i] = position t*M + i.
+  template <class Load>
+  NF_HD static void run(int t, cf* local, const cf* table, Load&& load) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) local[i] = load(source(t, i));
+    ct_level_run<FORWARD, N, F.count - 1, 1, M>(local, table);
+  }
+  // Outermost level: butterflies k1 = t + T*m; read(p) returns position p of the
+  // exchanged runs, write(x, v) receives output element x.
+  template <class Read, class Write>
+  NF_HD static void outer(int t, const cf* table, Read&& read, Write&& write) {
+#pragma unroll
+    for (int m = 0; m < M / T; ++m) {
+      const int k1 = t + T * m;
+      cf v[T];
+#pragma unroll
+      for (int j = 0; j < T; ++j) {
+        v[j] = read(j * M + k1);
+        if (j * k1 != 0) {
+          cf w = table[j * k1];
+          if (!FORWARD) w.i = -w.i;
+          v[j] = cmul_plain(v[j], w);
+        }
+      }
+      butterfly_ct<FORWARD, T>(v, table, N);
+#pragma unroll
+      for (int q = 0; q < T; ++q) write(k1 + M * q, v[q]);
+    }
+  }
+};
+
 // In-place project transform of a[0..n-1]; `table` holds w_n^m, m < n.
 // NC > 0: compile-time length (fft_ct above). NC == 0: the same butterflies in a
 // runtime loop nest for lengths n <= RCAP.

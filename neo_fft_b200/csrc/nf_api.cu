@@ -1134,10 +1134,11 @@ __global__ void fill_kernel(T* p, size_t n, T v) {
 
 cudaError_t run_kalman_advance(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, const nfd::KalmanArgs& a,
                                cudaStream_t st) {
-  const size_t per_block = size_t(d.bh) * d.K * sizeof(cf);
-  int nb = std::max(1, std::min(8, int((64 * 1024) / per_block)));
-  nb = std::min(nb, d.gx.count);
-  const size_t smem = per_block * size_t(nb);
+  // Blocks per CTA: enough column tasks (nb * K) for the 256 threads, within ~110 KB of
+  // shared memory (staged source window and spectra), so two CTAs fit on an SM.
+  int nb = std::max(1, std::min(d.gx.count, 256 / d.K));
+  while (nb > 1 && nfd::kalman_smem_bytes(d.bh, d.bw, d.gx.step, nb) > size_t(110) * 1024) --nb;
+  const size_t smem = nfd::kalman_smem_bytes(d.bh, d.bw, d.gx.step, nb);
   const dim3 grid((d.gx.count + nb - 1) / nb, d.gy.count);
   if (d.bh == d.bw) {
     switch (d.bw) {

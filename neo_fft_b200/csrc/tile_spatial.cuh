@@ -213,10 +213,6 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
   }
 }
 
-// Source samples per thread of the next block row loaded ahead, during the current
-// block row's column phase (software pipelining of the staging).
-constexpr int kStagePf = 4;
-
 // ALGO: 0 FFT3D, 1 DFTTest (the launch knows the plan's algorithm, so the other
 // algorithm's branches are compiled out), -1 read from the plan.
 template <int BHC, int BWC, int STORAGE, int SRC = kSrcPixels, int ALGO = -1>
@@ -326,9 +322,6 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     const int ry = in ? sy : reflect_axis(cy, gy), rx = in ? sx : reflect_axis(cx, gx);
     return load_sample<STORAGE>(J.src + ptrdiff_t(ry) * J.src_stride, rx);
   };
-  float pf[kStagePf];
-#pragma unroll
-  for (int j = 0; j < kStagePf; ++j) pf[j] = 0.0f;
   // No barrier between a block row's retire phase (accumulator ring and the output) and the
   // next block row's first phase (staging ring, or the column phase's spectrum and DC
   // buffers): they touch disjoint shared memory, and every later phase is behind a barrier.
@@ -336,21 +329,11 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     const int oy = by * gy.step;
     if (SRC == kSrcPixels && !kalman_L) {
       // ---- 0: stage the rows this block row adds ----------------------------
-      // The first kStagePf samples of each thread were loaded during the previous block
-      // row's column phase (registers `pf`); the rest, and the first block row, load here.
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
       const int nrows = oy + BH - r0;
-      int i = 0;
-      for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next(), ++i) {
+      for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
         const int cy = r0 + c.y;
-        float sv;
-        if (by > by_lo && i < kStagePf) {
-#pragma unroll
-          for (int j = 0; j < kStagePf; ++j)
-            if (j == i) sv = pf[j];
-        } else {
-          sv = source_sample(cy, cx0 + c.x);
-        }
+        const float sv = source_sample(cy, cx0 + c.x);
         const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
         if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
         ring_in[int(unsigned(cy) % unsigned(BH)) * S.ring_pitch + c.x] = v;
@@ -383,13 +366,6 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         nf::row_forward<BWC>(row, BW, spec + y * KNB + b, P.tww, codelet, NB);
       }
       __syncthreads();
-      if (by < by_hi) {  // next block row's first samples: loads in flight during phases B-E
-        const int noy = oy + gy.step, nr0 = max(noy, noy + BH - gy.step), nn = noy + BH - nr0;
-        Cursor2 c(tid, nthr, win);
-#pragma unroll
-        for (int j = 0; j < kStagePf; ++j, c.next())
-          if (c.y < nn) pf[j] = source_sample(nr0 + c.y, cx0 + c.x);
-      }
     }
     // ---- B: column forward, filter, column inverse --------------------------
     const int ncol = nbx * K;

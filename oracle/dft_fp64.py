@@ -193,7 +193,7 @@ class FFT3DFP64:
         self.last_z, self.last_kink = z.detach(), None
         # per block: smallest relative distance of q from the kink of max((q - a)/q, floor),
         # q = a / (1 - floor)
-        qk = a / (1.0 - fp.floor)
+        qk = a.detach() / (1.0 - fp.floor)
         self.last_kink = (torch.abs(q.detach() - qk) / qk).amin(dim=(-2, -1))
         return torch.where((z > 0) & (z < 1), z, z.detach().clamp(0.0, 1.0))
 

@@ -35,7 +35,36 @@ int check(std::mt19937& rng) {
   }
   return bad;
 }
+// The team form (lanes run one after another, the runs exchanged through a buffer)
+// against the single-thread transform.
+template <bool FWD, int N>
+int check_team(std::mt19937& rng) {
+  using Team = nf::TeamFFT<FWD, N>;
+  const auto tw = table(N);
+  std::normal_distribution<float> d(0.f, 1.f);
+  int bad = 0;
+  for (int trial = 0; trial < 20; ++trial) {
+    nf::cf in[N], ref[N], buf[N], out[N];
+    for (int i = 0; i < N; ++i) in[i] = ref[i] = {d(rng), d(rng)};
+    nf::fft_project<FWD, N>(ref, N, tw.data());
+    for (int t = 0; t < Team::T; ++t) {
+      nf::cf local[Team::M];
+      Team::run(t, local, tw.data(), [&](int k) { return in[k]; });
+      for (int i = 0; i < Team::M; ++i) buf[t * Team::M + i] = local[i];
+    }
+    for (int t = 0; t < Team::T; ++t)
+      Team::outer(t, tw.data(), [&](int p) { return buf[p]; }, [&](int x, nf::cf v) { out[x] = v; });
+    if (std::memcmp(out, ref, sizeof(out))) ++bad;
+  }
+  return bad;
+}
 } // namespace
+
+extern "C" int fft_team_mismatches() {
+  std::mt19937 rng(11);
+  return check_team<true, 48>(rng) + check_team<false, 48>(rng) + check_team<true, 64>(rng) +
+         check_team<false, 64>(rng) + check_team<true, 32>(rng) + check_team<false, 96>(rng);
+}
 
 extern "C" int fft_forms_mismatches() {
   std::mt19937 rng(7);

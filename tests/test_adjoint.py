@@ -249,17 +249,23 @@ def _fd_check(o, module_cfg, noisy, clean, n, s, kink_fn, z_fn, seed):
     z = z_fn()
     step, block = o.gx["step"], o.gx["block"]
     pix, ent = fd_coordinates(kink, xr.grad.numpy(), 48, 16, tr.grad.numpy(), step, block, seed, z=z)
-    worst = 0.0
+    g64x, g64t = xr.grad.numpy(), tr.grad.numpy()
+    rows = []
     for i, yy, xx in pix:
         # one pixel only moves its own patch: difference the loss of that patch
+        # h = 1e-6: the step moves every bin's power by far less than the rule's 1e-2 margin
+        # (DFTTest scales float samples by 255 before the transform)
         fd = central_difference(lambda v: ((o.forward(v, tab) - cd[i:i + 1]) ** 2).sum() / cd.numel(),
-                                xd[i:i + 1], (0, yy, xx), 1e-4)
-        worst = max(worst, abs(gx[i, yy, xx] - fd) / abs(fd))
+                                xd[i:i + 1], (0, yy, xx), 1e-6)
+        rows.append((abs(gx[i, yy, xx] - fd) / abs(fd), f"pixel {(i, yy, xx)}", gx[i, yy, xx], g64x[i, yy, xx], fd))
     for k in ent:
         fd = central_difference(lambda v: ((o.forward(xd, v) - cd) ** 2).mean(), tab, int(k), 1e-5 * float(tab[k]))
-        worst = max(worst, abs(gt[k] - fd) / abs(fd))
-    print(f"worst relative error {worst:.3g} over {len(pix) + len(ent)} coordinates")
-    assert worst <= 1e-4, worst
+        rows.append((abs(gt[k] - fd) / abs(fd), f"table {int(k)}", gt[k], g64t[k], fd))
+    rows.sort(key=lambda r: -r[0])
+    print(f"worst relative error {rows[0][0]:.3g} over {len(rows)} coordinates")
+    for r in rows[:6]:
+        print(f"  {r[1]}: rel {r[0]:.3g} gpu {r[2]:.9g} fp64-autograd {r[3]:.9g} central difference {r[4]:.9g}")
+    assert rows[0][0] <= 1e-4, rows[:6]
 
 
 @pytest.mark.gpu

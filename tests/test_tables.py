@@ -191,4 +191,7 @@ def test_project_transform_forms_identical():
             (ROOT / "neo_fft_b200" / "csrc" / "fft_core.cuh").stat().st_mtime > lib_path.stat().st_mtime:
         subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", "-fno-fast-math", "-ffp-contract=off",
                         f"-I{ROOT / 'neo_fft_b200' / 'csrc'}", str(src), "-o", str(lib_path)], check=True)
-    assert ctypes.CDLL(str(lib_path)).fft_forms_mismatches() == 0
+    lib = ctypes.CDLL(str(lib_path))
+    assert lib.fft_forms_mismatches() == 0
+    # the team form (a transform shared by four lanes, used by the 48x48 kernels) too
+    assert lib.fft_team_mismatches() == 0

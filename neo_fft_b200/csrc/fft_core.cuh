@@ -526,15 +526,14 @@ struct TeamFFT {
   static constexpr int T = F.r[0];  // lanes of a team
   static constexpr int M = N / T;   // elements per lane
   static_assert(F.count >= 2 && M % T == 0, "team transforms need M = N/T divisible by T");
-  static constexpr DigitReversal<N> perm{};
 
-  // Input element of run position i of lane t.
-  NF_HD static constexpr int source(int t, int i) { return t + perm.v[i]; }
-  // The lane's run after every level but the outermost: local[i] = position t*M + i.
+  // The lane's run after every level but the outermost: local[i] = position t*M + i, whose
+  // digit-reversed input is element t + perm[i].
   template <class Load>
   NF_HD static void run(int t, cf* local, const cf* table, Load&& load) {
+    constexpr DigitReversal<N> perm{};
 #pragma unroll
-    for (int i = 0; i < M; ++i) local[i] = load(source(t, i));
+    for (int i = 0; i < M; ++i) local[i] = load(t + perm.v[i]);
     ct_level_run<FORWARD, N, F.count - 1, 1, M>(local, table);
   }
   // Outermost level: butterflies k1 = t + T*m; read(p) returns position p of the

@@ -132,20 +132,22 @@ struct nf_clip_batch {
   std::vector<const nf_plan*> plans;  // distinct plans (sampled noise models are checked per launch)
   int bh = 0, bw = 0, storage = 0;
   int slice = 0;  // 0: FFT3D temporal clips; 1: DFTTest tmode 1 slice form
-  size_t smem1 = 0, smem2 = 0;
-  int nbc = 1, ctas2 = 1;
+  size_t smem1 = 0, smem2 = 0, smem2p = 0;
+  int nbc = 1, ctas2 = 1, ctas2p = 1;
   struct Step {
     nfd::SpectraWork w1{};
     nfd::VolumeSpectraWork w1v{};
     int items1 = 0;
-    nfd::BatchWork w2{};
+    nfd::BatchWork w2{};   // frames filtered across time (slot or slice spectra)
     int tiles2 = 0;
+    nfd::BatchWork w2p{};  // FFT3D clip-edge frames: single-frame pixel strips
+    int tiles2p = 0;
   };
   std::vector<Step> steps;
   void* dev = nullptr;      // plans | shapes | per-step job tables
   void* rings = nullptr;    // frame spectra, T per clip plane
   void* tspec = nullptr;    // slot pointer arrays of the temporal jobs
-  int* counters = nullptr;  // one work-queue head per step
+  int* counters = nullptr;  // two work-queue heads per step (temporal, clip-edge pixel)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t capture_stream = nullptr;
@@ -535,9 +537,18 @@ std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_p
     c.win_max = (c.nbx_max - 1) * d.gx.step + d.bw;
     int q = (c.win_max + 3) / 4;
     if (q % 2 == 0) ++q;  // odd float4 count: consecutive staged rows start in different banks
-    // Staging ring: pixel tiles only. FFT3D clip launches keep it for their single-frame
-    // fallback tiles at the clip edges; DFTTest slices and Kalman renders have no pixel tiles.
-    c.ring_pitch = work == StripWork::Slice || work == StripWork::Kalman ? 0 : 4 * q;
+    // Staging ring: pixel tiles only (DFTTest slices, Kalman renders and FFT3D temporal
+    // tiles have no pixel input). Temporal tiles of 48x48 blocks use it as the scratch
+    // through which their teams of four lanes exchange row-transform runs.
+    if (work == StripWork::Pixels) {
+      c.ring_pitch = 4 * q;
+    } else if (work == StripWork::Temporal && d.bh == 48 && d.bw == 48) {
+      int t = (nfd::team_scratch_floats(d.bw, 256) + d.bh - 1) / d.bh;
+      t = (t + 3) / 4;
+      c.ring_pitch = 4 * t;
+    } else {
+      c.ring_pitch = 0;
+    }
     c.th = d.gy.length;
     return c;
   };
@@ -1134,10 +1145,10 @@ __global__ void fill_kernel(T* p, size_t n, T v) {
 
 cudaError_t run_kalman_advance(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, const nfd::KalmanArgs& a,
                                cudaStream_t st) {
-  // Blocks per CTA: enough column tasks (nb * K) for the 256 threads, within ~110 KB of
-  // shared memory (staged source window and spectra), so two CTAs fit on an SM.
-  int nb = std::max(1, std::min(d.gx.count, 256 / d.K));
-  while (nb > 1 && nfd::kalman_smem_bytes(d.bh, d.bw, d.gx.step, nb) > size_t(110) * 1024) --nb;
+  // Blocks per CTA: up to eight (a 1080p plane of 32x32 blocks gives ~600 CTAs, several
+  // waves), within ~64 KB of shared memory (staged source window and spectra).
+  int nb = std::max(1, std::min(8, d.gx.count));
+  while (nb > 1 && nfd::kalman_smem_bytes(d.bh, d.bw, d.gx.step, nb) > size_t(64) * 1024) --nb;
   const size_t smem = nfd::kalman_smem_bytes(d.bh, d.bw, d.gx.step, nb);
   const dim3 grid((d.gx.count + nb - 1) / nb, d.gy.count);
   if (d.bh == d.bw) {
@@ -1944,6 +1955,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
         seg_h = h;
       }
     }
+    std::vector<nfd::StripShape> shapes_p;  // clip-edge pixel strips (FFT3D)
     for (const nf_plan* p : plans) {
       dplans.push_back(p->dev);
       nfd::StripShape S = pick_strip(p->dev, 0, b->slice ? StripWork::Slice : StripWork::Temporal);
@@ -1951,6 +1963,10 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       S.th = (p->t.gy.length + segs - 1) / segs;
       shapes.push_back(S);
       b->smem2 = std::max(b->smem2, nfd::strip_smem_bytes(b->bh, b->bw, S));
+      nfd::StripShape Sp = pick_strip(p->dev, 0, StripWork::Pixels);
+      Sp.th = S.th;
+      shapes_p.push_back(Sp);
+      if (!b->slice) b->smem2p = std::max(b->smem2p, nfd::strip_smem_bytes(b->bh, b->bw, Sp));
     }
     int max_count = 1, step = plans[0]->t.gx.step;
     for (const nf_plan* p : plans) max_count = std::max(max_count, p->t.gx.count);
@@ -2004,7 +2020,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
     std::vector<std::vector<nfd::SpectraJob>> pass1(static_cast<size_t>(nsteps));
     std::vector<std::vector<nfd::VolumeSpectraJob>> pass1v(static_cast<size_t>(nsteps));
     std::vector<std::vector<int>> pass1_base(static_cast<size_t>(nsteps), std::vector<int>(1, 0));
-    std::vector<Pass2> pass2(static_cast<size_t>(nsteps));
+    std::vector<Pass2> pass2(static_cast<size_t>(nsteps)), pass2p(static_cast<size_t>(nsteps));
     for (int s = 0; s < nsteps; ++s) {
       for (int i = 0; b->slice && i < count; ++i) {
         // DFTTest: step s is temporal block s, frames T*s .. T*s+T-1 clamped to the clip
@@ -2055,7 +2071,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
         nfd::PlaneJob job{fallback ? static_cast<const unsigned char*>(it.frames[t].data) : nullptr,
                           (long long)it.frames[t].stride_bytes, static_cast<unsigned char*>(it.dsts[t].data),
                           (long long)it.dsts[t].stride_bytes, nullptr, pi, 0, nullptr};
-        Pass2& q = pass2[size_t(s)];
+        Pass2& q = fallback ? pass2p[size_t(s)] : pass2[size_t(s)];
         q.jobs.push_back(job);
         if (fallback) {
           q.tspec_index.push_back(SIZE_MAX);
@@ -2063,7 +2079,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
           q.tspec_index.push_back(slot_ptrs.size());
           for (int j = 0; j < bt; ++j) slot_ptrs.push_back(frame_spec(i, t - left + j));
         }
-        const nfd::StripShape& S = shapes[size_t(pi)];
+        const nfd::StripShape& S = fallback ? shapes_p[size_t(pi)] : shapes[size_t(pi)];
         const int tx = (p.t.gx.length + S.tw - 1) / S.tw, ty = (p.t.gy.length + S.th - 1) / S.th;
         q.tiles_x.push_back(tx);
         q.base.push_back(q.base.back() + tx * ty);
@@ -2078,9 +2094,10 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
     }
     const auto* slots_dev = static_cast<const cf* const*>(b->tspec);
     Blob blob;
-    const size_t o_p = blob.add(dplans), o_s = blob.add(shapes);
+    const size_t o_p = blob.add(dplans), o_s = blob.add(shapes), o_sp = blob.add(shapes_p);
     struct Offsets {
       size_t j1 = SIZE_MAX, b1 = SIZE_MAX, j2 = SIZE_MAX, b2 = SIZE_MAX, t2 = SIZE_MAX;
+      size_t j2p = SIZE_MAX, b2p = SIZE_MAX, t2p = SIZE_MAX;
     };
     std::vector<Offsets> offs(static_cast<size_t>(nsteps));
     for (int s = 0; s < nsteps; ++s) {
@@ -2100,12 +2117,18 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
         o.b2 = blob.add(q.base);
         o.t2 = blob.add(q.tiles_x);
       }
+      const Pass2& qp = pass2p[size_t(s)];
+      if (!qp.jobs.empty()) {
+        o.j2p = blob.add(qp.jobs);
+        o.b2p = blob.add(qp.base);
+        o.t2p = blob.add(qp.tiles_x);
+      }
     }
     if ((ce = cudaMalloc(&b->dev, blob.bytes.size())) != cudaSuccess)
       return cuda_fail(err, len, ce, "device allocation failed");
     if ((ce = cudaMemcpy(b->dev, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
       return cuda_fail(err, len, ce, "clip batch upload failed");
-    if ((ce = cudaMalloc(&b->counters, sizeof(int) * size_t(nsteps))) != cudaSuccess)
+    if ((ce = cudaMalloc(&b->counters, 2 * sizeof(int) * size_t(nsteps))) != cudaSuccess)
       return cuda_fail(err, len, ce, "device allocation failed");
     auto* base = static_cast<unsigned char*>(b->dev);
     int sms = 148;
@@ -2137,11 +2160,22 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
         st.w2.job_tile_base = reinterpret_cast<const int*>(base + o.b2);
         st.w2.job_tiles_x = reinterpret_cast<const int*>(base + o.t2);
         st.w2.njobs = int(pass2[size_t(s)].jobs.size());
-        st.w2.counter = b->counters + s;
+        st.w2.counter = b->counters + 2 * s;
         st.tiles2 = pass2[size_t(s)].base.back();
+      }
+      if (o.j2p != SIZE_MAX) {
+        st.w2p.plans = reinterpret_cast<const nfd::DevPlan*>(base + o_p);
+        st.w2p.shapes = reinterpret_cast<const nfd::StripShape*>(base + o_sp);
+        st.w2p.jobs = reinterpret_cast<const nfd::PlaneJob*>(base + o.j2p);
+        st.w2p.job_tile_base = reinterpret_cast<const int*>(base + o.b2p);
+        st.w2p.job_tiles_x = reinterpret_cast<const int*>(base + o.t2p);
+        st.w2p.njobs = int(pass2p[size_t(s)].jobs.size());
+        st.w2p.counter = b->counters + 2 * s + 1;
+        st.tiles2p = pass2p[size_t(s)].base.back();
       }
     }
     b->ctas2 = per_sm * sms;
+    b->ctas2p = per_sm * sms;
     *out = b.release();
     return NF_OK;
   });
@@ -2152,7 +2186,7 @@ nf_status nf_clip_batch_launch(nf_clip_batch* b, void* stream, char* err, size_t
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (b->steps.empty()) return NF_OK;
   if (const nf_status ms = check_models(b->plans, err, len)) return ms;
-  cudaError_t e = cudaMemsetAsync(b->counters, 0, sizeof(int) * b->steps.size(), st);
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, 2 * sizeof(int) * b->steps.size(), st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
   for (const auto& s : b->steps) {
     if (s.items1 > 0) {
@@ -2164,6 +2198,17 @@ nf_status nf_clip_batch_launch(nf_clip_batch* b, void* stream, char* err, size_t
       const int ctas = std::max(1, std::min(b->ctas2, s.tiles2));
       if ((e = launch_temporal_shape(b->bh, b->bw, b->storage, b->slice, s.w2, ctas, b->smem2, st)) != cudaSuccess)
         return cuda_fail(err, len, e, "kernel launch failed");
+    }
+    if (s.w2p.njobs > 0) {  // clip-edge frames: single-frame pixel strips (FFT3D)
+      BatchGroup g;
+      g.bh = b->bh;
+      g.bw = b->bw;
+      g.storage = b->storage;
+      g.algo = 0;
+      g.ctas = std::max(1, std::min(b->ctas2p, s.tiles2p));
+      g.smem = b->smem2p;
+      g.work = s.w2p;
+      if ((e = launch_batch_group(g, st)) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
     }
   }
   return NF_OK;

@@ -213,6 +213,15 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
   }
 }
 
+// Block shapes whose temporal strips use team transforms (nf::TeamFFT over four lanes):
+// square 48x48, the largest non-codelet shape instantiated.
+template <int BHC, int BWC>
+__host__ __device__ constexpr bool team_block() {
+  return BHC == 48 && BWC == 48;
+}
+// Floats of team scratch a temporal strip of `threads` threads needs in its staging ring.
+__host__ __device__ inline int team_scratch_floats(int bw, int threads) { return (threads / 4) * 2 * bw; }
+
 // ALGO: 0 FFT3D, 1 DFTTest (the launch knows the plan's algorithm, so the other
 // algorithm's branches are compiled out), -1 read from the plan.
 template <int BHC, int BWC, int STORAGE, int SRC = kSrcPixels, int ALGO = -1>
@@ -233,6 +242,12 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const cf* kalman_L = J.kalman_L;
   const int NB = S.nbx_max;   // block stride of spec and ob
   const int OBW = BW + 4;     // ob row pitch (conflict-free float4 stores and overlap reads)
+  // FFT3D temporal tiles of 48x48 blocks share each 48-point transform among a team of
+  // four lanes (nf::TeamFFT): a lane holds 12 values instead of 48.
+  constexpr bool kTeam = SRC == kSrcTemporal && team_block<BHC, BWC>();
+  const int lane = threadIdx.x & 3, team = threadIdx.x >> 2, nteams = blockDim.x >> 2;
+  const unsigned team_mask = 0xFu << (threadIdx.x & 28);
+  (void)lane; (void)team; (void)nteams; (void)team_mask;
 
   const int tw = min(S.tw, gx.length - px0), th = min(S.th, gy.length - py0);
   const int X0 = px0 + gx.offset, Y0 = py0 + gy.offset;
@@ -421,17 +436,34 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         }
         __syncthreads();
       }
-      for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
-        const int k = c.y, b = c.x;
-        cf col[CAPH];
-        cf* sp = spec + k * NB + b;
+      if constexpr (kTeam) {
+        // Column inverses shared by teams of lanes, in place on the spectrum column: each
+        // lane gathers and transforms its run, the runs go back into the column, and each
+        // lane finishes the outermost butterflies of its own positions.
+        using TH = nf::TeamFFT<false, BHC>;
+        for (Cursor2 c(team, nteams, nbx); c.y < K; c.next()) {
+          cf* sp = spec + c.y * NB + c.x;
+          cf run[TH::M];
+          TH::run(lane, run, P.twh, [&](int y) { return sp[y * KNB]; });
+          __syncwarp(team_mask);  // every lane has gathered before any run is written back
+#pragma unroll
+          for (int i = 0; i < TH::M; ++i) sp[(lane * TH::M + i) * KNB] = run[i];
+          __syncwarp(team_mask);
+          TH::outer(lane, P.twh, [&](int q) { return sp[q * KNB]; }, [&](int y, cf v) { sp[y * KNB] = v; });
+        }
+      } else {
+        for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
+          const int k = c.y, b = c.x;
+          cf col[CAPH];
+          cf* sp = spec + k * NB + b;
 #pragma unroll UH
-        for (int y = 0; y < CAPH; ++y)
-          if (y < BH) col[y] = sp[y * KNB];
-        nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
+          for (int y = 0; y < CAPH; ++y)
+            if (y < BH) col[y] = sp[y * KNB];
+          nf::fft_1d<false, BHC>(col, BH, P.twh, codelet);
 #pragma unroll UH
-        for (int y = 0; y < CAPH; ++y)
-          if (y < BH) sp[y * KNB] = col[y];
+          for (int y = 0; y < CAPH; ++y)
+            if (y < BH) sp[y * KNB] = col[y];
+        }
       }
       __syncthreads();
     } else {
@@ -506,6 +538,37 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     }
     }
     // ---- C: row inverses and synthesis weighting -----------------------------
+    if constexpr (kTeam) {
+      // Row inverses shared by teams of lanes; the runs are exchanged through the team's
+      // scratch (the staging ring, which temporal tiles do not use).
+      using TW = nf::TeamFFT<false, BWC>;
+      cf* xs = reinterpret_cast<cf*>(ring_in) + team * BWC;
+      for (Cursor2 c(team, nteams, nbx); c.y < BH; c.next()) {
+        const int y = c.y, b = c.x;
+        const cf* bins = spec + y * KNB + b;
+        cf run[TW::M];
+        // the half spectrum mirrored as row_inverse does: conjugates above BW/2 (0 - im),
+        // the DC and Nyquist imaginary parts cleared
+        TW::run(lane, run, P.tww, [&](int x) {
+          cf v = bins[(x <= BW / 2 ? x : BW - x) * NB];
+          if (x > BW / 2) v.i = fsub(0.0f, v.i);
+          if (x == 0 || x == BW / 2) v.i = 0.0f;
+          return v;
+        });
+#pragma unroll
+        for (int i = 0; i < TW::M; ++i) xs[lane * TW::M + i] = run[i];
+        __syncwarp(team_mask);
+        float* o = ob + (y * NB + b) * OBW;
+        float guard = 0.0f;
+        TW::outer(lane, P.tww, [&](int q) { return xs[q]; }, [&](int x, cf v) {
+          const float r = fmul(v.r, fct);
+          guard = __fmaf_rn(r, 0.0f, guard);
+          o[x] = fmul(r, wxs[x]);
+        });
+        __syncwarp(team_mask);  // the scratch is reused by the team's next row
+        if (guard != guard) bad = true;
+      }
+    } else
     for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
       const int y = c.y, b = c.x;
       if (P.center && y != BH / 2) continue;

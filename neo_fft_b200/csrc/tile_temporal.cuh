@@ -6,7 +6,7 @@
 //   pass 2 (temporal_batch_kernel): the streaming strip (strip_tile in temporal mode)
 //     reads the T spectra of each block, filters across time and reconstructs.
 // Clip edges, where the host layer falls back to a single frame (filter.hpp:407-421),
-// run as pixel-mode strips in the same pass-2 launch.
+// run as pixel-mode strips of the batched spatial kernel beside pass 2.
 #pragma once
 #include "tile_spatial.cuh"
 
@@ -306,9 +306,10 @@ __global__ void __launch_bounds__(256) volume_spectra_batch_kernel(VolumeSpectra
   if (bad) atomicOr(P.err, kErrNonFinite);
 }
 
-// Pass 2: persistent strips over the step's jobs. FFT3D (SRC = kSrcTemporal): temporal
-// jobs carry tspec, clip-edge jobs filter their single source frame in pixel mode.
-// DFTTest (SRC = kSrcSlice): every job reconstructs one slice spectrum.
+// Pass 2: persistent strips over the step's jobs. FFT3D (SRC = kSrcTemporal): every job
+// carries the slot spectra of its frame (clip-edge frames, which filter their single
+// source frame, run as pixel strips in the batched spatial kernel). DFTTest (SRC =
+// kSrcSlice): every job reconstructs one slice spectrum.
 template <int BHC, int BWC, int STORAGE, int SRC>
 __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) temporal_batch_kernel(BatchWork W) {
   extern __shared__ float smem[];
@@ -340,8 +341,7 @@ __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) temporal
     if constexpr (SRC == kSrcSlice) {
       strip_tile<BHC, BWC, STORAGE, kSrcSlice, 1>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
     } else {
-      if (sJ.tspec) strip_tile<BHC, BWC, STORAGE, kSrcTemporal, 0>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
-      else strip_tile<BHC, BWC, STORAGE, kSrcPixels, 0>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+      strip_tile<BHC, BWC, STORAGE, kSrcTemporal, 0>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
     }
   }
 }

@@ -4,11 +4,9 @@
 //
 // Each CTA owns a run of NB consecutive blocks of one block row; every block is
 // visited exactly once, so each state bin has a single owner thread per frame and
-// the update is race-free. Stage: the run's BH source rows (its window of columns) are
-// read once with coalesced loads, reflected and decoded into shared memory. Rows:
-// thread = (block, row) -> windowed row transform into shared memory. Columns: thread =
-// (block, column) -> transform along y in registers, then the recursion over that
-// column's bins.
+// the update is race-free. Rows: thread = (block, row) -> reflected, windowed row
+// transform into shared memory. Columns: thread = (block, column) -> transform
+// along y in registers, then the recursion over that column's bins.
 #pragma once
 #include "tile_spatial.cuh"
 
@@ -23,12 +21,6 @@ struct KalmanArgs {
   const float* pattern;  // per-bin noise table or nullptr (uniform r0)
   int fp64;
 };
-
-// Shared layout (floats): stage [bh][pitch] | spec [nb][bh][K] complex.
-__host__ __device__ inline int kalman_stage_pitch(int bw, int step, int nb) { return ((nb - 1) * step + bw + 3) & ~3; }
-__host__ __device__ inline size_t kalman_smem_bytes(int bh, int bw, int step, int nb) {
-  return sizeof(float) * (size_t(bh) * kalman_stage_pitch(bw, step, nb) + 2 * size_t(nb) * bh * (bw / 2 + 1));
-}
 
 template <int BHC, int BWC, int STORAGE>
 __global__ void __launch_bounds__(256) kalman_advance_kernel(DevPlan P, int nb_per_cta, const unsigned char* src,
@@ -45,44 +37,38 @@ __global__ void __launch_bounds__(256) kalman_advance_kernel(DevPlan P, int nb_p
   constexpr bool kCodelet = BHC == BWC && (BWC == 8 || BWC == 16 || BWC == 32);
   const bool codelet = kCodelet || (BHC == 0 && P.codelet != 0);
   const DevAxis gx = P.gx, gy = P.gy;
-  const int pitch = kalman_stage_pitch(BW, gx.step, nb_per_cta);
-  float* stage = smem;
-  cf* spec = reinterpret_cast<cf*>(smem + BH * pitch);
+  cf* spec = reinterpret_cast<cf*>(smem);
   const int by = blockIdx.y;
   const int bx0 = blockIdx.x * nb_per_cta;
   const int nb = min(nb_per_cta, gx.count - bx0);
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const int oy = by * gy.step, cx0 = bx0 * gx.step;
-  const int win = (nb - 1) * gx.step + BW;
+  const int oy = by * gy.step;
   bool bad = false;
   // Legacy pad_source decodes without a finiteness check (src/algorithms/pad.hpp:47-82);
   // the recursion checks every consumed value instead.
-  for (Cursor2 c(tid, nthr, win); c.y < BH; c.next()) {
-    const int cy = oy + c.y, cx = cx0 + c.x;
-    const int sy = cy - gy.offset, sx = cx - gx.offset;
-    const bool in = unsigned(sy) < unsigned(gy.length) && unsigned(sx) < unsigned(gx.length);
-    const int ry = in ? sy : reflect_axis(cy, gy), rx = in ? sx : reflect_axis(cx, gx);
-    stage[c.y * pitch + c.x] = fsub(load_sample<STORAGE>(src + ptrdiff_t(ry) * src_stride, rx), P.dec_base);
-  }
-  __syncthreads();
   for (int task = tid; task < nb * BH; task += nthr) {
     const int b = task / BH, y = task - b * BH;
-    const float* in = stage + y * pitch + b * gx.step;
-    const float wy = P.wya[y];
+    const int ox = (bx0 + b) * gx.step;
+    const unsigned char* srow = src + ptrdiff_t(reflect_axis(oy + y, gy)) * src_stride;
     float row[CAPW];
 #pragma unroll UW
-    for (int x = 0; x < CAPW; ++x)
-      if (x < BW) row[x] = fmul(fmul(in[x], wy), P.wxa[x]);
-    nf::row_forward<BWC>(row, BW, spec + (b * BH + y) * K, P.tww, codelet);
+    for (int x = 0; x < CAPW; ++x) {
+      if (x < BW) {
+        const float s = load_sample<STORAGE>(srow, reflect_axis(ox + x, gx));
+        const float v = fsub(s, P.dec_base);
+        row[x] = fmul(fmul(v, P.wya[y]), P.wxa[x]);
+      }
+    }
+    nf::row_forward<BWC>(row, BW, spec + (size_t(b) * BH + y) * K, P.tww, codelet);
   }
   __syncthreads();
   for (int task = tid; task < nb * K; task += nthr) {
     const int b = task / K, k = task - b * K;
     cf col[CAPH];
-    const cf* sp = spec + b * BH * K + k;
+    const cf* sp = spec + size_t(b) * BH * K + k;
 #pragma unroll UH
     for (int y = 0; y < CAPH; ++y)
-      if (y < BH) col[y] = sp[y * K];
+      if (y < BH) col[y] = sp[size_t(y) * K];
     nf::fft_1d<true, BHC>(col, BH, P.twh, codelet);
     const size_t base = (size_t(by) * gx.count + (bx0 + b)) * P.bins;
 #pragma unroll UH

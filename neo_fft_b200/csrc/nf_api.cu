@@ -542,8 +542,8 @@ std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_p
     // through which their teams of four lanes exchange row-transform runs.
     if (work == StripWork::Pixels) {
       c.ring_pitch = 4 * q;
-    } else if (work == StripWork::Temporal && d.bh == 48 && d.bw == 48) {
-      int t = (nfd::team_scratch_floats(d.bw, 256) + d.bh - 1) / d.bh;
+    } else if (work == StripWork::Temporal && d.bh == 48 && d.bw == 48) {  // 512-thread CTAs
+      int t = (nfd::team_scratch_floats(d.bw, 512) + d.bh - 1) / d.bh;
       t = (t + 3) / 4;
       c.ring_pitch = 4 * t;
     } else {
@@ -1145,11 +1145,10 @@ __global__ void fill_kernel(T* p, size_t n, T v) {
 
 cudaError_t run_kalman_advance(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, const nfd::KalmanArgs& a,
                                cudaStream_t st) {
-  // Blocks per CTA: up to eight (a 1080p plane of 32x32 blocks gives ~600 CTAs, several
-  // waves), within ~64 KB of shared memory (staged source window and spectra).
-  int nb = std::max(1, std::min(8, d.gx.count));
-  while (nb > 1 && nfd::kalman_smem_bytes(d.bh, d.bw, d.gx.step, nb) > size_t(64) * 1024) --nb;
-  const size_t smem = nfd::kalman_smem_bytes(d.bh, d.bw, d.gx.step, nb);
+  const size_t per_block = size_t(d.bh) * d.K * sizeof(cf);
+  int nb = std::max(1, std::min(8, int((64 * 1024) / per_block)));
+  nb = std::min(nb, d.gx.count);
+  const size_t smem = per_block * size_t(nb);
   const dim3 grid((d.gx.count + nb - 1) / nb, d.gy.count);
   if (d.bh == d.bw) {
     switch (d.bw) {

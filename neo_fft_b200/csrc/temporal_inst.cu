@@ -34,7 +34,7 @@ cudaError_t temporal(const BatchWork& w, int ctas, size_t smem, cudaStream_t st)
   auto k = temporal_batch_kernel<NF_BH, NF_BW, ST, SRC>;
   cudaError_t e = prepare(k, smem);
   if (e != cudaSuccess) return e;
-  k<<<ctas, 256, smem, st>>>(w);
+  k<<<ctas, TemporalThreads<NF_BH, NF_BW, SRC>::value, smem, st>>>(w);
   return cudaGetLastError();
 }
 } // namespace

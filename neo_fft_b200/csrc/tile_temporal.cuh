@@ -310,8 +310,16 @@ __global__ void __launch_bounds__(256) volume_spectra_batch_kernel(VolumeSpectra
 // carries the slot spectra of its frame (clip-edge frames, which filter their single
 // source frame, run as pixel strips in the batched spatial kernel). DFTTest (SRC =
 // kSrcSlice): every job reconstructs one slice spectrum.
+// Threads of a pass-2 CTA: 512 for FFT3D temporal strips of 48x48 blocks (their team
+// transforms fit in 128 registers, so one CTA per SM runs 16 warps), 256 otherwise.
+template <int BHC, int BWC, int SRC>
+struct TemporalThreads {
+  static constexpr int value = (SRC == kSrcTemporal && team_block<BHC, BWC>()) ? 512 : 256;
+};
+
 template <int BHC, int BWC, int STORAGE, int SRC>
-__global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) temporal_batch_kernel(BatchWork W) {
+__global__ void __launch_bounds__(TemporalThreads<BHC, BWC, SRC>::value, StripOccupancy<BHC, BWC>::value)
+    temporal_batch_kernel(BatchWork W) {
   extern __shared__ float smem[];
   __shared__ int item;
   const int total = W.job_tile_base[W.njobs];

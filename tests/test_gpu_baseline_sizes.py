@@ -237,3 +237,30 @@ def test_b_dfttest_16_4k_yuv420p10(ref, cuda):
         stats["luma" if p == 0 else "chroma"] = s
     record("B4K DFTTest 16/12 ftype 0 flat curve, 3840x2160 YUV420P10 luma + chroma", vs_reference="bit-identical",
            vs_fp64=stats)
+
+
+def test_a_fft3d_bt1_32_640x360_gray8(ref, cuda):
+    """A: FFT3D bt=1, 32x32 / 16, sigma 2 on 24 frames of 640x360 GRAY8 (smooth gradient plus
+    sinusoids in [16, 235] plus noise sd 5), through the batched form."""
+    from neo_fft_b200.plan import Batch
+    from oracle.fp64_pipeline import FP64Plan
+    from tests.synth import gradient_sinusoid, to_format
+    w, h, n = 640, 360, 24
+    fmt = SampleFormat(8)
+    cfg = FFT3DConfig(bw=32, bh=32, ow=16, oh=16, sigma=2.0)
+    frames = [to_format(gradient_sinusoid(h, w, (1, 0, f)), 8, False, 5.0, (1, 0, f, 1)) for f in range(n)]
+    plan = Plan(w, h, fmt, cfg)
+    dev = [cuda.from_numpy(f).cuda() for f in frames]
+    outs = [cuda.empty_like(d) for d in dev]
+    Batch([(plan, dev[f], outs[f]) for f in range(n)]).launch()
+    plan.sync_status()
+    rp, fp = ref.RefPlan(w, h, fmt, cfg), FP64Plan(w, h, fmt, cfg)
+    worst = {"max_steps": 0, "frac_off_by_one": 0.0, "excess_over_half_step": 0.0}
+    for f in range(n):
+        gpu = outs[f].cpu().numpy()
+        check_parity(gpu, rp.process([frames[f]]), fmt)
+        s = int_vs_fp64(gpu, fp.process([frames[f]]), fp)
+        worst = {k: max(worst[k], s[k]) for k in worst}
+    assert worst["max_steps"] <= 1 and worst["frac_off_by_one"] <= 0.005, worst
+    record("A FFT3D bt=1 32/16 sigma 2, 640x360 GRAY8, 24 frames", vs_reference="bit-identical, 24 frames",
+           vs_fp64=worst)

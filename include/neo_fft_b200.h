@@ -195,6 +195,13 @@ nf_status nf_batch_graph_launch(nf_batch* batch, void* stream, char* err, size_t
 int nf_batch_geometry_count(const nf_batch* batch);
 int nf_batch_geometry(const nf_batch* batch);
 nf_status nf_batch_select_geometry(nf_batch* batch, int index, char* err, size_t err_len);
+/* Planes of the geometry in use whose interior block rows are staged by bulk-tensor
+ * copies prefetched one block row ahead (a 2-D tensor map per plane; planes whose base
+ * address or row stride is not a multiple of 16 bytes, or whose strips are wider than a
+ * tensor-map box, are staged by direct loads). A copy that does not arrive within about
+ * a second is reported by nf_batch_sync_status / nf_plan_sync_status as NF_DEVICE_ERROR
+ * "a source staging copy did not complete"; the outputs are still written. */
+int nf_batch_mapped_planes(const nf_batch* batch);
 void nf_batch_destroy(nf_batch* batch);
 
 /* Temporal clips in batched form: every output frame of every clip, with the host

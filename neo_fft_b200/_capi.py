@@ -106,6 +106,7 @@ PROTOTYPES = {
     "nf_batch_graph_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_batch_destroy": (None, [c_void_p]),
     "nf_batch_geometry_count": (c_int, [c_void_p]),
+    "nf_batch_mapped_planes": (c_int, [c_void_p]),
     "nf_batch_geometry": (c_int, [c_void_p]),
     "nf_batch_select_geometry": (c_int, [c_void_p, c_int, ctypes.c_char_p, c_size_t]),
     "nf_plan_process_planes_device": (c_int, [c_void_p, ctypes.POINTER(NfConstPlane), ctypes.POINTER(NfPlane), c_int,

@@ -536,8 +536,8 @@ struct TeamFFT {
     for (int i = 0; i < M; ++i) local[i] = load(t + perm.v[i]);
     ct_level_run<FORWARD, N, F.count - 1, 1, M>(local, table);
   }
-  // Outermost level: butterflies k1 = t + T*m; read(p) returns position p of the
-  // exchanged runs, write(x, v) receives output element x.
+  // Outermost level: butterflies k1 = t + T*m; read(j, i) returns element i of lane j's
+  // run (position j*M + i of the exchanged runs), write(x, v) receives output element x.
   template <class Read, class Write>
   NF_HD static void outer(int t, const cf* table, Read&& read, Write&& write) {
 #pragma unroll
@@ -546,7 +546,7 @@ struct TeamFFT {
       cf v[T];
 #pragma unroll
       for (int j = 0; j < T; ++j) {
-        v[j] = read(j * M + k1);
+        v[j] = read(j, k1);
         if (j * k1 != 0) {
           cf w = table[j * k1];
           if (!FORWARD) w.i = -w.i;

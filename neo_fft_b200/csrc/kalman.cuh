@@ -6,7 +6,8 @@
 // visited exactly once, so each state bin has a single owner thread per frame and
 // the update is race-free. Rows: thread = (block, row) -> reflected, windowed row
 // transform into shared memory. Columns: thread = (block, column) -> transform
-// along y in registers, then the recursion over that column's bins.
+// along y in registers, written back in place. Recursion: thread = bin of the run,
+// over the state arrays in their own order.
 #pragma once
 #include "tile_spatial.cuh"
 
@@ -65,33 +66,49 @@ __global__ void __launch_bounds__(256) kalman_advance_kernel(DevPlan P, int nb_p
   for (int task = tid; task < nb * K; task += nthr) {
     const int b = task / K, k = task - b * K;
     cf col[CAPH];
-    const cf* sp = spec + size_t(b) * BH * K + k;
+    cf* sp = spec + size_t(b) * BH * K + k;
 #pragma unroll UH
     for (int y = 0; y < CAPH; ++y)
       if (y < BH) col[y] = sp[size_t(y) * K];
     nf::fft_1d<true, BHC>(col, BH, P.twh, codelet);
-    const size_t base = (size_t(by) * gx.count + (bx0 + b)) * P.bins;
 #pragma unroll UH
-    for (int y = 0; y < CAPH; ++y) {
-      if (y < BH) {
-        const int kk = y * K + k;
-        const size_t i = base + kk;
-        cf L = A.last[i];
-        bool ok;
-        if (A.fp64) {
-          double c = A.cov64[i], q = A.proc64[i];
-          ok = kalman_bin_fp64(col[y], L, c, q, A.pattern, kk, P.kalman_r0, P.kalman_ratio2);
-          A.cov64[i] = c;
-          A.proc64[i] = q;
-        } else {
-          float c = A.cov32[i], q = A.proc32[i];
-          ok = kalman_bin(col[y], L, c, q, A.pattern, kk, P.kalman_r0, P.kalman_ratio2);
-          A.cov32[i] = c;
-          A.proc32[i] = q;
-        }
-        A.last[i] = L;
-        if (!ok) bad = true;
-      }
+    for (int y = 0; y < CAPH; ++y)
+      if (y < BH) sp[size_t(y) * K] = col[y];
+  }
+  __syncthreads();
+  // The recursion, one thread per bin: spec holds the run's blocks as [block][y*K + k],
+  // the state's own layout, and the run's blocks are consecutive in the state, so bin i
+  // of the run is state element base + i (coalesced; the arrays never alias).
+  const int bins = BH * K;
+  const int n = nb * bins;
+  const size_t base = (size_t(by) * gx.count + bx0) * size_t(bins);
+  cf* __restrict__ last = A.last + base;
+  const float* __restrict__ pattern = A.pattern;
+  if (A.fp64) {
+    double* __restrict__ cov = A.cov64 + base;
+    double* __restrict__ proc = A.proc64 + base;
+#pragma unroll 4
+    for (int i = tid; i < n; i += nthr) {
+      const int kk = i - (i / bins) * bins;
+      cf L = last[i];
+      double c = cov[i], q = proc[i];
+      if (!kalman_bin_fp64(spec[i], L, c, q, pattern, kk, P.kalman_r0, P.kalman_ratio2)) bad = true;
+      last[i] = L;
+      cov[i] = c;
+      proc[i] = q;
+    }
+  } else {
+    float* __restrict__ cov = A.cov32 + base;
+    float* __restrict__ proc = A.proc32 + base;
+#pragma unroll 4
+    for (int i = tid; i < n; i += nthr) {
+      const int kk = i - (i / bins) * bins;
+      cf L = last[i];
+      float c = cov[i], q = proc[i];
+      if (!kalman_bin(spec[i], L, c, q, pattern, kk, P.kalman_r0, P.kalman_ratio2)) bad = true;
+      last[i] = L;
+      cov[i] = c;
+      proc[i] = q;
     }
   }
   if (bad) atomicOr(P.err, kErrNonFinite);

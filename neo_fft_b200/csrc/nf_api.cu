@@ -14,6 +14,8 @@
 #include "dither.cuh"
 #include "plan_info.hpp"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -99,6 +101,7 @@ struct nf_kalman_state {
 // One persistent launch group: planes of one block shape and storage.
 struct BatchGroup {
   int bh = 0, bw = 0, storage = 0, algo = 0, ctas = 0;
+  int mapped = 0;  // planes staged through tensor maps
   size_t smem = 0;
   void* dev = nullptr;  // plans | shapes | jobs | tile_base | tiles_x
   nfd::BatchWork work{};
@@ -291,6 +294,49 @@ struct Blob {
     return add(v.data(), v.size() * sizeof(T));
   }
 };
+
+// Bulk-tensor staging of batched pixel strips. The driver's tensor-map encoder is
+// reached through the runtime's entry-point query (no link against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// Staged width of a strip shape in samples: the window rounded up to whole 4-sample
+// groups, plus the remainder of the start column's 16-byte rounding, in whole boxes of
+// 256 bytes (nfd::kStagingBoxBytes). 0 beyond eight boxes.
+int tma_box_width(const nfd::StripShape& S, int storage) {
+  const int align = 16 / storage, box = nfd::kStagingBoxBytes / storage;
+  const int w = (((S.win_max + 3) & ~3) + align - 1 + box - 1) / box * box;
+  return w <= 8 * box ? w : 0;
+}
+
+// The 2-D tensor map of a source plane with boxes of box_w x box_h samples, or false
+// when the plane breaks a tensor-map rule (16-byte aligned base and row stride).
+bool encode_plane_map(CUtensorMap* m, const void* base, int width, int height, long long stride, int storage, int box_w,
+                      int box_h) {
+  const auto fn = tensor_map_encoder();
+  if (!fn || box_w <= 0 || box_h <= 0 || box_h > 256 || stride <= 0 || (stride & 15) != 0 ||
+      (reinterpret_cast<uintptr_t>(base) & 15) != 0 || stride < (long long)width * storage)
+    return false;
+  const CUtensorMapDataType type = storage == nfd::kStoreU8    ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                   : storage == nfd::kStoreU16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16
+                                                                : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[2] = {cuuint64_t(width), cuuint64_t(height)};
+  const cuuint64_t strides[1] = {cuuint64_t(stride)};
+  const cuuint32_t box[2] = {cuuint32_t(box_w), cuuint32_t(box_h)};
+  const cuuint32_t elem_strides[2] = {1, 1};
+  return fn(m, type, 2, const_cast<void*>(base), dims, strides, box, elem_strides, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
 
 nfd::DevAxis dev_axis(const nfb::Axis& a) {
   return {a.length, a.block, a.overlap, a.step, a.count, a.cover, a.offset};
@@ -486,7 +532,9 @@ int plain_ctas(const nfd::DevPlan& d) { return (d.bh * d.bw <= 256 ? 2 : 1) * 14
 // What the tiles of a strip launch compute: pixels staged and transformed forward and
 // back (all phases), or spectra that are already in memory (FFT3D temporal pass 2,
 // DFTTest slices, Kalman render), whose tiles skip the staging ring and the forward rows.
-enum class StripWork { Pixels, Temporal, Slice, Kalman };
+// Pixels: pixel tiles of plain launches; Staged: pixel tiles of batches, whose shared
+// memory also holds the two raw boxes of the bulk-tensor staging.
+enum class StripWork { Pixels, Temporal, Slice, Kalman, Staged };
 
 // Modelled duration of one strip tile of `cols` x `rows` output samples: per block row,
 // rounds of 256 threads over the row phases (nb*bh real rows forward and inverse, weight
@@ -497,8 +545,9 @@ double tile_cost(const nfd::DevPlan& d, int cols, int rows, StripWork w) {
   const int K = d.bw / 2 + 1;
   const int nb = (cols + d.bw - d.gx.step + d.gx.step - 1) / d.gx.step;
   const int br = (rows + d.bh - d.gy.step + d.gy.step - 1) / d.gy.step + 2;
-  const double wrows = w == StripWork::Pixels ? 2.0 : 1.0;
-  const double wcols = w == StripWork::Pixels ? 3.0 : w == StripWork::Slice ? 1.0 : 2.0;
+  const bool px = w == StripWork::Pixels || w == StripWork::Staged;
+  const double wrows = px ? 2.0 : 1.0;
+  const double wcols = px ? 3.0 : w == StripWork::Slice ? 1.0 : 2.0;
   return (wrows * ((nb * d.bh + 255) / 256) + wcols * ((nb * K + 255) / 256)) * br;
 }
 
@@ -532,6 +581,8 @@ std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_p
   auto shape = [&](int nbx) {
     nfd::StripShape c;
     c.tab_floats = nfd::strip_table_floats(d);
+    c.tma_box_w = 0;
+    c.raw_bytes = 0;
     c.tw = std::min(std::max(d.gx.step, (nbx - edge) * d.gx.step), d.gx.length);
     c.nbx_max = (c.tw + d.bw - 1) / d.gx.step + 2;
     c.win_max = (c.nbx_max - 1) * d.gx.step + d.bw;
@@ -540,8 +591,13 @@ std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_p
     // Staging ring: pixel tiles only (DFTTest slices, Kalman renders and FFT3D temporal
     // tiles have no pixel input). Temporal tiles of 48x48 blocks use it as the scratch
     // through which their teams of four lanes exchange row-transform runs.
-    if (work == StripWork::Pixels) {
+    if (work == StripWork::Pixels || work == StripWork::Staged) {
       c.ring_pitch = 4 * q;
+      if (work == StripWork::Staged) {  // raw boxes: staged width x step samples, two buffers
+        c.tma_box_w = tma_box_width(c, d.storage);
+        c.raw_bytes = int((size_t(c.tma_box_w) * d.gy.step * size_t(d.storage) + 127) & ~size_t(127));
+        if (c.tma_box_w == 0) c.raw_bytes = 0;
+      }
     } else if (work == StripWork::Temporal && d.bh == 48 && d.bw == 48) {  // 512-thread CTAs
       int t = (nfd::team_scratch_floats(d.bw, 512) + d.bh - 1) / d.bh;
       t = (t + 3) / 4;
@@ -605,7 +661,11 @@ std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_p
                    [](const auto& a, const auto& b) { return a.first < b.first; });
   std::vector<nfd::StripShape> out;
   for (const auto& r : ranked) out.push_back(r.second);
-  if (out.empty()) out.push_back(shape(edge + 2));  // over the budget even at its narrowest
+  if (out.empty()) {  // over the budget even at its narrowest
+    nfd::StripShape c = shape(edge + 2);
+    if (nfd::strip_smem_bytes(d.bh, d.bw, c) > size_t(227) * 1024) c.tma_box_w = c.raw_bytes = 0;
+    out.push_back(c);
+  }
   std::lock_guard<std::mutex> lock(memo_mu);
   return memo.emplace(key, out).first->second;
 }
@@ -725,6 +785,7 @@ nf_status read_error_word(const nf_plan& p, cudaStream_t st, char* err, size_t l
   if (h) {
     cudaMemsetAsync(p.err, 0, sizeof(int), st);
     cudaStreamSynchronize(st);
+    if (h & nfd::kErrStaging) return fail(err, len, "a source staging copy did not complete", NF_DEVICE_ERROR);
     return fail(err, len, "non-finite sample or intermediate", NF_NON_FINITE);
   }
   return NF_OK;
@@ -946,7 +1007,7 @@ cudaError_t launch_volume_spectra_shape(int bh, int bw, int storage, const nfd::
 template <class SmemFn>
 int pass1_chunk(int bh, int bw, int T, bool slice, int max_count, SmemFn smem) {
   const int K = bw / 2 + 1, tt = slice ? T : 1;
-  const size_t budget = size_t(bh * bw <= 256 ? 100 : 200) * 1024;
+  const size_t budget = size_t(100) * 1024;  // two CTAs per SM (spectra_batch_kernel)
   int best_n = 1;
   double best = -1.0;
   if (slice) {  // DFTTest volumes: the widest chunk within 100 KB measured fastest
@@ -1692,7 +1753,7 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
     int nvar = 1;
     for (const auto& plans : group_plans)
       for (const nf_plan* p : plans)
-        nvar = std::max(nvar, std::min(kVariants, int(strip_candidates(p->dev, 0, StripWork::Pixels).size())));
+        nvar = std::max(nvar, std::min(kVariants, int(strip_candidates(p->dev, 0, StripWork::Staged).size())));
     const std::vector<BatchGroup> proto = b->groups;
     for (int v = 0; v < nvar; ++v) {
       std::vector<BatchGroup> groups = proto;
@@ -1703,7 +1764,7 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
         std::vector<nfd::StripShape> shapes;
         for (const nf_plan* p : plans) {
           dplans.push_back(p->dev);
-          const auto& cand = strip_candidates(p->dev, 0, StripWork::Pixels);
+          const auto& cand = strip_candidates(p->dev, 0, StripWork::Staged);
           shapes.push_back(cand[std::min(size_t(v), cand.size() - 1)]);
         }
         std::vector<Entry> mine;
@@ -1716,29 +1777,42 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
         std::vector<std::pair<const nfd::DevPlan*, int>> queue;
         for (auto& e : mine) queue.emplace_back(&plans[size_t(e.plan)]->dev, shapes[size_t(e.plan)].tw);
         const int seg_h =
-            batch_segment_height(queue, g.bh, (long long)(g.bh * g.bw <= 256 ? 2 : 1) * sms, StripWork::Pixels);
+            batch_segment_height(queue, g.bh, (long long)(g.bh * g.bw <= 256 ? 2 : 1) * sms, StripWork::Staged);
         for (size_t j = 0; j < plans.size(); ++j) {
           const int segs = std::max(1, (plans[j]->t.gy.length + seg_h - 1) / seg_h);
           shapes[j].th = (plans[j]->t.gy.length + segs - 1) / segs;
           g.smem = std::max(g.smem, nfd::strip_smem_bytes(g.bh, g.bw, shapes[j]));
         }
         std::vector<nfd::PlaneJob> jobs;
-        std::vector<int> base(1, 0), tiles_x;
+        std::vector<CUtensorMap> maps;
+        std::vector<int> base(1, 0), tiles_x, map_of;
         for (auto& e : mine) {
           const nfd::StripShape& S = shapes[size_t(e.plan)];
           const nf_plan* p = plans[size_t(e.plan)];
           const int tx = (p->t.gx.length + S.tw - 1) / S.tw, ty = (p->t.gy.length + S.th - 1) / S.th;
           jobs.push_back(e.job);
+          CUtensorMap m;
+          const bool mapped = S.tma_box_w > 0 && encode_plane_map(&m, e.job.src, p->t.gx.length, p->t.gy.length,
+                                                                   e.job.src_stride, g.storage,
+                                                                   nfd::kStagingBoxBytes / g.storage, p->t.gy.step);
+          map_of.push_back(mapped ? int(maps.size()) : -1);
+          if (mapped) maps.push_back(m);
+          g.mapped += mapped ? 1 : 0;
           tiles_x.push_back(tx);
           base.push_back(base.back() + tx * ty);
         }
         Blob blob;
         const size_t o_p = blob.add(dplans), o_s = blob.add(shapes), o_j = blob.add(jobs), o_b = blob.add(base),
-                     o_t = blob.add(tiles_x);
+                     o_t = blob.add(tiles_x), o_m = blob.add(maps);  // tensor maps: 256-byte aligned
         if ((ce = cudaMalloc(&g.dev, blob.bytes.size())) != cudaSuccess) {
           b->variants.push_back(groups);  // freed with the batch
           return cuda_fail(err, len, ce, "device allocation failed");
         }
+        for (size_t i = 0; i < jobs.size(); ++i)  // jobs point at their maps in device memory
+          if (map_of[i] >= 0) {
+            jobs[i].tmap = static_cast<unsigned char*>(g.dev) + o_m + size_t(map_of[i]) * sizeof(CUtensorMap);
+            std::memcpy(blob.bytes.data() + o_j + i * sizeof(nfd::PlaneJob), &jobs[i], sizeof(nfd::PlaneJob));
+          }
         if ((ce = cudaMemcpy(g.dev, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
           b->variants.push_back(groups);
           return cuda_fail(err, len, ce, "batch upload failed");
@@ -1852,6 +1926,12 @@ nf_status nf_batch_graph_launch(nf_batch* b, void* stream, char* err, size_t len
 
 int nf_batch_geometry_count(const nf_batch* b) { return b ? int(b->variants.size()) : 0; }
 int nf_batch_geometry(const nf_batch* b) { return b ? b->chosen : -1; }
+int nf_batch_mapped_planes(const nf_batch* b) {
+  int n = 0;
+  if (b)
+    for (const auto& g : b->groups) n += g.mapped;
+  return n;
+}
 
 nf_status nf_batch_select_geometry(nf_batch* b, int index, char* err, size_t len) {
   if (!b) return fail(err, len, "null batch", NF_INVALID_ARGUMENT);

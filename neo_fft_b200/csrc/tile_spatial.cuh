@@ -25,6 +25,7 @@
 #pragma once
 #include <type_traits>
 #include "device_plan.cuh"
+#include "tma.cuh"
 
 namespace nfd {
 
@@ -80,6 +81,9 @@ struct PlaneJob {
   // form, the T slots' spatial spectra (the strip filters across them); DFTTest slice
   // form, tspec[0] = the filtered spatial spectrum of slice zt (the strip reconstructs it).
   const cf* const* tspec;
+  // Batched pixel strips: 2-D tensor map of the source plane (boxes of tma_box_w x
+  // step samples) for the prefetched staging of interior block rows, or nullptr.
+  const void* tmap;
 };
 
 // Source of a strip's block spectra.
@@ -93,6 +97,8 @@ struct StripShape {
   int win_max;    // staged input columns: (nbx_max-1)*step + bw
   int ring_pitch; // floats per staged row: a multiple of 4 with an odd float4 count
   int tab_floats; // per-plan tables staged in shared memory
+  int tma_box_w;  // bulk-tensor staging: staged width in samples, whole boxes (0: none)
+  int raw_bytes;  // bytes of each of the two raw buffers (a multiple of 128)
 };
 
 // Floats of the per-plan tables a strip stages in shared memory (strip_tile).
@@ -108,13 +114,15 @@ __host__ __device__ inline int strip_table_floats(const DevPlan& P) {
 
 // Shared layout (floats): tables | ring_in [bh][ring_pitch] | spec [bh][K][nbx]
 // complex (block fastest) | ob [bh][nbx][bw+4] (synthesised rows, x fastest) |
-// acc [bh][tw] | dc [2*nbx] | colmap [tw] (overlap-add blocks of each strip column).
+// acc [bh][tw] | dc [2*nbx] | colmap [tw] (overlap-add blocks of each strip column) |
+// raw [2][raw_bytes] source boxes of the bulk-tensor staging (128-byte aligned).
 __host__ __device__ inline size_t strip_smem_bytes(int bh, int bw, const StripShape& s) {
   const size_t K = size_t(bw / 2 + 1);
   const size_t spec_cf = (size_t(s.nbx_max) * bh * K + 1) & ~size_t(1);  // keeps ob 16-byte aligned
   return sizeof(float) * (size_t(s.tab_floats) + size_t(bh) * s.ring_pitch + spec_cf * 2 +
                           size_t(bh) * s.nbx_max * (bw + 4) + size_t(bh) * s.tw + 2 * size_t(s.nbx_max) +
-                          size_t(s.tw));
+                          size_t(s.tw)) +
+         (s.raw_bytes > 0 ? 2 * size_t(s.raw_bytes) + 128 : 0);
 }
 
 // Walks the linear indices start, start + step, ... of a rows x width range as (y, x)
@@ -219,14 +227,15 @@ template <int BHC, int BWC>
 __host__ __device__ constexpr bool team_block() {
   return BHC == 48 && BWC == 48;
 }
-// Floats of team scratch a temporal strip of `threads` threads needs in its staging ring.
-__host__ __device__ inline int team_scratch_floats(int bw, int threads) { return (threads / 4) * 2 * bw; }
+// Floats of team scratch a temporal strip of `threads` threads needs in its staging ring:
+// per team of four lanes, bw + 4 complex values (four runs of bw/4 + 1).
+__host__ __device__ inline int team_scratch_floats(int bw, int threads) { return (threads / 4) * 2 * (bw + 4); }
 
 // ALGO: 0 FFT3D, 1 DFTTest (the launch knows the plan's algorithm, so the other
 // algorithm's branches are compiled out), -1 read from the plan.
 template <int BHC, int BWC, int STORAGE, int SRC = kSrcPixels, int ALGO = -1>
 __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, const StripShape& S, int px0, int py0,
-                                           float* smem) {
+                                           float* smem, TmaPipe* pipe = nullptr) {
   const bool fft3d = ALGO >= 0 ? ALGO == 0 : P.algo == 0;
   const int BH = BHC > 0 ? BHC : P.bh;
   const int BW = BWC > 0 ? BWC : P.bw;
@@ -270,6 +279,9 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   int* colmap = reinterpret_cast<int*>(dc + 2 * NB);
   const int tid = threadIdx.x, nthr = blockDim.x;
   bool bad = false;
+  // Raw boxes of the bulk-tensor staging, 128-byte aligned after colmap.
+  unsigned char* raw = reinterpret_cast<unsigned char*>(colmap + S.tw);
+  raw += (128 - (smem_u32(raw) & 127)) & 127;
 
   __syncthreads();  // shared memory may still be read by a previous work item
   // ---- per-plan tables into shared memory --------------------------------------
@@ -337,6 +349,26 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     const int ry = in ? sy : reflect_axis(cy, gy), rx = in ? sx : reflect_axis(cx, gx);
     return load_sample<STORAGE>(J.src + ptrdiff_t(ry) * J.src_stride, rx);
   };
+  // Bulk-tensor staging (batched pixel strips with a tensor map): the strip's staged
+  // columns lie inside the plane, and a block row after the tile's first whose `step` new
+  // rows lie inside it too is copied by the elected thread one block row ahead. The box
+  // starts at the staged columns rounded down to 16 bytes (xa); tma_shift is the
+  // remainder in samples.
+  constexpr int kElem = STORAGE == kStoreU8 ? 1 : (STORAGE == kStoreU16 ? 2 : 4);
+  constexpr int kBox = kStagingBoxBytes / kElem;  // samples per box row
+  const int sx0 = cx0 - gx.offset;
+  const bool tma_cols = SRC == kSrcPixels && pipe != nullptr && J.tmap != nullptr && S.tma_box_w > 0 && !kalman_L &&
+                        sx0 >= 0 && sx0 + win <= gx.length;
+  const int tma_xa = sx0 & ~(16 / kElem - 1), tma_shift = sx0 - tma_xa;
+  const unsigned tma_bytes = unsigned(S.tma_box_w) * unsigned(gy.step) * kElem;
+  auto tma_rows = [&](int b) {  // first plane row of block row b's new rows, or -1
+    const int y = b * gy.step + BH - gy.step - gy.offset;
+    return y >= 0 && y + gy.step <= gy.length ? y : -1;
+  };
+  // The dead flag is written only inside a staging phase and read only right after a
+  // barrier that no staging phase separates from the next, so every thread of the CTA
+  // takes the same staging path in a block row.
+  bool tma_on = tma_cols && *pipe->dead == 0;
   // No barrier between a block row's retire phase (accumulator ring and the output) and the
   // next block row's first phase (staging ring, or the column phase's spectrum and DC
   // buffers): they touch disjoint shared memory, and every later phase is behind a barrier.
@@ -344,16 +376,92 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     const int oy = by * gy.step;
     if (SRC == kSrcPixels && !kalman_L) {
       // ---- 0: stage the rows this block row adds ----------------------------
+      // Prefetch block row by + 1 into buffer (by + 1) & 1, last read while staging
+      // block row by - 1 (behind that phase's barrier).
+      if (tma_on && tid == 0 && by < by_hi) {
+        const int y1 = tma_rows(by + 1);
+        if (y1 >= 0) {
+          const int nb1 = (by + 1) & 1;
+          mbar_expect_tx(pipe->mbar + nb1, tma_bytes);
+          for (int k = 0; k * kBox < S.tma_box_w; ++k)
+            tma_load_2d(raw + nb1 * S.raw_bytes + k * kStagingBoxBytes * gy.step, J.tmap, tma_xa + k * kBox, y1,
+                        pipe->mbar + nb1);
+          pipe->pending |= 1u << nb1;
+        }
+      }
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
       const int nrows = oy + BH - r0;
-      for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
-        const int cy = r0 + c.y;
-        const float sv = source_sample(cy, cx0 + c.x);
-        const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
-        if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
-        ring_in[int(unsigned(cy) % unsigned(BH)) * S.ring_pitch + c.x] = v;
+      bool staged = false;
+      if (tma_on && by > by_lo && tma_rows(by) >= 0) {
+        const int b0 = by & 1;
+        const bool ok = mbar_wait_bounded(pipe->mbar + b0, (pipe->phase >> b0) & 1u, kStagingWaitCycles);
+        if (ok) {
+          pipe->phase ^= 1u << b0;
+          if (tid == 0) pipe->pending &= ~(1u << b0);
+        } else {  // the copy did not arrive: report it, stop prefetching, read directly
+          *pipe->dead = 1;
+          atomicOr(P.err, kErrStaging);
+        }
+        // Four samples per thread. Plane row tma_rows(by) + r, column tma_xa + i is sample
+        // (i / kBox) * kBox * step + r * kBox + i % kBox of the raw boxes. A thread whose
+        // wait ran out reads its samples directly.
+        const unsigned char* rb = raw + b0 * S.raw_bytes;
+        const int q4 = (win + 3) >> 2;
+        for (Cursor2 c(tid, nthr, q4); c.y < nrows; c.next()) {
+          const int x = c.x * 4;
+          float v[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) v[j] = 0.0f;
+          const int i0 = x + tma_shift;
+          if (ok && (tma_shift & 3) == 0) {
+            // the quad lies inside one box row: one 4-, 8- or 16-byte shared load
+            const int at = (i0 / kBox) * kBox * gy.step + c.y * kBox + i0 % kBox;
+            if constexpr (STORAGE == kStoreU8) {
+              const unsigned w = *reinterpret_cast<const unsigned*>(rb + at);
+#pragma unroll
+              for (int j = 0; j < 4; ++j) v[j] = float((w >> (8 * j)) & 0xffu);
+            } else if constexpr (STORAGE == kStoreU16) {
+              const uint2 w = *reinterpret_cast<const uint2*>(rb + 2 * at);
+              v[0] = float(w.x & 0xffffu);
+              v[1] = float(w.x >> 16);
+              v[2] = float(w.y & 0xffffu);
+              v[3] = float(w.y >> 16);
+            } else {
+              const float4 w = *reinterpret_cast<const float4*>(rb + 4 * at);
+              v[0] = w.x;
+              v[1] = w.y;
+              v[2] = w.z;
+              v[3] = w.w;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int i = i0 + j;
+              if (ok) v[j] = load_sample<STORAGE>(rb, (i / kBox) * kBox * gy.step + c.y * kBox + i % kBox);
+              else if (x + j < win) v[j] = source_sample(r0 + c.y, cx0 + x + j);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            v[j] = fmul(fsub(v[j], P.dec_base), P.dec_scale);
+            if (STORAGE == kStoreF32 && x + j < win && !isfin(v[j])) bad = true;
+          }
+          *reinterpret_cast<float4*>(ring_in + int(unsigned(r0 + c.y) % unsigned(BH)) * S.ring_pitch + x) =
+              make_float4(v[0], v[1], v[2], v[3]);
+        }
+        staged = true;
+      }
+      if (!staged) {
+        for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
+          const int cy = r0 + c.y;
+          const float sv = source_sample(cy, cx0 + c.x);
+          const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
+          if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
+          ring_in[int(unsigned(cy) % unsigned(BH)) * S.ring_pitch + c.x] = v;
+        }
       }
       __syncthreads();
+      tma_on = tma_on && *pipe->dead == 0;
       // ---- A: row transforms (block index fastest) --------------------------
       for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
         const int y = c.y, b = c.x;
@@ -449,7 +557,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
 #pragma unroll
           for (int i = 0; i < TH::M; ++i) sp[(lane * TH::M + i) * KNB] = run[i];
           __syncwarp(team_mask);
-          TH::outer(lane, P.twh, [&](int q) { return sp[q * KNB]; }, [&](int y, cf v) { sp[y * KNB] = v; });
+          TH::outer(lane, P.twh, [&](int j, int i) { return sp[(j * TH::M + i) * KNB]; },
+                    [&](int y, cf v) { sp[y * KNB] = v; });
         }
       } else {
         for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
@@ -541,8 +650,10 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     if constexpr (kTeam) {
       // Row inverses shared by teams of lanes; the runs are exchanged through the team's
       // scratch (the staging ring, which temporal tiles do not use).
+      // Scratch rows of M + 1 values, T + N values per team: a lane's run stores and the
+      // outer butterflies' reads then fall in distinct banks across the warp's teams.
       using TW = nf::TeamFFT<false, BWC>;
-      cf* xs = reinterpret_cast<cf*>(ring_in) + team * BWC;
+      cf* xs = reinterpret_cast<cf*>(ring_in) + team * (BWC + TW::T);
       for (Cursor2 c(team, nteams, nbx); c.y < BH; c.next()) {
         const int y = c.y, b = c.x;
         const cf* bins = spec + y * KNB + b;
@@ -556,11 +667,11 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
           return v;
         });
 #pragma unroll
-        for (int i = 0; i < TW::M; ++i) xs[lane * TW::M + i] = run[i];
+        for (int i = 0; i < TW::M; ++i) xs[lane * (TW::M + 1) + i] = run[i];
         __syncwarp(team_mask);
         float* o = ob + (y * NB + b) * OBW;
         float guard = 0.0f;
-        TW::outer(lane, P.tww, [&](int q) { return xs[q]; }, [&](int x, cf v) {
+        TW::outer(lane, P.tww, [&](int j, int i) { return xs[j * (TW::M + 1) + i]; }, [&](int x, cf v) {
           const float r = fmul(v.r, fct);
           guard = __fmaf_rn(r, 0.0f, guard);
           o[x] = fmul(r, wxs[x]);
@@ -720,6 +831,15 @@ template <int BHC, int BWC, int STORAGE, int ALGO>
 __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_batch_kernel(BatchWork W) {
   extern __shared__ float smem[];
   __shared__ int item;
+  __shared__ alignas(8) unsigned long long s_mbar[2];
+  __shared__ int s_dead;
+  if (threadIdx.x == 0) {
+    mbar_init(s_mbar, 1);
+    mbar_init(s_mbar + 1, 1);
+    mbar_init_fence();
+    s_dead = 0;
+  }
+  TmaPipe pipe{s_mbar, &s_dead, 0u, 0u};
   const int total = W.job_tile_base[W.njobs];
   for (;;) {
     __syncthreads();
@@ -746,8 +866,13 @@ __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value) spatial_
     __syncthreads();
     const int local = t - W.job_tile_base[lo];
     const int sx = local % W.job_tiles_x[lo], sy = local / W.job_tiles_x[lo];
-    strip_tile<BHC, BWC, STORAGE, kSrcPixels, ALGO>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem);
+    strip_tile<BHC, BWC, STORAGE, kSrcPixels, ALGO>(sP, sJ, sS, sx * sS.tw, sy * sS.th, smem, &pipe);
   }
+  // Copies still in flight after a wait ran out: wait for them once more (bounded)
+  // before the CTA's shared memory is released.
+  if (threadIdx.x == 0)
+    for (int b = 0; b < 2; ++b)
+      if (pipe.pending & (1u << b)) mbar_wait_bounded(s_mbar + b, (pipe.phase >> b) & 1u, kStagingWaitCycles);
 }
 
 } // namespace nfd

@@ -38,8 +38,15 @@ __host__ __device__ inline size_t spectra_smem_bytes(int bh, int bw, int step, i
   return sizeof(float) * (((size_t(bw + bh) + 3) & ~size_t(3)) + size_t(bh) * pitch + 2 * size_t(bh) * K * nbc);
 }
 
+// Two CTAs per SM for compile-time shapes: one CTA's staging loads overlap the other's
+// transforms (the host keeps a chunk within half the SM's shared memory).
+template <int BHC, int BWC>
+struct SpectraOccupancy {
+  static constexpr int value = BHC > 0 ? 2 : 1;
+};
+
 template <int BHC, int BWC, int STORAGE>
-__global__ void __launch_bounds__(256) spectra_batch_kernel(SpectraWork W) {
+__global__ void __launch_bounds__(256, SpectraOccupancy<BHC, BWC>::value) spectra_batch_kernel(SpectraWork W) {
   extern __shared__ float smem[];
   const int BH = BHC > 0 ? BHC : W.plans[0].bh;
   const int BW = BWC > 0 ? BWC : W.plans[0].bw;

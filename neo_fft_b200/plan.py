@@ -411,6 +411,11 @@ class Batch:
         return int(self._lib.nf_batch_geometry_count(self._h))
 
     @property
+    def mapped_planes(self) -> int:
+        """Planes staged through bulk-tensor copies (2-D tensor maps) in the geometry in use."""
+        return int(self._lib.nf_batch_mapped_planes(self._h))
+
+    @property
     def geometry(self) -> int:
         """Index of the geometry in use; -1 before the first launch has tuned."""
         return int(self._lib.nf_batch_geometry(self._h))

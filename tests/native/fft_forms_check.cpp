@@ -53,7 +53,8 @@ int check_team(std::mt19937& rng) {
       for (int i = 0; i < Team::M; ++i) buf[t * Team::M + i] = local[i];
     }
     for (int t = 0; t < Team::T; ++t)
-      Team::outer(t, tw.data(), [&](int p) { return buf[p]; }, [&](int x, nf::cf v) { out[x] = v; });
+      Team::outer(t, tw.data(), [&](int j, int i) { return buf[j * Team::M + i]; },
+                  [&](int x, nf::cf v) { out[x] = v; });
     if (std::memcmp(out, ref, sizeof(out))) ++bad;
   }
   return bad;

@@ -84,31 +84,62 @@ __global__ void __launch_bounds__(256) kalman_advance_kernel(DevPlan P, int nb_p
   const size_t base = (size_t(by) * gx.count + bx0) * size_t(bins);
   cf* __restrict__ last = A.last + base;
   const float* __restrict__ pattern = A.pattern;
+  // Eight bins per thread and step: their loads are issued together before the first
+  // recursion, so each thread keeps several state reads in flight.
+  constexpr int kStep = 8;
   if (A.fp64) {
     double* __restrict__ cov = A.cov64 + base;
     double* __restrict__ proc = A.proc64 + base;
-#pragma unroll 4
-    for (int i = tid; i < n; i += nthr) {
-      const int kk = i - (i / bins) * bins;
-      cf L = last[i];
-      double c = cov[i], q = proc[i];
-      if (!kalman_bin_fp64(spec[i], L, c, q, pattern, kk, P.kalman_r0, P.kalman_ratio2)) bad = true;
-      last[i] = L;
-      cov[i] = c;
-      proc[i] = q;
+    for (int i0 = tid; i0 < n; i0 += kStep * nthr) {
+      cf L[kStep];
+      double c[kStep], q[kStep];
+#pragma unroll
+      for (int j = 0; j < kStep; ++j) {
+        const int i = i0 + j * nthr;
+        if (i < n) {
+          L[j] = last[i];
+          c[j] = cov[i];
+          q[j] = proc[i];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kStep; ++j) {
+        const int i = i0 + j * nthr;
+        if (i < n) {
+          const int kk = i - (i / bins) * bins;
+          if (!kalman_bin_fp64(spec[i], L[j], c[j], q[j], pattern, kk, P.kalman_r0, P.kalman_ratio2)) bad = true;
+          last[i] = L[j];
+          cov[i] = c[j];
+          proc[i] = q[j];
+        }
+      }
     }
   } else {
     float* __restrict__ cov = A.cov32 + base;
     float* __restrict__ proc = A.proc32 + base;
-#pragma unroll 4
-    for (int i = tid; i < n; i += nthr) {
-      const int kk = i - (i / bins) * bins;
-      cf L = last[i];
-      float c = cov[i], q = proc[i];
-      if (!kalman_bin(spec[i], L, c, q, pattern, kk, P.kalman_r0, P.kalman_ratio2)) bad = true;
-      last[i] = L;
-      cov[i] = c;
-      proc[i] = q;
+    for (int i0 = tid; i0 < n; i0 += kStep * nthr) {
+      cf L[kStep];
+      float c[kStep], q[kStep];
+#pragma unroll
+      for (int j = 0; j < kStep; ++j) {
+        const int i = i0 + j * nthr;
+        if (i < n) {
+          L[j] = last[i];
+          c[j] = cov[i];
+          q[j] = proc[i];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kStep; ++j) {
+        const int i = i0 + j * nthr;
+        if (i < n) {
+          const int kk = i - (i / bins) * bins;
+          if (!kalman_bin(spec[i], L[j], c[j], q[j], pattern, kk, P.kalman_r0, P.kalman_ratio2)) bad = true;
+          last[i] = L[j];
+          cov[i] = c[j];
+          proc[i] = q[j];
+        }
+      }
     }
   }
   if (bad) atomicOr(P.err, kErrNonFinite);

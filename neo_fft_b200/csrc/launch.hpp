@@ -87,8 +87,8 @@ NF_DECLARE_VOLUME(48, 48)
 NF_DECLARE_VOLUME(0, 0)
 #undef NF_DECLARE_VOLUME
 #define NF_DECLARE_KALMAN(BH, BW)                                                                               \
-  cudaError_t launch_kalman_##BH##x##BW(const DevPlan& d, int nb, dim3 grid, size_t smem, const void* src,      \
-                                        ptrdiff_t ss, const KalmanArgs& a, cudaStream_t st);
+  cudaError_t launch_kalman_##BH##x##BW(const DevPlan& d, const void* src, ptrdiff_t ss, const KalmanArgs& a,   \
+                                        cudaStream_t st);
 NF_DECLARE_KALMAN(8, 8)
 NF_DECLARE_KALMAN(16, 16)
 NF_DECLARE_KALMAN(32, 32)

@@ -1206,22 +1206,17 @@ __global__ void fill_kernel(T* p, size_t n, T v) {
 
 cudaError_t run_kalman_advance(const nfd::DevPlan& d, const void* src, ptrdiff_t ss, const nfd::KalmanArgs& a,
                                cudaStream_t st) {
-  const size_t per_block = size_t(d.bh) * d.K * sizeof(cf);
-  int nb = std::max(1, std::min(8, int((64 * 1024) / per_block)));
-  nb = std::min(nb, d.gx.count);
-  const size_t smem = per_block * size_t(nb);
-  const dim3 grid((d.gx.count + nb - 1) / nb, d.gy.count);
   if (d.bh == d.bw) {
     switch (d.bw) {
-      case 8: return nfd::launch_kalman_8x8(d, nb, grid, smem, src, ss, a, st);
-      case 16: return nfd::launch_kalman_16x16(d, nb, grid, smem, src, ss, a, st);
-      case 32: return nfd::launch_kalman_32x32(d, nb, grid, smem, src, ss, a, st);
-      case 12: return nfd::launch_kalman_12x12(d, nb, grid, smem, src, ss, a, st);
-      case 48: return nfd::launch_kalman_48x48(d, nb, grid, smem, src, ss, a, st);
+      case 8: return nfd::launch_kalman_8x8(d, src, ss, a, st);
+      case 16: return nfd::launch_kalman_16x16(d, src, ss, a, st);
+      case 32: return nfd::launch_kalman_32x32(d, src, ss, a, st);
+      case 12: return nfd::launch_kalman_12x12(d, src, ss, a, st);
+      case 48: return nfd::launch_kalman_48x48(d, src, ss, a, st);
       default: break;
     }
   }
-  return nfd::launch_kalman_0x0(d, nb, grid, smem, src, ss, a, st);
+  return nfd::launch_kalman_0x0(d, src, ss, a, st);
 }
 
 void check_kalman_source(const nf_plan& p, const nf_const_plane& s) {

@@ -1,6 +1,8 @@
 // Instantiates the single-frame tile kernel for one block shape (NF_BH x NF_BW,
 // 0 = runtime shape) and its three sample storages.
 #include "launch.hpp"
+
+#include <algorithm>
 #include "tile_spatial.cuh"
 #include "kalman.cuh"
 
@@ -31,13 +33,55 @@ cudaError_t launch_batch(const BatchWork& w, int ctas, size_t smem, cudaStream_t
   k<<<ctas, 256, smem, st>>>(w);
   return cudaGetLastError();
 }
+// Kalman advance: runs of nb blocks of one block row per CTA of about nb * bh threads
+// (whole warps, 64..256). The run length minimises the modelled launch time: waves of the
+// grid over the resident CTAs (the occupancy the kernel really gets) times the CTA's
+// rounds of threads over rows, columns and bins (eight bins per thread and round) plus
+// one of setup; longer runs on ties.
 template <int ST>
-cudaError_t launch_kalman_one(const DevPlan& d, int nb, dim3 grid, size_t smem, const void* src, ptrdiff_t ss,
-                              const KalmanArgs& a, cudaStream_t st) {
+cudaError_t launch_kalman_one(const DevPlan& d, const void* src, ptrdiff_t ss, const KalmanArgs& a, cudaStream_t st) {
   auto k = kalman_advance_kernel<NF_BH, NF_BW, ST>;
-  cudaError_t e = prepare(k, smem);
+  const size_t per_block = size_t(d.bh) * d.K * sizeof(cf);
+  const int nb_max = std::max(1, std::min({8, int((64 * 1024) / per_block), d.gx.count}));
+  cudaError_t e = prepare(k, per_block * size_t(nb_max));
   if (e != cudaSuccess) return e;
-  k<<<grid, 256, smem, st>>>(d, nb, static_cast<const unsigned char*>(src), ss, a);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  // the choice of the last geometry this thread launched (frames of a clip repeat it)
+  struct Choice {
+    int dev = -1, cx = 0, cy = 0, bh = 0, bw = 0, st = 0, nb = 0, threads = 0;
+  };
+  thread_local Choice last;
+  if (last.dev == dev && last.cx == d.gx.count && last.cy == d.gy.count && last.bh == d.bh && last.bw == d.bw &&
+      last.st == ST) {
+    const dim3 grid((d.gx.count + last.nb - 1) / last.nb, d.gy.count);
+    k<<<grid, last.threads, per_block * size_t(last.nb), st>>>(d, last.nb, static_cast<const unsigned char*>(src), ss,
+                                                                 a);
+    return cudaGetLastError();
+  }
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  auto rounds = [](long long tasks, int threads) { return (tasks + threads - 1) / threads; };
+  int nb = nb_max, threads = 256;
+  long long best = -1;
+  for (int r = nb_max; r >= 1; --r) {
+    const int t = std::min(256, std::max(64, (r * d.bh + 31) / 32 * 32));
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, t, per_block * size_t(r)) != cudaSuccess || occ < 1)
+      continue;
+    const long long ctas = (long long)((d.gx.count + r - 1) / r) * d.gy.count;
+    const long long slots = (long long)occ * sms;
+    const long long cost = (ctas + slots - 1) / slots *
+                           (1 + rounds((long long)r * d.bh, t) + rounds((long long)r * d.K, t) +
+                            rounds((long long)r * d.bins, 8 * t));
+    if (best < 0 || cost < best) {
+      best = cost;
+      nb = r;
+      threads = t;
+    }
+  }
+  last = Choice{dev, d.gx.count, d.gy.count, d.bh, d.bw, ST, nb, threads};
+  const dim3 grid((d.gx.count + nb - 1) / nb, d.gy.count);
+  k<<<grid, threads, per_block * size_t(nb), st>>>(d, nb, static_cast<const unsigned char*>(src), ss, a);
   return cudaGetLastError();
 }
 } // namespace
@@ -66,11 +110,11 @@ cudaError_t launch_kalman_one(const DevPlan& d, int nb, dim3 grid, size_t smem, 
     if (storage == kStoreU16) return launch_batch<kStoreU16, 1>(w, ctas, smem, st);                             \
     return launch_batch<kStoreF32, 1>(w, ctas, smem, st);                                                        \
   }                                                                                                              \
-  cudaError_t launch_kalman_##BH##x##BW(const DevPlan& d, int nb, dim3 grid, size_t smem, const void* src,       \
-                                        ptrdiff_t ss, const KalmanArgs& a, cudaStream_t st) {                   \
-    if (d.storage == kStoreU8) return launch_kalman_one<kStoreU8>(d, nb, grid, smem, src, ss, a, st);           \
-    if (d.storage == kStoreU16) return launch_kalman_one<kStoreU16>(d, nb, grid, smem, src, ss, a, st);         \
-    return launch_kalman_one<kStoreF32>(d, nb, grid, smem, src, ss, a, st);                                      \
+  cudaError_t launch_kalman_##BH##x##BW(const DevPlan& d, const void* src, ptrdiff_t ss, const KalmanArgs& a,    \
+                                        cudaStream_t st) {                                                      \
+    if (d.storage == kStoreU8) return launch_kalman_one<kStoreU8>(d, src, ss, a, st);                           \
+    if (d.storage == kStoreU16) return launch_kalman_one<kStoreU16>(d, src, ss, a, st);                         \
+    return launch_kalman_one<kStoreF32>(d, src, ss, a, st);                                                      \
   }
 NF_DEFINE(NF_BH, NF_BW)
 } // namespace nfd

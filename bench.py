@@ -734,7 +734,7 @@ def run_profile(a):
       dft16_4k the same on a u16 3840x2160 plane (input+output larger than L2)
       fft3d32  FFT3D bw=bh=32, ow=oh=16, sigma 2, u8 640x360
       fft3d48  FFT3D bt=3 bw=bh=48, ow=oh=24, sigma 3, sharpen 0.3, u16 (10-bit) 3840x2160
-      kalman32 FFT3D bt=0 (Kalman advance), bw=bh=32, float 1920x1080
+      kalman32 FFT3D bt=0 (Kalman advance and render per launch), bw=bh=32, float 1920x1080
       dft12t5  DFTTest tbsize 5 tmode 1, sbsize 12 / sosize 9, ftype 1, float 1920x1080
       clip12t5 DFTTest tbsize 5 tmode 1 sbsize 12 / sosize 9 ftype 1, float 1920x1080 clip of 10
                frames as one clip batch (volume spectra pass + slice strips) per launch
@@ -785,8 +785,10 @@ def run_profile(a):
         plan = Plan(w, h, SampleFormat(32, True), FFT3DConfig(bw=32, bh=32, bt=0, sigma=2.5, kratio=2.0))
         state = plan.initial_kalman()
         src = torch.from_numpy(_plane(h, w, np.float32, 0, 1, 1)).to(dev)
+        out = torch.empty_like(src)
         for _ in range(a.launches):
             plan.advance_kalman(src, state)
+            plan.render_kalman(src, out, state)
         torch.cuda.synchronize()
         plan.sync_status()
         return

@@ -43,7 +43,9 @@ struct BatchWork;
   cudaError_t launch_spatial_##BH##x##BW(const DevPlan& d, const StripShape& s, dim3 grid, size_t smem,         \
                                          const PlaneJobs& job, cudaStream_t st);                                \
   cudaError_t launch_spatial_batch_##BH##x##BW(int storage, int algo, const BatchWork& w, int ctas, size_t smem, \
-                                               cudaStream_t st);
+                                               cudaStream_t st);                                                \
+  cudaError_t launch_kalman_render_##BH##x##BW(const DevPlan& d, const StripShape& s, dim3 grid, size_t smem,   \
+                                               const PlaneJobs& job, cudaStream_t st);
 NF_DECLARE_SPATIAL(8, 8)
 NF_DECLARE_SPATIAL(16, 16)
 NF_DECLARE_SPATIAL(32, 32)

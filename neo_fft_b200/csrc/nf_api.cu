@@ -527,7 +527,6 @@ Checked validate_call(const nf_plan& p, const nf_const_plane* sources, int n, co
 }
 
 // Resident CTAs of the plain launch: two per SM for blocks up to 16x16, else one.
-int plain_ctas(const nfd::DevPlan& d) { return (d.bh * d.bw <= 256 ? 2 : 1) * 148; }
 
 // What the tiles of a strip launch compute: pixels staged and transformed forward and
 // back (all phases), or spectra that are already in memory (FFT3D temporal pass 2,
@@ -535,6 +534,14 @@ int plain_ctas(const nfd::DevPlan& d) { return (d.bh * d.bw <= 256 ? 2 : 1) * 14
 // Pixels: pixel tiles of plain launches; Staged: pixel tiles of batches, whose shared
 // memory also holds the two raw boxes of the bulk-tensor staging.
 enum class StripWork { Pixels, Temporal, Slice, Kalman, Staged };
+
+// Resident CTAs of a plain strip launch: two per SM up to 16x16 blocks, and for Kalman
+// renders up to 32x32 (kalman_render_kernel); one otherwise.
+bool two_per_sm(const nfd::DevPlan& d, StripWork w) {
+  return d.bh * d.bw <= 256 || (w == StripWork::Kalman && d.bh * d.bw <= 1024 && d.bh == d.bw &&
+                                (d.bw == 8 || d.bw == 12 || d.bw == 16 || d.bw == 32));
+}
+int plain_ctas(const nfd::DevPlan& d, StripWork w) { return (two_per_sm(d, w) ? 2 : 1) * 148; }
 
 // Modelled duration of one strip tile of `cols` x `rows` output samples: per block row,
 // rounds of 256 threads over the row phases (nb*bh real rows forward and inverse, weight
@@ -608,8 +615,8 @@ std::vector<nfd::StripShape> strip_candidates(const nfd::DevPlan& d, int plain_p
     c.th = d.gy.length;
     return c;
   };
-  const size_t budget = size_t(d.bh * d.bw <= 256 ? 110 : 200) * 1024;
-  const int slots = plain_ctas(d);
+  const size_t budget = size_t(two_per_sm(d, work) ? 110 : 200) * 1024;
+  const int slots = plain_ctas(d, work);
   std::vector<std::pair<double, nfd::StripShape>> ranked;
   std::vector<double> costs;
   for (int nbx = edge + 2; nbx <= 128; ++nbx) {
@@ -736,6 +743,19 @@ cudaError_t run_spatial_planes(const nfd::DevPlan& d, const nfd::PlaneJobs& J, c
   const nfd::StripShape S = pick_strip(d, J.n, render ? StripWork::Kalman : StripWork::Pixels);
   const size_t smem = nfd::strip_smem_bytes(d.bh, d.bw, S);
   const dim3 grid((d.gx.length + S.tw - 1) / S.tw, (d.gy.length + S.th - 1) / S.th, J.n);
+  if (render) {
+    if (d.bh == d.bw) {
+      switch (d.bw) {
+        case 8: return nfd::launch_kalman_render_8x8(d, S, grid, smem, J, st);
+        case 16: return nfd::launch_kalman_render_16x16(d, S, grid, smem, J, st);
+        case 32: return nfd::launch_kalman_render_32x32(d, S, grid, smem, J, st);
+        case 12: return nfd::launch_kalman_render_12x12(d, S, grid, smem, J, st);
+        case 48: return nfd::launch_kalman_render_48x48(d, S, grid, smem, J, st);
+        default: break;
+      }
+    }
+    return nfd::launch_kalman_render_0x0(d, S, grid, smem, J, st);
+  }
   return launch_spatial_shape(d, S, grid, smem, J, st);
 }
 
@@ -1147,7 +1167,8 @@ nf_status run_two_pass(const nf_plan& p, const nfd::DevPlan& d, const nf_const_p
     w.job_tiles_x = reinterpret_cast<const int*>(b + o_hdr + offsetof(TwoPassHeader, tiles_x));
     w.njobs = 1;
     w.counter = reinterpret_cast<int*>(b + o_hdr + offsetof(TwoPassHeader, counter));
-    e = launch_temporal_shape(t.bh, t.bw, storage, slice ? 1 : 0, w, std::min(tx * ty, plain_ctas(d)), smem2, st);
+    const int ctas2 = std::min(tx * ty, plain_ctas(d, slice ? StripWork::Slice : StripWork::Temporal));
+    e = launch_temporal_shape(t.bh, t.bw, storage, slice ? 1 : 0, w, ctas2, smem2, st);
   }
   cudaFreeAsync(scratch, st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");

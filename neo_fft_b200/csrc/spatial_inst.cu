@@ -25,6 +25,15 @@ cudaError_t launch_one(const DevPlan& d, const StripShape& S, dim3 grid, size_t 
   k<<<grid, 256, smem, st>>>(d, S, job);
   return cudaGetLastError();
 }
+template <int ST>
+cudaError_t launch_render(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem, const PlaneJobs& job,
+                          cudaStream_t st) {
+  auto k = kalman_render_kernel<NF_BH, NF_BW, ST>;
+  cudaError_t e = prepare(k, smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, 256, smem, st>>>(d, S, job);
+  return cudaGetLastError();
+}
 template <int ST, int ALGO>
 cudaError_t launch_batch(const BatchWork& w, int ctas, size_t smem, cudaStream_t st) {
   auto k = spatial_batch_kernel<NF_BH, NF_BW, ST, ALGO>;
@@ -109,6 +118,12 @@ cudaError_t launch_kalman_one(const DevPlan& d, const void* src, ptrdiff_t ss, c
     if (storage == kStoreU8) return launch_batch<kStoreU8, 1>(w, ctas, smem, st);                               \
     if (storage == kStoreU16) return launch_batch<kStoreU16, 1>(w, ctas, smem, st);                             \
     return launch_batch<kStoreF32, 1>(w, ctas, smem, st);                                                        \
+  }                                                                                                              \
+  cudaError_t launch_kalman_render_##BH##x##BW(const DevPlan& d, const StripShape& S, dim3 grid, size_t smem,   \
+                                               const PlaneJobs& job, cudaStream_t st) {                         \
+    if (d.storage == kStoreU8) return launch_render<kStoreU8>(d, S, grid, smem, job, st);                       \
+    if (d.storage == kStoreU16) return launch_render<kStoreU16>(d, S, grid, smem, job, st);                     \
+    return launch_render<kStoreF32>(d, S, grid, smem, job, st);                                                  \
   }                                                                                                              \
   cudaError_t launch_kalman_##BH##x##BW(const DevPlan& d, const void* src, ptrdiff_t ss, const KalmanArgs& a,    \
                                         cudaStream_t st) {                                                      \

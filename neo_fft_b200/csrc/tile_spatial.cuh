@@ -87,9 +87,10 @@ struct PlaneJob {
 };
 
 // Source of a strip's block spectra.
-constexpr int kSrcPixels = 0;    // source pixels (or a Kalman estimate)
+constexpr int kSrcPixels = 0;    // source pixels
 constexpr int kSrcTemporal = 1;  // FFT3D bt=2..5 slot spectra, filtered across time here
 constexpr int kSrcSlice = 2;     // DFTTest tmode 1 filtered slice spectra
+constexpr int kSrcKalman = 3;    // FFT3D Kalman render: the state's estimate L (PlaneJob::kalman_L)
 
 struct StripShape {
   int tw, th;     // strip width and segment height (plane pixels)
@@ -249,6 +250,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   const bool codelet = kCodelet || (BHC == 0 && P.codelet != 0);
   const DevAxis gx = P.gx, gy = P.gy;
   const cf* kalman_L = J.kalman_L;
+  (void)kalman_L;
   const int NB = S.nbx_max;   // block stride of spec and ob
   const int OBW = BW + 4;     // ob row pitch (conflict-free float4 stores and overlap reads)
   // FFT3D temporal tiles of 48x48 blocks share each 48-point transform among a team of
@@ -357,8 +359,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   constexpr int kElem = STORAGE == kStoreU8 ? 1 : (STORAGE == kStoreU16 ? 2 : 4);
   constexpr int kBox = kStagingBoxBytes / kElem;  // samples per box row
   const int sx0 = cx0 - gx.offset;
-  const bool tma_cols = SRC == kSrcPixels && pipe != nullptr && J.tmap != nullptr && S.tma_box_w > 0 && !kalman_L &&
-                        sx0 >= 0 && sx0 + win <= gx.length;
+  const bool tma_cols = SRC == kSrcPixels && pipe != nullptr && J.tmap != nullptr && S.tma_box_w > 0 && sx0 >= 0 &&
+                        sx0 + win <= gx.length;
   const int tma_xa = sx0 & ~(16 / kElem - 1), tma_shift = sx0 - tma_xa;
   const unsigned tma_bytes = unsigned(S.tma_box_w) * unsigned(gy.step) * kElem;
   auto tma_rows = [&](int b) {  // first plane row of block row b's new rows, or -1
@@ -374,7 +376,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   // buffers): they touch disjoint shared memory, and every later phase is behind a barrier.
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
-    if (SRC == kSrcPixels && !kalman_L) {
+    if constexpr (SRC == kSrcPixels) {
       // ---- 0: stage the rows this block row adds ----------------------------
       // Prefetch block row by + 1 into buffer (by + 1) & 1, last read while staging
       // block row by - 1 (behind that phase's barrier).
@@ -583,7 +585,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       cf col[CAPH];
       cf* sp = spec + k * NB + b;  // + y*KNB
       if (active) {
-        if (kalman_L) {
+        if constexpr (SRC == kSrcKalman) {
           const cf* L = kalman_L + (size_t(by) * gx.count + (bx_lo + b)) * P.bins + k;
 #pragma unroll UH
           for (int y = 0; y < CAPH; ++y)
@@ -811,6 +813,21 @@ __global__ void __launch_bounds__(256, StripOccupancy<BHC, BWC>::value)
   extern __shared__ float smem[];
   strip_tile<BHC, BWC, STORAGE, kSrcPixels, ALGO>(P, J.job[blockIdx.z], S, blockIdx.x * S.tw, blockIdx.y * S.th,
                                                   smem);
+}
+
+// Kalman render (plan.cpp:471-477): the inverse transforms of the state's estimate and
+// the enhancement, per plain strip tile. Blocks up to 32x32 run two CTAs per SM (the
+// render holds one column transform at a time, with no staging ring or forward rows).
+template <int BHC, int BWC>
+struct RenderOccupancy {
+  static constexpr int value = (BHC > 0 && BHC * BWC <= 1024) ? 2 : 1;
+};
+
+template <int BHC, int BWC, int STORAGE>
+__global__ void __launch_bounds__(256, RenderOccupancy<BHC, BWC>::value)
+    kalman_render_kernel(DevPlan P, StripShape S, const __grid_constant__ PlaneJobs J) {
+  extern __shared__ float smem[];
+  strip_tile<BHC, BWC, STORAGE, kSrcKalman, 0>(P, J.job[blockIdx.z], S, blockIdx.x * S.tw, blockIdx.y * S.th, smem);
 }
 
 // Batched launch: a persistent grid pulls (plane, strip, segment) work items from

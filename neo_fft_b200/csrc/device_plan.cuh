@@ -163,6 +163,25 @@ NF_HD cf spectral_bin(cf x, const cf* grid, int k, float scale, const DevSpectra
   return out;
 }
 
+// spectral_bin<kFt0Ratio> (DFTTest ftype 0, plain Wiener ratio) with its error test
+// folded into one multiply-add: the gain is max((power - a)/(power + 1e-15), 0) with
+// a finite table value a >= 0, so it lies in [0, 1] and each output, a point between
+// the bin and the template term, is finite whenever the bin, the template term and the
+// power are. A non-finite bin, template term, power or table value makes the gain NaN,
+// and a NaN gain turns `guard` NaN (x * 0 is NaN for inf and NaN): the caller tests
+// guard once instead of three compares per bin.
+NF_HD cf ratio_bin(cf x, const cf* grid, int k, float scale, const DevSpectral& p, float& guard) {
+  const float a = p.primary ? p.primary[k] : p.a;
+  const float mr = grid ? fmul(scale, grid[k].r) : 0.0f;
+  const float mi = grid ? fmul(scale, grid[k].i) : 0.0f;
+  const float re = fsub(x.r, mr), im = fsub(x.i, mi);
+  const float power = fadd(fmul(re, re), fmul(im, im));
+  const float r = fdiv(fsub(power, a), fadd(power, 1e-15f));
+  const float gain = r < 0.0f ? 0.0f : r;
+  guard = nf::ffma(gain, 0.0f, guard);
+  return {fadd(fmul(gain, re), mr), fadd(fmul(gain, im), mi)};
+}
+
 // One bin of kalman_scalar (src/kernels/scalar/kalman.cpp:3-24) in binary32, the
 // reference's specified operation order. Returns false on a non-finite value.
 NF_HD bool kalman_bin(cf x, cf& last, float& cov, float& proc, const float* pattern, int k, float uniform,

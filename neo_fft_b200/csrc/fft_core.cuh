@@ -254,6 +254,123 @@ NF_HD void fft32(cf* v) {
   }
 }
 
+// Real-row forms of the 16-point codelet transform. The codelet transforms a real
+// row as complex data with zero imaginary parts and inverts a half spectrum after
+// mirroring it into a full conjugate-symmetric array (fft16x16_avx2.cpp:239-262 and
+// 400-430). On such data many of fft16's operations add or subtract an exact zero,
+// negate a value (0 - x), or recompute another operation's result with its sign or
+// its real and imaginary parts exchanged: with c = cos(pi/4) = sin(pi/4) in the
+// table, W16^6 * conj(z) = (-re, im) of W16^2 * z, and round(-a) = -round(a) under
+// round-to-nearest. These forms keep every other operation of fft16, in its order
+// and with its rounding, and skip those. Each result equals fft16's: an exactly
+// zero result may carry the other sign, and nothing else differs (a signed zero
+// changes no later nonzero value: every divisor in the pipeline is positive).
+
+// Bins 0..8 (at `stride`) of the forward transform of 16 real samples; the DC and
+// Nyquist imaginary parts are 0, as the codelet stores them.
+NF_HD void fft16_real_forward(const float* x, cf* X, int stride) {
+  // span 2 on the bit-reversed pairs
+  float s[16];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int p = ((j & 1) << 2) | (j & 2) | ((j & 4) >> 2);  // bit-reversed j (3 bits)
+    s[2 * j] = fadd(x[p], x[p + 8]);
+    s[2 * j + 1] = fsub(x[p], x[p + 8]);
+  }
+  // span 4, group g (positions 4g..4g+3): (R0, (p,-q), R2, (p,q)) with p = s[4g+1],
+  // q = s[4g+3]; the j-rotation of the real q only moves it into the imaginary part.
+  float R0[4], R2[4];
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    R0[g] = fadd(s[4 * g], s[4 * g + 2]);
+    R2[g] = fsub(s[4 * g], s[4 * g + 2]);
+  }
+  // span 8, half h (groups 2h and 2h+1, positions 8h..8h+7):
+  // (e0, c1, (R2, -R2'), c3, e4, conj(c3), (R2, R2'), conj(c1)).
+  float e0[2], e4[2];
+  cf c1[2], c3[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int g0 = 2 * h, g1 = 2 * h + 1;
+    e0[h] = fadd(R0[g0], R0[g1]);
+    e4[h] = fsub(R0[g0], R0[g1]);
+    const float p = s[4 * g0 + 1], q = s[4 * g0 + 3];
+    const cf v1 = cmul_codelet<true>(cf{s[4 * g1 + 1], -s[4 * g1 + 3]}, tw16r(2), tw16i(2));
+    c1[h] = {fadd(p, v1.r), fadd(-q, v1.i)};
+    c3[h] = {fsub(p, v1.r), fadd(q, v1.i)};  // W16^6 * (p',q') = (-v1.r, v1.i)
+  }
+  // span 16: X[k] = A[k] + W16^k B[k] for the two halves A and B.
+  const float ra = R2[0], rb = R2[1], ra2 = R2[2], rb2 = R2[3];
+  X[0] = {fadd(e0[0], e0[1]), 0.0f};
+  X[8 * stride] = {fsub(e0[0], e0[1]), 0.0f};
+  X[stride] = cadd(c1[0], cmul_codelet<true>(c1[1], tw16r(1), tw16i(1)));
+  const cf t2 = cmul_codelet<true>(cf{ra2, -rb2}, tw16r(2), tw16i(2));
+  X[2 * stride] = {fadd(ra, t2.r), fadd(-rb, t2.i)};
+  X[3 * stride] = cadd(c3[0], cmul_codelet<true>(c3[1], tw16r(3), tw16i(3)));
+  X[4 * stride] = {e4[0], -e4[1]};
+  X[5 * stride] = cadd(cf{c3[0].r, -c3[0].i}, cmul_codelet<true>(cf{c3[1].r, -c3[1].i}, tw16r(5), tw16i(5)));
+  X[6 * stride] = {fsub(ra, t2.r), fadd(rb, t2.i)};  // W16^6 * conj(B2) = (-t2.r, t2.i)
+  X[7 * stride] = cadd(cf{c1[0].r, -c1[0].i}, cmul_codelet<true>(cf{c1[1].r, -c1[1].i}, tw16r(7), tw16i(7)));
+}
+
+// Inverse of one real row from bins 0..8 (at `stride`): the 16 real outputs of fft16
+// over the mirrored half spectrum, times fct. The imaginary parts of the DC and
+// Nyquist bins reach only imaginary outputs and are not read.
+NF_HD void fft16_real_inverse(const cf* Y, int stride, float fct, float* out) {
+  const cf y0 = Y[0], y1 = Y[stride], y2 = Y[2 * stride], y3 = Y[3 * stride], y4 = Y[4 * stride],
+           y5 = Y[5 * stride], y6 = Y[6 * stride], y7 = Y[7 * stride], y8 = Y[8 * stride];
+  // span 2 over (Y0,Y8) (Y4,~Y4) (Y2,~Y6) (Y6,~Y2) (Y1,~Y7) (Y5,~Y3) (Y3,~Y5) (Y7,~Y1)
+  const float s0 = fadd(y0.r, y8.r), s1 = fsub(y0.r, y8.r);
+  const float y4r2 = fadd(y4.r, y4.r), y4i2 = fadd(y4.i, y4.i);
+  const cf P = {fadd(y2.r, y6.r), fsub(y2.i, y6.i)}, M = {fsub(y2.r, y6.r), fadd(y2.i, y6.i)};
+  const cf Q = {fadd(y1.r, y7.r), fsub(y1.i, y7.i)}, N = {fsub(y1.r, y7.r), fadd(y1.i, y7.i)};
+  const cf S = {fadd(y5.r, y3.r), fsub(y5.i, y3.i)}, T = {fsub(y5.r, y3.r), fadd(y5.i, y3.i)};
+  // span 4. Group 0: real parts only (these positions are never rotated later).
+  const float e0 = fadd(s0, y4r2), e2 = fsub(s0, y4r2), e1 = fsub(s1, y4i2), e3 = fadd(s1, y4i2);
+  // group 1: (2P.r, 0), (D, -D), (0, 2P.i), (Sg, Sg)
+  const float p2r = fadd(P.r, P.r), p2i = fadd(P.i, P.i);
+  const float D = fsub(M.r, M.i), Sg = fadd(M.r, M.i);
+  // group 2; group 3 is (~q8, (-q9.i, -q9.r), (-q10.r, q10.i), (q11.i, q11.r))
+  const cf q8 = cadd(Q, S), q10 = csub(Q, S);
+  const cf q9 = {fsub(N.r, T.i), fadd(N.i, T.r)}, q11 = {fadd(N.r, T.i), fsub(N.i, T.r)};
+  // span 8, half 0 (real parts)
+  const float b0 = fadd(e0, p2r), b4 = fsub(e0, p2r);
+  const float v1r = ffma(D, tw16r(2), fmul(D, tw16i(2)));
+  const float b1 = fadd(e1, v1r), b5 = fsub(e1, v1r);
+  const float b2 = fsub(e2, p2i), b6 = fadd(e2, p2i);
+  const float v3r = ffma(Sg, tw16r(6), -fmul(Sg, tw16i(6)));
+  const float b3 = fadd(e3, v3r), b7 = fsub(e3, v3r);
+  // span 8, half 1: f0 = (2 q8.r, 0), f4 = (0, 2 q8.i), f2 = (D2, -D2), f6 = (S2, S2)
+  const float f0r = fadd(q8.r, q8.r), f4i = fadd(q8.i, q8.i);
+  const cf w1 = cmul_codelet<false>(cf{-q9.i, -q9.r}, tw16r(2), tw16i(2));
+  const cf f1 = cadd(q9, w1), f5 = csub(q9, w1);
+  const float D2 = fsub(q10.r, q10.i), S2 = fadd(q10.r, q10.i);
+  const cf w3 = cmul_codelet<false>(cf{q11.i, q11.r}, tw16r(6), tw16i(6));
+  const cf f3 = cadd(q11, w3), f7 = csub(q11, w3);
+  // span 16, real parts: x[k] = b[k] + re(W16^k f[k]), x[k+8] = b[k] - re(W16^k f[k])
+  auto rot = [](cf f, float wr, float wi) { return ffma(f.r, wr, -fmul(f.i, wi)); };
+  const float t1 = rot(f1, tw16r(1), tw16i(1)), t3 = rot(f3, tw16r(3), tw16i(3));
+  const float t5 = rot(f5, tw16r(5), tw16i(5)), t7 = rot(f7, tw16r(7), tw16i(7));
+  const float t2 = ffma(D2, tw16r(2), fmul(D2, tw16i(2)));
+  const float t6 = ffma(S2, tw16r(6), -fmul(S2, tw16i(6)));
+  out[0] = fmul(fadd(b0, f0r), fct);
+  out[8] = fmul(fsub(b0, f0r), fct);
+  out[1] = fmul(fadd(b1, t1), fct);
+  out[9] = fmul(fsub(b1, t1), fct);
+  out[2] = fmul(fadd(b2, t2), fct);
+  out[10] = fmul(fsub(b2, t2), fct);
+  out[3] = fmul(fadd(b3, t3), fct);
+  out[11] = fmul(fsub(b3, t3), fct);
+  out[4] = fmul(fsub(b4, f4i), fct);
+  out[12] = fmul(fadd(b4, f4i), fct);
+  out[5] = fmul(fadd(b5, t5), fct);
+  out[13] = fmul(fsub(b5, t5), fct);
+  out[6] = fmul(fadd(b6, t6), fct);
+  out[14] = fmul(fsub(b6, t6), fct);
+  out[7] = fmul(fadd(b7, t7), fct);
+  out[15] = fmul(fsub(b7, t7), fct);
+}
+
 // ---------------------------------------------------------------------------
 // Project mixed-radix DIT transform for arbitrary lengths.
 // ---------------------------------------------------------------------------
@@ -643,6 +760,12 @@ NF_HD bool is_codelet_length(int n) { return n == 8 || n == 16 || n == 32; }
 // fft32x32_avx2.cpp:329-335); the project transform does the same for every even W.
 template <int WC>
 NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool codelet, int bin_stride = 1) {
+  if constexpr (WC == 16) {
+    if (codelet) {  // the real-row form of the 16-point codelet transform
+      fft16_real_forward(x, bins, bin_stride);
+      return;
+    }
+  }
   const int w = WC > 0 ? WC : w_rt;
   constexpr int CAP = WC > 0 ? WC : kMaxProject;
   constexpr int U = WC > 0 ? CAP : 1;
@@ -666,6 +789,12 @@ NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool
 template <int WC>
 NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf* table, bool codelet,
                        int bin_stride = 1) {
+  if constexpr (WC == 16) {
+    if (codelet) {  // the real-row form of the 16-point codelet transform
+      fft16_real_inverse(bins, bin_stride, fct, out);
+      return;
+    }
+  }
   const int w = WC > 0 ? WC : w_rt;
   constexpr int CAP = WC > 0 ? WC : kMaxProject;
   constexpr int U = WC > 0 ? CAP : 1;

@@ -605,9 +605,17 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         // column instead of a switch per bin.
         auto filter_column = [&](auto ft) {
           constexpr int FT = decltype(ft)::value;
+          if constexpr (FT == kFt0Ratio) {
+            float guard = 0.0f;
 #pragma unroll UH
-          for (int y = 0; y < CAPH; ++y)
-            if (y < BH) col[y] = spectral_bin<FT>(col[y], grid, y * K + k, g, filt, bad);
+            for (int y = 0; y < CAPH; ++y)
+              if (y < BH) col[y] = ratio_bin(col[y], grid, y * K + k, g, filt, guard);
+            if (guard != guard) bad = true;
+          } else {
+#pragma unroll UH
+            for (int y = 0; y < CAPH; ++y)
+              if (y < BH) col[y] = spectral_bin<FT>(col[y], grid, y * K + k, g, filt, bad);
+          }
         };
         if (ALGO == 1) {
           switch (filt.type) {

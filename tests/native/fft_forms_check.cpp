@@ -73,3 +73,57 @@ extern "C" int fft_forms_mismatches() {
          check<8>(rng) + check<9>(rng) + check<12>(rng) + check<15>(rng) + check<16>(rng) + check<20>(rng) +
          check<24>(rng) + check<32>(rng) + check<48>(rng) + check<64>(rng) + check<11>(rng) + check<13>(rng);
 }
+
+namespace {
+// Equal as numbers: +0 == -0 and NaN == NaN (the real-row forms may give an exact zero
+// the other sign and nothing else).
+bool same_value(float a, float b) { return (a != a && b != b) || a == b; }
+bool same_bits(float a, float b) { return std::memcmp(&a, &b, sizeof a) == 0; }
+
+float draw(std::mt19937& rng, bool structured) {
+  std::normal_distribution<float> d(0.f, 1.f);
+  if (!structured) return d(rng) * 300.0f;
+  const float pool[] = {0.0f, -0.0f, 1.0f, -1.0f, 2.5f, 2.5f, 1e-38f, -3e-39f, 1e38f, -1e38f,
+                        INFINITY, -INFINITY, NAN, 7.0f, 7.0f, 7.0f};
+  const unsigned pick = rng() % 24u;
+  return pick < 16 ? pool[pick] : d(rng);
+}
+} // namespace
+
+// The real-row forms of the 16-point codelet transform (row_forward<16>,
+// row_inverse<16>) against fft16 on complex data with zero imaginary parts and on the
+// mirrored half spectrum: identical bits on generic data, identical values (zero signs
+// aside, NaN where the other has NaN) on rows of zeros, repeats, infinities and NaNs.
+extern "C" int fft16_real_mismatches(int structured) {
+  std::mt19937 rng(structured ? 29 : 17);
+  int bad = 0;
+  auto same = [&](float a, float b) { return structured ? same_value(a, b) : same_bits(a, b); };
+  for (int trial = 0; trial < 4000; ++trial) {
+    float x[16];
+    // structured rows: a flat row, a row of one repeated pair, or draws from the pool
+    const int kind = structured ? trial % 3 : 2;
+    for (int k = 0; k < 16; ++k) x[k] = kind == 0 ? 5.0f : kind == 1 ? (k & 1 ? -2.0f : 2.0f) : draw(rng, structured);
+    if (structured && trial % 7 == 0) x[trial % 16] = -0.0f;
+    nf::cf got[9], ref[16];
+    nf::row_forward<16>(x, 16, got, nullptr, true);
+    for (int k = 0; k < 16; ++k) ref[k] = {x[k], 0.0f};
+    nf::fft16<true>(ref);
+    ref[8].i = 0.0f;
+    for (int k = 0; k < 9; ++k)
+      if (!same(got[k].r, ref[k].r) || !same(got[k].i, ref[k].i)) ++bad;
+    nf::cf bins[9];
+    for (int k = 0; k < 9; ++k) bins[k] = {draw(rng, structured), draw(rng, structured)};
+    if (structured && trial % 5 == 0)
+      for (int k = 0; k < 9; ++k) bins[k] = bins[trial % 9];
+    float out[16];
+    const float fct = 1.0f / 256.0f;
+    nf::row_inverse<16>(bins, 16, fct, out, nullptr, true);
+    nf::cf a[16];
+    for (int k = 0; k <= 8; ++k) a[k] = bins[k];
+    for (int k = 1; k < 8; ++k) a[16 - k] = {bins[k].r, 0.0f - bins[k].i};
+    nf::fft16<false>(a);
+    for (int k = 0; k < 16; ++k)
+      if (!same(out[k], a[k].r * fct)) ++bad;
+  }
+  return bad;
+}

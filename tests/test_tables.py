@@ -195,3 +195,8 @@ def test_project_transform_forms_identical():
     assert lib.fft_forms_mismatches() == 0
     # the team form (a transform shared by four lanes, used by the 48x48 kernels) too
     assert lib.fft_team_mismatches() == 0
+    # the real-row forms of the 16-point codelet transform (row_forward/row_inverse<16>):
+    # identical bits on generic rows; on rows of zeros, repeats, infinities and NaNs
+    # identical values, the sign of an exact zero aside
+    assert lib.fft16_real_mismatches(0) == 0
+    assert lib.fft16_real_mismatches(1) == 0

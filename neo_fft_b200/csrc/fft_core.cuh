@@ -267,7 +267,9 @@ NF_HD void fft32(cf* v) {
 // changes no later nonzero value: every divisor in the pipeline is positive).
 
 // Bins 0..8 (at `stride`) of the forward transform of 16 real samples; the DC and
-// Nyquist imaginary parts are 0, as the codelet stores them.
+// Nyquist imaginary parts are 0, as the codelet stores them. ALL: bins 9..15 too (the
+// halves of the 32-point transform).
+template <bool ALL = false>
 NF_HD void fft16_real_forward(const float* x, cf* X, int stride) {
   // span 2 on the bit-reversed pairs
   float s[16];
@@ -303,19 +305,35 @@ NF_HD void fft16_real_forward(const float* x, cf* X, int stride) {
   const float ra = R2[0], rb = R2[1], ra2 = R2[2], rb2 = R2[3];
   X[0] = {fadd(e0[0], e0[1]), 0.0f};
   X[8 * stride] = {fsub(e0[0], e0[1]), 0.0f};
-  X[stride] = cadd(c1[0], cmul_codelet<true>(c1[1], tw16r(1), tw16i(1)));
+  const cf t1 = cmul_codelet<true>(c1[1], tw16r(1), tw16i(1));
   const cf t2 = cmul_codelet<true>(cf{ra2, -rb2}, tw16r(2), tw16i(2));
+  const cf t3 = cmul_codelet<true>(c3[1], tw16r(3), tw16i(3));
+  const cf t5 = cmul_codelet<true>(cf{c3[1].r, -c3[1].i}, tw16r(5), tw16i(5));
+  const cf t7 = cmul_codelet<true>(cf{c1[1].r, -c1[1].i}, tw16r(7), tw16i(7));
+  const cf a5 = {c3[0].r, -c3[0].i}, a7 = {c1[0].r, -c1[0].i};
+  X[stride] = cadd(c1[0], t1);
   X[2 * stride] = {fadd(ra, t2.r), fadd(-rb, t2.i)};
-  X[3 * stride] = cadd(c3[0], cmul_codelet<true>(c3[1], tw16r(3), tw16i(3)));
+  X[3 * stride] = cadd(c3[0], t3);
   X[4 * stride] = {e4[0], -e4[1]};
-  X[5 * stride] = cadd(cf{c3[0].r, -c3[0].i}, cmul_codelet<true>(cf{c3[1].r, -c3[1].i}, tw16r(5), tw16i(5)));
+  X[5 * stride] = cadd(a5, t5);
   X[6 * stride] = {fsub(ra, t2.r), fadd(rb, t2.i)};  // W16^6 * conj(B2) = (-t2.r, t2.i)
-  X[7 * stride] = cadd(cf{c1[0].r, -c1[0].i}, cmul_codelet<true>(cf{c1[1].r, -c1[1].i}, tw16r(7), tw16i(7)));
+  X[7 * stride] = cadd(a7, t7);
+  if constexpr (ALL) {  // X[k + 8] = A[k] - W16^k B[k]
+    X[9 * stride] = csub(c1[0], t1);
+    X[10 * stride] = {fsub(ra, t2.r), fsub(-rb, t2.i)};
+    X[11 * stride] = csub(c3[0], t3);
+    X[12 * stride] = {e4[0], e4[1]};
+    X[13 * stride] = csub(a5, t5);
+    X[14 * stride] = {fadd(ra, t2.r), fsub(rb, t2.i)};
+    X[15 * stride] = csub(a7, t7);
+  }
 }
 
 // Inverse of one real row from bins 0..8 (at `stride`): the 16 real outputs of fft16
-// over the mirrored half spectrum, times fct. The imaginary parts of the DC and
-// Nyquist bins reach only imaginary outputs and are not read.
+// over the mirrored half spectrum, times fct (SCALE) or unscaled (the even half of the
+// 32-point inverse). The imaginary parts of the DC and Nyquist bins reach only
+// imaginary outputs and are not read.
+template <bool SCALE = true>
 NF_HD void fft16_real_inverse(const cf* Y, int stride, float fct, float* out) {
   const cf y0 = Y[0], y1 = Y[stride], y2 = Y[2 * stride], y3 = Y[3 * stride], y4 = Y[4 * stride],
            y5 = Y[5 * stride], y6 = Y[6 * stride], y7 = Y[7 * stride], y8 = Y[8 * stride];
@@ -353,22 +371,74 @@ NF_HD void fft16_real_inverse(const cf* Y, int stride, float fct, float* out) {
   const float t5 = rot(f5, tw16r(5), tw16i(5)), t7 = rot(f7, tw16r(7), tw16i(7));
   const float t2 = ffma(D2, tw16r(2), fmul(D2, tw16i(2)));
   const float t6 = ffma(S2, tw16r(6), -fmul(S2, tw16i(6)));
-  out[0] = fmul(fadd(b0, f0r), fct);
-  out[8] = fmul(fsub(b0, f0r), fct);
-  out[1] = fmul(fadd(b1, t1), fct);
-  out[9] = fmul(fsub(b1, t1), fct);
-  out[2] = fmul(fadd(b2, t2), fct);
-  out[10] = fmul(fsub(b2, t2), fct);
-  out[3] = fmul(fadd(b3, t3), fct);
-  out[11] = fmul(fsub(b3, t3), fct);
-  out[4] = fmul(fsub(b4, f4i), fct);
-  out[12] = fmul(fadd(b4, f4i), fct);
-  out[5] = fmul(fadd(b5, t5), fct);
-  out[13] = fmul(fsub(b5, t5), fct);
-  out[6] = fmul(fadd(b6, t6), fct);
-  out[14] = fmul(fsub(b6, t6), fct);
-  out[7] = fmul(fadd(b7, t7), fct);
-  out[15] = fmul(fsub(b7, t7), fct);
+  auto put = [fct](float v) { return SCALE ? fmul(v, fct) : v; };
+  out[0] = put(fadd(b0, f0r));
+  out[8] = put(fsub(b0, f0r));
+  out[1] = put(fadd(b1, t1));
+  out[9] = put(fsub(b1, t1));
+  out[2] = put(fadd(b2, t2));
+  out[10] = put(fsub(b2, t2));
+  out[3] = put(fadd(b3, t3));
+  out[11] = put(fsub(b3, t3));
+  out[4] = put(fsub(b4, f4i));
+  out[12] = put(fadd(b4, f4i));
+  out[5] = put(fadd(b5, t5));
+  out[13] = put(fsub(b5, t5));
+  out[6] = put(fadd(b6, t6));
+  out[14] = put(fsub(b6, t6));
+  out[7] = put(fadd(b7, t7));
+  out[15] = put(fsub(b7, t7));
+}
+
+// Real-row forms of the 32-point codelet transform, on the same terms as the 16-point
+// ones. Forward: fft32's even and odd halves of a real row are real 16-point
+// transforms (fft16_real_forward<true>), combined with the W32 table as fft32 does; the
+// DC term's twiddle is (1, 0) and W32^8 multiplies a real value. Bins 0..16 at
+// `stride`, the Nyquist imaginary part 0.
+NF_HD void fft32_real_forward(const float* x, cf* X, int stride) {
+  float xe[16], xo[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    xe[m] = x[2 * m];
+    xo[m] = x[2 * m + 1];
+  }
+  cf E[16], O[16];
+  fft16_real_forward<true>(xe, E, 1);
+  fft16_real_forward<true>(xo, O, 1);
+  // W32^0 * O[0] = (O0, O0 * -0 + 0): the imaginary part is +0, or NaN for inf and NaN
+  X[0] = {fadd(E[0].r, O[0].r), ffma(O[0].r, -0.0f, 0.0f)};
+  X[16 * stride] = {fsub(E[0].r, O[0].r), 0.0f};
+#pragma unroll
+  for (int k = 1; k < 16; ++k) {
+    if (k == 8) {  // O[8] is real: W32^8 * O[8] = (O8 * cos, -O8)
+      X[8 * stride] = {fadd(E[8].r, fmul(O[8].r, tw32r(8))), -O[8].r};
+    } else {
+      X[k * stride] = cadd(E[k], cmul_codelet<true>(O[k], tw32r(k), tw32i(k)));
+    }
+  }
+}
+
+// Inverse of one real row from bins 0..16 (at `stride`), times fct. fft32's even half of
+// the mirrored spectrum is itself a mirrored 16-point half spectrum (bins 0, 2, .., 16),
+// whose real outputs fft16_real_inverse gives; the odd half is transformed as fft32 does,
+// and only the real parts of its W32 products are formed.
+NF_HD void fft32_real_inverse(const cf* Y, int stride, float fct, float* out) {
+  float ev[16];
+  fft16_real_inverse<false>(Y, 2 * stride, 1.0f, ev);
+  cf o[16];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const cf y = Y[(2 * m + 1) * stride];
+    o[m] = y;
+    o[15 - m] = {y.r, -y.i};
+  }
+  fft16<false>(o);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const float t = ffma(o[k].r, tw32r(k), -fmul(o[k].i, tw32i(k)));
+    out[k] = fmul(fadd(ev[k], t), fct);
+    out[k + 16] = fmul(fsub(ev[k], t), fct);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -760,9 +830,10 @@ NF_HD bool is_codelet_length(int n) { return n == 8 || n == 16 || n == 32; }
 // fft32x32_avx2.cpp:329-335); the project transform does the same for every even W.
 template <int WC>
 NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool codelet, int bin_stride = 1) {
-  if constexpr (WC == 16) {
-    if (codelet) {  // the real-row form of the 16-point codelet transform
-      fft16_real_forward(x, bins, bin_stride);
+  if constexpr (WC == 16 || WC == 32) {
+    if (codelet) {  // the real-row forms of the 16- and 32-point codelet transforms
+      if constexpr (WC == 16) fft16_real_forward(x, bins, bin_stride);
+      else fft32_real_forward(x, bins, bin_stride);
       return;
     }
   }
@@ -789,9 +860,10 @@ NF_HD void row_forward(const float* x, int w_rt, cf* bins, const cf* table, bool
 template <int WC>
 NF_HD void row_inverse(const cf* bins, int w_rt, float fct, float* out, const cf* table, bool codelet,
                        int bin_stride = 1) {
-  if constexpr (WC == 16) {
-    if (codelet) {  // the real-row form of the 16-point codelet transform
-      fft16_real_inverse(bins, bin_stride, fct, out);
+  if constexpr (WC == 16 || WC == 32) {
+    if (codelet) {  // the real-row forms of the 16- and 32-point codelet transforms
+      if constexpr (WC == 16) fft16_real_inverse(bins, bin_stride, fct, out);
+      else fft32_real_inverse(bins, bin_stride, fct, out);
       return;
     }
   }

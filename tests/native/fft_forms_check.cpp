@@ -127,3 +127,37 @@ extern "C" int fft16_real_mismatches(int structured) {
   }
   return bad;
 }
+
+// The same check for the 32-point real-row forms against fft32.
+extern "C" int fft32_real_mismatches(int structured) {
+  std::mt19937 rng(structured ? 31 : 19);
+  int bad = 0;
+  auto same = [&](float a, float b) { return structured ? same_value(a, b) : same_bits(a, b); };
+  for (int trial = 0; trial < 3000; ++trial) {
+    float x[32];
+    const int kind = structured ? trial % 3 : 2;
+    for (int k = 0; k < 32; ++k) x[k] = kind == 0 ? 5.0f : kind == 1 ? (k & 1 ? -2.0f : 2.0f) : draw(rng, structured);
+    if (structured && trial % 7 == 0) x[trial % 32] = -0.0f;
+    nf::cf got[17], ref[32];
+    nf::row_forward<32>(x, 32, got, nullptr, true);
+    for (int k = 0; k < 32; ++k) ref[k] = {x[k], 0.0f};
+    nf::fft32<true>(ref);
+    ref[16].i = 0.0f;
+    for (int k = 0; k < 17; ++k)
+      if (!same(got[k].r, ref[k].r) || !same(got[k].i, ref[k].i)) ++bad;
+    nf::cf bins[17];
+    for (int k = 0; k < 17; ++k) bins[k] = {draw(rng, structured), draw(rng, structured)};
+    if (structured && trial % 5 == 0)
+      for (int k = 0; k < 17; ++k) bins[k] = bins[trial % 17];
+    float out[32];
+    const float fct = 1.0f / 1024.0f;
+    nf::row_inverse<32>(bins, 32, fct, out, nullptr, true);
+    nf::cf a[32];
+    for (int k = 0; k <= 16; ++k) a[k] = bins[k];
+    for (int k = 1; k < 16; ++k) a[32 - k] = {bins[k].r, 0.0f - bins[k].i};
+    nf::fft32<false>(a);
+    for (int k = 0; k < 32; ++k)
+      if (!same(out[k], a[k].r * fct)) ++bad;
+  }
+  return bad;
+}

@@ -200,3 +200,6 @@ def test_project_transform_forms_identical():
     # identical values, the sign of an exact zero aside
     assert lib.fft16_real_mismatches(0) == 0
     assert lib.fft16_real_mismatches(1) == 0
+    # and of the 32-point one
+    assert lib.fft32_real_mismatches(0) == 0
+    assert lib.fft32_real_mismatches(1) == 0

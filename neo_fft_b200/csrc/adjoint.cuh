@@ -228,12 +228,16 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
   // No barrier between a block row's retire phase (accumulator ring and the cover gradient) and
   // the next block row's staging (source and gradient rings): they touch disjoint shared memory,
   // and every later phase is behind a barrier.
+  // The phases' thread-to-(row, column) walks, divided once per tile (a division inside the
+  // block-row loop is not hoisted by the compiler).
+  const Cursor2 walk_win(tid, nthr, win), walk_nbx(tid, nthr, nbx), walk_tw(tid, nthr, tw),
+      walk_tw4(tid, nthr, max(tw >> 2, 1));
   for (int by = by_lo; by <= by_hi; ++by) {
     const int oy = by * gy.step;
     // ---- stage source rows (decoded) and upstream-gradient rows -------------
     const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
     const int nrows = oy + BH - r0;
-    for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
+    for (Cursor2 c = walk_win; c.y < nrows; c.next()) {
       const int rr = c.y, xx = c.x;
       const int cy = r0 + rr, cx = cx0 + xx;
       const float* srow = reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(J.src) +
@@ -254,7 +258,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     }
     __syncthreads();
     // ---- rows: forward spectrum rows and gradient rows ----------------------
-    for (Cursor2 c(tid, nthr, nbx); c.y < 2 * BH; c.next()) {
+    for (Cursor2 c = walk_nbx; c.y < 2 * BH; c.next()) {
       const int which = c.y >= BH ? 1 : 0, y = c.y - which * BH, b = c.x;
       const float* in = (which ? gring : ring) + size_t((oy + y) % BH) * S.ring_pitch + b * gx.step;
       float row[CAPW];
@@ -272,7 +276,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     // ---- columns: forward transforms, DC exchange, per-bin adjoint -----------
     // (k = 0 tasks come first, so every block's DC is exchanged in the first pass)
     const int ncol = nbx * K;
-    Cursor2 cb(tid, nthr, nbx);
+    Cursor2 cb = walk_nbx;
     for (int base = 0; base < ncol; base += nthr, cb.next()) {
       const bool active = cb.y < K;  // task < ncol
       const int k = active ? cb.y : 0, b = active ? cb.x : 0;
@@ -317,7 +321,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     }
     __syncthreads();
     // ---- columns: template-ratio gradient, adjoint of r2c, inverse -----------
-    for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
+    for (Cursor2 c = walk_nbx; c.y < K; c.next()) {
       const int k = c.y, b = c.x;
       cf x[CAPH];
       cf* sp = spec + size_t(k) * NB + b;
@@ -347,7 +351,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
       da_tile[i] = s;
     }
     // ---- rows: unnormalised inverse, analysis-window weighting ---------------
-    for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
+    for (Cursor2 c = walk_nbx; c.y < BH; c.next()) {
       const int y = c.y, b = c.x;
       float row[CAPW];
       nf::row_inverse<BWC>(spec + size_t(y) * K * NB + b, BW, 1.0f, row, P.tww, codelet, NB);
@@ -361,7 +365,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     const int ylo = max(oy, Y0), yhi = min(oy + BH, Y0 + th);
     if (ola4) {  // four columns per thread, one 16-byte load per block (as in strip_tile)
       const int adv4 = (OBW - gx.step) >> 2;
-      for (Cursor2 c(tid, nthr, tw >> 2); c.y < yhi - ylo; c.next()) {
+      for (Cursor2 c = walk_tw4; c.y < yhi - ylo; c.next()) {
         const int Y = ylo + c.y, xx = c.x << 2, ly = Y - oy;
         float4* a = reinterpret_cast<float4*>(acc + size_t(Y % BH) * S.tw + xx);
         const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
@@ -375,7 +379,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
         *a = sacc;
       }
     }
-    for (Cursor2 c(tid, nthr, tw); !ola4 && c.y < yhi - ylo; c.next()) {
+    for (Cursor2 c = walk_tw; !ola4 && c.y < yhi - ylo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = ylo + yy, ly = Y - oy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;
@@ -388,7 +392,7 @@ __device__ __forceinline__ void adjoint_tile(const DevPlan& P, const AdjointJob&
     }
     __syncthreads();
     const int rlo = max(oy, Y0), rhi = min(by == by_hi ? Y0 + th : oy + gy.step, Y0 + th);
-    for (Cursor2 c(tid, nthr, tw); c.y < rhi - rlo; c.next()) {
+    for (Cursor2 c = walk_tw; c.y < rhi - rlo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = rlo + yy;
       float* a = acc + size_t(Y % BH) * S.tw + xx;

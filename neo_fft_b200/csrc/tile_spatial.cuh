@@ -150,10 +150,11 @@ struct Cursor2 {
 // Warm L2 with one block row of slot spectra (nslots x bins runs of nbx values at
 // `at` + bin * cnt in each slot) while the current row is filtered and reconstructed:
 // one prefetch per 128-byte line, each at an element address inside its run.
+// `walk` is the thread's walk over rows of prefetch_lines(nbx) lines.
+__host__ __device__ inline int prefetch_lines(int nbx) { return (nbx * int(sizeof(cf)) + 127) / 128 + 1; }
 __device__ __forceinline__ void prefetch_row_l2(const cf* const* slots, int nslots, size_t at, int bins, size_t cnt,
-                                                int nbx) {
-  const int lines = (nbx * int(sizeof(cf)) + 127) / 128 + 1;
-  for (Cursor2 q(threadIdx.x, blockDim.x, lines); q.y < nslots * bins; q.next()) {
+                                                int nbx, const Cursor2& walk) {
+  for (Cursor2 q = walk; q.y < nslots * bins; q.next()) {
     const int z = q.y / bins, kk = q.y - z * bins;
     const uintptr_t lo = reinterpret_cast<uintptr_t>(slots[z] + at + size_t(kk) * cnt);
     const uintptr_t hi = lo + size_t(nbx) * sizeof(cf);
@@ -169,7 +170,7 @@ template <int TC>
 __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const PlaneJob& J, const DevSpectral& filt,
                                                          const cf* grid, float grid0, cf* spec, const float* dc, int NB,
                                                          int nbx, int nel, size_t row_base, size_t cnt, int T,
-                                                         float invT, bool& bad) {
+                                                         float invT, bool& bad, const Cursor2& walk) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   // loop invariants in registers: slot pointers, temporal twiddles, scalars
   const cf* slot[TC];
@@ -187,7 +188,7 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
   (void)T;
   const int nrow_e = nel / nbx;  // bins
 #pragma unroll 2
-  for (Cursor2 c(tid, nthr, nbx); c.y < nrow_e; c.next()) {
+  for (Cursor2 c = walk; c.y < nrow_e; c.next()) {
     const int kk = c.y, b = c.x;
     const size_t at = row_base + size_t(kk) * cnt + b;
     cf v[TC];
@@ -371,6 +372,12 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
   // barrier that no staging phase separates from the next, so every thread of the CTA
   // takes the same staging path in a block row.
   bool tma_on = tma_cols && *pipe->dead == 0;
+  // The phases' thread-to-(row, column) walks, divided once per tile: the widths do not
+  // change between block rows, and a division left in the loop is not hoisted by the
+  // compiler (it cannot prove the divisor nonzero).
+  const Cursor2 walk_nbx(tid, nthr, nbx), walk_tw(tid, nthr, tw), walk_tw4(tid, nthr, max(tw >> 2, 1));
+  const Cursor2 walk_win(tid, nthr, win), walk_q4(tid, nthr, (win + 3) >> 2);
+  const Cursor2 walk_lines(tid, nthr, prefetch_lines(nbx)), walk_team(team, nteams, nbx);
   // No barrier between a block row's retire phase (accumulator ring and the output) and the
   // next block row's first phase (staging ring, or the column phase's spectrum and DC
   // buffers): they touch disjoint shared memory, and every later phase is behind a barrier.
@@ -409,7 +416,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         // wait ran out reads its samples directly.
         const unsigned char* rb = raw + b0 * S.raw_bytes;
         const int q4 = (win + 3) >> 2;
-        for (Cursor2 c(tid, nthr, q4); c.y < nrows; c.next()) {
+        for (Cursor2 c = walk_q4; c.y < nrows; c.next()) {
           const int x = c.x * 4;
           float v[4];
 #pragma unroll
@@ -454,7 +461,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         staged = true;
       }
       if (!staged) {
-        for (Cursor2 c(tid, nthr, win); c.y < nrows; c.next()) {
+        for (Cursor2 c = walk_win; c.y < nrows; c.next()) {
           const int cy = r0 + c.y;
           const float sv = source_sample(cy, cx0 + c.x);
           const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
@@ -465,7 +472,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       __syncthreads();
       tma_on = tma_on && *pipe->dead == 0;
       // ---- A: row transforms (block index fastest) --------------------------
-      for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
+      for (Cursor2 c = walk_nbx; c.y < BH; c.next()) {
         const int y = c.y, b = c.x;
         const float* in = ring_in + int(unsigned(oy + y) % unsigned(BH)) * S.ring_pitch + b * gx.step;
         float row[CAPW];
@@ -500,8 +507,8 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const cf* S = J.tspec[0] + size_t(by) * bins * size_t(gx.count) + size_t(bx_lo);
       if (by < by_hi)
         prefetch_row_l2(J.tspec, 1, size_t(by + 1) * bins * size_t(gx.count) + size_t(bx_lo), bins,
-                        size_t(gx.count), nbx);
-      for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
+                        size_t(gx.count), nbx, walk_lines);
+      for (Cursor2 c = walk_nbx; c.y < K; c.next()) {
         const int k = c.y, b = c.x;
         cf col[CAPH];
 #pragma unroll UH
@@ -524,21 +531,21 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const size_t cnt = size_t(gx.count);
       const size_t row_base = size_t(by) * bins * cnt + size_t(bx_lo);
       const float invT = fdiv(1.0f, float(T));
-      if (by < by_hi) prefetch_row_l2(J.tspec, T, row_base + size_t(bins) * cnt, bins, cnt, nbx);
+      if (by < by_hi) prefetch_row_l2(J.tspec, T, row_base + size_t(bins) * cnt, bins, cnt, nbx, walk_lines);
       for (int b = tid; b < nbx; b += nthr) dc[b] = J.tspec[c][row_base + b].r;
       __syncthreads();
       const int nel = bins * nbx;
       switch (T) {  // compile-time slot counts keep the slot values in registers
-        case 2: temporal_filter_elements<2>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
-        case 3: temporal_filter_elements<3>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
-        case 4: temporal_filter_elements<4>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
-        default: temporal_filter_elements<5>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad); break;
+        case 2: temporal_filter_elements<2>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad, walk_nbx); break;
+        case 3: temporal_filter_elements<3>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad, walk_nbx); break;
+        case 4: temporal_filter_elements<4>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad, walk_nbx); break;
+        default: temporal_filter_elements<5>(P, J, filt, grid, grid0, spec, dc, NB, nbx, nel, row_base, cnt, T, invT, bad, walk_nbx); break;
       }
       __syncthreads();
       if (enh.enh) {
         for (int b = tid; b < nbx; b += nthr) dc[NB + b] = spec[b].r;  // recovered DC
         __syncthreads();
-        for (Cursor2 c(tid, nthr, nbx); c.y < bins; c.next()) {
+        for (Cursor2 c = walk_nbx; c.y < bins; c.next()) {
           const int kk = c.y, b = c.x;
           const float g2 = grid ? fdiv(fmul(P.mean_scale, dc[NB + b]), grid0) : 0.0f;
           cf* sp = spec + kk * NB + b;
@@ -551,7 +558,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         // lane gathers and transforms its run, the runs go back into the column, and each
         // lane finishes the outermost butterflies of its own positions.
         using TH = nf::TeamFFT<false, BHC>;
-        for (Cursor2 c(team, nteams, nbx); c.y < K; c.next()) {
+        for (Cursor2 c = walk_team; c.y < K; c.next()) {
           cf* sp = spec + c.y * NB + c.x;
           cf run[TH::M];
           TH::run(lane, run, P.twh, [&](int y) { return sp[y * KNB]; });
@@ -563,7 +570,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
                     [&](int y, cf v) { sp[y * KNB] = v; });
         }
       } else {
-        for (Cursor2 c(tid, nthr, nbx); c.y < K; c.next()) {
+        for (Cursor2 c = walk_nbx; c.y < K; c.next()) {
           const int k = c.y, b = c.x;
           cf col[CAPH];
           cf* sp = spec + k * NB + b;
@@ -578,7 +585,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       }
       __syncthreads();
     } else {
-    Cursor2 cb(tid, nthr, nbx);
+    Cursor2 cb = walk_nbx;
     for (int base = 0; base < ncol; base += nthr, cb.next()) {
       const bool active = cb.y < K;  // task < ncol
       const int k = active ? cb.y : 0, b = active ? cb.x : 0;
@@ -664,7 +671,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       // outer butterflies' reads then fall in distinct banks across the warp's teams.
       using TW = nf::TeamFFT<false, BWC>;
       cf* xs = reinterpret_cast<cf*>(ring_in) + team * (BWC + TW::T);
-      for (Cursor2 c(team, nteams, nbx); c.y < BH; c.next()) {
+      for (Cursor2 c = walk_team; c.y < BH; c.next()) {
         const int y = c.y, b = c.x;
         const cf* bins = spec + y * KNB + b;
         cf run[TW::M];
@@ -690,7 +697,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         if (guard != guard) bad = true;
       }
     } else
-    for (Cursor2 c(tid, nthr, nbx); c.y < BH; c.next()) {
+    for (Cursor2 c = walk_nbx; c.y < BH; c.next()) {
       const int y = c.y, b = c.x;
       if (P.center && y != BH / 2) continue;
       float row[CAPW];
@@ -726,7 +733,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       // share their first block and block count, so one 16-byte load per block serves
       // all four, each component summed in the same block order as the scalar path.
       const int adv4 = (OBW - gx.step) >> 2;
-      for (Cursor2 c(tid, nthr, tw >> 2); c.y < yhi - ylo; c.next()) {
+      for (Cursor2 c = walk_tw4; c.y < yhi - ylo; c.next()) {
         const int Y = ylo + c.y, xx = c.x << 2, ly = Y - oy;
         float4* a = reinterpret_cast<float4*>(acc + int(unsigned(Y) % unsigned(BH)) * S.tw + xx);
         const int cm = colmap[xx], nblk = (cm >> 10) & 1023;
@@ -759,7 +766,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         }
       }
     }
-    for (Cursor2 c(tid, nthr, tw); !ola4 && c.y < yhi - ylo; c.next()) {
+    for (Cursor2 c = walk_tw; !ola4 && c.y < yhi - ylo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = ylo + yy, X = X0 + xx, ly = Y - oy;
       float* a = acc + int(unsigned(Y) % unsigned(BH)) * S.tw + xx;
@@ -786,7 +793,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     __syncthreads();
     // ---- E: retire rows that no later block row touches ---------------------
     const int rlo = max(oy, Y0), rhi = min(by == by_hi ? Y0 + th : oy + gy.step, Y0 + th);
-    for (Cursor2 c(tid, nthr, tw); c.y < rhi - rlo; c.next()) {
+    for (Cursor2 c = walk_tw; c.y < rhi - rlo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = rlo + yy;
       float* a = acc + int(unsigned(Y) % unsigned(BH)) * S.tw + xx;

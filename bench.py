@@ -681,14 +681,23 @@ def other_configs(args, dev):
             for f in range(n):
                 kp.advance_kalman(kf[f], state)
                 kp.render_kalman(kf[f], kout, state)
+
+        def seq_step():
+            for f in range(n):
+                kp.step_kalman(kf[f], kout, state)
         ms = measure(seq, max(2, min(steps, 3)), 1)
-        d1[mode] = {"plain": n * w * h / (ms / 1e3) / 1e6, "plain_ms": ms}
+        ms_step = measure(seq_step, max(2, min(steps, 3)), 1)
+        d1[mode] = {"plain": n * w * h / (ms / 1e3) / 1e6, "plain_ms": ms,
+                    "step": n * w * h / (ms_step / 1e3) / 1e6, "step_ms": ms_step}
         del state
     kp.sync_status()
     out["D1"] = {"workload": "FFT3D bt=0 Kalman 32x32 sigma 2.5 kratio 2, 240 sequential distinct 1920x1080 float32 "
-                             "frames, advance + render per frame", "unit": "Mpx/s", **d1,
+                             "frames", "unit": "Mpx/s", **d1,
                  "plain": d1["binary64_variance"]["plain"], "plain_ms": d1["binary64_variance"]["plain_ms"],
-                 "form": "binary64-variance state (the figure under plain); binary32 beside it"}
+                 "step": d1["binary64_variance"]["step"], "step_ms": d1["binary64_variance"]["step_ms"],
+                 "form": "binary64-variance state (the figures under plain and step; binary32 beside them); plain = "
+                         "nf_kalman_advance_device + nf_kalman_render_device per frame, step = nf_kalman_step_device "
+                         "per frame (one pass over the blocks, then the ordered overlap-add)"}
     del kf
     torch.cuda.empty_cache()
 
@@ -735,6 +744,8 @@ def run_profile(a):
       fft3d32  FFT3D bw=bh=32, ow=oh=16, sigma 2, u8 640x360
       fft3d48  FFT3D bt=3 bw=bh=48, ow=oh=24, sigma 3, sharpen 0.3, u16 (10-bit) 3840x2160
       kalman32 FFT3D bt=0 (Kalman advance and render per launch), bw=bh=32, float 1920x1080
+      kalman32_step the same as one Kalman step per launch (advance with the render's
+               inverse transforms, then the ordered overlap-add)
       dft12t5  DFTTest tbsize 5 tmode 1, sbsize 12 / sosize 9, ftype 1, float 1920x1080
       clip12t5 DFTTest tbsize 5 tmode 1 sbsize 12 / sosize 9 ftype 1, float 1920x1080 clip of 10
                frames as one clip batch (volume spectra pass + slice strips) per launch
@@ -780,15 +791,18 @@ def run_profile(a):
         plan = Plan(w, h, SampleFormat(10), FFT3DConfig(bw=48, bh=48, ow=24, oh=24, bt=3, sigma=3.0, sharpen=0.3))
         srcs = [torch.from_numpy(_plane(h, w, np.uint16, 64, 940, f)).to(dev) for f in range(3)]
         targets = ()
-    elif wl == "kalman32":
+    elif wl in ("kalman32", "kalman32_step"):
         w, h = 1920, 1080
         plan = Plan(w, h, SampleFormat(32, True), FFT3DConfig(bw=32, bh=32, bt=0, sigma=2.5, kratio=2.0))
         state = plan.initial_kalman()
         src = torch.from_numpy(_plane(h, w, np.float32, 0, 1, 1)).to(dev)
         out = torch.empty_like(src)
         for _ in range(a.launches):
-            plan.advance_kalman(src, state)
-            plan.render_kalman(src, out, state)
+            if wl == "kalman32_step":
+                plan.step_kalman(src, out, state)
+            else:
+                plan.advance_kalman(src, state)
+                plan.render_kalman(src, out, state)
         torch.cuda.synchronize()
         plan.sync_status()
         return

@@ -156,6 +156,13 @@ nf_status nf_kalman_advance_device(const nf_plan* plan, nf_const_plane source, n
                                    char* err, size_t err_len);
 nf_status nf_kalman_render_device(const nf_plan* plan, nf_const_plane source, nf_plane dst,
                                   const nf_kalman_state* state, void* stream, char* err, size_t err_len);
+/* Kalman step: advance_kalman(source, state) then render_kalman(source, dst, state) of
+ * the same frame (the sequence filter.hpp:198 and :225 run for each output frame), in one
+ * pass over the blocks: each block is transformed forward once and back once and its
+ * state read and written once. Results and error reporting equal the two calls above.
+ * Takes stream-ordered scratch of bh*bw floats per block from the library's pool. */
+nf_status nf_kalman_step_device(const nf_plan* plan, nf_const_plane source, nf_plane dst, nf_kalman_state* state,
+                                void* stream, char* err, size_t err_len);
 /* Host-memory variants: the plane is staged through the plan's device buffers and
  * the call synchronises `stream` (NF_NON_FINITE like the reference). */
 nf_status nf_kalman_advance_host(const nf_plan* plan, nf_const_plane source, nf_kalman_state* state, void* stream,

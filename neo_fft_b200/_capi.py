@@ -96,6 +96,8 @@ PROTOTYPES = {
     "nf_kalman_advance_device": (c_int, [c_void_p, NfConstPlane, c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_kalman_render_device": (c_int, [c_void_p, NfConstPlane, NfPlane, c_void_p, c_void_p,
                                         ctypes.c_char_p, c_size_t]),
+    "nf_kalman_step_device": (c_int, [c_void_p, NfConstPlane, NfPlane, c_void_p, c_void_p,
+                                        ctypes.c_char_p, c_size_t]),
     "nf_kalman_advance_host": (c_int, [c_void_p, NfConstPlane, c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_kalman_render_host": (c_int, [c_void_p, NfConstPlane, NfPlane, c_void_p, c_void_p, ctypes.c_char_p,
                                       c_size_t]),

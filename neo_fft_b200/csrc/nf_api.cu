@@ -1595,6 +1595,67 @@ nf_status nf_kalman_render_device(const nf_plan* p, nf_const_plane source, nf_pl
     return NF_OK;
   });
 }
+// Kalman step: nf_kalman_advance_device followed by nf_kalman_render_device of the same
+// frame, in two launches (the advance kernel renders each run of blocks it advanced into
+// a buffer of synthesised blocks, then kalman_ola_kernel adds them per pixel). The buffer
+// is stream-ordered scratch of the library's pool: bh * bw floats per block.
+nf_status nf_kalman_step_device(const nf_plan* p, nf_const_plane source, nf_plane dst, nf_kalman_state* state,
+                                void* stream, char* err, size_t len) {
+  return guarded(err, len, [&]() -> nf_status {
+    nfb::require(p && state, "null plan or state");
+    check_kalman_source(*p, source);
+    nfb::require(state->count == size_t(p->t.gx.count) * p->t.gy.count * p->t.bins, "Kalman state shape differs");
+    nfb::require(!p->t.needs_pattern || p->model_ready.load(std::memory_order_acquire),
+                 "Kalman sampled model not initialized");
+    nfb::require(dst.width == p->t.gx.length && dst.height == p->t.gy.length, "frame dimensions differ from plan");
+    const size_t elem = size_t(storage_of(p->t.format));
+    const size_t de = plane_extent(dst.width, dst.height, dst.stride_bytes, elem);
+    check_pointer(dst.data, elem);
+    disjoint(source.data, plane_extent(source.width, source.height, source.stride_bytes, elem), dst.data, de);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t synth_bytes = size_t(p->t.gx.count) * p->t.gy.count * size_t(p->t.bh) * p->t.bw * sizeof(float);
+    void* synth = nullptr;
+    cudaError_t e = scratch_alloc(&synth, synth_bytes, st);
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "device allocation failed");
+    nfd::KalmanArgs a{state->last,
+                      state->fp64 ? nullptr : static_cast<float*>(state->covariance),
+                      state->fp64 ? nullptr : static_cast<float*>(state->process),
+                      state->fp64 ? static_cast<double*>(state->covariance) : nullptr,
+                      state->fp64 ? static_cast<double*>(state->process) : nullptr,
+                      p->t.spectral.primary.empty() && !p->t.needs_pattern ? nullptr : p->dev.filt.primary,
+                      state->fp64,
+                      static_cast<float*>(synth)};
+    nfd::DevPlan d = p->dev;
+    d.fft3d_mode = nfd::kEnhanceOnly;  // the render enhances the estimate (plan.cpp:471-477)
+    e = run_kalman_advance(d, source.data, source.stride_bytes, a, st);
+    if (e == cudaSuccess) {
+      // four (two) pixels per thread when they share their covering blocks: 16 (8)-byte loads
+      const int per = ((d.gx.step | d.bw | d.gx.offset) & 3) == 0 ? 4 : ((d.gx.step | d.bw | d.gx.offset) & 1) == 0 ? 2 : 1;
+      const dim3 grid((unsigned((dst.width + per - 1) / per) + 255) / 256, unsigned(dst.height));
+      auto* out = static_cast<unsigned char*>(dst.data);
+      const long long ds = (long long)dst.stride_bytes;
+      const float* sy = static_cast<const float*>(synth);
+      auto ola = [&](auto storage, auto v) {
+        nfd::kalman_ola_kernel<decltype(storage)::value, decltype(v)::value><<<grid, 256, 0, st>>>(d, sy, out, ds);
+      };
+      using U8 = std::integral_constant<int, nfd::kStoreU8>;
+      using U16 = std::integral_constant<int, nfd::kStoreU16>;
+      using F32 = std::integral_constant<int, nfd::kStoreF32>;
+      auto by_width = [&](auto storage) {
+        if (per == 4) ola(storage, std::integral_constant<int, 4>{});
+        else if (per == 2) ola(storage, std::integral_constant<int, 2>{});
+        else ola(storage, std::integral_constant<int, 1>{});
+      };
+      if (d.storage == nfd::kStoreU8) by_width(U8{});
+      else if (d.storage == nfd::kStoreU16) by_width(U16{});
+      else by_width(F32{});
+      e = cudaGetLastError();
+    }
+    cudaFreeAsync(synth, st);
+    if (e != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+    return NF_OK;
+  });
+}
 namespace {
 // Copies a host plane into the plan's staging buffer (slot `slot` of `nslots`).
 nf_status stage_host_plane(const nf_plan& p, const nf_const_plane& s, int slot, int nslots, cudaStream_t st,

@@ -48,24 +48,35 @@ cudaError_t launch_batch(const BatchWork& w, int ctas, size_t smem, cudaStream_t
 // rounds of threads over rows, columns and bins (eight bins per thread and round) plus
 // one of setup; longer runs on ties.
 template <int ST>
-cudaError_t launch_kalman_one(const DevPlan& d, const void* src, ptrdiff_t ss, const KalmanArgs& a, cudaStream_t st) {
-  auto k = kalman_advance_kernel<NF_BH, NF_BW, ST>;
-  const size_t per_block = size_t(d.bh) * d.K * sizeof(cf);
-  const int nb_max = std::max(1, std::min({8, int((64 * 1024) / per_block), d.gx.count}));
-  cudaError_t e = prepare(k, per_block * size_t(nb_max));
+cudaError_t launch_kalman_one(const DevPlan& d, const void* src, ptrdiff_t ss, const KalmanArgs& args,
+                              cudaStream_t st) {
+  // Kalman step (a.synth set): the same run geometry, the run's estimate DCs after its
+  // spectra, and the render's inverse columns and rows in the cost of a run. Runs stage
+  // their old state in shared memory by bulk copies when every run's slice of the state
+  // arrays starts on 16 bytes (a bin count that is a multiple of four).
+  KalmanArgs a = args;
+  const uintptr_t arrays = reinterpret_cast<uintptr_t>(a.last) |
+                           (a.fp64 ? reinterpret_cast<uintptr_t>(a.cov64) | reinterpret_cast<uintptr_t>(a.proc64)
+                                   : reinterpret_cast<uintptr_t>(a.cov32) | reinterpret_cast<uintptr_t>(a.proc32));
+  a.staged = (d.bins & 3) == 0 && (arrays & 15) == 0;
+  const bool step = a.synth != nullptr;
+  auto k = step ? kalman_advance_kernel<NF_BH, NF_BW, ST, true> : kalman_advance_kernel<NF_BH, NF_BW, ST, false>;
+  auto smem_of = [&](int r) { return kalman_smem(d.bins, r, step, a.fp64, a.staged).bytes; };
+  int nb_max = std::max(1, std::min(8, d.gx.count));
+  while (nb_max > 1 && smem_of(nb_max) > size_t(200) * 1024) --nb_max;
+  cudaError_t e = prepare(k, smem_of(nb_max));
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   // the choice of the last geometry this thread launched (frames of a clip repeat it)
   struct Choice {
-    int dev = -1, cx = 0, cy = 0, bh = 0, bw = 0, st = 0, nb = 0, threads = 0;
+    int dev = -1, cx = 0, cy = 0, bh = 0, bw = 0, st = 0, step = 0, fp64 = 0, nb = 0, threads = 0;
   };
   thread_local Choice last;
   if (last.dev == dev && last.cx == d.gx.count && last.cy == d.gy.count && last.bh == d.bh && last.bw == d.bw &&
-      last.st == ST) {
+      last.st == ST && last.step == int(step) && last.fp64 == a.fp64) {
     const dim3 grid((d.gx.count + last.nb - 1) / last.nb, d.gy.count);
-    k<<<grid, last.threads, per_block * size_t(last.nb), st>>>(d, last.nb, static_cast<const unsigned char*>(src), ss,
-                                                                 a);
+    k<<<grid, last.threads, smem_of(last.nb), st>>>(d, last.nb, static_cast<const unsigned char*>(src), ss, a);
     return cudaGetLastError();
   }
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -75,22 +86,23 @@ cudaError_t launch_kalman_one(const DevPlan& d, const void* src, ptrdiff_t ss, c
   for (int r = nb_max; r >= 1; --r) {
     const int t = std::min(256, std::max(64, (r * d.bh + 31) / 32 * 32));
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, t, per_block * size_t(r)) != cudaSuccess || occ < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, t, smem_of(r)) != cudaSuccess || occ < 1)
       continue;
     const long long ctas = (long long)((d.gx.count + r - 1) / r) * d.gy.count;
     const long long slots = (long long)occ * sms;
-    const long long cost = (ctas + slots - 1) / slots *
-                           (1 + rounds((long long)r * d.bh, t) + rounds((long long)r * d.K, t) +
-                            rounds((long long)r * d.bins, 8 * t));
+    const long long per_run = 1 + rounds((long long)r * d.bh, t) + rounds((long long)r * d.K, t) +
+                              rounds((long long)r * d.bins, 8 * t) +
+                              (step ? rounds((long long)r * d.K, t) + rounds((long long)r * d.bh, t) : 0);
+    const long long cost = (ctas + slots - 1) / slots * per_run;
     if (best < 0 || cost < best) {
       best = cost;
       nb = r;
       threads = t;
     }
   }
-  last = Choice{dev, d.gx.count, d.gy.count, d.bh, d.bw, ST, nb, threads};
+  last = Choice{dev, d.gx.count, d.gy.count, d.bh, d.bw, ST, int(step), a.fp64, nb, threads};
   const dim3 grid((d.gx.count + nb - 1) / nb, d.gy.count);
-  k<<<grid, threads, per_block * size_t(nb), st>>>(d, nb, static_cast<const unsigned char*>(src), ss, a);
+  k<<<grid, threads, smem_of(nb), st>>>(d, nb, static_cast<const unsigned char*>(src), ss, a);
   return cudaGetLastError();
 }
 } // namespace

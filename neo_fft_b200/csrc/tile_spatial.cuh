@@ -171,7 +171,6 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
                                                          const cf* grid, float grid0, cf* spec, const float* dc, int NB,
                                                          int nbx, int nel, size_t row_base, size_t cnt, int T,
                                                          float invT, bool& bad, const Cursor2& walk) {
-  const int tid = threadIdx.x, nthr = blockDim.x;
   // loop invariants in registers: slot pointers, temporal twiddles, scalars
   const cf* slot[TC];
   cf tf[TC * TC], ti[TC];
@@ -415,7 +414,6 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         // (i / kBox) * kBox * step + r * kBox + i % kBox of the raw boxes. A thread whose
         // wait ran out reads its samples directly.
         const unsigned char* rb = raw + b0 * S.raw_bytes;
-        const int q4 = (win + 3) >> 2;
         for (Cursor2 c = walk_q4; c.y < nrows; c.next()) {
           const int x = c.x * 4;
           float v[4];

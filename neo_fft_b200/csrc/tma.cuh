@@ -78,4 +78,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, 
       : "memory");
 }
 
+// `bytes` bytes from global `src` into shared `dst` with one bulk copy (both addresses
+// 16-byte aligned, `bytes` a multiple of 16); completion is counted on `b`. This GPU's
+// own memory only, no cluster sharing.
+__device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, unsigned bytes, unsigned long long* b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(b))
+               : "memory");
+}
+
 }  // namespace nfd

@@ -333,6 +333,17 @@ class Plan:
         C.raise_for(st, err.value)
         return dst
 
+    def step_kalman(self, source, dst, state: "KalmanState", stream=None):
+        """advance_kalman(source, state) then render_kalman(source, dst, state) in one pass
+        over the blocks (nf_kalman_step_device): the same results and errors."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        err = ctypes.create_string_buffer(512)
+        st = self._lib.nf_kalman_step_device(self._h, _plane(source, True), _plane(dst, False), state._h,
+                                             ctypes.c_void_p(s), err, 512)
+        C.raise_for(st, err.value)
+        return dst
+
 
 class KalmanState:
     """Device-resident Kalman state (kernels/kalman.hpp:5-14)."""

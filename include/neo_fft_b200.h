@@ -221,8 +221,13 @@ void nf_batch_destroy(nf_batch* batch);
  *  - DFTTest tmode 1 with tosize 0 and smode 1 (clips of at least tbsize frames): the
  *    temporal blocks of temporal_grid.hpp:5-40 each serve tbsize output frames, so each
  *    block's volume is transformed and filtered once for all of them.
- * Items must share the algorithm, block shape and sample storage; planes must stay
- * allocated while the batch is used, and outputs must not overlap any frame of their clip. */
+ *  - Other DFTTest temporal plans (tmode 0 with the clamped centred window of
+ *    filter.hpp:289-296; tmode 1 with tosize > 0, whose outputs add their covering
+ *    temporal blocks; smode 0): one filter call per output frame inside the batch's
+ *    launch and graph, since their frames share no transform between outputs.
+ * The grouped items (the first two kinds) must share the algorithm, block shape and sample
+ * storage; planes must stay allocated while the batch is used, and outputs must not
+ * overlap any frame of their clip. */
 typedef struct nf_clip_batch nf_clip_batch;
 typedef struct nf_clip_item {
   const nf_plan* plan;

@@ -147,6 +147,18 @@ struct nf_clip_batch {
     int tiles2p = 0;
   };
   std::vector<Step> steps;
+  // DFTTest clips whose output frames share no transform (tmode 0: a frame's slot weight
+  // depends on its place in each output's window; tmode 1 with tosize > 0: an output adds
+  // several temporal blocks in temporal-block order over the whole tile; smode 0): one
+  // filter call per output frame with the host layer's frame selection, in the batch's
+  // launch and its graph.
+  struct FrameCall {
+    const nf_plan* plan;
+    std::vector<nf_const_plane> sources;
+    std::vector<int> targets;
+    nf_plane dst;
+  };
+  std::vector<FrameCall> calls;
   void* dev = nullptr;      // plans | shapes | per-step job tables
   void* rings = nullptr;    // frame spectra, T per clip plane
   void* tspec = nullptr;    // slot pointer arrays of the temporal jobs
@@ -2030,6 +2042,52 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(out && count > 0 && items, "null clip batch output or items");
     auto b = std::make_unique<nf_clip_batch>();
+    // DFTTest temporal clips outside the two-pass slice form become per-frame calls; the
+    // rest are grouped into the two passes below.
+    std::vector<nf_clip_item> grouped;
+    for (int i = 0; i < count; ++i) {
+      const nf_clip_item& it = items[i];
+      nfb::require(it.plan != nullptr && it.frames && it.dsts && it.nframes > 0, "invalid clip item");
+      const nf_plan& p = *it.plan;
+      const bool per_frame = p.t.algo == nfb::Algo::DFTTest && p.t.temporal_size >= 2 &&
+                             !(p.t.temporal_ola && p.t.temporal_overlap == 0 && !p.t.center &&
+                               p.t.temporal_size <= nfd::kMaxVolumeSlots);
+      if (!per_frame) {
+        grouped.push_back(it);
+        continue;
+      }
+      nfb::require(!dithers(p.t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
+      nfb::require(!p.t.preview, "pshow previews run through nf_plan_process_device");
+      nfb::require(it.nframes >= p.t.temporal_size || !p.t.temporal_ola, "DFTTest clips must hold at least tbsize frames");
+      const int N = it.nframes, T = p.t.temporal_size;
+      const size_t elem = size_t(storage_of(p.t.format));
+      for (int n = 0; n < N; ++n) {
+        nf_clip_batch::FrameCall c{&p, {}, {}, it.dsts[n]};
+        if (p.t.temporal_ola) {  // the covering temporal blocks (temporal_grid.hpp:5-40)
+          for (const auto& blk : nfb::temporal_blocks(n, N, T, p.t.temporal_overlap)) {
+            c.targets.push_back(blk.target);
+            for (int z = 0; z < T; ++z) c.sources.push_back(it.frames[blk.slots[size_t(z)]]);
+          }
+        } else {  // slots clamp(n - T/2 + j, 0, N - 1) (filter.hpp:289-296)
+          for (int j = 0; j < T; ++j) c.sources.push_back(it.frames[std::min(std::max(n - T / 2 + j, 0), N - 1)]);
+        }
+        validate_call(p, c.sources.data(), int(c.sources.size()), c.targets.empty() ? nullptr : c.targets.data(),
+                      int(c.targets.size()), c.dst);
+        const size_t de = plane_extent(c.dst.width, c.dst.height, c.dst.stride_bytes, elem);
+        for (int g = 0; g < N; ++g)  // outputs are written while other outputs still read the clip
+          disjoint(it.frames[g].data,
+                   plane_extent(it.frames[g].width, it.frames[g].height, it.frames[g].stride_bytes, elem),
+                   c.dst.data, de);
+        b->calls.push_back(std::move(c));
+      }
+      if (std::find(b->plans.begin(), b->plans.end(), &p) == b->plans.end()) b->plans.push_back(&p);
+    }
+    if (grouped.empty()) {
+      *out = b.release();
+      return NF_OK;
+    }
+    items = grouped.data();
+    count = int(grouped.size());
     std::vector<const nf_plan*> plans;
     std::vector<int> plan_of(static_cast<size_t>(count));
     for (int i = 0; i < count; ++i) {
@@ -2040,8 +2098,7 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
                          p.t.temporal_size <= 5;
       const bool dft = p.t.algo == nfb::Algo::DFTTest && p.t.temporal_ola && p.t.temporal_overlap == 0 &&
                        !p.t.center && p.t.temporal_size >= 2 && p.t.temporal_size <= nfd::kMaxVolumeSlots;
-      nfb::require(fft3d || dft,
-                   "clip batches take FFT3D plans with bt 2..5 or DFTTest plans with tmode 1, tosize 0 and smode 1");
+      nfb::require(fft3d || dft, "clip batches take FFT3D plans with bt 2..5 or DFTTest plans with tbsize >= 2");
       const int storage = storage_of(p.t.format);
       if (i == 0) {
         b->bh = p.t.bh;
@@ -2079,7 +2136,10 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
       }
       plan_of[size_t(i)] = pi;
     }
+    const std::vector<const nf_plan*> call_plans = b->plans;  // plans of the per-frame calls
     b->plans = plans;
+    for (const nf_plan* q : call_plans)
+      if (std::find(b->plans.begin(), b->plans.end(), q) == b->plans.end()) b->plans.push_back(q);
     // strips of pass 2 (tall segments: the batch supplies the parallelism) and the
     // block-column chunk of pass 1
     std::vector<nfd::DevPlan> dplans;
@@ -2340,8 +2400,14 @@ nf_status nf_clip_batch_create(const nf_clip_item* items, int count, nf_clip_bat
 nf_status nf_clip_batch_launch(nf_clip_batch* b, void* stream, char* err, size_t len) {
   if (!b) return fail(err, len, "null clip batch", NF_INVALID_ARGUMENT);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (b->steps.empty()) return NF_OK;
   if (const nf_status ms = check_models(b->plans, err, len)) return ms;
+  for (const auto& c : b->calls) {
+    const nf_status s = filter_device(*c.plan, c.plan->dev, c.sources.data(), int(c.sources.size()),
+                                      c.targets.empty() ? nullptr : c.targets.data(), int(c.targets.size()), c.dst, st,
+                                      err, len);
+    if (s != NF_OK) return s;
+  }
+  if (b->steps.empty()) return NF_OK;
   cudaError_t e = cudaMemsetAsync(b->counters, 0, 2 * sizeof(int) * b->steps.size(), st);
   if (e != cudaSuccess) return cuda_fail(err, len, e, "queue reset failed");
   for (const auto& s : b->steps) {

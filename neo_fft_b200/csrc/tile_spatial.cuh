@@ -47,8 +47,9 @@ __device__ __forceinline__ int floor_div_i(int v, int d) { return v >= 0 ? v / d
 // (acc+0.5)+base, DFTTest integer acc*scale+0.5, clipped to [0, peak] and
 // truncated; FFT3D float clipped to [0,1]; DFTTest float acc*scale unclipped.
 // ALGO: 0 FFT3D, 1 DFTTest known at compile time, -1 read from the plan.
-template <int STORAGE, int ALGO = -1>
-__device__ __forceinline__ void store_sample(unsigned char* row, int x, float acc, const DevPlan& P) {
+// `P`: the plan, or an OutConv copy of its conversion fields taken before a loop.
+template <int STORAGE, int ALGO = -1, class Conv = DevPlan>
+__device__ __forceinline__ void store_sample(unsigned char* row, int x, float acc, const Conv& P) {
   const bool fft3d = ALGO >= 0 ? ALGO == 0 : P.algo == 0;
   if (STORAGE == kStoreU8 && P.raw_out) {  // dithered u8 output: the dither pass converts
     reinterpret_cast<float*>(row)[x] = acc;
@@ -65,6 +66,15 @@ __device__ __forceinline__ void store_sample(unsigned char* row, int x, float ac
   const float c = v < 0.0f ? 0.0f : (P.out_peak < v ? P.out_peak : v);
   if (STORAGE == kStoreU8) row[x] = (unsigned char)(c);
   else reinterpret_cast<unsigned short*>(row)[x] = (unsigned short)(c);
+}
+
+// The output conversion fields of a plan, read once before a loop of stores.
+struct OutConv {
+  int algo, raw_out;
+  float out_base, out_scale, out_peak;
+};
+__device__ __forceinline__ OutConv out_conv(const DevPlan& P) {
+  return {P.algo, P.raw_out, P.out_base, P.out_scale, P.out_peak};
 }
 
 // One plane to filter: source/destination (device memory, signed byte strides) and
@@ -399,6 +409,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       }
       const int r0 = by == by_lo ? oy : max(oy, oy + BH - gy.step);
       const int nrows = oy + BH - r0;
+      const float dec_base = P.dec_base, dec_scale = P.dec_scale;  // read once, not per sample
       bool staged = false;
       if (tma_on && by > by_lo && tma_rows(by) >= 0) {
         const int b0 = by & 1;
@@ -450,7 +461,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
           }
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            v[j] = fmul(fsub(v[j], P.dec_base), P.dec_scale);
+            v[j] = fmul(fsub(v[j], dec_base), dec_scale);
             if (STORAGE == kStoreF32 && x + j < win && !isfin(v[j])) bad = true;
           }
           *reinterpret_cast<float4*>(ring_in + int(unsigned(r0 + c.y) % unsigned(BH)) * S.ring_pitch + x) =
@@ -462,7 +473,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         for (Cursor2 c = walk_win; c.y < nrows; c.next()) {
           const int cy = r0 + c.y;
           const float sv = source_sample(cy, cx0 + c.x);
-          const float v = fmul(fsub(sv, P.dec_base), P.dec_scale);
+          const float v = fmul(fsub(sv, dec_base), dec_scale);
           if (STORAGE == kStoreF32 && !isfin(v)) bad = true;  // decoded integers are finite
           ring_in[int(unsigned(cy) % unsigned(BH)) * S.ring_pitch + c.x] = v;
         }
@@ -694,10 +705,11 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         __syncwarp(team_mask);  // the scratch is reused by the team's next row
         if (guard != guard) bad = true;
       }
-    } else
+    } else {
+    const int center = P.center;
     for (Cursor2 c = walk_nbx; c.y < BH; c.next()) {
       const int y = c.y, b = c.x;
-      if (P.center && y != BH / 2) continue;
+      if (center && y != BH / 2) continue;
       float row[CAPW];
       nf::row_inverse<BWC>(spec + y * KNB + b, BW, SRC == kSrcSlice ? fct3 : fct, row, P.tww, codelet, NB);
       float* o = ob + (y * NB + b) * OBW;
@@ -722,6 +734,7 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
         for (int x = 0; x < CAPW; ++x)
           if (x < BW) o[x] = row[x];
       }
+    }
     }
     __syncthreads();
     // ---- D: ordered overlap-add into the ring accumulator --------------------
@@ -791,13 +804,14 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
     __syncthreads();
     // ---- E: retire rows that no later block row touches ---------------------
     const int rlo = max(oy, Y0), rhi = min(by == by_hi ? Y0 + th : oy + gy.step, Y0 + th);
+    const OutConv oc = out_conv(P);
     for (Cursor2 c = walk_tw; c.y < rhi - rlo; c.next()) {
       const int yy = c.y, xx = c.x;
       const int Y = rlo + yy;
       float* a = acc + int(unsigned(Y) % unsigned(BH)) * S.tw + xx;
       const float v = *a;
       if (!isfin(v)) bad = true;
-      store_sample<STORAGE, ALGO>(J.dst + ptrdiff_t(Y - gy.offset) * J.dst_stride, px0 + xx, v, P);
+      store_sample<STORAGE, ALGO>(J.dst + ptrdiff_t(Y - gy.offset) * J.dst_stride, px0 + xx, v, oc);
       *a = 0.0f;
     }
   }

@@ -686,8 +686,11 @@ class ROI:
 class ClipBatch:
     """Temporal clips in batched form: `clips` is a list of (plan, frames, dsts) with
     device tensors; every output frame is filtered with the host layer's frame selection
-    (FFT3D bt 2..5: temporal.fft3d_slots; DFTTest tmode 1 with tosize 0:
-    temporal.temporal_blocks). Equal to per-frame process_at."""
+    (FFT3D bt 2..5: temporal.fft3d_slots; DFTTest tmode 1: temporal.temporal_blocks;
+    DFTTest tmode 0: the clamped centred window). FFT3D and DFTTest tmode 1 with tosize 0
+    share each frame's transforms between outputs (two passes); the other DFTTest modes run
+    one filter call per output frame inside the batch's launch and graph. Equal to
+    per-frame process_at."""
 
     def __init__(self, clips):
         self._lib = C.load()

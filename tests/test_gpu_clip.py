@@ -131,10 +131,6 @@ def test_clip_batch_rejects_invalid_items(cuda):
     d = [cuda.empty_like(f) for f in fr]
     with pytest.raises(ValueError, match="bt 2..5"):
         ClipBatch([(Plan(96, 64, fmt, FFT3DConfig(bw=16, bh=16, bt=1)), fr, d)])
-    with pytest.raises(ValueError, match="tmode 1, tosize 0"):
-        ClipBatch([(Plan(96, 64, fmt, DFTConfig(tbsize=3)), fr, d)])  # tmode 0
-    with pytest.raises(ValueError, match="tmode 1, tosize 0"):
-        ClipBatch([(Plan(96, 64, fmt, DFTConfig(tbsize=3, temporal_mode=1, temporal_overlap=1)), fr, d)])
     with pytest.raises(ValueError, match="at least tbsize"):
         ClipBatch([(Plan(96, 64, fmt, DFTConfig(tbsize=5, temporal_mode=1)), fr, d)])
     p16 = Plan(96, 64, fmt, FFT3DConfig(bw=16, bh=16, bt=3))
@@ -143,3 +139,50 @@ def test_clip_batch_rejects_invalid_items(cuda):
         ClipBatch([(p16, fr, d), (p32, fr, [cuda.empty_like(f) for f in fr])])
     with pytest.raises(ValueError):
         ClipBatch([(p16, fr, [fr[1], d[1], d[2], d[3]])])  # an output overlaps a frame of the clip
+
+
+def _per_frame_window(cuda, plan, frames, tmode, overlap=0):
+    """One process_at per output frame with the host layer's selection: tmode 0 the clamped
+    centred window (filter.hpp:289-296), tmode 1 the covering temporal blocks."""
+    n, T = len(frames), plan.temporal_size
+    outs = []
+    for t in range(n):
+        o = cuda.empty_like(frames[t])
+        if tmode == 0:
+            plan.process_at([frames[min(max(t - T // 2 + j, 0), n - 1)] for j in range(T)], o)
+        else:
+            blocks = temporal_blocks(t, n, T, overlap)
+            plan.process_at([frames[j] for b in blocks for j in b["slots"]], o, targets=[b["target"] for b in blocks])
+        outs.append(o)
+    return outs
+
+
+def test_clip_batch_per_frame_dfttest_modes(cuda):
+    """DFTTest tmode 0, tmode 1 with tosize > 0 and smode 0 clips in one clip batch beside a
+    grouped tmode 1 clip: every output equals its per-frame call, plain and from the graph."""
+    fmt = SampleFormat(16)
+    w, h, n = 120, 90, 7
+    cases = [
+        (DFTConfig(block=16, overlap=8, tbsize=3, ftype=0, sigma=6.0), 0, 0),  # tmode 0
+        (DFTConfig(block=16, overlap=8, tbsize=5, ftype=1, sigma=8.0), 0, 0),  # tmode 0, T=5
+        (DFTConfig(block=12, overlap=6, tbsize=4, temporal_mode=1, temporal_overlap=2, ftype=0, sigma=5.0), 1, 2),
+        (DFTConfig(block=9, mode=0, tbsize=3, ftype=0, sigma=4.0), 0, 0),  # smode 0 (centre)
+        (DFTConfig(block=16, overlap=8, tbsize=3, temporal_mode=1, ftype=0, sigma=6.0), 1, 0),  # grouped
+    ]
+    clips, expect = [], []
+    for i, (cfg, tmode, overlap) in enumerate(cases):
+        plan = Plan(w, h, fmt, cfg)
+        frames = _clip(cuda, n, h, w, fmt, 120 + i)
+        dsts = [cuda.empty_like(f) for f in frames]
+        clips.append((plan, frames, dsts))
+        expect.append(_per_frame_window(cuda, plan, frames, tmode, overlap))
+    batch = ClipBatch(clips)
+    for graph in (False, True):
+        for _, _, dsts in clips:
+            for d in dsts:
+                d.fill_(0)
+        batch.launch(graph=graph)
+        for (plan, _, dsts), exp in zip(clips, expect):
+            for t, (got, e) in enumerate(zip(dsts, exp)):
+                assert cuda.equal(got, e), (plan, t, graph)
+            plan.sync_status()

@@ -266,12 +266,16 @@ __global__ void __launch_bounds__(256) kalman_ola_kernel(DevPlan P, const float*
                                                          long long dst_stride) {
   const DevAxis gx = P.gx, gy = P.gy;
   const int BH = P.bh, BW = P.bw;
+  // the last covering block is the one starting at or before the pixel; the one before it
+  // covers the pixel too when the pixel lies within its block length (one division per axis)
   const int Y = blockIdx.y, cy = Y + gy.offset;
-  const int by1 = min(gy.count - 1, cy / gy.step), by0 = max(0, floor_div_i(cy - BH, gy.step) + 1);
+  const int by1 = min(gy.count - 1, cy / gy.step);
+  const int by0 = by1 > 0 && cy - (by1 - 1) * gy.step < BH ? by1 - 1 : by1;
   const int X = (blockIdx.x * blockDim.x + threadIdx.x) * V;
   if (X >= gx.length) return;
   const int cx = X + gx.offset;
-  const int bx1 = min(gx.count - 1, cx / gx.step), bx0 = max(0, floor_div_i(cx - BW, gx.step) + 1);
+  const int bx1 = min(gx.count - 1, cx / gx.step);
+  const int bx0 = bx1 > 0 && cx - (bx1 - 1) * gx.step < BW ? bx1 - 1 : bx1;
   using Vec = typename std::conditional<V == 4, float4, typename std::conditional<V == 2, float2, float>::type>::type;
   Vec v[2][2];
 #pragma unroll

@@ -191,7 +191,7 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
   }
 #pragma unroll
   for (int i = 0; i < TC * TC; ++i) tf[i] = P.tfwd[i];
-  const float mean_scale = P.mean_scale, lower = P.lower, noise_mult = P.noise_mult, noise_uniform = P.noise_uniform;
+  const float lower = P.lower, noise_mult = P.noise_mult, noise_uniform = P.noise_uniform;
   const float* primary = filt.primary;
   const float fT = float(TC);
   (void)T;
@@ -205,8 +205,7 @@ __device__ __forceinline__ void temporal_filter_elements(const DevPlan& P, const
     for (int j = 0; j < TC; ++j) v[j] = slot[j][at];
     cf gT = {0.0f, 0.0f};
     if (grid) {
-      const float g = fdiv(fmul(mean_scale, dc[b]), grid0);
-      if (!isfin(g)) bad = true;
+      const float g = dc[b];  // the block's template scale
       const cf M = {fmul(g, grid[kk].r), fmul(g, grid[kk].i)};
       gT = {fmul(M.r, fT), fmul(M.i, fT)};
     }
@@ -541,7 +540,16 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       const size_t row_base = size_t(by) * bins * cnt + size_t(bx_lo);
       const float invT = fdiv(1.0f, float(T));
       if (by < by_hi) prefetch_row_l2(J.tspec, T, row_base + size_t(bins) * cnt, bins, cnt, nbx, walk_lines);
-      for (int b = tid; b < nbx; b += nthr) dc[b] = J.tspec[c][row_base + b].r;
+      // each block's template scale, mean_scale * DC(centre slot) / grid DC, once per block
+      // (the filter below reads it for every bin of the block)
+      for (int b = tid; b < nbx; b += nthr) {
+        float g = 0.0f;
+        if (grid) {
+          g = fdiv(fmul(P.mean_scale, J.tspec[c][row_base + b].r), grid0);
+          if (!isfin(g)) bad = true;
+        }
+        dc[b] = g;
+      }
       __syncthreads();
       const int nel = bins * nbx;
       switch (T) {  // compile-time slot counts keep the slot values in registers
@@ -552,11 +560,12 @@ __device__ __forceinline__ void strip_tile(const DevPlan& P, const PlaneJob& J, 
       }
       __syncthreads();
       if (enh.enh) {
-        for (int b = tid; b < nbx; b += nthr) dc[NB + b] = spec[b].r;  // recovered DC
+        // template scale of each block's recovered spectrum, once per block
+        for (int b = tid; b < nbx; b += nthr) dc[NB + b] = grid ? fdiv(fmul(P.mean_scale, spec[b].r), grid0) : 0.0f;
         __syncthreads();
         for (Cursor2 c = walk_nbx; c.y < bins; c.next()) {
           const int kk = c.y, b = c.x;
-          const float g2 = grid ? fdiv(fmul(P.mean_scale, dc[NB + b]), grid0) : 0.0f;
+          const float g2 = dc[NB + b];
           cf* sp = spec + kk * NB + b;
           *sp = spectral_bin<-2>(*sp, grid, kk, g2, enh, bad);  // enh is always type -2
         }

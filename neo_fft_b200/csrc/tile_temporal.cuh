@@ -178,7 +178,10 @@ __device__ __forceinline__ void volume_time(const DevPlan& P, const VolumeSpectr
 #pragma unroll
     for (int z = 0; z < CAP; ++z)
       if (z < T) bp[size_t(z) * slot] = line[z];
-    if (kk == 0) dc[b] = line[0].r;
+    // the block's template scale from its volume DC, once per block (the filter reads it per bin)
+    if (kk == 0)
+      dc[b] = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f) ? fdiv(fmul(P.mean_scale, line[0].r), P.grid[0].r)
+                                                                      : 0.0f;
   }
   __syncthreads();
   const size_t cnt = size_t(P.gx.count);
@@ -189,8 +192,7 @@ __device__ __forceinline__ void volume_time(const DevPlan& P, const VolumeSpectr
     for (Cursor2 c(tid, nthr, nb); c.y < bins; c.next()) {
       const int kk = c.y, b = c.x;
       const cf* bp = spec + size_t(kk) * nbc + b;
-      const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
-                          ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
+      const float g = dc[b];  // the block's template scale
       cf line[CAP];
 #pragma unroll
       for (int z = 0; z < CAP; ++z)

@@ -134,12 +134,18 @@ __global__ void __launch_bounds__(256) volume_tile_kernel(DevPlan P, VolumeShape
         // ---- T: temporal transform and filter per bin ------------------------
         const int nbin = nb * BH * K;
         if (fft3d) {
-          for (int task = tid; task < nbin; task += nthr) {
-            const int b = task / int(slot_bins), kk = task - b * int(slot_bins);
-            cf* bp = spec + b * blk_bins + kk;
+          // each block's template scale from the centre slot's DC, once per block
+          for (int b = tid; b < nb; b += nthr) {
             const float g = P.grid ? fdiv(fmul(P.mean_scale, spec[b * blk_bins + size_t(c) * slot_bins].r), P.grid[0].r)
                                    : 0.0f;
             if (P.grid && !isfin(g)) bad = true;
+            dc[b] = g;
+          }
+          __syncthreads();
+          for (int task = tid; task < nbin; task += nthr) {
+            const int b = task / int(slot_bins), kk = task - b * int(slot_bins);
+            cf* bp = spec + b * blk_bins + kk;
+            const float g = dc[b];
             const cf M = P.grid ? cf{fmul(g, P.grid[kk].r), fmul(g, P.grid[kk].i)} : cf{0.0f, 0.0f};
             const cf gT = {fmul(M.r, float(T)), fmul(M.i, float(T))};
             cf Fv[5];
@@ -176,7 +182,10 @@ __global__ void __launch_bounds__(256) volume_tile_kernel(DevPlan P, VolumeShape
             for (int z = 0; z < T; ++z) line[z] = bp[size_t(z) * slot_bins];
             nf::fft_project<true, 0, 16>(line, T, P.twt);
             for (int z = 0; z < T; ++z) bp[size_t(z) * slot_bins] = line[z];
-            if (kk == 0) dc[b] = line[0].r;
+            // the block's template scale from its volume DC, once per block (the filter reads it per bin)
+            if (kk == 0)
+              dc[b] = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f) ? fdiv(fmul(P.mean_scale, line[0].r), P.grid[0].r)
+                                                                              : 0.0f;
           }
           __syncthreads();
           // The filter type fixed at compile time per branch (no switch per element).
@@ -185,8 +194,7 @@ __global__ void __launch_bounds__(256) volume_tile_kernel(DevPlan P, VolumeShape
             for (int task = tid; task < nbin; task += nthr) {
               const int b = task / int(slot_bins), kk = task - b * int(slot_bins);
               cf* bp = spec + b * blk_bins + kk;
-              const float g = (P.grid && P.mean_scale != 0.0f && P.grid[0].r != 0.0f)
-                                  ? fdiv(fmul(P.mean_scale, dc[b]), P.grid[0].r) : 0.0f;
+              const float g = dc[b];  // the block's template scale
               cf line[15];
               for (int z = 0; z < T; ++z)
                 line[z] = spectral_bin<FT>(bp[size_t(z) * slot_bins], P.grid, z * int(slot_bins) + kk, g, P.filt, bad);

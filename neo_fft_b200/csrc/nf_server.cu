@@ -392,8 +392,11 @@ struct nf_frame_server {
             else check(nf_kalman_state_create(plans[size_t(p)], 0, &cur.planes[size_t(p)], err, sizeof err), err);
             cur.bytes += nf_kalman_state_bytes(cur.planes[size_t(p)]);
           }
+          // frames before n are advanced; frame n is advanced and rendered together below
+          // (nf_kalman_step_device: the same results as advance then render)
           for (int f = replay_start + 1; f <= n; ++f) {
             upload(b, f);
+            if (f == n) break;
             for (int p = 0; p < planes; ++p)
               if (plans[size_t(p)])
                 check(nf_kalman_advance_device(plans[size_t(p)], device_plane(b.src, 0, p), cur.planes[size_t(p)], st,
@@ -414,9 +417,14 @@ struct nf_frame_server {
         if (plans[size_t(p)] && state) {
           const auto& in = info[size_t(p)];
           if (d.width != in.width || d.height != in.height) raise(NF_INVALID_ARGUMENT, "frame dimensions differ from plan");
-          check(nf_kalman_render_device(plans[size_t(p)], device_plane(b.src, 0, p), out_plane(b.out, 0, p),
-                                        (*state)[size_t(p)], st, err, sizeof err),
-                err);
+          if (have_n)
+            check(nf_kalman_step_device(plans[size_t(p)], device_plane(b.src, 0, p), out_plane(b.out, 0, p),
+                                        cur.planes[size_t(p)], st, err, sizeof err),
+                  err);
+          else
+            check(nf_kalman_render_device(plans[size_t(p)], device_plane(b.src, 0, p), out_plane(b.out, 0, p),
+                                          (*state)[size_t(p)], st, err, sizeof err),
+                  err);
           check(cudaMemcpy2DAsync(d.data, size_t(d.stride_bytes), slot(b.out, 0, p), pitch[size_t(p)],
                                   size_t(in.width) * size_t(in.elem), size_t(in.height), cudaMemcpyDefault, st),
                 "output copy failed");

@@ -188,6 +188,13 @@ typedef struct nf_batch_item {
   nf_plane dst;
 } nf_batch_item;
 nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** batch, char* err, size_t err_len);
+/* The same with each item's frame and plane numbers (the `frame` and `plane` arguments of
+ * nf_plan_process_device; NULL arrays mean 0). They seed the noise of dithered 8-bit DFTTest
+ * output (dither.cpp:4-41, plan.cpp:617-623), so this form also takes dithered items: the
+ * batch filters them into a float accumulator of its own and runs the dither pass per item,
+ * with outputs equal to nf_plan_process_device(..., frame, plane, ...). */
+nf_status nf_batch_create_indexed(const nf_batch_item* items, const int* frames, const int* planes, int count,
+                                  nf_batch** batch, char* err, size_t err_len);
 /* Enqueues the batch on `stream`: no allocation. The first call outside a stream
  * capture also tunes the strip geometry: it launches each of up to three candidate
  * geometries once (after a warm-up launch; all write the same outputs) and waits for

@@ -104,6 +104,8 @@ PROTOTYPES = {
     "nf_kalman_state_read": (c_int, [c_void_p, _FP, _FP, _FP, c_size_t]),
     "nf_batch_create": (c_int, [ctypes.POINTER(NfBatchItem), c_int, ctypes.POINTER(c_void_p), ctypes.c_char_p,
                                 c_size_t]),
+    "nf_batch_create_indexed": (c_int, [ctypes.POINTER(NfBatchItem), _IP, _IP, c_int, ctypes.POINTER(c_void_p),
+                                        ctypes.c_char_p, c_size_t]),
     "nf_batch_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_batch_graph_launch": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, c_size_t]),
     "nf_batch_destroy": (None, [c_void_p]),

@@ -108,6 +108,20 @@ struct BatchGroup {
 };
 
 struct nf_batch {
+  // Dithered 8-bit DFTTest items (nf_batch_create_indexed): the batch filters them into a
+  // float accumulator plane, then the dither pass writes the item's output (plan.cpp:617-623),
+  // as nf_plan_process_device does.
+  struct DitherJob {
+    const nf_plan* plan;
+    float* acc;
+    size_t pitch;  // bytes per accumulator row
+    float* boundary;
+    unsigned char* dst;
+    long long dst_stride;
+    int width, height, frame, plane;
+  };
+  std::vector<DitherJob> dithers;
+  void* dither_mem = nullptr;
   std::vector<BatchGroup> groups;                 // the strip geometry in use (one of `variants`)
   std::vector<std::vector<BatchGroup>> variants;  // candidate geometries, timed on the first launch
   bool tuned = false;
@@ -125,6 +139,7 @@ struct nf_batch {
       for (auto& g : v)
         if (g.dev) cudaFree(g.dev);
     if (counters) cudaFree(counters);
+    if (dither_mem) cudaFree(dither_mem);
   }
 };
 
@@ -1778,10 +1793,16 @@ nf_status nf_kalman_state_read(const nf_kalman_state* s, float* last, float* cov
   return NF_OK;
 }
 
-nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out, char* err, size_t len) {
+namespace {
+// frames / plane_ids: each item's frame and plane numbers (nf_plan_process_device's `frame`
+// and `plane`), or null: they seed the noise of dithered 8-bit DFTTest output, which only
+// the indexed form accepts.
+nf_status batch_create(const nf_batch_item* items, const int* frames, const int* plane_ids, int count, bool indexed,
+                       nf_batch** out, char* err, size_t len) {
   return guarded(err, len, [&]() -> nf_status {
     nfb::require(out && (count == 0 || items), "null batch output or items");
     auto b = std::make_unique<nf_batch>();
+    std::vector<std::pair<size_t, int>> dithered;  // (entry, item) of dithered items
     struct Entry {
       int group, plan;
       nfd::PlaneJob job;
@@ -1790,15 +1811,20 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
     };
     std::vector<Entry> entries;
     std::vector<std::vector<const nf_plan*>> group_plans;
+    std::vector<std::vector<char>> group_raw;  // per group plan: filters into a dither accumulator
     for (int i = 0; i < count; ++i) {
       const nf_batch_item& it = items[i];
       nfb::require(it.plan != nullptr, "null plan in batch");
       const nf_plan& p = *it.plan;
       nfb::require(!p.t.kalman && (p.t.temporal_size == 1 || p.t.algo == nfb::Algo::FFT3D) && !p.t.temporal_ola,
                    "batch items must be single-frame plans");
-      nfb::require(!dithers(p.t), "dithered 8-bit DFTTest output runs through nf_plan_process_device");
+      const bool dith = dithers(p.t);
+      nfb::require(!dith || indexed,
+                   "dithered 8-bit DFTTest output runs through nf_plan_process_device or nf_batch_create_indexed");
       nfb::require(!p.t.preview, "pshow previews run through nf_plan_process_device");
       validate_call(p, &it.source, 1, nullptr, 0, it.dst);
+      nfb::require(!dith || ((!frames || frames[i] >= 0) && (!plane_ids || plane_ids[i] >= 0)),
+                   "invalid dither coordinates or mode");
       if (std::find(b->plans.begin(), b->plans.end(), &p) == b->plans.end()) b->plans.push_back(&p);
       const int storage = storage_of(p.t.format), algo = p.t.algo == nfb::Algo::FFT3D ? 0 : 1;
       int gi = -1;
@@ -1815,22 +1841,50 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
         g.algo = algo;
         b->groups.push_back(g);
         group_plans.emplace_back();
+        group_raw.emplace_back();
       }
+      // a dithered item's plan enters its group a second time, keeping the raw accumulator
       auto& plans = group_plans[size_t(gi)];
+      auto& raws = group_raw[size_t(gi)];
       int pi = -1;
       for (size_t j = 0; j < plans.size(); ++j)
-        if (plans[j] == &p) pi = int(j);
+        if (plans[j] == &p && raws[j] == char(dith)) pi = int(j);
       if (pi < 0) {
         pi = int(plans.size());
         plans.push_back(&p);
+        raws.push_back(char(dith));
       }
       Entry e{gi, pi,
               {static_cast<const unsigned char*>(it.source.data), (long long)it.source.stride_bytes,
                static_cast<unsigned char*>(it.dst.data), (long long)it.dst.stride_bytes, nullptr, pi},
               0, 0, (long long)p.t.gx.count * p.t.gy.count};
+      if (dith) dithered.emplace_back(entries.size(), i);
       entries.push_back(e);
     }
     cudaError_t ce;
+    if (!dithered.empty()) {  // accumulator planes and dither boundary rows, 256-byte aligned
+      auto up = [](size_t v) { return (v + 255) & ~size_t(255); };
+      size_t bytes = 0;
+      for (const auto& d : dithered) {
+        const nf_plan& p = *items[d.second].plan;
+        bytes += up(size_t(p.t.gx.length) * sizeof(float)) * size_t(p.t.gy.length) + up(size_t(p.t.gx.length) * sizeof(float));
+      }
+      if ((ce = cudaMalloc(&b->dither_mem, bytes)) != cudaSuccess) return cuda_fail(err, len, ce, "device allocation failed");
+      auto* at = static_cast<unsigned char*>(b->dither_mem);
+      for (const auto& d : dithered) {
+        const nf_batch_item& it = items[d.second];
+        const nf_plan& p = *it.plan;
+        const int W = p.t.gx.length, H = p.t.gy.length;
+        const size_t pitch = up(size_t(W) * sizeof(float));
+        nf_batch::DitherJob j{&p, reinterpret_cast<float*>(at), pitch, reinterpret_cast<float*>(at + pitch * size_t(H)),
+                              static_cast<unsigned char*>(it.dst.data), (long long)it.dst.stride_bytes, W, H,
+                              frames ? frames[d.second] : 0, plane_ids ? plane_ids[d.second] : 0};
+        at += pitch * size_t(H) + up(size_t(W) * sizeof(float));
+        entries[d.first].job.dst = reinterpret_cast<unsigned char*>(j.acc);
+        entries[d.first].job.dst_stride = (long long)pitch;
+        b->dithers.push_back(j);
+      }
+    }
     if (!b->groups.empty() &&
         (ce = cudaMalloc(&b->counters, sizeof(int) * b->groups.size())) != cudaSuccess)
       return cuda_fail(err, len, ce, "device allocation failed");
@@ -1851,8 +1905,10 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
         const auto& plans = group_plans[gi];
         std::vector<nfd::DevPlan> dplans;
         std::vector<nfd::StripShape> shapes;
-        for (const nf_plan* p : plans) {
+        for (size_t j = 0; j < plans.size(); ++j) {
+          const nf_plan* p = plans[j];
           dplans.push_back(p->dev);
+          if (group_raw[gi][j]) dplans.back().raw_out = 1;  // the dither pass converts
           const auto& cand = strip_candidates(p->dev, 0, StripWork::Staged);
           shapes.push_back(cand[std::min(size_t(v), cand.size() - 1)]);
         }
@@ -1925,6 +1981,15 @@ nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out,
     return NF_OK;
   });
 }
+} // namespace
+
+nf_status nf_batch_create(const nf_batch_item* items, int count, nf_batch** out, char* err, size_t len) {
+  return batch_create(items, nullptr, nullptr, count, false, out, err, len);
+}
+nf_status nf_batch_create_indexed(const nf_batch_item* items, const int* frames, const int* planes, int count,
+                                  nf_batch** out, char* err, size_t len) {
+  return batch_create(items, frames, planes, count, true, out, err, len);
+}
 
 namespace {
 cudaError_t launch_groups(nf_batch& b, const std::vector<BatchGroup>& groups, cudaStream_t st) {
@@ -1981,6 +2046,12 @@ nf_status nf_batch_launch(nf_batch* b, void* stream, char* err, size_t len) {
   cudaError_t e = cudaSuccess;
   if (!b->tuned && (e = tune_batch(*b, st)) != cudaSuccess) return cuda_fail(err, len, e, "batch tuning failed");
   if ((e = launch_groups(*b, b->groups, st)) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  for (const auto& d : b->dithers) {  // the dither pass of each dithered item (as process_dithered)
+    nfd::dither_kernel<<<1, std::min(nfd::kDitherRows, d.height), 0, st>>>(
+        d.acc, (long long)(d.pitch / sizeof(float)), d.dst, d.dst_stride, d.width, d.height, d.plan->t.dither,
+        unsigned(d.plan->t.dither_seed), unsigned(d.frame), unsigned(d.plane), d.boundary, d.plan->dev.err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(err, len, e, "kernel launch failed");
+  }
   return NF_OK;
 }
 

@@ -398,16 +398,24 @@ class Batch:
     replays a captured CUDA graph. Outputs equal per-plane `Plan.process_at`."""
 
     def __init__(self, items):
-        """items: iterable of (plan, source_tensor, dst_tensor)."""
+        """items: iterable of (plan, source_tensor, dst_tensor) or (plan, source_tensor,
+        dst_tensor, frame, plane); frame and plane (default 0) are process_at's, and items
+        that carry them may be dithered 8-bit DFTTest planes (nf_batch_create_indexed)."""
         self._lib = C.load()
-        items = list(items)
+        items = [tuple(it) for it in items]
         self._keep = items  # planes must stay alive while the batch exists
-        arr = (C.NfBatchItem * len(items))(*[C.NfBatchItem(p._h.value, _plane(s, True), _plane(d, False))
-                                             for p, s, d in items])
-        self._plans = [p for p, _, _ in items]
+        arr = (C.NfBatchItem * len(items))(*[C.NfBatchItem(it[0]._h.value, _plane(it[1], True), _plane(it[2], False))
+                                             for it in items])
+        self._plans = [it[0] for it in items]
         self._h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(512)
-        C.raise_for(self._lib.nf_batch_create(arr, len(items), ctypes.byref(self._h), err, 512), err.value)
+        if any(len(it) == 5 for it in items):
+            frames = (ctypes.c_int * len(items))(*[int(it[3]) if len(it) == 5 else 0 for it in items])
+            planes = (ctypes.c_int * len(items))(*[int(it[4]) if len(it) == 5 else 0 for it in items])
+            C.raise_for(self._lib.nf_batch_create_indexed(arr, frames, planes, len(items), ctypes.byref(self._h), err,
+                                                          512), err.value)
+        else:
+            C.raise_for(self._lib.nf_batch_create(arr, len(items), ctypes.byref(self._h), err, 512), err.value)
 
     def launch(self, graph: bool = False, stream=None) -> None:
         import torch

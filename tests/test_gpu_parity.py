@@ -1,7 +1,7 @@
 """GPU parity: the sm_100a path (through the C ABI) against the reference core compiled
 from its own sources, on identical seeded inputs.
 
-The bar (north star): float output within 2e-5 of full scale, integer output within
+The parity bar: float output within 2e-5 of full scale, integer output within
 ±1 LSB on at most 0.01 % of pixels. The GPU path restates the reference's arithmetic
 step by step, so these cases are expected to be bit-identical; `exact=False` cases
 (binary32 pow for f0beta outside {1, 0.5}) use the tolerance.

@@ -78,15 +78,18 @@ def test_fp64_reevaluation_matches_reference(name, w, h, fmt, cfg, nsrc):
     check(ref_out, fp.process(srcs), fp, fmt)
 
 
-@pytest.mark.parametrize("ftype", [0, 1])
-def test_fp64_temporal_overlap_add_matches_reference(ftype):
+@pytest.mark.parametrize("ftype,tbsize,tosize", [(0, 5, 0), (1, 5, 0), (0, 4, 2), (0, 5, 2)])
+def test_fp64_temporal_overlap_add_matches_reference(ftype, tbsize, tosize):
+    """tmode 1, with and without overlapping temporal blocks (tosize > 0: an output adds the
+    slices of every temporal block that covers it)."""
     w, h, n = 96, 80, 9
     fmt = SampleFormat(32, True)
-    cfg = DFTConfig(block=12, overlap=9, tbsize=5, temporal_mode=1, ftype=ftype, sigma=8.0)
+    cfg = DFTConfig(block=12, overlap=9, tbsize=tbsize, temporal_mode=1, temporal_overlap=tosize, ftype=ftype,
+                    sigma=8.0)
     clip = [plane(h, w, 32, True, seed=(62, f)) for f in range(n)]
     rp, fp = R.RefPlan(w, h, fmt, cfg), FP64Plan(w, h, fmt, cfg)
     for t in (0, 2, 4, 8):
-        blocks = temporal_blocks(t, n, 5, 0)
+        blocks = temporal_blocks(t, n, tbsize, tosize)
         srcs = [clip[s] for b in blocks for s in b["slots"]]
         tg = [b["target"] for b in blocks]
         check(rp.process(srcs, targets=tg), fp.process(srcs, targets=tg), fp, fmt, threshold=ftype == 1)

@@ -59,6 +59,9 @@ cudaError_t launch_kalman_one(const DevPlan& d, const void* src, ptrdiff_t ss, c
                            (a.fp64 ? reinterpret_cast<uintptr_t>(a.cov64) | reinterpret_cast<uintptr_t>(a.proc64)
                                    : reinterpret_cast<uintptr_t>(a.cov32) | reinterpret_cast<uintptr_t>(a.proc32));
   a.staged = (d.bins & 3) == 0 && (arrays & 15) == 0;
+  // Large blocks keep the state in global memory: one block's spectra and staged state must
+  // fit the run's shared-memory budget (128x128 blocks in binary64 variance need 266 KB).
+  if (a.staged && kalman_smem(d.bins, 1, a.synth != nullptr, a.fp64, 1).bytes > size_t(200) * 1024) a.staged = 0;
   const bool step = a.synth != nullptr;
   auto k = step ? kalman_advance_kernel<NF_BH, NF_BW, ST, true> : kalman_advance_kernel<NF_BH, NF_BW, ST, false>;
   auto smem_of = [&](int r) { return kalman_smem(d.bins, r, step, a.fp64, a.staged).bytes; };

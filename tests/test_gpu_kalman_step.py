@@ -28,6 +28,8 @@ CASES = [
      True),
     ("u10 48/24 sharpen", 200, 150, SampleFormat(10), FFT3DConfig(bw=48, bh=48, ow=24, oh=24, bt=0, sigma=3.0,
                                                                    kratio=2.0, sharpen=0.3), False),
+    # 45 bins per block: runs keep the state in global memory (no 16-byte bulk copies)
+    ("u8 9 state unstaged", 90, 66, SampleFormat(8), FFT3DConfig(bw=9, bh=9, bt=0, sigma=2.0, kratio=2.0), True),
 ]
 
 

@@ -43,6 +43,19 @@ def test_defaults_match_reference_structs():
     assert (d.block, d.overlap, d.mode, d.swin, d.twin, d.ftype, d.tbsize, d.zmean) == (16, 12, 1, 0, 7, 0, 1, 1)
 
 
+def test_header_is_plain_c():
+    """The C ABI compiles as C99 with warnings as errors and links against the library (the
+    calls a C, cgo or FFI host makes); the entry points that need no GPU give the defaults."""
+    import subprocess
+    exe = ROOT / "tests" / "_build" / "c_abi_check"
+    exe.parent.mkdir(exist_ok=True)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", f"-I{ROOT / 'include'}",
+                    str(ROOT / "tests" / "native" / "c_abi_check.c"), "-o", str(exe), f"-L{ROOT / 'neo_fft_b200'}",
+                    "-lneofft_b200", f"-Wl,-rpath,{ROOT / 'neo_fft_b200'}"], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert out == ["1", "32", "1", "16", "12", str(16 << 20)]
+
+
 def test_invalid_config_rejected_on_host():
     from neo_fft_b200.plan import DFTConfig, FFT3DConfig, Plan, SampleFormat
     with pytest.raises(ValueError, match="FFT3D bt outside -1..5"):

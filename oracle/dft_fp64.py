@@ -130,7 +130,9 @@ class FFT3DFP64:
     blocks (v*wy)*wx, r2c, degrid template M = degrid * X0/G0 * G with G = r2c(wy*wx),
     gain max((q - a)/q, floor) with q = |X - M|^2 + 1e-15 (kernels/scalar/spectral.cpp:18-22)
     times the sharpen/dehalo factor S(q)D(q) (algorithms/fft3d_profile.cpp:69-81; windows in
-    binary64 as in oracle/fp64_pipeline.py), Y = gain*R + M, c2r / (bw*bh), synthesis wxs*wys,
+    binary64 as in oracle/fp64_pipeline.py), Y = gain*R + M; for varying-sigma plans the
+    enhancement is a second pass on Y with its own template term (plan.cpp:476-481, 325-329);
+    c2r / (bw*bh), synthesis wxs*wys,
     overlap-add, output clamp(z, 0, 1) whose gradient passes where 0 < z < 1.
 
     forward(x [B, H, W] float64 tensor, table [bh*(bw/2+1)] float64 tensor) -> [B, H, W]; the
@@ -176,16 +178,30 @@ class FFT3DFP64:
         r = (q - a) / q
         gain = torch.where(r >= fp.floor, r, torch.full_like(r, fp.floor))
         e = fp.enh
-        if e.active:
-            s = torch.ones_like(q)
-            d = torch.ones_like(q)
+
+        def enhancement(qq):  # S(q) * D(q)
+            s = torch.ones_like(qq)
+            d = torch.ones_like(qq)
             if e.sharpen and e.b != 0:
-                s = 1.0 + e.sharpen * t(e.sw).reshape(bh, K) * torch.sqrt(q * e.b / ((q + e.a) * (q + e.b)))
+                s = 1.0 + e.sharpen * t(e.sw).reshape(bh, K) * torch.sqrt(qq * e.b / ((qq + e.a) * (qq + e.b)))
             if e.dehalo:
-                qc = q + e.c
-                d = qc / (qc + e.dehalo * t(e.hw).reshape(bh, K) * q)
-            gain = gain * s * d
-        out_blocks = torch.fft.irfft2(gain * R + mean, s=(bh, bw)) * ws
+                qc = qq + e.c
+                d = qc / (qc + e.dehalo * t(e.hw).reshape(bh, K) * qq)
+            return s * d
+
+        if e.active and fp.table is None:  # uniform sigma: enhancement fused into the Wiener gain
+            gain = gain * enhancement(q)
+        Y = gain * R + mean
+        if e.active and fp.table is not None:
+            # varying sigma (plan.cpp:476-481): the Wiener output is enhanced in a second pass
+            # whose template term is recomputed from that output's DC (enhance, plan.cpp:325-329)
+            if fp.grid is not None:
+                mean2 = (fp.mean_scale * Y[..., 0, 0].real / grid[0, 0].real)[..., None, None] * grid
+            else:
+                mean2 = torch.zeros_like(Y)
+            R2 = Y - mean2
+            Y = enhancement(R2.real ** 2 + R2.imag ** 2 + 1e-15) * R2 + mean2
+        out_blocks = torch.fft.irfft2(Y, s=(bh, bw)) * ws
         cols = out_blocks.permute(0, 3, 4, 1, 2).reshape(B, bh * bw, ny * nx)
         acc = F.fold(cols, output_size=(ch, cw), kernel_size=(bh, bw), stride=(sy, sx))[:, 0]
         oy, ox = self.gy["offset"], self.gx["offset"]

@@ -403,6 +403,8 @@ class Batch:
         that carry them may be dithered 8-bit DFTTest planes (nf_batch_create_indexed)."""
         self._lib = C.load()
         items = [tuple(it) for it in items]
+        if any(len(it) not in (3, 5) for it in items):
+            raise ValueError("batch items are (plan, source, dst) or (plan, source, dst, frame, plane)")
         self._keep = items  # planes must stay alive while the batch exists
         arr = (C.NfBatchItem * len(items))(*[C.NfBatchItem(it[0]._h.value, _plane(it[1], True), _plane(it[2], False))
                                              for it in items])

@@ -66,6 +66,14 @@ def test_invalid_config_rejected_on_host():
         Plan(64, 64, SampleFormat(9), DFTConfig())
 
 
+def test_batch_item_shapes_checked_on_host():
+    """A batch item carries both frame and plane numbers or neither; a 4-tuple is an error,
+    not an item whose frame is silently dropped."""
+    from neo_fft_b200.plan import Batch
+    with pytest.raises(ValueError, match="batch items are"):
+        Batch([(None, None, None, 3)])
+
+
 def _build_facade_check():
     import subprocess
     exe = ROOT / "tests" / "_build" / "facade_check"

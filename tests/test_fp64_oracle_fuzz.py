@@ -1,7 +1,9 @@
 """Seeded random configurations: the binary64 re-evaluation (oracle/fp64_pipeline.py)
 against the reference core compiled from its own sources, on the CPU. Draws cover both
 algorithms, every sample format, odd and non-square blocks, overlaps, windows, filter
-types, temporal sizes and modes, enhancement, degrid and sigma curves; the bar is the one
+types, temporal sizes and modes, enhancement, degrid and sigma curves. A draw the reference
+rejects is rejected by the re-evaluation too (it takes its validation and geometry from the
+reference's plan); otherwise the bar is the one
 of tests/test_fp64_oracle.py (the reference's own binary32 rounding only), with the
 threshold allowance wherever a gain switches at a threshold (DFTTest ftype 1, and ftype 3,
 whose gain switches at pmin/pmax) and the error scaled by the gain where it exceeds 1."""
@@ -55,22 +57,19 @@ def _fft3d(rng):
     return cfg
 
 
-def _outcome(fn):
-    try:
-        return fn(), None
-    except (ValueError, RuntimeError) as e:  # the oracle maps the reference's exceptions
-        return None, type(e)
-
-
 @pytest.mark.parametrize("seed", range(160))
 def test_random_configuration_fp64_matches_reference(seed):
     rng = np.random.default_rng([700, seed])
     fmt = FORMATS[int(rng.integers(0, len(FORMATS)))]
     cfg = _dft(rng) if rng.random() < 0.55 else _fft3d(rng)
     w, h = int(rng.integers(24, 120)), int(rng.integers(24, 96))
-    rp, err = _outcome(lambda: R.RefPlan(w, h, fmt, cfg))
-    if err is not None:
-        pytest.skip(f"the reference rejects the draw ({err.__name__})")
+    try:
+        rp = R.RefPlan(w, h, fmt, cfg)
+    except ValueError as e:
+        with pytest.raises(ValueError) as mine:
+            FP64Plan(w, h, fmt, cfg)
+        assert str(mine.value) == str(e)
+        return
     fp = FP64Plan(w, h, fmt, cfg)
     is_dft = isinstance(cfg, DFTConfig)
     T = cfg.tbsize if is_dft else max(cfg.bt, 1)
@@ -82,9 +81,7 @@ def test_random_configuration_fp64_matches_reference(seed):
         targets = [b["target"] for b in blocks]
     else:
         srcs = frames[:T]
-    ref_out, err = _outcome(lambda: rp.process(srcs, targets=targets))
-    if err is not None:
-        pytest.skip(f"the reference rejects the input ({err.__name__})")
+    ref_out = rp.process(srcs, targets=targets)
     threshold = is_dft and cfg.ftype in (1, 3)
     # DFTTest ftype 2/3/4 multiply by the sigma table (or sigma2): the largest of them bounds
     # the gain; the other filters' gains stay within 1

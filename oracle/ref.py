@@ -77,6 +77,8 @@ def load() -> ctypes.CDLL:
             "ref_plan_publish_pattern": (ci, [vp, FP, ci, cp, cs]),
             "ref_dither": (ci, [FP, ci, ci, ci, ctypes.POINTER(ctypes.c_ubyte), ci, ci, ci, ci, ci, cp, cs]),
             "ref_dither_hash": (ctypes.c_uint, [ctypes.c_uint] * 5),
+            "ref_temporal_blocks": (ci, [ci, ci, ci, ci, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ci),
+                                         ctypes.POINTER(ci), ci, ctypes.POINTER(ci), cp, cs]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -233,6 +235,22 @@ class RefKalman:
         if getattr(self, "h", None):
             self.lib.ref_kalman_destroy(self.h)
             self.h = None
+
+
+def temporal_blocks(frame: int, length: int, size: int, overlap: int) -> list[dict]:
+    """The reference's covering temporal blocks of an output frame
+    (src/algorithms/temporal_grid.hpp:24-40): start, target slice and clamped slots."""
+    cap = 16
+    starts = (ctypes.c_longlong * cap)()
+    targets = (ctypes.c_int * cap)()
+    slots = (ctypes.c_int * (cap * 15))()
+    count = ctypes.c_int()
+    err = ctypes.create_string_buffer(256)
+    _raise(load().ref_temporal_blocks(frame, length, size, overlap, starts, targets, slots, cap, ctypes.byref(count),
+                                      err, 256), err)
+    assert count.value <= cap
+    return [{"start": starts[i], "target": targets[i], "slots": list(slots[i * size:(i + 1) * size])}
+            for i in range(count.value)]
 
 
 def fp(a: np.ndarray):

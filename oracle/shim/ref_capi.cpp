@@ -7,12 +7,14 @@
 // Nothing here is linked into the product library.
 #include "algorithms/plan.hpp"
 #include "algorithms/dft_noise.hpp"
+#include "algorithms/temporal_grid.hpp"
 #include "kernels/dither.hpp"
 #include "neo_fft_b200.h"
 #include "fft_core.cuh"
 
 #include <cmath>
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <memory>
@@ -313,6 +315,20 @@ int ref_dither(const float* src, int w, int h, int src_stride, unsigned char* ds
 }
 unsigned ref_dither_hash(unsigned seed, unsigned n, unsigned p, unsigned y, unsigned x) {
   return dither_hash(seed, n, p, y, x);
+}
+// The covering temporal blocks of an output frame (temporal_grid.hpp): up to `cap`
+// blocks, each with its start, target slice and `size` clamped slots.
+int ref_temporal_blocks(int frame, int length, int size, int overlap, long long* starts, int* targets, int* slots,
+                        int cap, int* count, char* err, size_t len) {
+  return guarded(err, len, [&] {
+    const auto blocks = temporal_blocks(frame, length, size, overlap);
+    *count = int(blocks.size());
+    for (int i = 0; i < std::min(cap, *count); ++i) {
+      starts[i] = blocks[size_t(i)].start;
+      targets[i] = blocks[size_t(i)].target;
+      for (int z = 0; z < size; ++z) slots[i * size + z] = blocks[size_t(i)].slots[size_t(z)];
+    }
+  });
 }
 } // extern "C"
 

@@ -119,3 +119,28 @@ def test_temporal_lattice_examples():
     assert [x["slots"] for x in b] == [[2, 3, 4, 4], [4, 4, 4, 4]]
     with pytest.raises(ValueError, match="DFTTest temporal heavy overlap requires divisible step"):
         temporal_blocks(0, 10, 5, 3)
+
+
+def test_temporal_lattice_equals_reference(ref):
+    """neo_fft_b200.temporal.temporal_blocks (the tmode 1 frame selection of the clip forms,
+    the frame server and the shards) equals the reference's temporal_grid.hpp:24-40 for every
+    tbsize 1..15, every tosize 0..tbsize (invalid and heavy ones included), clips of tbsize - 1
+    to 40 frames and every frame index from -1 to the clip length: the same blocks, targets and
+    clamped slots, or the same error text."""
+    from neo_fft_b200.temporal import temporal_blocks
+    checked = rejected = 0
+    for size in range(1, 16):
+        for overlap in range(0, size + 1):
+            for length in sorted({size - 1, size, size + 1, 2 * size + 3, 40}):
+                for frame in range(-1, length + 1):
+                    try:
+                        want = ref.temporal_blocks(frame, length, size, overlap)
+                    except ValueError as e:
+                        with pytest.raises(ValueError) as mine:
+                            temporal_blocks(frame, length, size, overlap)
+                        assert str(mine.value) == str(e), (frame, length, size, overlap)
+                        rejected += 1
+                        continue
+                    assert temporal_blocks(frame, length, size, overlap) == want, (frame, length, size, overlap)
+                    checked += 1
+    assert checked == 7888 and rejected > 0, (checked, rejected)  # 7,888 valid (frame, clip, tbsize, tosize)

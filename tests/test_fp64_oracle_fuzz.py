@@ -87,3 +87,39 @@ def test_random_configuration_fp64_matches_reference(seed):
     # the gain; the other filters' gains stay within 1
     gain = max([cfg.sigma, cfg.sigma2] + list(cfg.slocation[1::2])) if is_dft and cfg.ftype >= 2 else 1.0
     check(ref_out, fp.process(srcs, targets=targets), fp, fmt, threshold=threshold, gain=gain)
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_kalman_sequence_fp64_matches_reference(seed):
+    """FFT3D bt=0 (Kalman) over 8 frames of a slowly varying clip, random block shape,
+    overlap, sigma, kratio, enhancement and format: every rendered frame within the bar.
+    A motion-test decision within binary32 rounding of its threshold (counted by the
+    re-evaluation) may go the other way in the reference; such frames take the
+    threshold allowance."""
+    from oracle.fp64_pipeline import FP64Kalman
+    rng = np.random.default_rng([702, seed])
+    fmt = FORMATS[int(rng.integers(0, len(FORMATS)))]
+    bw = int(rng.choice([8, 12, 16, 20, 32]))
+    bh = bw if rng.random() < 0.7 else int(rng.choice([8, 16, 32]))
+    cfg = FFT3DConfig(bw=bw, bh=bh, ow=int(rng.integers(0, bw // 2 + 1)), oh=int(rng.integers(0, bh // 2 + 1)),
+                      bt=0, sigma=float(rng.uniform(1.0, 4.0)), kratio=float(rng.uniform(1.5, 3.0)),
+                      sharpen=float(rng.choice([0.0, 0.0, 0.3])), dehalo=float(rng.choice([0.0, 0.0, 0.4])))
+    w, h = int(rng.integers(40, 120)), int(rng.integers(32, 96))
+    try:
+        rp = R.RefPlan(w, h, fmt, cfg)
+    except ValueError as e:
+        with pytest.raises(ValueError) as mine:
+            FP64Plan(w, h, fmt, cfg)
+        assert str(mine.value) == str(e)
+        return
+    fp = FP64Plan(w, h, fmt, cfg)
+    st, k = rp.kalman_state(), FP64Kalman(fp)
+    base = plane(h, w, fmt.bits, fmt.floating, seed=(703, seed, 0)).astype(np.float64)
+    sd = 0.02 if fmt.floating else 0.02 * fp.peak
+    dtype = np.float32 if fmt.floating else np.uint8 if fmt.bits == 8 else np.uint16
+    for _ in range(8):
+        v = base + rng.standard_normal((h, w)) * sd
+        src = (v if fmt.floating else np.clip(np.round(v), 0, fp.peak)).astype(dtype)
+        rp.advance_kalman(src, st)
+        k.advance(src)
+        check(rp.render_kalman(src, st), k.render(), fp, fmt, threshold=k.ambiguous > 0)

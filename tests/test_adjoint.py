@@ -463,3 +463,52 @@ def test_training_step_replays_from_a_cuda_graph(cuda):
         torch.cuda.synchronize()
         assert torch.equal(static_x.grad, eager[0]) and torch.equal(m.table.grad, eager[1])
     m.plan.sync_status()
+
+
+@pytest.mark.parametrize("seed", range(64))
+def test_fp64_restatements_random_configurations(ref, seed):
+    """The differentiable binary64 restatements (oracle/dft_fp64.py) against the reference
+    core on seeded random configurations of what they cover: DFTTest tbsize 1 ftype 0/1/2
+    (block, overlap, window, zmean, sigma) and FFT3D bt=1 (block shape, overlap, window type,
+    sigma curve, beta, degrid, sharpen, dehalo), float planes. The bar is the fixed cases'
+    1e-6 of full scale, times the gain where DFTTest ftype 2 multiplies by sigma > 1; ftype 1,
+    a hard threshold, allows a switched bin (1e-3 on at most 2 % of pixels)."""
+    import torch
+    from oracle.dft_fp64 import DFTTestFP64, FFT3DFP64
+    rng = np.random.default_rng([37, seed])
+    w, h = int(rng.integers(40, 130)), int(rng.integers(32, 100))
+    x = plane(h, w, 32, True, seed=(37, seed, 0))
+    threshold, gain = False, 1.0
+    if rng.random() < 0.5:
+        block = int(rng.choice([8, 12, 16]))
+        ftype = int(rng.integers(0, 3))
+        cfg = DFTConfig(block=block, overlap=int(rng.choice([block // 4, block // 2, 3 * block // 4])), ftype=ftype,
+                        swin=int(rng.integers(0, 12)), zmean=bool(rng.integers(0, 2)),
+                        sigma=float(rng.uniform(4.0, 30.0)) if ftype != 2 else float(rng.uniform(0.3, 2.0)))
+        threshold, gain = ftype == 1, max(1.0, cfg.sigma) if ftype == 2 else 1.0
+        make = DFTTestFP64
+    else:
+        bw = int(rng.choice([8, 12, 16, 32]))
+        bh = bw if rng.random() < 0.7 else int(rng.choice([8, 16]))
+        cfg = FFT3DConfig(bw=bw, bh=bh, ow=int(rng.integers(0, bw // 2 + 1)), oh=int(rng.integers(0, bh // 2 + 1)),
+                          wintype=int(rng.integers(0, 3)), sigma=float(rng.uniform(1.0, 4.0)),
+                          beta=float(rng.uniform(1.0, 2.0)), degrid=float(rng.choice([0.0, 1.0])),
+                          sharpen=float(rng.choice([0.0, 0.3])), dehalo=float(rng.choice([0.0, 0.3])))
+        if rng.random() < 0.3:
+            cfg.sigma2, cfg.sigma3, cfg.sigma4 = (float(rng.uniform(1.0, 4.0)) for _ in range(3))
+        make = FFT3DFP64
+    try:
+        exp = ref.RefPlan(w, h, SampleFormat(32, True), cfg).process(x)
+    except ValueError:
+        with pytest.raises(ValueError):
+            make(w, h, cfg)
+        return
+    o = make(w, h, cfg)
+    plan_table = getattr(getattr(o, "fp", None), "table", None)  # a varying-sigma FFT3D plan's own curve
+    table = np.asarray(plan_table if plan_table is not None else o.uniform_table(), np.float64)
+    got = o.forward(torch.from_numpy(x).double()[None], torch.from_numpy(table))[0].numpy()
+    e = np.abs(got - exp) / max(1.0, float(np.abs(exp).max()))
+    if threshold:
+        assert e.max() <= 1e-3 and np.mean(e > 1e-6) <= 0.02
+    else:
+        assert e.max() <= 1e-6 * gain

@@ -412,7 +412,7 @@ def run_ours(args):
                 "per_plane_host_api_value": host_plane_value,
                 "per_plane_host_api_8_threads_value": host_threads_value},
         "gpu_launches": args.steps,
-        # The binding roof is the FP32 pipe (358 flops per algorithmic byte against a ridge of
+        # The binding roof is the FP32 pipe (193 flops per algorithmic byte against a ridge of
         # ~11): achieved = algorithmic flops per launch / the launch's CUDA-event time; the
         # peak is nominal (no FP32 peak is measured on this pool). The HBM fraction and the
         # DRAM traffic of the same launch sit beside it.

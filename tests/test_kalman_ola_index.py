@@ -61,3 +61,24 @@ def test_pixel_groups_share_blocks_and_stay_in_rows():
             if V > 1:  # the vector load starts on a V-element boundary of the row
                 for b in range(b0, b1 + 1):
                     assert (c - b * a["step"]) % V == 0
+
+
+def test_axis_formula_equals_reference(ref):
+    """The axis formula above is the reference's own: every axis of the sweep that the
+    reference accepts as a plane width equals the geometry of a reference FFT3D plan built on
+    it (the oracle library)."""
+    from neo_fft_b200.plan import FFT3DConfig, SampleFormat
+    checked = 0
+    for a in AXES:
+        if a["length"] > 400:  # the wide planes add nothing to the formula check
+            continue
+        overlap = a["block"] - a["step"]
+        try:
+            plan = ref.RefPlan(a["length"], 32, SampleFormat(8), FFT3DConfig(bw=a["block"], bh=8, ow=overlap, oh=0,
+                                                                              bt=0, sigma=2.0))
+        except ValueError:  # padding beyond one reflection of a narrow plane: no plan to compare
+            continue
+        assert {k: plan.x[k] for k in ("length", "block", "step", "count", "cover", "offset")} == \
+            {k: a[k] for k in ("length", "block", "step", "count", "cover", "offset")}, a
+        checked += 1
+    assert checked > 100

@@ -79,7 +79,8 @@ def _build_facade_check():
     exe = ROOT / "tests" / "_build" / "facade_check"
     exe.parent.mkdir(exist_ok=True)
     src = ROOT / "tests" / "native" / "facade_check.cpp"
-    subprocess.run(["g++", "-std=c++17", "-O1", f"-I{ROOT / 'include'}", f"-I{ROOT / 'oracle' / 'shim'}", str(src),
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Wpedantic", "-Werror", f"-I{ROOT / 'include'}",
+                    f"-I{ROOT / 'oracle' / 'shim'}", str(src),
                     "-o", str(exe), f"-L{ROOT / 'neo_fft_b200'}", "-lneofft_b200",
                     f"-Wl,-rpath,{ROOT / 'neo_fft_b200'}"], check=True)
     return exe
@@ -112,7 +113,8 @@ def test_reference_roi_code_compiles_against_facade():
 
 def test_cpp_facade_compiles_and_links():
     """include/neo_fft_b200/plan.hpp (the reference Plan's class signature over the
-    C ABI) compiles against a span2d provider and links to the library."""
+    C ABI) compiles without warnings (-Wall -Wextra -Wpedantic) against a span2d provider
+    and links to the library."""
     assert _build_facade_check().exists()
 
 

@@ -167,3 +167,18 @@ def test_cpp_facade_matches_python_path(cuda):
         o = cuda.empty_like(frames[0])
         seek.frame(n, lambda f, p: frames[f], [o])
         assert int(got[f"seek{n}"]) == fnv(o.cpu().numpy().tobytes()), n
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """The product path has no CPU fallback: without the CUDA library, loading it raises."""
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        C.load(tmp_path / "libneofft_b200.so")
+
+
+def test_product_modules_do_not_import_the_oracle():
+    """Nothing under neo_fft_b200/ imports, links or runs oracle/ (the oracle is test
+    infrastructure); the package's sources name it nowhere."""
+    pkg = ROOT / "neo_fft_b200"
+    offenders = [p for p in list(pkg.glob("*.py")) + list((pkg / "csrc").glob("*"))
+                 if p.is_file() and re.search(r"\boracle\b", p.read_text(errors="replace"))]
+    assert not offenders, offenders

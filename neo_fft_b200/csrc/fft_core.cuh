@@ -751,6 +751,16 @@ struct TeamFFT {
 // NC > 0: compile-time length (fft_ct above). NC == 0: the same butterflies in a
 // runtime loop nest for lengths n <= RCAP.
 constexpr int kMaxProject = 128;
+// The runtime loop nest keeps one radix's values in buffers of kMaxRadix: a length whose
+// largest factor exceeds it (a prime side of 67..127) has no runtime transform, and plans
+// reject such block sides (largest_radix below).
+constexpr int kMaxRadix = kMaxProject < 64 ? kMaxProject : 64;
+NF_HD constexpr int largest_radix(int n) {
+  const Factors f = factorize(n);
+  int m = 1;
+  for (int l = 0; l < f.count; ++l) m = f.r[l] > m ? f.r[l] : m;
+  return m;
+}
 template <bool FORWARD, int NC, int RCAP = kMaxProject>
 NF_HD void fft_project(cf* a, int n_rt, const cf* table) {
   if constexpr (NC > 0) {
@@ -779,8 +789,8 @@ NF_HD void fft_project(cf* a, int n_rt, const cf* table) {
       const int tw_step = n / len;
       for (int base = 0; base < n; base += len) {
         for (int k1 = 0; k1 < inner; ++k1) {
-          cf t[kMaxProject < 64 ? kMaxProject : 64];
-          cf scratch[kMaxProject < 64 ? kMaxProject : 64];
+          cf t[kMaxRadix];
+          cf scratch[kMaxRadix];
           for (int j = 0; j < r; ++j) {
             cf v = a[base + j * inner + k1];
             const int e = j * k1;

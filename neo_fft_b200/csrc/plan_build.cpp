@@ -152,6 +152,8 @@ void validate_dft(const nf_dft_config& c) {
 void gpu_block_limits(int bh, int bw, int t) {
   require(bh <= nf::kMaxProject && bw <= nf::kMaxProject,
           "block size exceeds the GPU tile limit of 128 samples per side");
+  require(nf::largest_radix(bh) <= nf::kMaxRadix && nf::largest_radix(bw) <= nf::kMaxRadix,
+          "block side has a prime factor above 64, beyond the GPU transform's radix limit");
   require((long long)bh * (bw / 2 + 1) * t <= 16384, "block volume exceeds the GPU tile limit");
 }
 

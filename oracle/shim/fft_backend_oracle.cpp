@@ -26,6 +26,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <stdexcept>
 #include <vector>
 
 namespace {
@@ -48,6 +49,13 @@ const nf::cf* table(int n) {
 
 bool codelet_shape(int h, int w) { return h == w && (w == 8 || w == 16 || w == 32); }
 
+// The stand-in transform covers lengths up to 128 whose factors are at most 64 (the
+// product's limits); other lengths are refused rather than transformed wrongly.
+void stand_in_length(int n) {
+  if (n < 1 || n > nf::kMaxProject || nf::largest_radix(n) > nf::kMaxRadix)
+    throw std::invalid_argument("transform length outside the oracle's stand-in transform");
+}
+
 void r2c_one(int h, int w, const float* in, std::size_t in_rs, cfloat* out, std::size_t out_rs) {
   if (codelet_shape(h, w)) {
     if (w == 8) neo_fft::codelet::fft8x8_r2c(in, in_rs, out, out_rs);
@@ -55,6 +63,8 @@ void r2c_one(int h, int w, const float* in, std::size_t in_rs, cfloat* out, std:
     else neo_fft::codelet::fft32x32_r2c(in, in_rs, out, out_rs);
     return;
   }
+  stand_in_length(h);
+  stand_in_length(w);
   nf::block_r2c(in, int(in_rs), reinterpret_cast<nf::cf*>(out), int(out_rs), h, w, table(h), table(w));
 }
 void c2r_one(int h, int w, const cfloat* in, std::size_t in_rs, float* out, std::size_t out_rs, float fct) {
@@ -64,6 +74,8 @@ void c2r_one(int h, int w, const cfloat* in, std::size_t in_rs, float* out, std:
     else neo_fft::codelet::fft32x32_c2r(in, in_rs, out, out_rs, fct);
     return;
   }
+  stand_in_length(h);
+  stand_in_length(w);
   nf::block_c2r(reinterpret_cast<const nf::cf*>(in), int(in_rs), out, int(out_rs), h, w, fct, table(h),
                 table(w));
 }
@@ -86,6 +98,7 @@ void batch_c2r(std::size_t batch, int h, int w, const cfloat* in, std::size_t in
 
 // Temporal axis over T slices of `bins` complex values each (in place).
 void temporal_axis(int t, std::size_t bins, cfloat* v, bool forward) {
+  stand_in_length(t);
   std::vector<nf::cf> line(static_cast<std::size_t>(t));
   const nf::cf* tw = table(t);
   for (std::size_t k = 0; k < bins; ++k) {

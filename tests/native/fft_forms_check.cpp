@@ -161,3 +161,21 @@ extern "C" int fft32_real_mismatches(int structured) {
   }
   return bad;
 }
+
+// The runtime project transform of length n (1..kMaxProject, factors at most kMaxRadix; 1 is
+// returned for other lengths) on interleaved complex data, forward or inverse (unnormalised),
+// with the plan builders' binary32 twiddle table: the Python side compares it with a binary64
+// DFT for every length.
+extern "C" int project_fft(int n, int forward, const float* in, float* out) {
+  if (n < 1 || n > nf::kMaxProject || nf::largest_radix(n) > nf::kMaxRadix) return 1;
+  const auto tw = table(n);
+  std::vector<nf::cf> a(static_cast<size_t>(n));
+  for (int i = 0; i < n; ++i) a[size_t(i)] = {in[2 * i], in[2 * i + 1]};
+  if (forward) nf::fft_project<true, 0>(a.data(), n, tw.data());
+  else nf::fft_project<false, 0>(a.data(), n, tw.data());
+  for (int i = 0; i < n; ++i) {
+    out[2 * i] = a[size_t(i)].r;
+    out[2 * i + 1] = a[size_t(i)].i;
+  }
+  return 0;
+}

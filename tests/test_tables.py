@@ -203,3 +203,66 @@ def test_project_transform_forms_identical():
     # and of the 32-point one
     assert lib.fft32_real_mismatches(0) == 0
     assert lib.fft32_real_mismatches(1) == 0
+
+
+def _largest_prime_factor(n):
+    p, m, best = 2, n, 1
+    while m > 1:
+        while m % p == 0:
+            m //= p
+            best = p
+        p += 1
+    return best
+
+
+def test_project_transform_every_length_vs_binary64():
+    """The project transform (the stand-in for PocketFFT on every non-codelet length: block
+    sides, 48-point team transforms, temporal axes) against a binary64 DFT for every length
+    1..128 whose prime factors are at most 64, forward and inverse, on seeded complex data:
+    within the reference's FFT test tolerance (3e-5 of the largest output,
+    tests/unit/foundation.cpp:65-75). The primes 67..127 exceed the runtime transform's radix
+    buffers: the transform refuses them, and so do plans (next test)."""
+    import numpy as np
+    src = ROOT / "tests" / "native" / "fft_forms_check.cpp"
+    lib_path = ROOT / "tests" / "_build" / "libfft_forms.so"
+    lib_path.parent.mkdir(exist_ok=True)
+    if not lib_path.exists() or src.stat().st_mtime > lib_path.stat().st_mtime or \
+            (ROOT / "neo_fft_b200" / "csrc" / "fft_core.cuh").stat().st_mtime > lib_path.stat().st_mtime:
+        subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", "-fno-fast-math", "-ffp-contract=off",
+                        f"-I{ROOT / 'neo_fft_b200' / 'csrc'}", str(src), "-o", str(lib_path)], check=True)
+    lib = ctypes.CDLL(str(lib_path))
+    fp = ctypes.POINTER(ctypes.c_float)
+    lib.project_fft.argtypes = [ctypes.c_int, ctypes.c_int, fp, fp]
+    rng = np.random.default_rng(128)
+    worst = 0.0
+    for n in range(1, 129):
+        for forward in (1, 0):
+            x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+            inp = np.ascontiguousarray(np.stack([x.real, x.imag], -1), np.float32)
+            out = np.zeros_like(inp)
+            rc = lib.project_fft(n, forward, inp.ctypes.data_as(fp), out.ctypes.data_as(fp))
+            if _largest_prime_factor(n) > 64:
+                assert rc == 1
+                continue
+            assert rc == 0
+            got = out[:, 0].astype(np.float64) + 1j * out[:, 1]
+            xd = x.astype(np.complex128)
+            exp = np.fft.fft(xd) if forward else np.fft.ifft(xd) * n
+            err = np.abs(got - exp).max() / max(1.0, np.abs(exp).max())
+            worst = max(worst, err)
+            assert err <= 3e-5, (n, forward, err)
+    assert worst > 0.0
+
+
+def test_block_sides_beyond_the_radix_limit_rejected():
+    """Block sides with a prime factor above 64 (67..127) are refused at plan creation, before
+    any device work, for both algorithms."""
+    from neo_fft_b200.plan import DFTConfig, FFT3DConfig, Plan, SampleFormat
+    msg = "block side has a prime factor above 64"
+    for side in (67, 97, 127):
+        with pytest.raises(ValueError, match=msg):
+            Plan(400, 300, SampleFormat(8), FFT3DConfig(bw=side, bh=16, ow=0, oh=0))
+        with pytest.raises(ValueError, match=msg):
+            Plan(400, 300, SampleFormat(8), FFT3DConfig(bw=16, bh=side, ow=0, oh=0))
+        with pytest.raises(ValueError, match=msg):
+            Plan(400, 300, SampleFormat(8), DFTConfig(block=side, overlap=0))

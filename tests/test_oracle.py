@@ -170,3 +170,27 @@ def test_kernel_bin_arithmetic_equals_reference_kernels(ref):
     counts = dict(line.split() for line in r.stdout.splitlines())
     assert r.returncode == 0, r.stdout
     assert len(counts) == 15 and all(int(v) == 0 for k, v in counts.items() if k != "overflow_only"), counts
+
+
+def test_project_transform_random_shapes_vs_binary64(ref):
+    """The 2-D real transforms of non-codelet block shapes (fft_core.cuh block_r2c/block_c2r,
+    reached through the oracle's stand-in backend) against binary64 for 48 seeded random shapes
+    with sides 1..128 whose prime factors are at most 64: forward within 3e-5 of the largest
+    output (tests/unit/foundation.cpp:65-75), the round trip within 8e-6 of the largest input."""
+    rng = np.random.default_rng(64)
+    lib = ref.load()
+    done = 0
+    while done < 48:
+        h, w = (int(v) for v in rng.integers(1, 129, 2))
+        if any(max(p for p in range(1, n + 1) if n % p == 0 and all(p % q for q in range(2, p))) > 64
+               for n in (h, w)) or (h == w and w in (8, 16, 32)):
+            continue
+        x = rng.standard_normal((h, w)).astype(np.float32)
+        got = ref.r2c(x)
+        exp = np.fft.rfft2(x.astype(np.float64))
+        assert np.abs(got - exp).max() <= 3e-5 * max(1.0, np.abs(exp).max()), (h, w)
+        spec = np.ascontiguousarray(np.stack([got.real, got.imag], -1).astype(np.float32))
+        y = np.zeros((h, w), np.float32)
+        lib.ref_fft_c2r(h, w, ref.fp(spec), ref.fp(y))
+        assert np.abs(y - x).max() <= 8e-6 * max(1.0, np.abs(x).max()), (h, w)
+        done += 1

@@ -266,3 +266,57 @@ def test_block_sides_beyond_the_radix_limit_rejected():
             Plan(400, 300, SampleFormat(8), FFT3DConfig(bw=16, bh=side, ow=0, oh=0))
         with pytest.raises(ValueError, match=msg):
             Plan(400, 300, SampleFormat(8), DFTConfig(block=side, overlap=0))
+
+
+@pytest.mark.parametrize("seed", range(200))
+def test_random_configuration_tables_match_reference(tb, ref, seed):
+    """Seeded random configurations (both algorithms, every format, odd and non-square
+    blocks, overlaps, windows, ftypes, temporal modes, curves, enhancement): the product's
+    host plan builder and the reference either reject the draw with the same text, or both
+    build it with the same geometry and, for DFTTest, the same 3-D window and primary table
+    (FFT3D: the same sigma profile when sigma varies). A GPU limit the reference does not
+    have is the only other outcome allowed."""
+    from tests.test_fp64_oracle_fuzz import FORMATS, _dft, _fft3d
+    rng = np.random.default_rng([800, seed])
+    fmt = FORMATS[int(rng.integers(0, len(FORMATS)))]
+    cfg = _dft(rng) if rng.random() < 0.55 else _fft3d(rng)
+    w, h = int(rng.integers(16, 160)), int(rng.integers(16, 120))
+    algo = 0 if isinstance(cfg, FFT3DConfig) else 1
+    try:
+        rp, ref_msg = ref.RefPlan(w, h, fmt, cfg), None
+    except ValueError as e:
+        rp, ref_msg = None, str(e)
+    try:
+        sizes, big, scal = _product_tables(tb, algo, w, h, fmt, cfg)
+        msg = None
+    except ValueError as e:
+        msg = str(e)
+    if msg is not None and ref_msg is None:
+        assert "GPU" in msg, (cfg, msg)
+        return
+    assert msg == ref_msg, (cfg, msg, ref_msg)
+    if msg is not None:
+        return
+    assert (sizes[5], sizes[6], sizes[7], sizes[8], sizes[9], sizes[10]) == (
+        rp.x["count"], rp.y["count"], rp.x["cover"], rp.y["cover"], rp.x["offset"], rp.y["offset"]), cfg
+    err = ctypes.create_string_buffer(256)
+    if algo == 1:
+        hwin = np.zeros(sizes[4], np.float32)
+        w1 = np.zeros(1, np.float32)
+        assert ref.load().ref_dft_window_3d(cfg.tbsize, cfg.block, 0 if cfg.mode == 0 else cfg.overlap, cfg.mode,
+                                            cfg.swin, cfg.twin, cfg.sbeta, cfg.tbeta, cfg.temporal_mode,
+                                            cfg.temporal_overlap, ref.fp(hwin), ref.fp(w1), err, 256) == 0
+        assert np.array_equal(hwin, big[4][: sizes[4]]), cfg
+        if sizes[1]:
+            c, keep = cfg.to_c()
+            exp = np.zeros(sizes[1], np.float32)
+            div = w1[0] if cfg.ftype < 2 else np.float32(1)
+            assert ref.load().ref_dft_profile(ctypes.byref(c), div, ref.fp(exp), err, 256) == 0
+            assert np.array_equal(big[1][: sizes[1]], exp), cfg
+    elif cfg.sigma2 is not None and sizes[1]:
+        # the reference's sample-domain factor (plan.cpp:103): 1/255 for float planes
+        factor = np.float32(1.0) / np.float32(255) if fmt.floating else np.float32(1 << (fmt.bits - 8))
+        sig = np.array([cfg.sigma, cfg.sigma2, cfg.sigma3, cfg.sigma4], np.float32) * factor
+        exp = np.zeros(cfg.bh * (cfg.bw // 2 + 1), np.float32)
+        assert ref.load().ref_fft3d_profile(cfg.bw, cfg.bh, ref.fp(sig), ref.fp(exp), err, 256) == 0
+        assert np.array_equal(big[1][: sizes[1]], exp), cfg

@@ -55,4 +55,23 @@ int tb_plan(int algo, int w, int h, nf_format f, const void* cfg, int* sizes, fl
     return 2;
   }
 }
+// The product's C++ temporal lattice (plan_build.cpp, used by the clip batches and the frame
+// server): up to `cap` blocks with start, target and `size` slots; 1 with the text on error.
+int tb_temporal_blocks(int frame, int length, int size, int overlap, long long* starts, int* targets, int* slots,
+                       int cap, int* count, char* err, size_t len) {
+  try {
+    const auto blocks = nfb::temporal_blocks(frame, length, size, overlap);
+    *count = int(blocks.size());
+    for (int i = 0; i < cap && i < *count; ++i) {
+      starts[i] = blocks[size_t(i)].start;
+      targets[i] = blocks[size_t(i)].target;
+      for (int z = 0; z < size; ++z) slots[i * size + z] = blocks[size_t(i)].slots[z];
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    std::strncpy(err, e.what(), len - 1);
+    err[len - 1] = 0;
+    return 1;
+  }
+}
 }

@@ -320,3 +320,36 @@ def test_random_configuration_tables_match_reference(tb, ref, seed):
         exp = np.zeros(cfg.bh * (cfg.bw // 2 + 1), np.float32)
         assert ref.load().ref_fft3d_profile(cfg.bw, cfg.bh, ref.fp(sig), ref.fp(exp), err, 256) == 0
         assert np.array_equal(big[1][: sizes[1]], exp), cfg
+
+
+def test_cpp_temporal_lattice_equals_reference(tb, ref):
+    """The C++ temporal lattice the clip batches and the frame server use
+    (plan_build.cpp temporal_blocks) equals the reference's temporal_grid.hpp:24-40 for every
+    tbsize 1..15, tosize 0..tbsize and frame of clips up to 40 frames, error texts included."""
+    cap = 16
+    ci, ip = ctypes.c_int, ctypes.POINTER(ctypes.c_int)
+    tb.tb_temporal_blocks.argtypes = [ci, ci, ci, ci, ctypes.POINTER(ctypes.c_longlong), ip, ip, ci, ip,
+                                      ctypes.c_char_p, ctypes.c_size_t]
+    starts = (ctypes.c_longlong * cap)()
+    targets = (ctypes.c_int * cap)()
+    slots = (ctypes.c_int * (cap * 15))()
+    count = ctypes.c_int()
+    err = ctypes.create_string_buffer(256)
+    checked = 0
+    for size in range(1, 16):
+        for overlap in range(0, size + 1):
+            for length in sorted({size - 1, size, size + 1, 2 * size + 3, 40}):
+                for frame in range(-1, length + 1):
+                    rc = tb.tb_temporal_blocks(frame, length, size, overlap, starts, targets, slots, cap,
+                                               ctypes.byref(count), err, 256)
+                    try:
+                        want = ref.temporal_blocks(frame, length, size, overlap)
+                    except ValueError as e:
+                        assert rc == 1 and err.value.decode() == str(e), (frame, length, size, overlap)
+                        continue
+                    assert rc == 0 and count.value == len(want), (frame, length, size, overlap)
+                    got = [{"start": starts[i], "target": targets[i], "slots": list(slots[i * size:(i + 1) * size])}
+                           for i in range(count.value)]
+                    assert got == want, (frame, length, size, overlap)
+                    checked += 1
+    assert checked == 7888
